@@ -1,0 +1,317 @@
+/*
+ * nectar_b200.h — C ABI of the B200 path-tracing back end.
+ *
+ * This is the drop-in boundary for NectarRender's path-tracing hot path. The
+ * reference exposes that path through its pybind11 module `_pathtracer`
+ * (nectar_render/csrc/bindings/bindings.cpp:16-30); the classes it binds are
+ * backed here by plain C entry points with opaque handles, plain pointers and
+ * sizes, and integer status codes. The pybind11 module shipped in
+ * nectarrender_b200/csrc/pathtracer_module.cpp re-creates the reference's
+ * Python names on top of these functions.
+ *
+ * Conventions
+ *  - Every function returns NR_OK (0) or a negative NR_ERR_* code; the last
+ *    error message of the calling thread is available from nr_last_error().
+ *    The reference throws std::runtime_error in the same situations
+ *    (e.g. nectar_render/csrc/engine/include/engine/camera.h:317-319,
+ *    nectar_render/csrc/hittable/include/hittable/registry.h:113-117).
+ *  - Images are planar CHW float32, index c*H*W + y*W + x, exactly the AOV
+ *    layout of nectar_render/csrc/data/include/data/render_layers.h:28-55 and
+ *    nectar_render/csrc/data/include/data/utils.h:9-21.
+ *  - Resolution follows the reference's camera: resolution[0] is the image
+ *    height H and resolution[1] its width W when buffers are sized
+ *    (camera.h:176-178), while the pixel-to-sensor mapping uses
+ *    resolution[0] as its horizontal extent (camera.h:269-272). Square images
+ *    are therefore the only fully consistent case, exactly as in the reference.
+ *  - No function allocates on, or touches, a GPU until nr_scene_build /
+ *    nr_render_create. Without a usable CUDA device these return
+ *    NR_ERR_NO_DEVICE; there is no CPU fallback.
+ */
+#ifndef NECTAR_B200_H
+#define NECTAR_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NR_ABI_VERSION 1
+
+/* status codes ------------------------------------------------------------ */
+#define NR_OK 0
+#define NR_ERR_INVALID (-1)   /* bad argument or handle                       */
+#define NR_ERR_CUDA (-2)      /* a CUDA runtime call failed                   */
+#define NR_ERR_LIMIT (-3)     /* a registry/capacity limit was exceeded       */
+#define NR_ERR_IO (-4)        /* a file could not be read or parsed           */
+#define NR_ERR_NO_DEVICE (-5) /* no usable CUDA device                        */
+#define NR_ERR_STATE (-6)     /* call out of order (e.g. render before build) */
+#define NR_ERR_DEVICE (-7)    /* a kernel reported an error word (overflow)   */
+
+/* limits of the reference registries -------------------------------------- */
+#define NR_MAX_OBJECTS 1024   /* registry.h:104  MAX_REGISTRY_ENTRIES          */
+#define NR_MAX_MATERIALS 4096 /* material/registry.h:11 MAX_MATERIAL_COUNT     */
+
+/* enums: values mirror the reference enums ------------------------------- */
+/* HittableType, nectar_render/csrc/hittable/include/hittable/hittable.h:13-15 */
+enum {
+  NR_HITTABLE_NULL = 0,
+  NR_HITTABLE_QUAD = 1,
+  NR_HITTABLE_SPHERE = 2,
+  NR_HITTABLE_CUBE = 3,
+  NR_HITTABLE_MESH = 4,
+  NR_HITTABLE_CONSTANT_MEDIUM = 5,
+  NR_HITTABLE_OBJECT_LIGHT = 6
+};
+/* MaterialType, nectar_render/csrc/material/include/material/material.h:374-376 */
+enum {
+  NR_MATERIAL_NULL = 0,
+  NR_MATERIAL_LAMBERTIAN = 1,
+  NR_MATERIAL_PBR = 2,
+  NR_MATERIAL_DIELECTRIC = 3,
+  NR_MATERIAL_EMISSIVE = 4,
+  NR_MATERIAL_ISOTROPIC = 5
+};
+/* TextureType, nectar_render/csrc/material/include/material/texture.h:6 */
+enum { NR_TEXTURE_CONSTANT = 0, NR_TEXTURE_IMAGE = 1 };
+/* SkylightType, nectar_render/csrc/light/include/skylight.h:131 */
+enum { NR_SKY_NULL = 0, NR_SKY_SIMPLE = 1, NR_SKY_HDRI = 2 };
+/* LayerType, nectar_render/csrc/data/include/data/render_layers.h:11-14 */
+enum {
+  NR_LAYER_BEAUTY = 0,
+  NR_LAYER_DIFFUSE = 1,
+  NR_LAYER_SPECULAR = 2,
+  NR_LAYER_OBJECT_NORMAL = 3,
+  NR_LAYER_WORLD_NORMAL = 4,
+  NR_LAYER_SHADOW = 5,
+  NR_LAYER_DEPTH = 6,
+  NR_LAYER_EMISSION = 7,
+  NR_LAYER_OBJECT_ID = 8
+};
+/* TonemapMethod, nectar_render/csrc/data/include/data/stream.h:12 */
+enum { NR_TONEMAP_REINHARD = 0, NR_TONEMAP_REINHARD_EXTENDED = 1, NR_TONEMAP_ACES = 2 };
+
+/* Integrator modes.
+ * NR_MODE_REFERENCE reproduces the reference sampler draw for draw
+ *   (nectar_render/csrc/engine/src/trace.cu:11-79 and brdf.cu:4-35).
+ * NR_MODE_PERF keeps every BSDF but adds next-event estimation with
+ *   power-heuristic MIS toward lights[0] and toward the HDRI (importance
+ *   sampled through an alias table). It converges to the same image. */
+enum { NR_MODE_REFERENCE = 0, NR_MODE_PERF = 1 };
+
+/* Integrator schedules: one persistent megakernel with path regeneration, or
+ * the wavefront pipeline (generate / extend / shade / shadow / accumulate). */
+enum { NR_SCHEDULE_MEGAKERNEL = 0, NR_SCHEDULE_WAVEFRONT = 1 };
+
+/* scene description --------------------------------------------------------- */
+
+/* One texture slot: Texture::from_color / Texture::from_image (texture.h:145-177). */
+typedef struct nr_texture_desc {
+  int32_t type;  /* NR_TEXTURE_CONSTANT or NR_TEXTURE_IMAGE                   */
+  int32_t image; /* image id from nr_scene_add_image (IMAGE only)             */
+  float scale;   /* texture_scale (IMAGE only)                                */
+  float rgb[3];  /* constant_color (CONSTANT only)                            */
+} nr_texture_desc;
+
+/* One material (Material::lambertian/pbr/dielectric/emissive/isotropic,
+ * material.h:453-532). Texture slots: LAMBERTIAN, EMISSIVE, ISOTROPIC use
+ * tex[0]; PBR uses albedo, roughness, metallic, emission, normal in tex[0..4]. */
+typedef struct nr_material_desc {
+  int32_t type;     /* NR_MATERIAL_*                     */
+  float ior;        /* DIELECTRIC                        */
+  float brightness; /* EMISSIVE                          */
+  float tint[3];    /* DIELECTRIC                        */
+  nr_texture_desc tex[5];
+} nr_material_desc;
+
+/* One hittable (Hittable::quad/cube/sphere/mesh/object_light/constant_medium,
+ * hittable.h:148-277). For OBJECT_LIGHT and CONSTANT_MEDIUM, wrapped_type and
+ * the transform/radius/mesh fields describe the bound object, whose transform
+ * the wrapper inherits (hittable.h:231-233, 261-263). */
+typedef struct nr_object_desc {
+  int32_t type;         /* NR_HITTABLE_*                                  */
+  int32_t wrapped_type; /* bound object type for OBJECT_LIGHT / MEDIUM    */
+  int32_t material;     /* material id; 0 = default purple Lambertian     */
+  int32_t mesh;         /* mesh id for MESH (or a wrapped MESH)           */
+  float position[3];
+  float rotation[3]; /* Euler degrees, R = Rz*Ry*Rx (matrix.h:94-96)      */
+  float scale[3];
+  float radius;  /* SPHERE (or wrapped SPHERE)                             */
+  float density; /* CONSTANT_MEDIUM                                        */
+} nr_object_desc;
+
+/* CameraParams (nectar_render/csrc/engine/include/engine/camera.h:351-405). */
+typedef struct nr_camera_desc {
+  float resolution[2];
+  float position[3];
+  float rotation[3];
+  uint32_t samples_per_pixel;
+  float focal_length;
+  float focus_distance;
+  float aperture;
+  float sensor_width;
+  float shutter_speed;
+} nr_camera_desc;
+
+/* TraceConfig (nectar_render/csrc/engine/include/engine/trace.h:10-19) plus
+ * this back end's schedule, mode and accumulator options. */
+typedef struct nr_render_config {
+  uint32_t ray_depth;
+  uint32_t seed;
+  int32_t rr_enabled;       /* do_rr_termination                            */
+  uint32_t rr_start_bounce; /* rr_start_bounce                              */
+  float rr_survival;        /* rr_survival_chance                           */
+  int32_t mode;             /* NR_MODE_*                                    */
+  int32_t schedule;         /* NR_SCHEDULE_*                                */
+  int32_t fp64_accumulate;  /* also keep an FP64 sum of the beauty layer    */
+  uint32_t layer_mask;      /* bit i enables LayerType i (default 0x13)      */
+} nr_render_config;
+
+/* StreamConfig display fields (nectar_render/csrc/data/include/data/stream.h:13-30). */
+typedef struct nr_stream_config {
+  int32_t linear_to_gamma;
+  int32_t apply_white_balance;
+  float wb_temperature;
+  float wb_tint;
+  int32_t apply_tonemapping;
+  int32_t tm_method;
+  float tm_white_point;
+  float tm_alpha;
+} nr_stream_config;
+
+/* Statistics of a built scene. */
+typedef struct nr_scene_stats {
+  uint32_t n_objects;
+  uint32_t n_materials;
+  uint32_t n_lights;
+  uint64_t n_triangles;
+  uint64_t binary_nodes;     /* binary SAH tree nodes, all meshes + top level */
+  uint64_t wide_nodes;       /* 8-wide compressed nodes after collapse        */
+  double sah_cost_binary;    /* SAH cost of the largest mesh's binary tree     */
+  double build_ms;           /* device time of the last nr_scene_build         */
+  uint64_t device_bytes;     /* scene bytes resident in HBM                    */
+} nr_scene_stats;
+
+/* Per-launch counters for the roofline (filled when counters are enabled). */
+typedef struct nr_trace_counters {
+  uint64_t rays;        /* extension + shadow ray queries                    */
+  uint64_t node_visits; /* wide-node fetches (80 B each)                     */
+  uint64_t tri_tests;   /* triangle records fetched (48 B each)              */
+  uint64_t obj_tests;   /* instance/primitive records fetched                */
+  uint64_t paths;       /* pixel-samples completed                           */
+} nr_trace_counters;
+
+typedef struct nr_scene nr_scene;
+typedef struct nr_render nr_render;
+
+/* library ------------------------------------------------------------------ */
+int nr_abi_version(void);
+const char* nr_last_error(void);
+/* Number of CUDA devices visible (0 without a GPU; never fails). */
+int nr_device_count(void);
+
+/* scene (replaces Scene / HittablesRegistry / MaterialRegisty:
+ * nectar_render/csrc/scene/include/scene.h:15-77,
+ * nectar_render/csrc/hittable/include/hittable/registry.h:101-265,
+ * nectar_render/csrc/material/include/material/registry.h:8-103) ---------- */
+int nr_scene_create(nr_scene** out);
+int nr_scene_destroy(nr_scene* scene);
+/* Material id 0 always exists: the default purple Lambertian
+ * (material/registry.h:23-25, material.h:650-652). */
+int nr_scene_add_material(nr_scene* scene, const nr_material_desc* desc, uint32_t* out_id);
+/* uint8 planar CHW image for IMAGE textures (texture.h:8-26). */
+int nr_scene_add_image(nr_scene* scene, const uint8_t* chw, uint32_t C, uint32_t H, uint32_t W,
+                       uint32_t* out_id);
+/* Mesh from arrays (Mesh::set_geometry, mesh.h:169-175): positions/normals/
+ * tangents are float[3*n_vertices], uvs float[2*n_vertices] (NULL = zeros),
+ * triangles uint32[3*n_triangles]. */
+int nr_scene_add_mesh(nr_scene* scene, const float* positions, const float* normals,
+                      const float* tangents, const float* uvs, uint32_t n_vertices,
+                      const uint32_t* triangles, uint32_t n_triangles, uint32_t* out_id);
+/* Wavefront OBJ file (parse_obj_file, mesh.h:39-141): triangulated faces,
+ * vertices deduplicated on the (v, vt, vn) index triple, smooth normals when
+ * the file has none, per-vertex tangents from uv gradients. */
+int nr_scene_load_obj(nr_scene* scene, const char* path, uint32_t* out_id);
+/* Appends a hittable; OBJECT_LIGHT objects are also lights. Scene(hittables,
+ * lights, sky) appends lights after the hittables (scene.h:31-39). */
+int nr_scene_add_object(nr_scene* scene, const nr_object_desc* desc, uint32_t* out_id);
+int nr_scene_set_sky_null(nr_scene* scene);
+/* Skylight::simple (skylight.h:211-222). */
+int nr_scene_set_sky_simple(nr_scene* scene, const float start_rgb[3], const float end_rgb[3]);
+/* Skylight::hdri from float planar CHW data (skylight.h:54-69, texture.h:28-47). */
+int nr_scene_set_sky_hdri(nr_scene* scene, const float* chw, uint32_t C, uint32_t H, uint32_t W,
+                          float rotation_deg, float intensity);
+/* Skylight::hdri(path) from a Radiance RGBE .hdr file (stbi_loadf semantics). */
+int nr_scene_load_hdr(nr_scene* scene, const char* path, float rotation_deg, float intensity);
+/* HDRISkylightConfig rotation/intensity (skylight.h:14-21) after creation. */
+int nr_scene_set_hdri_params(nr_scene* scene, float rotation_deg, float intensity);
+/* Uploads the scene and builds every BVH on the GPU (Scene::build,
+ * nectar_render/csrc/scene/src/scene.cpp:68-76). Must precede nr_render_create. */
+int nr_scene_build(nr_scene* scene);
+int nr_scene_get_stats(const nr_scene* scene, nr_scene_stats* out);
+/* Binary SAH tree of mesh `mesh_id` as built on the GPU, for checks:
+ * nodes as float[8] {lo.xyz, hi.xyz, left|prim, right|count} bit patterns
+ * (int32 stored in the float slots). Pass NULL to query the count. */
+int nr_scene_get_binary_bvh(const nr_scene* scene, uint32_t mesh_id, float* nodes8,
+                            uint64_t* n_nodes, uint32_t* prim_order);
+
+/* render (replaces RenderEngine + RenderLayers + trace_full:
+ * nectar_render/csrc/engine/include/engine/engine.h:274-380,
+ * nectar_render/csrc/engine/src/engine.cpp:42-74,
+ * nectar_render/csrc/engine/src/trace.cu:47-94,
+ * nectar_render/csrc/data/include/data/render_layers.h:57-190) ----------- */
+int nr_render_config_default(nr_render_config* cfg);
+int nr_render_create(nr_scene* scene, const nr_camera_desc* camera, const nr_render_config* cfg,
+                     nr_render** out);
+int nr_render_destroy(nr_render* render);
+/* Clears the accumulated layers; the next sample index is 1 (engine.cpp:216-220). */
+int nr_render_reset(nr_render* render);
+/* Renders sample indices [first, first+count) and folds each into the running
+ * mean avg*(n-1)/n + s/n with n = sample index (data.cu:28-50). The reference
+ * render() loop is first = 1, count = samples_per_pixel - 1 (engine.cpp:43). */
+int nr_render_samples(nr_render* render, uint32_t first, uint32_t count);
+/* Renders one sample index and writes its raw per-sample layers (the
+ * reference's sample_aovs before accumulation) to host float CHW buffers;
+ * any pointer may be NULL. Used for per-sample parity. */
+int nr_render_sample_layers(nr_render* render, uint32_t sample_idx, float* beauty_chw,
+                            float* diffuse_chw, float* world_normal_chw, uint32_t* primary_prim);
+/* Device pointer of an accumulated layer (DataObject::device_ptr,
+ * nectar_render/csrc/data/include/data/data_object.h:163-166). */
+int nr_render_layer_device_ptr(nr_render* render, int32_t layer, uint64_t* out_ptr);
+/* Copies an accumulated layer to a host float CHW buffer of C*H*W floats. */
+int nr_render_read_layer(nr_render* render, int32_t layer, float* host_chw);
+/* FP64 running sum of beauty (when fp64_accumulate), divided by the count. */
+int nr_render_read_beauty_fp64(nr_render* render, double* host_chw);
+/* Display transform of a layer (process_stream_kernel, stream.cu:146-159):
+ * white balance -> tonemap -> sqrt gamma -> clamp -> uint8 CHW, into host memory. */
+int nr_render_readback(nr_render* render, int32_t layer, const nr_stream_config* cfg,
+                       uint8_t* host_chw);
+/* Same transform in float before quantisation (the RMSE domain). */
+int nr_render_display_float(nr_render* render, int32_t layer, const nr_stream_config* cfg,
+                            float* host_chw);
+int nr_render_dims(const nr_render* render, uint32_t* C, uint32_t* H, uint32_t* W);
+/* Counters of the last nr_render_samples call when enabled. */
+int nr_render_set_counters(nr_render* render, int32_t enabled);
+int nr_render_get_counters(const nr_render* render, nr_trace_counters* out);
+/* Device time in milliseconds of the last nr_render_samples call (CUDA events
+ * on the render stream). */
+int nr_render_last_ms(const nr_render* render, double* out_ms);
+/* Opaque cudaStream_t of the render (for callers that time or order work). */
+int nr_render_stream(const nr_render* render, uint64_t* out_stream);
+
+/* device-pointer level (callers that own their buffers) -------------------- */
+/* Fused running-mean accumulate of one sample layer into an average layer on
+ * the given stream: avg = avg*(n-1)/n + s/n (accumulate_samples_kernel,
+ * nectar_render/csrc/data/src/data.cu:28-50). Pointers are device float CHW. */
+int nr_accumulate_device(float* avg, const float* sample, uint32_t C, uint32_t H, uint32_t W,
+                         uint32_t sample_idx, uint64_t stream);
+/* Display transform of a device float CHW buffer into device uint8 CHW
+ * (process_stream_kernel, nectar_render/csrc/data/src/stream.cu:146-159). */
+int nr_display_device(const float* src, uint8_t* dst, uint32_t C, uint32_t H, uint32_t W,
+                      const nr_stream_config* cfg, uint64_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NECTAR_B200_H */

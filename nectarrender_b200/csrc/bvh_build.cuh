@@ -1,0 +1,39 @@
+// bvh_build.cuh — GPU BVH construction interface.
+#pragma once
+#include <vector>
+#include "scene_device.cuh"
+
+namespace nr {
+
+// Binary node as produced by the builder (both levels). Leaves have
+// left == right == -1 and reference the primitive range [start, start+count)
+// of the output primitive order.
+struct BinNode {
+  float lo[3], hi[3];
+  int32_t left, right;
+  uint32_t start, count;
+};
+
+struct BuildResult {
+  // device buffers owned by the caller after the build
+  BinNode* d_nodes = nullptr;   // n_nodes binary nodes, root = 0
+  uint32_t* d_order = nullptr;  // leaf order -> input primitive index
+  Bvh2Node* d_bvh2 = nullptr;   // inner nodes, 64 B layout, root = 0
+  Bvh8Node* d_bvh8 = nullptr;   // compressed 8-wide nodes, root = 0
+  uint32_t* d_order8 = nullptr; // wide-leaf order -> input primitive index
+  uint32_t n_nodes = 0;
+  uint32_t n_bvh2 = 0;
+  uint32_t n_bvh8 = 0;
+  double sah_cost = 0.0;  // binary tree, leaf size 1, unit costs (node 1, prim 1)
+  float build_ms = 0.0f;
+};
+
+// Builds the binary SAH tree over `n` primitive boxes given as device arrays
+// lo[i] = (x, y, z, _), hi[i] = (x, y, z, _) and derives the 2-wide and
+// 8-wide traversal layouts. Returns a cudaError_t value.
+int build_bvh(const float4* d_lo, const float4* d_hi, uint32_t n, bool want_bvh8,
+              BuildResult& out, cudaStream_t st);
+
+void free_build(BuildResult& r);
+
+}  // namespace nr

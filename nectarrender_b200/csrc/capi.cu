@@ -1,0 +1,1264 @@
+// capi.cu — host side of the back end and its extern "C" entry points.
+//
+// Scene state mirrors the reference's registries (HittablesRegistry,
+// MaterialRegisty, Skylight: nectar_render/csrc/hittable/include/hittable/
+// registry.h:101-265, nectar_render/csrc/material/include/material/
+// registry.h:8-103, nectar_render/csrc/light/include/skylight.h:138-254) but
+// is uploaded as flat arrays (scene_device.cuh) and every BVH is built on the
+// GPU (bvh_build.cu). Values the reference computes on the host (object
+// transforms, camera parameters, the n-rooks sample pattern, the top-level
+// leaf order that decides lights[0]) are computed here with the same host
+// arithmetic; values it computes on the device (cube face transforms, the
+// HDRI rotation, white-balance gains) are computed by device kernels.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <numeric>
+#include <random>
+#include <string>
+#include <vector>
+
+#include "../../include/nectar_b200.h"
+#include "bvh_build.cuh"
+#include "host_io.h"
+#include "image_ops.cuh"
+#include "integrator.cuh"
+
+using namespace nr;
+
+// ---------------------------------------------------------------------------
+// errors
+
+static thread_local std::string g_last_error;
+
+static int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+static int cuda_fail(cudaError_t e, const char* what) {
+  return fail(NR_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+#define CU(call, what)                                 \
+  do {                                                 \
+    cudaError_t e__ = (call);                          \
+    if (e__ != cudaSuccess) return cuda_fail(e__, what); \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// host math with the reference's expression order
+// (core/matrix.h:64-96, core/utils.h:12-22, core/transform.h:125-134)
+
+namespace {
+
+struct HM3 {
+  float m[3][3];
+};
+float h_deg2rad(float degrees) { return degrees * 0.01745329; }
+HM3 h_rot_x(float a) {
+  float c = cosf(a), s = sinf(a);
+  return HM3{{{1, 0, 0}, {0, c, -s}, {0, s, c}}};
+}
+HM3 h_rot_y(float a) {
+  float c = cosf(a), s = sinf(a);
+  return HM3{{{c, 0, s}, {0, 1, 0}, {-s, 0, c}}};
+}
+HM3 h_rot_z(float a) {
+  float c = cosf(a), s = sinf(a);
+  return HM3{{{c, -s, 0}, {s, c, 0}, {0, 0, 1}}};
+}
+HM3 h_mul(const HM3& a, const HM3& b) {
+  HM3 r;
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) {
+      r.m[i][j] = 0;
+      for (int k = 0; k < 3; k++) r.m[i][j] += a.m[i][k] * b.m[k][j];
+    }
+  return r;
+}
+HM3 h_T(const HM3& a) {
+  HM3 r;
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) r.m[i][j] = a.m[j][i];
+  return r;
+}
+HM3 h_euler_rad(float x, float y, float z) { return h_mul(h_mul(h_rot_z(z), h_rot_y(y)), h_rot_x(x)); }
+HM3 h_euler_deg(const float r[3]) {
+  return h_euler_rad(h_deg2rad(r[0]), h_deg2rad(r[1]), h_deg2rad(r[2]));
+}
+
+struct HXform {
+  HM3 R, invR;
+  float pos[3], scale[3], inv_s[3];
+};
+// Transform(position, rotation_deg, scale)
+HXform h_xform(const float p[3], const float r[3], const float s[3]) {
+  HXform x;
+  x.R = h_euler_deg(r);
+  x.invR = h_T(h_euler_deg(r));
+  for (int k = 0; k < 3; ++k) {
+    x.pos[k] = p[k];
+    x.scale[k] = s[k];
+    x.inv_s[k] = 1.0f / ((s[k] + 1e-8f) + 1e-8f);
+  }
+  return x;
+}
+// Transform(position): identity rotation from Euler zeros, unit scale
+HXform h_xform_pos(const float p[3]) {
+  HXform x;
+  x.R = h_euler_rad(0.0f, 0.0f, 0.0f);
+  x.invR = h_T(h_euler_rad(0.0f, 0.0f, 0.0f));
+  for (int k = 0; k < 3; ++k) {
+    x.pos[k] = p[k];
+    x.scale[k] = 1.0f;
+    x.inv_s[k] = 1.0f;
+  }
+  return x;
+}
+
+// AABB of the reference (hittable/include/bvh/aabb.h): intervals per axis.
+struct HBox {
+  float lo[3], hi[3];
+};
+// AABB::transformed(...).buffer() (aabb.h:60-91)
+HBox h_transformed(const HBox& b, const HXform& x) {
+  float c[8][3] = {{b.lo[0], b.lo[1], b.lo[2]}, {b.hi[0], b.lo[1], b.lo[2]},
+                   {b.lo[0], b.hi[1], b.lo[2]}, {b.hi[0], b.hi[1], b.lo[2]},
+                   {b.lo[0], b.lo[1], b.hi[2]}, {b.hi[0], b.lo[1], b.hi[2]},
+                   {b.lo[0], b.hi[1], b.hi[2]}, {b.hi[0], b.hi[1], b.hi[2]}};
+  float mn[3] = {1e32f, 1e32f, 1e32f}, mx[3] = {-1e32f, -1e32f, -1e32f};
+  for (int i = 0; i < 8; ++i) {
+    float s[3] = {c[i][0] * x.scale[0], c[i][1] * x.scale[1], c[i][2] * x.scale[2]};
+    float w[3];
+    for (int r = 0; r < 3; ++r)
+      w[r] = x.R.m[r][0] * s[0] + x.R.m[r][1] * s[1] + x.R.m[r][2] * s[2] + x.pos[r];
+    for (int k = 0; k < 3; ++k) {
+      mn[k] = fminf(mn[k], w[k]);
+      mx[k] = fmaxf(mx[k], w[k]);
+    }
+  }
+  HBox o;
+  for (int k = 0; k < 3; ++k) {
+    float lo = mn[k] <= mx[k] ? mn[k] : mx[k];
+    float hi = mn[k] <= mx[k] ? mx[k] : mn[k];
+    if (hi - lo < 1e-4f) {
+      float pad = 1e-4f / 2.0f;
+      lo = lo - pad;
+      hi = hi + pad;
+    }
+    o.lo[k] = lo;
+    o.hi[k] = hi;
+  }
+  return o;
+}
+
+// Leaf order of the reference's top-level BVH<T>::build
+// (hittable/include/bvh/bvh.h:35-320): 16 centroid bins, cost A_L*N_L +
+// A_R*N_R, std::partition by bin, std::sort median split as fallback. Only
+// the order is needed here: the reference's lights[0] is the first light in
+// that order (registry.h:216-263).
+struct RefOrder {
+  const std::vector<HBox>& boxes;
+  std::vector<int32_t> order;
+  static constexpr int kB = 16;
+  explicit RefOrder(const std::vector<HBox>& b) : boxes(b) {
+    order.resize(b.size());
+    std::iota(order.begin(), order.end(), 0);
+    if (!order.empty()) rec(0, (int32_t)order.size());
+  }
+  static float area(const HBox& b) {
+    float dx = b.hi[0] - b.lo[0], dy = b.hi[1] - b.lo[1], dz = b.hi[2] - b.lo[2];
+    return 2.0f * (dx * dy + dy * dz + dz * dx);
+  }
+  static HBox join(const HBox& a, const HBox& b) {
+    HBox r;
+    for (int k = 0; k < 3; ++k) {
+      r.lo[k] = a.lo[k] <= b.lo[k] ? a.lo[k] : b.lo[k];
+      r.hi[k] = a.hi[k] >= b.hi[k] ? a.hi[k] : b.hi[k];
+    }
+    return r;
+  }
+  void rec(int32_t start, int32_t end) {
+    if (end - start == 1) return;
+    float cmin[3] = {1e32f, 1e32f, 1e32f}, cmax[3] = {-1e32f, -1e32f, -1e32f};
+    for (int32_t i = start; i < end; ++i) {
+      const HBox& b = boxes[order[i]];
+      for (int k = 0; k < 3; ++k) {
+        float c = (b.lo[k] + b.hi[k]) * 0.5f;
+        cmin[k] = fminf(cmin[k], c);
+        cmax[k] = fmaxf(cmax[k], c);
+      }
+    }
+    float best_cost = 1e32f;
+    int32_t best_axis = -1, best_bin = -1;
+    for (int a = 0; a < 3; ++a) {
+      float extent = cmax[a] - cmin[a];
+      if (extent < 1e-4f) continue;
+      int32_t cnt[kB] = {0};
+      HBox bb[kB];
+      for (int32_t i = start; i < end; ++i) {
+        const HBox& b = boxes[order[i]];
+        float c = (b.lo[a] + b.hi[a]) * 0.5f;
+        int32_t bin = (int32_t)(kB * (c - cmin[a]) / extent);
+        bin = bin < 0 ? 0 : (bin >= kB ? kB - 1 : bin);
+        cnt[bin]++;
+        bb[bin] = cnt[bin] == 1 ? b : join(bb[bin], b);
+      }
+      HBox lb[kB], rb[kB];
+      int32_t lc[kB], rc[kB];
+      HBox run{};
+      int32_t rcount = 0;
+      bool started = false;
+      for (int i = 0; i < kB; ++i) {
+        if (cnt[i] > 0) {
+          run = started ? join(run, bb[i]) : bb[i];
+          started = true;
+        }
+        rcount += cnt[i];
+        lb[i] = run;
+        lc[i] = rcount;
+      }
+      rcount = 0;
+      started = false;
+      for (int i = kB - 1; i >= 0; --i) {
+        if (cnt[i] > 0) {
+          run = started ? join(run, bb[i]) : bb[i];
+          started = true;
+        }
+        rcount += cnt[i];
+        rb[i] = run;
+        rc[i] = rcount;
+      }
+      for (int i = 0; i < kB - 1; ++i) {
+        if (lc[i] == 0 || rc[i + 1] == 0) continue;
+        float cost = area(lb[i]) * lc[i] + area(rb[i + 1]) * rc[i + 1];
+        if (cost < best_cost) {
+          best_cost = cost;
+          best_axis = a;
+          best_bin = i;
+        }
+      }
+    }
+    if (best_axis == -1) {
+      HBox comb = boxes[order[start]];
+      for (int32_t i = start + 1; i < end; ++i) comb = join(comb, boxes[order[i]]);
+      float lx = comb.hi[0] - comb.lo[0], ly = comb.hi[1] - comb.lo[1], lz = comb.hi[2] - comb.lo[2];
+      best_axis = (lx > ly && lx > lz) ? 0 : (ly > lz ? 1 : 2);
+    }
+    if (best_bin == -1) {
+      int a = best_axis;
+      std::sort(order.begin() + start, order.begin() + end,
+                [&](int32_t x, int32_t y) { return boxes[x].lo[a] < boxes[y].lo[a]; });
+      int32_t mid = start + (end - start) / 2;
+      rec(start, mid);
+      rec(mid, end);
+      return;
+    }
+    int a = best_axis;
+    float c_min = cmin[a], extent = cmax[a] - c_min;
+    auto it = std::partition(order.begin() + start, order.begin() + end, [&](int32_t i) {
+      const HBox& b = boxes[i];
+      float c = (b.lo[a] + b.hi[a]) * 0.5f;
+      int32_t bin = (int32_t)(kB * (c - c_min) / extent);
+      bin = bin < 0 ? 0 : (bin >= kB ? kB - 1 : bin);
+      return bin <= best_bin;
+    });
+    int32_t mid = (int32_t)(it - order.begin());
+    rec(start, mid);
+    rec(mid, end);
+  }
+};
+
+template <typename T>
+cudaError_t upload(T*& d, const T* h, size_t n, cudaStream_t st) {
+  cudaError_t e = cudaMalloc(&d, sizeof(T) * (n ? n : 1));
+  if (e != cudaSuccess) return e;
+  if (n) e = cudaMemcpyAsync(d, h, sizeof(T) * n, cudaMemcpyHostToDevice, st);
+  return e;
+}
+
+struct MeshGpu {
+  float* pos = nullptr;       // 3 per vertex
+  float* nor = nullptr;
+  float* tan = nullptr;
+  float* uv = nullptr;
+  uint32_t* vidx = nullptr;   // 3 per triangle
+  TriRecord* tris2 = nullptr;
+  TriRecord* tris8 = nullptr;
+  BuildResult bvh;
+  void release() {
+    cudaFree(pos);
+    cudaFree(nor);
+    cudaFree(tan);
+    cudaFree(uv);
+    cudaFree(vidx);
+    cudaFree(tris2);
+    cudaFree(tris8);
+    free_build(bvh);
+    *this = MeshGpu{};
+  }
+};
+
+// triangle boxes for the builder
+__global__ void k_tri_boxes(const float* pos, const uint32_t* vidx, uint32_t n, float4* lo,
+                            float4* hi) {
+  uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  float v[3][3];
+  for (int k = 0; k < 3; ++k)
+    for (int c = 0; c < 3; ++c) v[k][c] = pos[3 * vidx[3 * t + k] + c];
+  float mn[3], mx[3];
+  for (int c = 0; c < 3; ++c) {
+    mn[c] = fminf(v[0][c], fminf(v[1][c], v[2][c]));
+    mx[c] = fmaxf(v[0][c], fmaxf(v[1][c], v[2][c]));
+  }
+  lo[t] = make_float4(mn[0], mn[1], mn[2], 0.f);
+  hi[t] = make_float4(mx[0], mx[1], mx[2], 0.f);
+}
+
+// triangle records in a leaf order; .e1.w flags a zero-extent box (any axis)
+__global__ void k_tri_records(const float* pos, const uint32_t* vidx, const uint32_t* order,
+                              uint32_t n, TriRecord* out) {
+  uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  uint32_t t = order[s];
+  float v[3][3];
+  for (int k = 0; k < 3; ++k)
+    for (int c = 0; c < 3; ++c) v[k][c] = pos[3 * vidx[3 * t + k] + c];
+  bool flat = false;
+  for (int c = 0; c < 3; ++c) {
+    float mn = fminf(v[0][c], fminf(v[1][c], v[2][c]));
+    float mx = fmaxf(v[0][c], fmaxf(v[1][c], v[2][c]));
+    if (mx == mn) flat = true;
+  }
+  TriRecord r;
+  r.v0 = make_float4(v[0][0], v[0][1], v[0][2], __uint_as_float(t));
+  r.e1 = make_float4(__fsub_rn(v[1][0], v[0][0]), __fsub_rn(v[1][1], v[0][1]),
+                     __fsub_rn(v[1][2], v[0][2]), __uint_as_float(flat ? 1u : 0u));
+  r.e2 = make_float4(__fsub_rn(v[2][0], v[0][0]), __fsub_rn(v[2][1], v[0][1]),
+                     __fsub_rn(v[2][2], v[0][2]), 0.f);
+  out[s] = r;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// scene
+
+struct HostImage8 {
+  uint32_t C, H, W;
+  std::vector<uint8_t> chw;
+};
+
+struct nr_scene {
+  std::vector<nr_material_desc> materials;
+  std::vector<HostImage8> images;
+  std::vector<HostMesh> meshes;
+  std::vector<nr_object_desc> objects;
+  int32_t sky_type = NR_SKY_NULL;
+  float sky_start[3] = {1.0f, 1.0f, 1.0f};
+  float sky_end[3] = {0.5f, 0.7f, 1.0f};
+  HostImageF hdri;
+  float hdri_rotation = 0.0f;
+  float hdri_intensity = 1.0f;
+
+  // device state
+  bool built = false;
+  cudaStream_t stream = nullptr;
+  std::vector<uint8_t*> d_images;
+  std::vector<MeshGpu> d_meshes;
+  DevMaterial* d_materials = nullptr;
+  DevObject* d_objects = nullptr;
+  DevMesh* d_mesh_table = nullptr;
+  float* d_hdri = nullptr;
+  BuildResult tlas;
+  DevScene dev{};
+  nr_scene_stats stats{};
+  std::vector<int32_t> ref_leaf_order;
+  int32_t light = -1;
+
+  void release_device() {
+    for (auto p : d_images) cudaFree(p);
+    d_images.clear();
+    for (auto& m : d_meshes) m.release();
+    d_meshes.clear();
+    cudaFree(d_materials);
+    cudaFree(d_objects);
+    cudaFree(d_mesh_table);
+    cudaFree(d_hdri);
+    d_materials = nullptr;
+    d_objects = nullptr;
+    d_mesh_table = nullptr;
+    d_hdri = nullptr;
+    free_build(tlas);
+    built = false;
+  }
+  ~nr_scene() {
+    release_device();
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+static nr_material_desc default_material() {
+  // Material::lambertian(Color::purple()) (material.h:650-652)
+  nr_material_desc m{};
+  m.type = NR_MATERIAL_LAMBERTIAN;
+  m.tex[0].type = NR_TEXTURE_CONSTANT;
+  m.tex[0].rgb[0] = 1.0f;
+  m.tex[0].rgb[1] = 0.0f;
+  m.tex[0].rgb[2] = 1.0f;
+  m.tex[0].scale = 1.0f;
+  return m;
+}
+
+static bool device_available() {
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return n > 0;
+}
+
+static int base_type(const nr_object_desc& o) {
+  return (o.type == NR_HITTABLE_OBJECT_LIGHT || o.type == NR_HITTABLE_CONSTANT_MEDIUM)
+             ? o.wrapped_type
+             : o.type;
+}
+
+static HXform object_xform(const nr_object_desc& o) {
+  return base_type(o) == NR_HITTABLE_SPHERE ? h_xform_pos(o.position)
+                                            : h_xform(o.position, o.rotation, o.scale);
+}
+
+static HBox object_local_box(const nr_scene* s, const nr_object_desc& o) {
+  HBox b;
+  int t = base_type(o);
+  if (t == NR_HITTABLE_SPHERE) {
+    float r = o.radius + 1e-8f;
+    for (int k = 0; k < 3; ++k) {
+      b.lo[k] = -r;
+      b.hi[k] = r;
+    }
+  } else if (t == NR_HITTABLE_MESH) {
+    const HostMesh& m = s->meshes[o.mesh];
+    float mn[3] = {1e32f, 1e32f, 1e32f}, mx[3] = {-1e32f, -1e32f, -1e32f};
+    for (size_t i = 0; i < m.positions.size() / 3; ++i)
+      for (int k = 0; k < 3; ++k) {
+        mn[k] = fminf(mn[k], m.positions[3 * i + k]);
+        mx[k] = fmaxf(mx[k], m.positions[3 * i + k]);
+      }
+    for (int k = 0; k < 3; ++k) {
+      b.lo[k] = mn[k];
+      b.hi[k] = mx[k];
+    }
+  } else {
+    for (int k = 0; k < 3; ++k) {
+      b.lo[k] = -0.5f;
+      b.hi[k] = 0.5f;
+    }
+  }
+  return b;
+}
+
+static DevTexture make_tex(const nr_scene* s, const nr_texture_desc& t) {
+  DevTexture d{};
+  d.type = t.type;
+  d.r = t.rgb[0];
+  d.g = t.rgb[1];
+  d.b = t.rgb[2];
+  d.scale = t.scale;
+  if (t.type == NR_TEXTURE_IMAGE && t.image >= 0 && (size_t)t.image < s->images.size()) {
+    d.data = s->d_images[t.image];
+    d.C = s->images[t.image].C;
+    d.H = s->images[t.image].H;
+    d.W = s->images[t.image].W;
+  }
+  return d;
+}
+
+extern "C" {
+
+int nr_abi_version(void) { return NR_ABI_VERSION; }
+const char* nr_last_error(void) { return g_last_error.c_str(); }
+int nr_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
+int nr_scene_create(nr_scene** out) {
+  if (!out) return fail(NR_ERR_INVALID, "nr_scene_create: null output");
+  nr_scene* s = new nr_scene();
+  s->materials.push_back(default_material());
+  *out = s;
+  return NR_OK;
+}
+
+int nr_scene_destroy(nr_scene* scene) {
+  delete scene;
+  return NR_OK;
+}
+
+int nr_scene_add_material(nr_scene* s, const nr_material_desc* d, uint32_t* out_id) {
+  if (!s || !d) return fail(NR_ERR_INVALID, "nr_scene_add_material: null argument");
+  if (d->type < NR_MATERIAL_NULL || d->type > NR_MATERIAL_ISOTROPIC)
+    return fail(NR_ERR_INVALID, "nr_scene_add_material: unknown material type");
+  if (s->materials.size() >= NR_MAX_MATERIALS)
+    return fail(NR_ERR_LIMIT,
+                "Maximum material count reached. Unable to register additional materials.");
+  for (int k = 0; k < 5; ++k)
+    if (d->tex[k].type == NR_TEXTURE_IMAGE &&
+        (d->tex[k].image < 0 || (size_t)d->tex[k].image >= s->images.size()))
+      return fail(NR_ERR_INVALID, "nr_scene_add_material: texture references an unknown image");
+  s->materials.push_back(*d);
+  if (out_id) *out_id = (uint32_t)(s->materials.size() - 1);
+  s->built = false;
+  return NR_OK;
+}
+
+int nr_scene_add_image(nr_scene* s, const uint8_t* chw, uint32_t C, uint32_t H, uint32_t W,
+                       uint32_t* out_id) {
+  if (!s || !chw || C < 3 || H == 0 || W == 0)
+    return fail(NR_ERR_INVALID, "nr_scene_add_image: need a CHW image with at least 3 channels");
+  HostImage8 im{C, H, W, std::vector<uint8_t>(chw, chw + (size_t)C * H * W)};
+  s->images.push_back(std::move(im));
+  if (out_id) *out_id = (uint32_t)(s->images.size() - 1);
+  s->built = false;
+  return NR_OK;
+}
+
+int nr_scene_add_mesh(nr_scene* s, const float* positions, const float* normals,
+                      const float* tangents, const float* uvs, uint32_t n_vertices,
+                      const uint32_t* triangles, uint32_t n_triangles, uint32_t* out_id) {
+  if (!s || !positions || !triangles || n_vertices == 0 || n_triangles == 0)
+    return fail(NR_ERR_INVALID, "nr_scene_add_mesh: empty mesh");
+  if (n_triangles >= (1u << 22))
+    return fail(NR_ERR_LIMIT, "nr_scene_add_mesh: at most 4194303 triangles per mesh");
+  for (size_t i = 0; i < (size_t)n_triangles * 3; ++i)
+    if (triangles[i] >= n_vertices)
+      return fail(NR_ERR_INVALID, "nr_scene_add_mesh: triangle index out of range");
+  HostMesh m;
+  m.positions.assign(positions, positions + 3 * (size_t)n_vertices);
+  m.normals = normals ? std::vector<float>(normals, normals + 3 * (size_t)n_vertices)
+                      : std::vector<float>(3 * (size_t)n_vertices, 0.0f);
+  m.tangents = tangents ? std::vector<float>(tangents, tangents + 3 * (size_t)n_vertices)
+                        : std::vector<float>(3 * (size_t)n_vertices, 0.0f);
+  m.uvs = uvs ? std::vector<float>(uvs, uvs + 2 * (size_t)n_vertices)
+              : std::vector<float>(2 * (size_t)n_vertices, 0.0f);
+  m.triangles.assign(triangles, triangles + 3 * (size_t)n_triangles);
+  s->meshes.push_back(std::move(m));
+  if (out_id) *out_id = (uint32_t)(s->meshes.size() - 1);
+  s->built = false;
+  return NR_OK;
+}
+
+int nr_scene_load_obj(nr_scene* s, const char* path, uint32_t* out_id) {
+  if (!s || !path) return fail(NR_ERR_INVALID, "nr_scene_load_obj: null argument");
+  HostMesh m;
+  std::string err;
+  if (!load_obj(path, m, err)) return fail(NR_ERR_IO, err);
+  if (m.triangles.empty()) return fail(NR_ERR_INVALID, std::string("OBJ has no faces: ") + path);
+  if (m.triangles.size() / 3 >= (1u << 22))
+    return fail(NR_ERR_LIMIT, "nr_scene_load_obj: at most 4194303 triangles per mesh");
+  s->meshes.push_back(std::move(m));
+  if (out_id) *out_id = (uint32_t)(s->meshes.size() - 1);
+  s->built = false;
+  return NR_OK;
+}
+
+int nr_scene_add_object(nr_scene* s, const nr_object_desc* d, uint32_t* out_id) {
+  if (!s || !d) return fail(NR_ERR_INVALID, "nr_scene_add_object: null argument");
+  if (s->objects.size() >= NR_MAX_OBJECTS)
+    return fail(NR_ERR_LIMIT, "Hittables registry exceeded maximum registry entries [1024].");
+  int bt = base_type(*d);
+  if (d->type < NR_HITTABLE_QUAD || d->type > NR_HITTABLE_OBJECT_LIGHT)
+    return fail(NR_ERR_INVALID, "nr_scene_add_object: unknown hittable type");
+  if (bt < NR_HITTABLE_QUAD || bt > NR_HITTABLE_MESH)
+    return fail(NR_ERR_INVALID, "nr_scene_add_object: a wrapper must bind a quad, sphere, cube or mesh");
+  if (bt == NR_HITTABLE_MESH && (d->mesh < 0 || (size_t)d->mesh >= s->meshes.size()))
+    return fail(NR_ERR_INVALID, "nr_scene_add_object: unknown mesh id");
+  if (d->material < 0 || (size_t)d->material >= s->materials.size())
+    return fail(NR_ERR_INVALID, "nr_scene_add_object: unknown material id");
+  s->objects.push_back(*d);
+  if (out_id) *out_id = (uint32_t)(s->objects.size() - 1);
+  s->built = false;
+  return NR_OK;
+}
+
+int nr_scene_set_sky_null(nr_scene* s) {
+  if (!s) return fail(NR_ERR_INVALID, "null scene");
+  s->sky_type = NR_SKY_NULL;
+  s->built = false;
+  return NR_OK;
+}
+
+int nr_scene_set_sky_simple(nr_scene* s, const float a[3], const float b[3]) {
+  if (!s || !a || !b) return fail(NR_ERR_INVALID, "null argument");
+  s->sky_type = NR_SKY_SIMPLE;
+  for (int k = 0; k < 3; ++k) {
+    s->sky_start[k] = a[k];
+    s->sky_end[k] = b[k];
+  }
+  s->built = false;
+  return NR_OK;
+}
+
+int nr_scene_set_sky_hdri(nr_scene* s, const float* chw, uint32_t C, uint32_t H, uint32_t W,
+                          float rotation, float intensity) {
+  if (!s) return fail(NR_ERR_INVALID, "null scene");
+  s->sky_type = NR_SKY_HDRI;
+  s->hdri = HostImageF{};
+  if (chw) {
+    if (C < 3 || H == 0 || W == 0)
+      return fail(NR_ERR_INVALID, "nr_scene_set_sky_hdri: need at least 3 channels");
+    s->hdri.C = C;
+    s->hdri.H = H;
+    s->hdri.W = W;
+    s->hdri.chw.assign(chw, chw + (size_t)C * H * W);
+  }
+  s->hdri_rotation = rotation;
+  s->hdri_intensity = intensity;
+  s->built = false;
+  return NR_OK;
+}
+
+int nr_scene_load_hdr(nr_scene* s, const char* path, float rotation, float intensity) {
+  if (!s || !path) return fail(NR_ERR_INVALID, "null argument");
+  HostImageF im;
+  std::string err;
+  if (!load_hdr(path, im, err)) return fail(NR_ERR_IO, err);
+  s->sky_type = NR_SKY_HDRI;
+  s->hdri = std::move(im);
+  s->hdri_rotation = rotation;
+  s->hdri_intensity = intensity;
+  s->built = false;
+  return NR_OK;
+}
+
+int nr_scene_set_hdri_params(nr_scene* s, float rotation, float intensity) {
+  if (!s) return fail(NR_ERR_INVALID, "null scene");
+  s->hdri_rotation = rotation;
+  s->hdri_intensity = intensity;
+  s->built = false;
+  return NR_OK;
+}
+
+int nr_scene_build(nr_scene* s) {
+  if (!s) return fail(NR_ERR_INVALID, "null scene");
+  if (s->objects.empty()) return fail(NR_ERR_INVALID, "Hittables list cannot be empty.");
+  if (!device_available()) return fail(NR_ERR_NO_DEVICE, "no CUDA device is available");
+  s->release_device();
+  if (!s->stream) CU(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "stream");
+  cudaStream_t st = s->stream;
+  cudaEvent_t e0, e1;
+  CU(cudaEventCreate(&e0), "event");
+  CU(cudaEventCreate(&e1), "event");
+  CU(cudaEventRecord(e0, st), "event");
+
+  // device-built constants: cube faces and the HDRI rotation
+  M3 hdri_rot;
+  CU(launch_init_constants(s->hdri_rotation, &hdri_rot, st), "init constants");
+
+  // images and materials
+  for (auto& im : s->images) {
+    uint8_t* d = nullptr;
+    CU(upload(d, im.chw.data(), im.chw.size(), st), "upload image");
+    s->d_images.push_back(d);
+  }
+  std::vector<DevMaterial> mats(s->materials.size());
+  for (size_t i = 0; i < s->materials.size(); ++i) {
+    const nr_material_desc& m = s->materials[i];
+    DevMaterial& d = mats[i];
+    d.type = m.type;
+    d.ior = m.ior;
+    d.brightness = m.brightness;
+    for (int k = 0; k < 3; ++k) d.tint[k] = m.tint[k];
+    for (int k = 0; k < 5; ++k) d.tex[k] = make_tex(s, m.tex[k]);
+  }
+  CU(upload(s->d_materials, mats.data(), mats.size(), st), "upload materials");
+
+  // meshes: GPU BVH per mesh
+  uint64_t n_tris_total = 0, bin_nodes = 0, wide_nodes = 0, dev_bytes = 0;
+  double largest_sah = 0.0;
+  uint32_t largest_n = 0;
+  std::vector<DevMesh> table(s->meshes.size());
+  s->d_meshes.resize(s->meshes.size());
+  for (size_t mi = 0; mi < s->meshes.size(); ++mi) {
+    const HostMesh& hm = s->meshes[mi];
+    MeshGpu& g = s->d_meshes[mi];
+    uint32_t nv = (uint32_t)(hm.positions.size() / 3), nt = (uint32_t)(hm.triangles.size() / 3);
+    CU(upload(g.pos, hm.positions.data(), hm.positions.size(), st), "upload mesh");
+    CU(upload(g.nor, hm.normals.data(), hm.normals.size(), st), "upload mesh");
+    CU(upload(g.tan, hm.tangents.data(), hm.tangents.size(), st), "upload mesh");
+    CU(upload(g.uv, hm.uvs.data(), hm.uvs.size(), st), "upload mesh");
+    CU(upload(g.vidx, hm.triangles.data(), hm.triangles.size(), st), "upload mesh");
+    float4 *lo = nullptr, *hi = nullptr;
+    CU(cudaMalloc(&lo, sizeof(float4) * nt), "alloc boxes");
+    CU(cudaMalloc(&hi, sizeof(float4) * nt), "alloc boxes");
+    k_tri_boxes<<<(nt + 255) / 256, 256, 0, st>>>(g.pos, g.vidx, nt, lo, hi);
+    int be = build_bvh(lo, hi, nt, true, g.bvh, st);
+    cudaFree(lo);
+    cudaFree(hi);
+    if (be != 0) return cuda_fail((cudaError_t)be, "mesh BVH build");
+    CU(cudaMalloc(&g.tris2, sizeof(TriRecord) * nt), "alloc tris");
+    CU(cudaMalloc(&g.tris8, sizeof(TriRecord) * nt), "alloc tris");
+    k_tri_records<<<(nt + 255) / 256, 256, 0, st>>>(g.pos, g.vidx, g.bvh.d_order, nt, g.tris2);
+    k_tri_records<<<(nt + 255) / 256, 256, 0, st>>>(g.pos, g.vidx, g.bvh.d_order8, nt, g.tris8);
+    CU(cudaGetLastError(), "triangle records");
+    DevMesh& d = table[mi];
+    d.tris2 = g.tris2;
+    d.tris8 = g.tris8;
+    d.bvh2 = g.bvh.d_bvh2;
+    d.bvh8 = g.bvh.d_bvh8;
+    d.tri_vidx = g.vidx;
+    d.vnormal = g.nor;
+    d.vtangent = g.tan;
+    d.vuv = g.uv;
+    d.n_tris = nt;
+    d.n_bvh2 = g.bvh.n_bvh2;
+    d.n_bvh8 = g.bvh.n_bvh8;
+    n_tris_total += nt;
+    bin_nodes += g.bvh.n_nodes;
+    wide_nodes += g.bvh.n_bvh8;
+    dev_bytes += (uint64_t)nt * (2 * sizeof(TriRecord) + 12) + (uint64_t)nv * 44 +
+                 (uint64_t)g.bvh.n_bvh2 * sizeof(Bvh2Node) + (uint64_t)g.bvh.n_bvh8 * sizeof(Bvh8Node);
+    if (nt >= largest_n) {
+      largest_n = nt;
+      largest_sah = g.bvh.sah_cost;
+    }
+  }
+  CU(upload(s->d_mesh_table, table.data(), table.size(), st), "upload mesh table");
+
+  // objects (registry order) and their world boxes
+  std::vector<DevObject> objs(s->objects.size());
+  std::vector<HBox> boxes(s->objects.size());
+  std::vector<float4> blo(s->objects.size()), bhi(s->objects.size());
+  for (size_t i = 0; i < s->objects.size(); ++i) {
+    const nr_object_desc& o = s->objects[i];
+    HXform x = object_xform(o);
+    DevObject& d = objs[i];
+    memset(&d, 0, sizeof(d));
+    for (int r = 0; r < 3; ++r)
+      for (int c = 0; c < 3; ++c) {
+        d.R.m[r][c] = x.R.m[r][c];
+        d.invR.m[r][c] = x.invR.m[r][c];
+      }
+    d.pos = V3{x.pos[0], x.pos[1], x.pos[2]};
+    d.scale = V3{x.scale[0], x.scale[1], x.scale[2]};
+    d.inv_s = V3{x.inv_s[0], x.inv_s[1], x.inv_s[2]};
+    d.type = o.type;
+    d.wrapped_type = o.wrapped_type;
+    d.material = (uint32_t)o.material;
+    d.mesh = (uint32_t)std::max(0, o.mesh);
+    d.radius = o.radius + 1e-8f;
+    d.neg_inv_density = -1.0f / (o.density + 1e-8f);
+    d.object_id = (uint32_t)i;
+    boxes[i] = h_transformed(object_local_box(s, o), x);
+    blo[i] = make_float4(boxes[i].lo[0], boxes[i].lo[1], boxes[i].lo[2], 0.f);
+    bhi[i] = make_float4(boxes[i].hi[0], boxes[i].hi[1], boxes[i].hi[2], 0.f);
+  }
+  CU(upload(s->d_objects, objs.data(), objs.size(), st), "upload objects");
+  float4 *dlo = nullptr, *dhi = nullptr;
+  CU(upload(dlo, blo.data(), blo.size(), st), "upload boxes");
+  CU(upload(dhi, bhi.data(), bhi.size(), st), "upload boxes");
+  int be = build_bvh(dlo, dhi, (uint32_t)objs.size(), true, s->tlas, st);
+  cudaFree(dlo);
+  cudaFree(dhi);
+  if (be != 0) return cuda_fail((cudaError_t)be, "top-level BVH build");
+
+  // lights[0]: first OBJECT_LIGHT in the reference's top-level leaf order
+  RefOrder ro(boxes);
+  s->ref_leaf_order = ro.order;
+  s->light = -1;
+  uint32_t n_lights = 0;
+  for (int32_t idx : ro.order)
+    if (s->objects[idx].type == NR_HITTABLE_OBJECT_LIGHT) {
+      if (s->light < 0) s->light = idx;
+      n_lights++;
+    }
+
+  // sky
+  DevSky sky{};
+  sky.type = s->sky_type;
+  for (int k = 0; k < 3; ++k) {
+    sky.start[k] = s->sky_start[k];
+    sky.end[k] = s->sky_end[k];
+  }
+  sky.rotation = s->hdri_rotation;
+  sky.intensity = s->hdri_intensity;
+  sky.rot = hdri_rot;
+  if (s->sky_type == NR_SKY_HDRI && !s->hdri.chw.empty()) {
+    CU(upload(s->d_hdri, s->hdri.chw.data(), s->hdri.chw.size(), st), "upload hdri");
+    sky.data = s->d_hdri;
+    sky.C = (int)s->hdri.C;
+    sky.H = (int)s->hdri.H;
+    sky.W = (int)s->hdri.W;
+    dev_bytes += s->hdri.chw.size() * 4;
+  }
+
+  DevScene& ds = s->dev;
+  ds = DevScene{};
+  ds.objects = s->d_objects;
+  ds.n_objects = (uint32_t)objs.size();
+  ds.materials = s->d_materials;
+  ds.n_materials = (uint32_t)mats.size();
+  ds.meshes = s->d_mesh_table;
+  ds.n_meshes = (uint32_t)table.size();
+  ds.tlas2 = s->tlas.d_bvh2;
+  ds.tlas8 = s->tlas.d_bvh8;
+  ds.tlas_prims = s->tlas.d_order;
+  ds.n_tlas2 = s->tlas.n_bvh2;
+  ds.n_tlas8 = s->tlas.n_bvh8;
+  ds.light = s->light;
+  ds.use_bvh8 = 1;
+  ds.sky = sky;
+
+  CU(cudaEventRecord(e1, st), "event");
+  CU(cudaEventSynchronize(e1), "build");
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+
+  nr_scene_stats& S = s->stats;
+  S.n_objects = (uint32_t)objs.size();
+  S.n_materials = (uint32_t)mats.size();
+  S.n_lights = n_lights;
+  S.n_triangles = n_tris_total;
+  S.binary_nodes = bin_nodes + s->tlas.n_nodes;
+  S.wide_nodes = wide_nodes + s->tlas.n_bvh8;
+  S.sah_cost_binary = largest_sah;
+  S.build_ms = ms;
+  S.device_bytes = dev_bytes;
+  s->built = true;
+  return NR_OK;
+}
+
+int nr_scene_get_stats(const nr_scene* s, nr_scene_stats* out) {
+  if (!s || !out) return fail(NR_ERR_INVALID, "null argument");
+  if (!s->built) return fail(NR_ERR_STATE, "scene is not built");
+  *out = s->stats;
+  return NR_OK;
+}
+
+int nr_scene_get_binary_bvh(const nr_scene* s, uint32_t mesh_id, float* nodes8, uint64_t* n_nodes,
+                            uint32_t* prim_order) {
+  if (!s || !n_nodes) return fail(NR_ERR_INVALID, "null argument");
+  if (!s->built) return fail(NR_ERR_STATE, "scene is not built");
+  if (mesh_id >= s->d_meshes.size()) return fail(NR_ERR_INVALID, "unknown mesh id");
+  const BuildResult& b = s->d_meshes[mesh_id].bvh;
+  *n_nodes = b.n_nodes;
+  if (nodes8) {
+    std::vector<BinNode> h(b.n_nodes);
+    CU(cudaMemcpy(h.data(), b.d_nodes, sizeof(BinNode) * b.n_nodes, cudaMemcpyDeviceToHost),
+       "read nodes");
+    for (size_t i = 0; i < h.size(); ++i) {
+      float* o = nodes8 + 8 * i;
+      for (int k = 0; k < 3; ++k) {
+        o[k] = h[i].lo[k];
+        o[3 + k] = h[i].hi[k];
+      }
+      int32_t a = h[i].left >= 0 ? h[i].left : (int32_t)h[i].start;
+      int32_t c = h[i].left >= 0 ? h[i].right : -(int32_t)h[i].count;
+      memcpy(o + 6, &a, 4);
+      memcpy(o + 7, &c, 4);
+    }
+  }
+  if (prim_order) {
+    uint32_t nt = s->d_meshes[mesh_id].bvh.n_nodes ? (uint32_t)(s->meshes[mesh_id].triangles.size() / 3) : 0;
+    CU(cudaMemcpy(prim_order, b.d_order, sizeof(uint32_t) * nt, cudaMemcpyDeviceToHost), "read order");
+  }
+  return NR_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// render
+
+struct nr_render {
+  nr_scene* scene = nullptr;
+  nr_camera_desc cam{};
+  nr_render_config cfg{};
+  uint32_t W = 0, H = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  float* layer[9] = {nullptr};
+  uint32_t layer_c[9] = {0};
+  double* beauty64 = nullptr;
+  uint32_t n64 = 0;
+  float* raw[3] = {nullptr, nullptr, nullptr};
+  uint32_t* raw_primary = nullptr;
+  uint32_t* work = nullptr;
+  uint32_t* err = nullptr;
+  unsigned long long* counters = nullptr;
+  V2* pattern = nullptr;
+  uint8_t* disp8 = nullptr;
+  float* dispf = nullptr;
+  V3* wb_scratch = nullptr;
+  DevCamera dcam{};
+  int rtl = 0;
+  bool counters_on = false;
+  nr_trace_counters last{};
+  double last_ms = 0.0;
+  ~nr_render() {
+    for (auto p : layer) cudaFree(p);
+    cudaFree(beauty64);
+    for (auto p : raw) cudaFree(p);
+    cudaFree(raw_primary);
+    cudaFree(work);
+    cudaFree(err);
+    cudaFree(counters);
+    cudaFree(pattern);
+    cudaFree(disp8);
+    cudaFree(dispf);
+    cudaFree(wb_scratch);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+// Draw order of multi-draw constructor arguments in the reference's device
+// build; see DESIGN notes on argument evaluation order.
+static int g_device_rtl = 0;
+
+extern "C" {
+
+int nr_render_config_default(nr_render_config* c) {
+  if (!c) return fail(NR_ERR_INVALID, "null config");
+  memset(c, 0, sizeof(*c));
+  c->ray_depth = 8;
+  c->seed = 54321;
+  c->rr_enabled = 1;
+  c->rr_start_bounce = 3;
+  c->rr_survival = 0.95f;
+  c->mode = NR_MODE_REFERENCE;
+  c->schedule = NR_SCHEDULE_MEGAKERNEL;
+  c->fp64_accumulate = 0;
+  c->layer_mask = (1u << NR_LAYER_BEAUTY) | (1u << NR_LAYER_DIFFUSE) | (1u << NR_LAYER_WORLD_NORMAL);
+  return NR_OK;
+}
+
+// n-rooks pattern of SampleGenerator::generate_n_rooks (camera.h:45-61). The
+// two jitter draws of each Vector2(...) are evaluated right to left by the
+// reference's host compiler, so the y jitter is drawn first.
+static std::vector<V2> n_rooks(uint32_t n, uint32_t seed) {
+  std::vector<uint32_t> perm(n);
+  std::iota(perm.begin(), perm.end(), 0);
+  std::mt19937 rng(seed);
+  std::shuffle(perm.begin(), perm.end(), rng);
+  std::uniform_real_distribution<float> jitter(0.0f, 1.0f);
+  std::vector<V2> out(n);
+  for (uint32_t i = 0; i < n; ++i) {
+    float jy = jitter(rng);
+    float jx = jitter(rng);
+    out[i] = V2{(i + jx) / (float)n, (perm[i] + jy) / (float)n};
+  }
+  return out;
+}
+
+int nr_render_create(nr_scene* s, const nr_camera_desc* c, const nr_render_config* cfg,
+                     nr_render** out) {
+  if (!s || !c || !cfg || !out) return fail(NR_ERR_INVALID, "nr_render_create: null argument");
+  if (!s->built) return fail(NR_ERR_STATE, "nr_render_create: scene is not built");
+  if (c->samples_per_pixel == 0) return fail(NR_ERR_INVALID, "samples_per_pixel must be > 0");
+  if (c->resolution[0] < 1.0f || c->resolution[1] < 1.0f)
+    return fail(NR_ERR_INVALID, "resolution must be at least 1x1");
+  std::unique_ptr<nr_render> r(new nr_render());
+  r->scene = s;
+  r->cam = *c;
+  r->cfg = *cfg;
+  r->H = (uint32_t)c->resolution[0];
+  r->W = (uint32_t)c->resolution[1];
+  if ((uint64_t)r->W * r->H * (uint64_t)c->samples_per_pixel > 0xffffffffull)
+    return fail(NR_ERR_LIMIT, "pixel count x samples exceeds the 32-bit sample stream");
+  r->rtl = g_device_rtl;
+  CU(cudaStreamCreateWithFlags(&r->stream, cudaStreamNonBlocking), "stream");
+  CU(cudaEventCreate(&r->ev0), "event");
+  CU(cudaEventCreate(&r->ev1), "event");
+  size_t hw = (size_t)r->W * r->H;
+  static const uint32_t kC[9] = {3, 3, 3, 3, 3, 1, 1, 3, 3};
+  for (int l = 0; l < 9; ++l) {
+    if (!(cfg->layer_mask & (1u << l))) continue;
+    r->layer_c[l] = kC[l];
+    CU(cudaMalloc(&r->layer[l], sizeof(float) * kC[l] * hw), "alloc layer");
+    CU(cudaMemsetAsync(r->layer[l], 0, sizeof(float) * kC[l] * hw, r->stream), "clear layer");
+  }
+  if (cfg->fp64_accumulate) {
+    CU(cudaMalloc(&r->beauty64, sizeof(double) * 3 * hw), "alloc fp64");
+    CU(cudaMemsetAsync(r->beauty64, 0, sizeof(double) * 3 * hw, r->stream), "clear fp64");
+  }
+  CU(cudaMalloc(&r->work, 4), "alloc");
+  CU(cudaMalloc(&r->err, 4), "alloc");
+  CU(cudaMemsetAsync(r->err, 0, 4, r->stream), "clear");
+  CU(cudaMalloc(&r->counters, 8 * 5), "alloc");
+  CU(cudaMalloc(&r->wb_scratch, sizeof(V3)), "alloc");
+  std::vector<V2> pat = n_rooks(c->samples_per_pixel, cfg->seed);
+  CU(upload(r->pattern, pat.data(), pat.size(), r->stream), "upload pattern");
+  // CameraParams::build (camera.h:124-136)
+  HM3 R = h_euler_deg(c->rotation);
+  DevCamera& d = r->dcam;
+  d.res_x = c->resolution[0];
+  d.res_y = c->resolution[1];
+  d.position = V3{c->position[0], c->position[1], c->position[2]};
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) d.R.m[i][j] = R.m[i][j];
+  d.shutter_time = 1.0f / (c->shutter_speed + 1e-8f);
+  float aperture_radius = c->aperture / 2.0f;
+  d.defocus_angle = 2.0f * atanf(aperture_radius / (c->focus_distance + 1e-8f));
+  d.defocus_radius = c->focus_distance * tanf(d.defocus_angle / 2.0f);
+  float aspect = c->resolution[1] / c->resolution[0];
+  d.uvw_x = c->sensor_width;
+  d.uvw_y = -c->sensor_width * aspect;
+  d.focal_length = c->focal_length;
+  d.focus_distance = c->focus_distance;
+  d.W = r->W;
+  d.H = r->H;
+  d.pattern = r->pattern;
+  CU(cudaStreamSynchronize(r->stream), "render create");
+  *out = r.release();
+  return NR_OK;
+}
+
+int nr_render_destroy(nr_render* r) {
+  if (r) cudaStreamSynchronize(r->stream);
+  delete r;
+  return NR_OK;
+}
+
+int nr_render_reset(nr_render* r) {
+  if (!r) return fail(NR_ERR_INVALID, "null render");
+  size_t hw = (size_t)r->W * r->H;
+  for (int l = 0; l < 9; ++l)
+    if (r->layer[l]) CU(cudaMemsetAsync(r->layer[l], 0, sizeof(float) * r->layer_c[l] * hw, r->stream), "clear");
+  if (r->beauty64) CU(cudaMemsetAsync(r->beauty64, 0, sizeof(double) * 3 * hw, r->stream), "clear");
+  r->n64 = 0;
+  CU(cudaStreamSynchronize(r->stream), "reset");
+  return NR_OK;
+}
+
+static KernelParams make_params(nr_render* r, uint32_t first, uint32_t count, bool raw) {
+  KernelParams P;
+  memset(&P, 0, sizeof(P));
+  P.scene = r->scene->dev;
+  P.scene.use_bvh8 = 1;
+  P.cam = r->dcam;
+  P.W = r->W;
+  P.H = r->H;
+  P.first_sample = first;
+  P.n_samples = count;
+  P.seed = r->cfg.seed;
+  P.depth = r->cfg.ray_depth;
+  P.rr_enabled = r->cfg.rr_enabled;
+  P.rr_start = r->cfg.rr_start_bounce;
+  P.rr_survival = r->cfg.rr_survival;
+  P.mode = r->cfg.mode;
+  P.rtl = r->rtl;
+  P.write_raw = raw ? 1 : 0;
+  if (raw) {
+    P.beauty = r->raw[0];
+    P.diffuse = r->raw[1];
+    P.normal = r->raw[2];
+    P.primary = r->raw_primary;
+  } else {
+    P.beauty = r->layer[NR_LAYER_BEAUTY];
+    P.diffuse = r->layer[NR_LAYER_DIFFUSE];
+    P.normal = r->layer[NR_LAYER_WORLD_NORMAL];
+    P.beauty64 = r->beauty64;
+  }
+  P.work_counter = r->work;
+  P.err = r->err;
+  P.counters = r->counters;
+  return P;
+}
+
+static int run_kernel(nr_render* r, const KernelParams& P) {
+  CU(cudaMemsetAsync(r->work, 0, 4, r->stream), "clear work counter");
+  if (r->counters_on) CU(cudaMemsetAsync(r->counters, 0, 8 * 5, r->stream), "clear counters");
+  CU(cudaEventRecord(r->ev0, r->stream), "event");
+  CU(launch_megakernel(P, r->counters_on, r->stream), "launch integrator");
+  CU(cudaEventRecord(r->ev1, r->stream), "event");
+  CU(cudaEventSynchronize(r->ev1), "integrator");
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, r->ev0, r->ev1);
+  r->last_ms = ms;
+  uint32_t herr = 0;
+  CU(cudaMemcpy(&herr, r->err, 4, cudaMemcpyDeviceToHost), "read error word");
+  if (herr) {
+    cudaMemset(r->err, 0, 4);
+    return fail(NR_ERR_DEVICE, "integrator error word 0x" + std::to_string(herr) +
+                                   " (traversal stack overflow)");
+  }
+  if (r->counters_on) {
+    unsigned long long c[5];
+    CU(cudaMemcpy(c, r->counters, sizeof(c), cudaMemcpyDeviceToHost), "read counters");
+    r->last.rays = c[0];
+    r->last.node_visits = c[1];
+    r->last.tri_tests = c[2];
+    r->last.obj_tests = c[3];
+    r->last.paths = c[4];
+  }
+  return NR_OK;
+}
+
+int nr_render_samples(nr_render* r, uint32_t first, uint32_t count) {
+  if (!r) return fail(NR_ERR_INVALID, "null render");
+  if (count == 0) return NR_OK;
+  if (first == 0) return fail(NR_ERR_INVALID, "sample indices start at 1");
+  if ((uint64_t)first + count > r->cam.samples_per_pixel)
+    return fail(NR_ERR_INVALID, "sample index beyond samples_per_pixel");
+  KernelParams P = make_params(r, first, count, false);
+  int rc = run_kernel(r, P);
+  if (rc == NR_OK) r->n64 = first + count - 1;
+  return rc;
+}
+
+int nr_render_sample_layers(nr_render* r, uint32_t sample_idx, float* beauty, float* diffuse,
+                            float* normal, uint32_t* primary) {
+  if (!r) return fail(NR_ERR_INVALID, "null render");
+  if (sample_idx >= r->cam.samples_per_pixel)
+    return fail(NR_ERR_INVALID, "sample index beyond samples_per_pixel");
+  size_t hw = (size_t)r->W * r->H;
+  for (int k = 0; k < 3; ++k)
+    if (!r->raw[k]) CU(cudaMalloc(&r->raw[k], sizeof(float) * 3 * hw), "alloc raw");
+  if (!r->raw_primary) CU(cudaMalloc(&r->raw_primary, sizeof(uint32_t) * hw), "alloc raw");
+  KernelParams P = make_params(r, sample_idx, 1, true);
+  int rc = run_kernel(r, P);
+  if (rc != NR_OK) return rc;
+  if (beauty) CU(cudaMemcpy(beauty, r->raw[0], sizeof(float) * 3 * hw, cudaMemcpyDeviceToHost), "read");
+  if (diffuse) CU(cudaMemcpy(diffuse, r->raw[1], sizeof(float) * 3 * hw, cudaMemcpyDeviceToHost), "read");
+  if (normal) CU(cudaMemcpy(normal, r->raw[2], sizeof(float) * 3 * hw, cudaMemcpyDeviceToHost), "read");
+  if (primary) CU(cudaMemcpy(primary, r->raw_primary, sizeof(uint32_t) * hw, cudaMemcpyDeviceToHost), "read");
+  return NR_OK;
+}
+
+int nr_render_layer_device_ptr(nr_render* r, int32_t layer, uint64_t* out) {
+  if (!r || !out || layer < 0 || layer > 8) return fail(NR_ERR_INVALID, "bad layer");
+  *out = (uint64_t)(uintptr_t)r->layer[layer];
+  return NR_OK;
+}
+
+int nr_render_read_layer(nr_render* r, int32_t layer, float* host) {
+  if (!r || !host || layer < 0 || layer > 8) return fail(NR_ERR_INVALID, "bad layer");
+  if (!r->layer[layer]) return fail(NR_ERR_STATE, "layer is not enabled");
+  size_t n = (size_t)r->layer_c[layer] * r->W * r->H;
+  CU(cudaMemcpy(host, r->layer[layer], sizeof(float) * n, cudaMemcpyDeviceToHost), "read layer");
+  return NR_OK;
+}
+
+int nr_render_read_beauty_fp64(nr_render* r, double* host) {
+  if (!r || !host) return fail(NR_ERR_INVALID, "null argument");
+  if (!r->beauty64) return fail(NR_ERR_STATE, "fp64 accumulation is not enabled");
+  size_t n = (size_t)3 * r->W * r->H;
+  CU(cudaMemcpy(host, r->beauty64, sizeof(double) * n, cudaMemcpyDeviceToHost), "read fp64");
+  double inv = r->n64 ? 1.0 / (double)r->n64 : 0.0;
+  for (size_t i = 0; i < n; ++i) host[i] *= inv;
+  return NR_OK;
+}
+
+static int display(nr_render* r, int32_t layer, const nr_stream_config* c, uint8_t* h8, float* hf) {
+  if (!r || !c || layer < 0 || layer > 8) return fail(NR_ERR_INVALID, "bad argument");
+  if (!r->layer[layer] || r->layer_c[layer] != 3)
+    return fail(NR_ERR_STATE, "display needs an enabled 3-channel layer");
+  size_t hw = (size_t)r->W * r->H;
+  if (h8 && !r->disp8) CU(cudaMalloc(&r->disp8, 3 * hw), "alloc");
+  if (hf && !r->dispf) CU(cudaMalloc(&r->dispf, sizeof(float) * 3 * hw), "alloc");
+  DisplayParams p{};
+  p.linear_to_gamma = c->linear_to_gamma;
+  p.apply_white_balance = c->apply_white_balance;
+  p.wb_tint = c->wb_tint;
+  p.apply_tonemapping = c->apply_tonemapping;
+  p.tm_method = c->tm_method;
+  p.tm_white_point = c->tm_white_point;
+  p.tm_alpha = c->tm_alpha;
+  CU(display_params_resolve(p, c->wb_temperature, r->wb_scratch, r->stream), "white balance");
+  CU(launch_display(r->layer[layer], h8 ? r->disp8 : nullptr, hf ? r->dispf : nullptr, hw, p,
+                    r->stream),
+     "display");
+  if (h8) CU(cudaMemcpyAsync(h8, r->disp8, 3 * hw, cudaMemcpyDeviceToHost, r->stream), "read");
+  if (hf) CU(cudaMemcpyAsync(hf, r->dispf, sizeof(float) * 3 * hw, cudaMemcpyDeviceToHost, r->stream), "read");
+  CU(cudaStreamSynchronize(r->stream), "display");
+  return NR_OK;
+}
+
+int nr_render_readback(nr_render* r, int32_t layer, const nr_stream_config* c, uint8_t* h8) {
+  if (!h8) return fail(NR_ERR_INVALID, "null output");
+  return display(r, layer, c, h8, nullptr);
+}
+
+int nr_render_display_float(nr_render* r, int32_t layer, const nr_stream_config* c, float* hf) {
+  if (!hf) return fail(NR_ERR_INVALID, "null output");
+  return display(r, layer, c, nullptr, hf);
+}
+
+int nr_render_dims(const nr_render* r, uint32_t* C, uint32_t* H, uint32_t* W) {
+  if (!r) return fail(NR_ERR_INVALID, "null render");
+  if (C) *C = 3;
+  if (H) *H = r->H;
+  if (W) *W = r->W;
+  return NR_OK;
+}
+
+int nr_render_set_counters(nr_render* r, int32_t on) {
+  if (!r) return fail(NR_ERR_INVALID, "null render");
+  r->counters_on = on != 0;
+  return NR_OK;
+}
+
+int nr_render_get_counters(const nr_render* r, nr_trace_counters* out) {
+  if (!r || !out) return fail(NR_ERR_INVALID, "null argument");
+  *out = r->last;
+  return NR_OK;
+}
+
+int nr_render_last_ms(const nr_render* r, double* out) {
+  if (!r || !out) return fail(NR_ERR_INVALID, "null argument");
+  *out = r->last_ms;
+  return NR_OK;
+}
+
+int nr_render_stream(const nr_render* r, uint64_t* out) {
+  if (!r || !out) return fail(NR_ERR_INVALID, "null argument");
+  *out = (uint64_t)(uintptr_t)r->stream;
+  return NR_OK;
+}
+
+int nr_accumulate_device(float* avg, const float* smp, uint32_t C, uint32_t H, uint32_t W,
+                         uint32_t sample_idx, uint64_t stream) {
+  if (!avg || !smp || sample_idx == 0) return fail(NR_ERR_INVALID, "bad argument");
+  CU(launch_accumulate(avg, smp, (size_t)C * H * W, sample_idx, (cudaStream_t)(uintptr_t)stream),
+     "accumulate");
+  return NR_OK;
+}
+
+int nr_display_device(const float* src, uint8_t* dst, uint32_t C, uint32_t H, uint32_t W,
+                      const nr_stream_config* c, uint64_t stream) {
+  if (!src || !dst || !c || C != 3) return fail(NR_ERR_INVALID, "bad argument");
+  cudaStream_t st = (cudaStream_t)(uintptr_t)stream;
+  DisplayParams p{};
+  p.linear_to_gamma = c->linear_to_gamma;
+  p.apply_white_balance = c->apply_white_balance;
+  p.wb_tint = c->wb_tint;
+  p.apply_tonemapping = c->apply_tonemapping;
+  p.tm_method = c->tm_method;
+  p.tm_white_point = c->tm_white_point;
+  p.tm_alpha = c->tm_alpha;
+  V3* scratch = nullptr;
+  if (p.apply_white_balance) {
+    CU(cudaMalloc(&scratch, sizeof(V3)), "alloc");
+    cudaError_t e = display_params_resolve(p, c->wb_temperature, scratch, st);
+    cudaFree(scratch);
+    if (e != cudaSuccess) return cuda_fail(e, "white balance");
+  }
+  CU(launch_display(src, dst, nullptr, (size_t)H * W, p, st), "display");
+  return NR_OK;
+}
+
+}  // extern "C"

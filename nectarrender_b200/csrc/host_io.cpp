@@ -1,0 +1,360 @@
+// host_io.cpp — scene file readers: Wavefront OBJ meshes and Radiance RGBE
+// (.hdr) images.
+//
+// OBJ follows the reference loader parse_obj_file
+// (nectar_render/csrc/hittable/include/hittable/mesh.h:39-141), which drives
+// tinyobjloader with triangulation on: quads are split along the shorter
+// diagonal and larger polygons are fanned (tinyobjloader ear-clips those),
+// vertices are deduplicated on the (v, vt, vn) index triple in order of first
+// use, missing normals become the normalised sum of face normals (or +y when
+// that sum is zero), and per-vertex tangents are the orthogonalised sum of
+// per-face uv-gradient tangents ((1,0,0) for faces with degenerate uvs).
+//
+// HDR implements the Radiance picture format (G. Ward, "Real Pixels",
+// Graphics Gems II; the RGBE encoding with flat or new-style run-length
+// scanlines), decoding a texel (r, g, b, e) with e != 0 to m * 2^(e - 136) for
+// each mantissa m, and to 0 when e == 0: the conversion stbi_loadf performs
+// for the reference (nectar_render/csrc/material/include/material/texture.h:28-47).
+#include "host_io.h"
+
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <sstream>
+#include <unordered_map>
+
+namespace nr {
+
+namespace {
+
+struct Key {
+  int v, vt, vn;
+  bool operator==(const Key& o) const { return v == o.v && vt == o.vt && vn == o.vn; }
+};
+struct KeyHash {
+  size_t operator()(const Key& k) const {
+    size_t h = std::hash<int>()(k.v);
+    h = h * 1000003u ^ std::hash<int>()(k.vt);
+    h = h * 1000003u ^ std::hash<int>()(k.vn);
+    return h;
+  }
+};
+
+// host vector helpers with the reference's operation order
+struct H3 {
+  float x, y, z;
+};
+inline H3 sub(H3 a, H3 b) { return H3{a.x - b.x, a.y - b.y, a.z - b.z}; }
+inline H3 add(H3 a, H3 b) { return H3{a.x + b.x, a.y + b.y, a.z + b.z}; }
+inline H3 muls(H3 a, float t) { return H3{a.x * t, a.y * t, a.z * t}; }
+inline float lsq(H3 v) {
+  float o = v.x * v.x + v.y * v.y;
+  o += v.z * v.z;
+  return o;
+}
+inline float len(H3 v) { return sqrtf(lsq(v)); }
+inline H3 nrm(H3 v) {
+  float r = 1.0f / len(v);
+  return H3{v.x * r, v.y * r, v.z * r};
+}
+inline H3 crs(H3 u, H3 v) {
+  return H3{u.y * v.z - u.z * v.y, u.z * v.x - u.x * v.z, u.x * v.y - u.y * v.x};
+}
+inline float dt(H3 u, H3 v) { return u.x * v.x + u.y * v.y + u.z * v.z; }
+
+// OBJ index: 1-based, negative = relative to the end
+int resolve(long idx, size_t count) {
+  if (idx > 0) return (int)(idx - 1);
+  if (idx < 0) return (int)((long)count + idx);
+  return -1;
+}
+
+}  // namespace
+
+bool load_obj(const std::string& path, HostMesh& out, std::string& err) {
+  std::ifstream f(path);
+  if (!f) {
+    err = "Failed to load OBJ '" + path + "': cannot open file";
+    return false;
+  }
+  std::vector<float> vpos, vnor, vtex;
+  struct Corner {
+    int v, vt, vn;
+  };
+  std::vector<Corner> tris;  // 3 per triangle
+  std::string line;
+  std::vector<Corner> poly;
+  size_t lineno = 0;
+  while (std::getline(f, line)) {
+    ++lineno;
+    const char* s = line.c_str();
+    while (*s == ' ' || *s == '\t') ++s;
+    if (s[0] == 'v' && (s[1] == ' ' || s[1] == '\t')) {
+      char* e;
+      float a = strtof(s + 2, &e);
+      float b = strtof(e, &e);
+      float c = strtof(e, &e);
+      vpos.push_back(a);
+      vpos.push_back(b);
+      vpos.push_back(c);
+    } else if (s[0] == 'v' && s[1] == 'n' && (s[2] == ' ' || s[2] == '\t')) {
+      char* e;
+      float a = strtof(s + 3, &e);
+      float b = strtof(e, &e);
+      float c = strtof(e, &e);
+      vnor.push_back(a);
+      vnor.push_back(b);
+      vnor.push_back(c);
+    } else if (s[0] == 'v' && s[1] == 't' && (s[2] == ' ' || s[2] == '\t')) {
+      char* e;
+      float a = strtof(s + 3, &e);
+      float b = strtof(e, &e);
+      vtex.push_back(a);
+      vtex.push_back(b);
+    } else if (s[0] == 'f' && (s[1] == ' ' || s[1] == '\t')) {
+      poly.clear();
+      const char* p = s + 2;
+      while (*p) {
+        while (*p == ' ' || *p == '\t') ++p;
+        if (!*p || *p == '\r' || *p == '#') break;
+        char* e;
+        long vi = strtol(p, &e, 10), ti = 0, ni = 0;
+        if (e == p) {
+          err = "Failed to load OBJ '" + path + "': bad face at line " + std::to_string(lineno);
+          return false;
+        }
+        p = e;
+        if (*p == '/') {
+          ++p;
+          if (*p != '/') {
+            ti = strtol(p, &e, 10);
+            p = e;
+          }
+          if (*p == '/') {
+            ++p;
+            ni = strtol(p, &e, 10);
+            p = e;
+          }
+        }
+        Corner c{resolve(vi, vpos.size() / 3), ti ? resolve(ti, vtex.size() / 2) : -1,
+                 ni ? resolve(ni, vnor.size() / 3) : -1};
+        if (c.v < 0 || (size_t)c.v >= vpos.size() / 3) {
+          err = "Failed to load OBJ '" + path + "': vertex index out of range at line " +
+                std::to_string(lineno);
+          return false;
+        }
+        poly.push_back(c);
+        while (*p && *p != ' ' && *p != '\t') ++p;
+      }
+      if (poly.size() == 4) {
+        // quads split along the shorter diagonal, as tinyobjloader does
+        auto coord = [&](int v, int k) { return vpos[3 * (size_t)v + k]; };
+        float e02x = coord(poly[2].v, 0) - coord(poly[0].v, 0);
+        float e02y = coord(poly[2].v, 1) - coord(poly[0].v, 1);
+        float e02z = coord(poly[2].v, 2) - coord(poly[0].v, 2);
+        float e13x = coord(poly[3].v, 0) - coord(poly[1].v, 0);
+        float e13y = coord(poly[3].v, 1) - coord(poly[1].v, 1);
+        float e13z = coord(poly[3].v, 2) - coord(poly[1].v, 2);
+        float s02 = e02x * e02x + e02y * e02y + e02z * e02z;
+        float s13 = e13x * e13x + e13y * e13y + e13z * e13z;
+        const int a[6] = {0, 1, 2, 0, 2, 3}, b[6] = {0, 1, 3, 1, 2, 3};
+        for (int k = 0; k < 6; ++k) tris.push_back(poly[s02 < s13 ? a[k] : b[k]]);
+      } else {
+        // larger polygons are fanned (tinyobjloader ear-clips them)
+        for (size_t k = 2; k < poly.size(); ++k) {
+          tris.push_back(poly[0]);
+          tris.push_back(poly[k - 1]);
+          tris.push_back(poly[k]);
+        }
+      }
+    }
+  }
+  bool has_normals = !vnor.empty();
+  out = HostMesh{};
+  std::unordered_map<Key, uint32_t, KeyHash> uniq;
+  uniq.reserve(tris.size());
+  std::vector<H3> P, N, T;
+  std::vector<float> UV;
+  out.triangles.reserve(tris.size());
+  for (size_t i = 0; i < tris.size(); ++i) {
+    const Corner& c = tris[i];
+    Key k{c.v, c.vt, c.vn};
+    auto it = uniq.find(k);
+    if (it != uniq.end()) {
+      out.triangles.push_back(it->second);
+      continue;
+    }
+    uint32_t id = (uint32_t)P.size();
+    P.push_back(H3{vpos[3 * c.v], vpos[3 * c.v + 1], vpos[3 * c.v + 2]});
+    N.push_back(c.vn >= 0 ? H3{vnor[3 * c.vn], vnor[3 * c.vn + 1], vnor[3 * c.vn + 2]}
+                          : H3{0.f, 0.f, 0.f});
+    UV.push_back(c.vt >= 0 ? vtex[2 * c.vt] : 0.0f);
+    UV.push_back(c.vt >= 0 ? vtex[2 * c.vt + 1] : 0.0f);
+    T.push_back(H3{0.f, 0.f, 0.f});
+    uniq.emplace(k, id);
+    out.triangles.push_back(id);
+  }
+  size_t nt = out.triangles.size() / 3;
+  const uint32_t* tr = out.triangles.data();
+  if (!has_normals) {
+    for (size_t t = 0; t < nt; ++t) {
+      uint32_t a = tr[3 * t], b = tr[3 * t + 1], c = tr[3 * t + 2];
+      H3 fn = nrm(crs(sub(P[b], P[a]), sub(P[c], P[a])));
+      N[a] = add(N[a], fn);
+      N[b] = add(N[b], fn);
+      N[c] = add(N[c], fn);
+    }
+    for (auto& n : N) n = len(n) < 1e-8f ? H3{0.f, 1.f, 0.f} : nrm(n);
+  }
+  for (size_t t = 0; t < nt; ++t) {
+    uint32_t a = tr[3 * t], b = tr[3 * t + 1], c = tr[3 * t + 2];
+    H3 e1 = sub(P[b], P[a]), e2 = sub(P[c], P[a]);
+    float du1 = UV[2 * b] - UV[2 * a], dv1 = UV[2 * b + 1] - UV[2 * a + 1];
+    float du2 = UV[2 * c] - UV[2 * a], dv2 = UV[2 * c + 1] - UV[2 * a + 1];
+    float denom = du1 * dv2 - du2 * dv1;
+    H3 tg = fabsf(denom) < 1e-8f ? H3{1.f, 0.f, 0.f}
+                                 : muls(sub(muls(e1, dv2), muls(e2, dv1)), 1.0f / denom);
+    T[a] = add(T[a], tg);
+    T[b] = add(T[b], tg);
+    T[c] = add(T[c], tg);
+  }
+  for (size_t i = 0; i < T.size(); ++i) {
+    H3 t = sub(T[i], muls(N[i], dt(T[i], N[i])));
+    T[i] = len(t) < 1e-8f ? H3{1.f, 0.f, 0.f} : nrm(t);
+  }
+  size_t nv = P.size();
+  out.positions.resize(3 * nv);
+  out.normals.resize(3 * nv);
+  out.tangents.resize(3 * nv);
+  out.uvs = UV;
+  for (size_t i = 0; i < nv; ++i) {
+    out.positions[3 * i] = P[i].x;
+    out.positions[3 * i + 1] = P[i].y;
+    out.positions[3 * i + 2] = P[i].z;
+    out.normals[3 * i] = N[i].x;
+    out.normals[3 * i + 1] = N[i].y;
+    out.normals[3 * i + 2] = N[i].z;
+    out.tangents[3 * i] = T[i].x;
+    out.tangents[3 * i + 1] = T[i].y;
+    out.tangents[3 * i + 2] = T[i].z;
+  }
+  return true;
+}
+
+namespace {
+inline void rgbe_to_float(const uint8_t* in, float* out) {
+  if (in[3] != 0) {
+    float f = (float)ldexp(1.0f, (int)in[3] - (int)(128 + 8));
+    out[0] = in[0] * f;
+    out[1] = in[1] * f;
+    out[2] = in[2] * f;
+  } else {
+    out[0] = out[1] = out[2] = 0.0f;
+  }
+}
+}  // namespace
+
+bool load_hdr(const std::string& path, HostImageF& out, std::string& err) {
+  FILE* f = fopen(path.c_str(), "rb");
+  if (!f) {
+    err = "Failed to load HDRI: cannot open '" + path + "'";
+    return false;
+  }
+  std::vector<uint8_t> data;
+  {
+    uint8_t buf[1 << 16];
+    size_t n;
+    while ((n = fread(buf, 1, sizeof(buf), f)) > 0) data.insert(data.end(), buf, buf + n);
+    fclose(f);
+  }
+  size_t pos = 0;
+  auto read_line = [&](std::string& l) {
+    l.clear();
+    while (pos < data.size() && data[pos] != '\n') l.push_back((char)data[pos++]);
+    if (pos < data.size()) ++pos;
+    return true;
+  };
+  std::string l;
+  read_line(l);
+  if (l != "#?RADIANCE" && l != "#?RGBE") {
+    err = "Failed to load HDRI: not a Radiance file";
+    return false;
+  }
+  bool fmt_ok = false;
+  while (pos < data.size()) {
+    read_line(l);
+    if (l.empty()) break;
+    if (l == "FORMAT=32-bit_rle_rgbe") fmt_ok = true;
+  }
+  if (!fmt_ok) {
+    err = "Failed to load HDRI: unsupported format";
+    return false;
+  }
+  read_line(l);
+  int H = 0, W = 0;
+  if (sscanf(l.c_str(), "-Y %d +X %d", &H, &W) != 2 || H <= 0 || W <= 0) {
+    err = "Failed to load HDRI: unsupported image orientation";
+    return false;
+  }
+  out.C = 3;
+  out.H = (uint32_t)H;
+  out.W = (uint32_t)W;
+  std::vector<float> hwc((size_t)H * W * 3);
+  std::vector<uint8_t> scan((size_t)W * 4);
+  for (int y = 0; y < H; ++y) {
+    if (pos + 4 > data.size()) {
+      err = "Failed to load HDRI: truncated file";
+      return false;
+    }
+    bool rle = W >= 8 && W < 32768 && data[pos] == 2 && data[pos + 1] == 2 &&
+               !(data[pos + 2] & 0x80) && (((int)data[pos + 2] << 8) | data[pos + 3]) == W;
+    if (!rle) {
+      // flat scanlines for the whole remaining image
+      size_t need = (size_t)(H - y) * W * 4;
+      if (pos + need > data.size()) {
+        err = "Failed to load HDRI: truncated file";
+        return false;
+      }
+      for (; y < H; ++y)
+        for (int x = 0; x < W; ++x, pos += 4) rgbe_to_float(&data[pos], &hwc[((size_t)y * W + x) * 3]);
+      break;
+    }
+    pos += 4;
+    for (int ch = 0; ch < 4; ++ch) {
+      int x = 0;
+      while (x < W) {
+        if (pos >= data.size()) {
+          err = "Failed to load HDRI: truncated file";
+          return false;
+        }
+        int count = data[pos++];
+        if (count > 128) {
+          count -= 128;
+          if (count > W - x || pos >= data.size()) {
+            err = "Failed to load HDRI: bad run";
+            return false;
+          }
+          uint8_t v = data[pos++];
+          for (int k = 0; k < count; ++k) scan[(size_t)(x++) * 4 + ch] = v;
+        } else {
+          if (count == 0 || count > W - x || pos + count > data.size()) {
+            err = "Failed to load HDRI: bad dump";
+            return false;
+          }
+          for (int k = 0; k < count; ++k) scan[(size_t)(x++) * 4 + ch] = data[pos++];
+        }
+      }
+    }
+    for (int x = 0; x < W; ++x) rgbe_to_float(&scan[(size_t)x * 4], &hwc[((size_t)y * W + x) * 3]);
+  }
+  // planar CHW, as the reference's load_image_float (texture.h:28-47)
+  size_t hw = (size_t)H * W;
+  out.chw.resize(hw * 3);
+  for (size_t c = 0; c < 3; ++c)
+    for (size_t i = 0; i < hw; ++i) out.chw[c * hw + i] = hwc[i * 3 + c];
+  return true;
+}
+
+}  // namespace nr

@@ -1,0 +1,217 @@
+"""Checker libraries for the path-tracing hot path — TEST INFRASTRUCTURE.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
+this package, and only to check or time against it; the product never calls
+it.
+
+* ``Oracle``  — liboracle.so, the CPU restatement of the reference integrator
+  (oracle.cpp), pinned against the reference itself;
+* ``RefCPU``  — _ref/libref_cpu.so, the reference's own integrator headers
+  compiled for the host (built here by oracle/Makefile from the reference
+  sources, shipped as a binary);
+* ``RefCUDA`` — _ref/libref_cuda.so, the reference's CUDA path compiled for
+  sm_100a.
+
+Parity is pinned: the restatement is compared bit for bit with RefCPU on the
+same seeded scenes (tests/test_oracle_pin.py), and RefCPU/RefCUDA are the
+reference code.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+from nectarrender_b200.capi import CameraDesc, MaterialDesc, ObjectDesc, RenderConfig
+from nectarrender_b200.capi import camera_desc, material_desc, object_desc, render_config
+from nectarrender_b200.scenes import SKY_HDRI, SKY_SIMPLE, SceneSpec
+
+HERE = Path(__file__).resolve().parent
+ORACLE_SO = HERE / "liboracle.so"
+REF_CPU_SO = HERE / "_ref" / "libref_cpu.so"
+REF_CUDA_SO = HERE / "_ref" / "libref_cuda.so"
+REF_SRC = Path("/root/reference/nectar_render/csrc")
+
+
+def build(reference: bool | None = None) -> None:
+    """make -C oracle (reference targets only where the reference sources exist)."""
+    targets = [str(ORACLE_SO)]
+    if reference is None:
+        reference = REF_SRC.exists()
+    if reference:
+        targets += [str(REF_CPU_SO), str(REF_CUDA_SO)]
+    r = subprocess.run(["make", "-C", str(HERE), *targets], capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("oracle build failed:\n" + r.stdout[-4000:] + r.stderr[-4000:])
+
+
+class OrMesh(C.Structure):
+    _fields_ = [("obj_path", C.c_char_p), ("positions", C.POINTER(C.c_float)),
+                ("normals", C.POINTER(C.c_float)), ("tangents", C.POINTER(C.c_float)),
+                ("uvs", C.POINTER(C.c_float)), ("n_vertices", C.c_uint32),
+                ("triangles", C.POINTER(C.c_uint32)), ("n_triangles", C.c_uint32)]
+
+
+class OrScene(C.Structure):
+    _fields_ = [("materials", C.POINTER(MaterialDesc)), ("n_materials", C.c_uint32),
+                ("objects", C.POINTER(ObjectDesc)), ("n_objects", C.c_uint32),
+                ("meshes", C.POINTER(OrMesh)), ("n_meshes", C.c_uint32),
+                ("sky_type", C.c_int32), ("sky_start", C.c_float * 3), ("sky_end", C.c_float * 3),
+                ("hdri", C.POINTER(C.c_float)), ("hdri_C", C.c_uint32), ("hdri_H", C.c_uint32),
+                ("hdri_W", C.c_uint32), ("hdri_rotation", C.c_float), ("hdri_intensity", C.c_float),
+                ("hdri_path", C.c_char_p)]
+
+
+class OrRequest(C.Structure):
+    _fields_ = [("first", C.c_uint32), ("count", C.c_uint32), ("mode", C.c_int32),
+                ("draw_rtl", C.c_int32), ("row_begin", C.c_uint32), ("row_end", C.c_uint32),
+                ("threads", C.c_int32), ("beauty", C.POINTER(C.c_float)),
+                ("diffuse", C.POINTER(C.c_float)), ("normal", C.POINTER(C.c_float)),
+                ("primary", C.POINTER(C.c_uint32)), ("beauty64", C.POINTER(C.c_double))]
+
+
+def _f(a):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+class _Lib:
+    prefix = ""
+    path: Path
+
+    def __init__(self):
+        if not self.path.exists():
+            raise FileNotFoundError(f"{self.path} not built (oracle/Makefile)")
+        self.lib = C.CDLL(str(self.path))
+        getattr(self.lib, self.prefix + "mesh_sah").restype = C.c_double
+        self._keep: list = []
+
+    def load_obj(self, path: str):
+        fn = getattr(self.lib, self.prefix + "load_obj")
+        cap_v, cap_t = 1 << 23, 1 << 23
+        nv, nt = C.c_uint32(), C.c_uint32()
+        P = np.zeros(3 * cap_v, np.float32)
+        N, T = np.zeros_like(P), np.zeros_like(P)
+        UV = np.zeros(2 * cap_v, np.float32)
+        tris = np.zeros(3 * cap_t, np.uint32)
+        rc = fn(path.encode(), _f(P), _f(N), _f(T), _f(UV), tris.ctypes.data_as(C.POINTER(C.c_uint32)),
+                C.byref(nv), C.byref(nt), cap_v, cap_t)
+        if rc != 0:
+            raise RuntimeError(f"load_obj failed ({rc}) for {path}")
+        v, t = nv.value, nt.value
+        return (P[:3 * v].copy(), N[:3 * v].copy(), T[:3 * v].copy(), UV[:2 * v].copy(),
+                tris[:3 * t].copy())
+
+    def load_hdr(self, path: str):
+        fn = getattr(self.lib, self.prefix + "load_hdr")
+        cap = 64 << 20
+        buf = np.zeros(cap, np.float32)
+        c, h, w = C.c_uint32(), C.c_uint32(), C.c_uint32()
+        rc = fn(path.encode(), _f(buf), C.byref(c), C.byref(h), C.byref(w), C.c_uint64(cap))
+        if rc != 0:
+            raise RuntimeError(f"load_hdr failed ({rc}) for {path}")
+        return buf[:c.value * h.value * w.value].reshape(c.value, h.value, w.value).copy()
+
+    def or_scene(self, spec: SceneSpec) -> OrScene:
+        keep = []
+        mats = [MaterialDesc()]
+        d0 = mats[0]
+        d0.type = 1
+        d0.tex[0].rgb = (C.c_float * 3)(1.0, 0.0, 1.0)
+        d0.tex[0].scale = 1.0
+        objs = []
+        for i, o in enumerate(spec.objects):
+            mats.append(material_desc(o["material"]))
+            objs.append(object_desc(o, i + 1))
+        mat_arr = (MaterialDesc * len(mats))(*mats)
+        obj_arr = (ObjectDesc * len(objs))(*objs)
+        meshes = []
+        for p in spec.meshes:
+            P, N, T, UV, tris = self.load_obj(p)
+            keep += [P, N, T, UV, tris]
+            m = OrMesh(p.encode(), _f(P), _f(N), _f(T), _f(UV), len(P) // 3,
+                       tris.ctypes.data_as(C.POINTER(C.c_uint32)), len(tris) // 3)
+            meshes.append(m)
+        mesh_arr = (OrMesh * max(1, len(meshes)))(*meshes)
+        s = OrScene()
+        s.materials, s.n_materials = mat_arr, len(mats)
+        s.objects, s.n_objects = obj_arr, len(objs)
+        s.meshes, s.n_meshes = mesh_arr, len(meshes)
+        s.sky_type = spec.sky["type"]
+        if spec.sky["type"] == SKY_SIMPLE:
+            s.sky_start = (C.c_float * 3)(*spec.sky["start"])
+            s.sky_end = (C.c_float * 3)(*spec.sky["end"])
+        if spec.sky["type"] == SKY_HDRI:
+            img = self.load_hdr(spec.sky["path"])
+            keep.append(img)
+            s.hdri = _f(img)
+            s.hdri_C, s.hdri_H, s.hdri_W = img.shape
+            s.hdri_rotation = spec.sky.get("rotation", 0.0)
+            s.hdri_intensity = spec.sky.get("intensity", 1.0)
+            s.hdri_path = spec.sky["path"].encode()
+        keep += [mat_arr, obj_arr, mesh_arr]
+        self._keep = keep
+        return s
+
+    def render(self, spec: SceneSpec, first: int, count: int = 1, mode: int = 1,
+               rows: tuple[int, int] | None = None, threads: int = 0, draw_rtl: int = 1,
+               fp64: bool = False, cfg: RenderConfig | None = None):
+        """mode 0: raw layers of sample `first`; mode 1: running mean of
+        samples [first, first+count). Returns (beauty, diffuse, normal,
+        primary, beauty64) as numpy arrays."""
+        s = self.or_scene(spec)
+        cam = camera_desc(spec.camera)
+        cfg = cfg or render_config(spec)
+        H, W = int(spec.camera["resolution"][0]), int(spec.camera["resolution"][1])
+        b = np.zeros((3, H, W), np.float32)
+        d, n = np.zeros_like(b), np.zeros_like(b)
+        p = np.full((H, W), 0xffffffff, np.uint32)
+        b64 = np.zeros((3, H, W), np.float64) if fp64 else None
+        r0, r1 = rows or (0, H)
+        req = OrRequest(first, count, mode, draw_rtl, r0, r1, threads, _f(b), _f(d), _f(n),
+                        p.ctypes.data_as(C.POINTER(C.c_uint32)),
+                        b64.ctypes.data_as(C.POINTER(C.c_double)) if fp64 else None)
+        rc = getattr(self.lib, self.prefix + "render")(C.byref(s), C.byref(cam), C.byref(cfg),
+                                                        C.byref(req))
+        if rc != 0:
+            raise RuntimeError(f"{self.prefix}render failed ({rc})")
+        return b, d, n, p, b64
+
+    def mesh_sah(self, spec: SceneSpec, mesh: int = 0) -> tuple[float, int]:
+        P, N, T, UV, tris = self.load_obj(spec.meshes[mesh])
+        m = OrMesh(spec.meshes[mesh].encode(), _f(P), _f(N), _f(T), _f(UV), len(P) // 3,
+                   tris.ctypes.data_as(C.POINTER(C.c_uint32)), len(tris) // 3)
+        nn = C.c_uint64()
+        v = getattr(self.lib, self.prefix + "mesh_sah")(C.byref(m), C.byref(nn))
+        return float(v), int(nn.value)
+
+    def uniforms(self, seed: int, sub: int, count: int) -> np.ndarray:
+        out = np.zeros(count, np.float32)
+        getattr(self.lib, self.prefix + "uniforms")(seed, sub, count, _f(out))
+        return out
+
+
+class Oracle(_Lib):
+    prefix = "oracle_"
+    path = ORACLE_SO
+
+    def n_rooks(self, n: int, seed: int, draw_rtl: int = 1) -> np.ndarray:
+        out = np.zeros(2 * n, np.float32)
+        self.lib.oracle_n_rooks(n, seed, draw_rtl, _f(out))
+        return out.reshape(n, 2)
+
+
+class RefCPU(_Lib):
+    prefix = "refcpu_"
+    path = REF_CPU_SO
+
+    def n_rooks(self, n: int, seed: int) -> np.ndarray:
+        out = np.zeros(2 * n, np.float32)
+        self.lib.refcpu_n_rooks(n, seed, _f(out))
+        return out.reshape(n, 2)
+
+    def render(self, spec, first, count=1, mode=1, rows=None, threads=0, draw_rtl=1, fp64=False,
+               cfg=None):
+        # the reference's host build evaluates multi-draw arguments right to left
+        return super().render(spec, first, count, mode, rows, threads, 1, fp64, cfg)
