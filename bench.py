@@ -1,0 +1,383 @@
+#!/usr/bin/env python3
+"""Benchmark of the path-tracing hot path: pixel-samples per second.
+
+Workload (default): the BVH/mesh stress scene — a 1,310,720-triangle
+displaced icosphere, 256 spheres, a 2048x1024 procedural HDRI, 1920x1080
+pixels, depth 12 — rendered with the reference-compatible integrator. One
+step renders `--spp-per-step` samples per pixel over the full image (the
+reference's render() loop body for that many sample indices). The scene is
+seeded synthetic data (see nectarrender_b200/scenes.py).
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference]
+
+N > 1 runs one process per GPU under torch.distributed (NCCL): each rank
+renders its own slice of sample indices (weak scaling, no collective inside
+the timed region); the per-rank images are combined by one all-reduce after
+timing. `--impl reference` times the reference's own integrator compiled
+for the host (oracle/_ref/libref_cpu.so, all host threads) on the same scene,
+rank 0 only.
+
+Prints one JSON line (rank 0).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+sys.path.insert(0, str(HERE))
+
+import numpy as np
+
+from nectarrender_b200 import scenes
+
+METRIC = "samples/s (pixel-samples per second, mesh-stress scene)"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--spp-per-step", type=int, default=4)
+    p.add_argument("--levels", type=int, default=8)
+    p.add_argument("--res", default="1080x1920", help="HxW as CameraParams.resolution")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-reference-cuda", action="store_true")
+    p.add_argument("--cpu-seconds", type=float, default=12.0)
+    return p.parse_args()
+
+
+def workload(args):
+    h, w = (int(x) for x in args.res.split("x"))
+    total = args.warmup + args.steps + 1
+    spec = scenes.mesh_stress(levels=args.levels, res_h=h, res_w=w,
+                              spp=max(256, args.spp_per_step * total * max(1, args.gpus)))
+    return spec, h, w
+
+
+def config_json(args, h, w, spec, l2):
+    return {"workload": f"mesh_stress: icosphere L{args.levels} "
+                        f"({20 * 4 ** args.levels} tris) + 256 spheres + 2048x1024 HDRI, "
+                        f"{w}x{h}, depth {spec.ray_depth}",
+            "width": w, "height": h, "ray_depth": spec.ray_depth,
+            "spp_per_step": args.spp_per_step, "integrator": "reference-compatible megakernel",
+            "parallelism": f"sample-sharded x{args.gpus}", "l2": l2}
+
+
+# ---------------------------------------------------------------------------
+# clocks
+
+class Clocks:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except FileNotFoundError:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        self.out = ""
+        if self.p:
+            self.p.terminate()
+            try:
+                self.out, _ = self.p.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+
+    def summary(self):
+        rows = []
+        for line in (getattr(self, "out", "") or "").splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                rows.append((float(f[1]), float(f[2]), float(f[3]), f[5:9]))
+            except ValueError:
+                continue
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        load = [r for r in rows if r[2] > 250.0] or rows
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in load for n, v in zip(names, r[3]) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(r[0] for r in load), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+# reference arm: the reference's integrator compiled for the host
+
+def cpu_reference(spec):
+    """The reference's integrator compiled for the host (oracle/_ref), else
+    the oracle port; the scene is built once, outside any timing."""
+    import oracle
+    try:
+        lib, kind = oracle.RefCPU(), "reference"
+    except (FileNotFoundError, OSError):
+        lib, kind = oracle.Oracle(), "port"
+    return lib.open_scene(spec), kind
+
+
+def cpu_reference_rate(spec, h, w, seconds: float):
+    """Row bands of 1 spp at full resolution, doubling until ~`seconds` of
+    CPU work; returns (rows, seconds, kind, cores)."""
+    handle, kind = cpu_reference(spec)
+    cores = os.cpu_count() or 1
+    rows, done, t_total = 4, 0, 0.0
+    while t_total < seconds and done < h:
+        r1 = min(h, done + rows)
+        t0 = time.perf_counter()
+        handle.render(1, 1, mode=0, rows=(done, r1), threads=cores)
+        t_total += time.perf_counter() - t0
+        done = r1
+        rows *= 2
+    return done, t_total, kind, cores
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    spec, h, w = workload(args)
+    handle, kind = cpu_reference(spec)
+    cores = os.cpu_count() or 1
+    per_step_rows = max(4, h // 128)
+    times = []
+    for i in range(args.warmup + args.steps):
+        r0 = (i * per_step_rows) % max(1, h - per_step_rows)
+        t0 = time.perf_counter()
+        handle.render(1, 1, mode=0, rows=(r0, r0 + per_step_rows), threads=cores)
+        if i >= args.warmup:
+            times.append(time.perf_counter() - t0)
+    t = sum(times)
+    value = per_step_rows * w * args.steps / t
+    sample_desc = (f"{per_step_rows} rows x {w} px x 1 spp per step of the {w}x{h} frame; "
+                   f"scene parsed and host BVH built once before timing")
+    line = {"metric": METRIC, "value": value, "unit": "samples/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded scene generator)", "impl": "reference",
+            "config": config_json(args, h, w, spec, "n/a (CPU)"),
+            "cpu_baseline": {"value": value, "unit": "samples/s", "cores": cores, "kind": kind,
+                             "sample": sample_desc},
+            "e2e": {"value": value, "unit": "samples/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# our arm
+
+def run_ours(args):
+    import ctypes
+    import torch
+    from nectarrender_b200 import capi, library, pathtracer
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    spec, h, w = workload(args)
+    lib = library()
+    t_build = time.perf_counter()
+    scene = capi.Scene(spec)
+    build_wall = time.perf_counter() - t_build
+    stats = scene.stats()
+    render = capi.Render(scene)
+    stream_handle = ctypes.c_uint64()
+    lib.nr_render_stream(render.h, ctypes.byref(stream_handle))
+    stream = torch.cuda.ExternalStream(stream_handle.value)
+    S = args.spp_per_step
+    # sample indices of this rank: disjoint slices per step
+    def first_index(step):
+        return 1 + (step * world + rank) * S
+
+    # warm-up
+    for i in range(args.warmup):
+        render.samples(first_index(i), S)
+    # counting launch (outside timing) for the roofline's algorithmic bytes
+    render.counters(True)
+    render.samples(first_index(args.warmup), S)
+    counts = render.last_counters()
+    render.counters(False)
+    l2_flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    with Clocks(local) as clk:
+        for k in range(args.steps):
+            l2_flush.zero_()  # evict the scene from L2 between timed steps
+            torch.cuda.synchronize()
+            ev[k][0].record(stream)
+            render.samples(first_index(args.warmup + 1 + k), S)
+            ev[k][1].record(stream)
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    t_ms = sum(step_ms)
+    if dist:
+        tt = torch.tensor([t_ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_ms = float(tt.item())
+    samples = float(w * h * S * args.steps * world)
+    value = samples / (t_ms * 1e-3)
+
+    # combine the ranks' accumulators once (after timing)
+    combine_ms = None
+    if dist:
+        img = torch.from_numpy(render.layer(0)).cuda()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        dist.all_reduce(img)
+        torch.cuda.synchronize()
+        combine_ms = 1e3 * (time.perf_counter() - t0)
+
+    # roofline of the integrator kernel from counted record fetches
+    # wide nodes 80 B, triangle records 48 B, object records 128 B, and the
+    # running-mean load+store of 3 layers x 3 channels x 4 B per pixel
+    per_launch_bytes = (counts["node_visits"] * 80 + counts["tri_tests"] * 48 +
+                        counts["obj_tests"] * 128 + w * h * 72)
+    kernel_ms = t_ms / args.steps
+    achieved = per_launch_bytes / (kernel_ms * 1e-3) / 1e9
+    peaks = {}
+    try:
+        peaks = json.loads((HERE / "MEASURED_PEAKS.json").read_text())
+        peak, peak_src = float(peaks["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        peak, peak_src = 6650.0, "fallback"
+    traffic = None
+    tp = HERE / "profiles" / "megakernel_traffic.json"
+    if tp.exists():
+        try:
+            t = json.loads(tp.read_text())
+            traffic = t["dram_bytes_per_sample"] * w * h * S
+        except (OSError, KeyError, ValueError):
+            traffic = None
+
+    # end to end through the public API: render + display readback to host
+    e2e = None
+    if rank == 0:
+        pt = pathtracer()
+        e2e = e2e_public_api(pt, spec, S, args)
+
+    ref_cuda = None
+    if rank == 0 and not args.no_reference_cuda:
+        ref_cuda = reference_cuda_rate(spec, w, h)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        done, secs, kind, cores = cpu_reference_rate(spec, h, w, args.cpu_seconds)
+        cpu = {"value": done * w / secs, "unit": "samples/s", "cores": cores, "kind": kind,
+               "sample": f"rows 0..{done} of the {w}x{h} frame at 1 spp, all host threads "
+                         f"(scene parsed and host BVH built once before timing)"}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "samples/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_ms / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded scene generator)",
+                "config": config_json(args, h, w, spec, "flushed between timed steps (256 MiB write)"),
+                "clocks": clk.summary(),
+                "e2e": e2e,
+                "gpu_launches": args.steps,
+                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                             "frac": achieved / peak, "traffic": traffic,
+                             "peak_source": peak_src,
+                             "algorithmic_bytes_per_launch": per_launch_bytes,
+                             "counts_per_launch": counts},
+                "cpu_baseline": cpu,
+                "reference_cuda": ref_cuda,
+                "scene": {"build_ms_device": stats["build_ms"], "build_wall_s": build_wall,
+                          "triangles": stats["n_triangles"], "wide_nodes": stats["wide_nodes"],
+                          "sah_cost_binary": stats["sah_cost_binary"]},
+                "step_ms": step_ms}
+        if combine_ms is not None:
+            line["combine_allreduce_ms"] = combine_ms
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def e2e_public_api(pt, spec, S, args):
+    """RenderEngine.render() for S samples + TransferStream.readback() (uint8
+    CHW to host), timed per step with the host clock around the public calls
+    (each call synchronises); camera parameters travel host->device per step."""
+    scene, cam, keep = scenes.to_pathtracer(spec, pt)
+    params = cam.parameters()
+    params.samples_per_pixel = S + 1
+    cam = pt.engine.camera.Camera(params)
+    eng = pt.engine.RenderEngine(cam, spec.ray_depth, spec.seed)
+    eng.set_scene(scene)
+    st = eng.stream()
+    cfg = pt.data.StreamConfig()
+    cfg.apply_denoising = False
+    st.update_config(cfg)
+    times = []
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        eng.set_n_samples(S + 1)   # re-creates the render: camera + pattern H2D, layers cleared
+        eng.render()
+        ptr = st.readback()
+        dt = time.perf_counter() - t0
+        if i >= args.warmup:
+            times.append(dt)
+    w, h = int(spec.camera["resolution"][1]), int(spec.camera["resolution"][0])
+    v = w * h * S * len(times) / sum(times)
+    h2d = 56 + 8 * (S + 1) + 1024
+    return {"value": v, "unit": "samples/s", "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": 3 * w * h,
+            "path": "_pathtracer RenderEngine.render + TransferStream.readback (uint8 CHW)"}
+
+
+def reference_cuda_rate(spec, w, h):
+    """The reference's CUDA path (sm_100a build) on the same scene: 2 samples,
+    its render loop timed with CUDA events."""
+    try:
+        import oracle
+        rc = oracle.RefCUDA()
+        res = rc.render(spec, 1, count=2, mode=1)
+        ms = res[3]
+        return {"value": w * h * 2 / (ms * 1e-3), "unit": "samples/s", "samples": 2,
+                "note": "reference trace_full + accumulate loop compiled for sm_100a, same scene"}
+    except Exception as e:  # noqa: BLE001 - reported, not fatal
+        return {"unavailable": repr(e)[:200]}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

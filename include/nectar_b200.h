@@ -210,6 +210,13 @@ int nr_abi_version(void);
 const char* nr_last_error(void);
 /* Number of CUDA devices visible (0 without a GPU; never fails). */
 int nr_device_count(void);
+/* Order in which NR_MODE_REFERENCE consumes random draws for the reference's
+ * constructor calls that take several draws as arguments (Vector3::random,
+ * Quad::random, random_in_unit_disk; C++ leaves it unspecified): 0 = left to
+ * right, as the reference's CUDA device code does (measured on sm_100a),
+ * 1 = right to left, as its host-compiled code does. */
+int nr_device_draw_order(void);
+int nr_set_draw_order(int right_to_left);
 
 /* scene (replaces Scene / HittablesRegistry / MaterialRegisty:
  * nectar_render/csrc/scene/include/scene.h:15-77,
@@ -229,6 +236,11 @@ int nr_scene_add_image(nr_scene* scene, const uint8_t* chw, uint32_t C, uint32_t
 int nr_scene_add_mesh(nr_scene* scene, const float* positions, const float* normals,
                       const float* tangents, const float* uvs, uint32_t n_vertices,
                       const uint32_t* triangles, uint32_t n_triangles, uint32_t* out_id);
+/* Reads back mesh `mesh_id` as stored (after OBJ parsing): pass NULL
+ * arrays to query n_vertices / n_triangles first. Needs no GPU. */
+int nr_scene_get_mesh(const nr_scene* scene, uint32_t mesh_id, float* positions, float* normals,
+                      float* tangents, float* uvs, uint32_t* triangles, uint32_t* n_vertices,
+                      uint32_t* n_triangles);
 /* Wavefront OBJ file (parse_obj_file, mesh.h:39-141): triangulated faces,
  * vertices deduplicated on the (v, vt, vn) index triple, smooth normals when
  * the file has none, per-vertex tangents from uv gradients. */

@@ -67,8 +67,10 @@ class TraceCounters(C.Structure):
 
 # symbols declared in include/nectar_b200.h
 EXPORTS = [
-    "nr_abi_version", "nr_last_error", "nr_device_count", "nr_scene_create", "nr_scene_destroy",
-    "nr_scene_add_material", "nr_scene_add_image", "nr_scene_add_mesh", "nr_scene_load_obj",
+    "nr_abi_version", "nr_last_error", "nr_device_count", "nr_device_draw_order",
+    "nr_set_draw_order", "nr_scene_create", "nr_scene_destroy",
+    "nr_scene_add_material", "nr_scene_add_image", "nr_scene_add_mesh", "nr_scene_get_mesh",
+    "nr_scene_load_obj",
     "nr_scene_add_object", "nr_scene_set_sky_null", "nr_scene_set_sky_simple",
     "nr_scene_set_sky_hdri", "nr_scene_load_hdr", "nr_scene_set_hdri_params", "nr_scene_build",
     "nr_scene_get_stats", "nr_scene_get_binary_bvh", "nr_render_config_default",
@@ -78,6 +80,12 @@ EXPORTS = [
     "nr_render_dims", "nr_render_set_counters", "nr_render_get_counters", "nr_render_last_ms",
     "nr_render_stream", "nr_accumulate_device", "nr_display_device",
 ]
+
+
+def device_draw_order() -> int:
+    """0: multi-draw constructor arguments consume draws left to right (the
+    reference's CUDA build), 1: right to left (its host build)."""
+    return int(library().nr_device_draw_order())
 
 
 def _check(rc: int, what: str) -> None:
@@ -189,6 +197,20 @@ class Scene:
         s = SceneStats()
         _check(self.lib.nr_scene_get_stats(self.h, C.byref(s)), "nr_scene_get_stats")
         return {k: getattr(s, k) for k, _ in SceneStats._fields_}
+
+    def mesh(self, mesh_id: int = 0):
+        """(positions, normals, tangents, uvs, triangles) as stored after parsing."""
+        nv, nt = C.c_uint32(), C.c_uint32()
+        _check(self.lib.nr_scene_get_mesh(self.h, mesh_id, None, None, None, None, None,
+                                          C.byref(nv), C.byref(nt)), "nr_scene_get_mesh")
+        P = np.zeros(3 * nv.value, np.float32)
+        N, T = np.zeros_like(P), np.zeros_like(P)
+        UV = np.zeros(2 * nv.value, np.float32)
+        tris = np.zeros(3 * nt.value, np.uint32)
+        _check(self.lib.nr_scene_get_mesh(self.h, mesh_id, _fptr(P), _fptr(N), _fptr(T), _fptr(UV),
+                                          tris.ctypes.data_as(C.POINTER(C.c_uint32)),
+                                          C.byref(nv), C.byref(nt)), "nr_scene_get_mesh")
+        return P, N, T, UV, tris
 
     def binary_bvh(self, mesh_id: int = 0) -> tuple[np.ndarray, np.ndarray]:
         n = C.c_uint64()

@@ -496,6 +496,18 @@ __global__ void k_split_large(const Task* tasks, uint32_t n_tasks, const TaskBin
     si.bin = so.bin;
     si.nleft = so.nl;
   }
+  if (si.nleft == 0 || si.nleft >= T.count) {
+    // cannot happen with consistent binning; guarantees progress regardless
+    atomicOr(err, 16u);
+    si.axis = -1;
+    si.bin = -1;
+    si.nleft = T.count / 2;
+    for (int k = 0; k < 6; ++k) { so.lbox[k] = pbox[k]; so.rbox[k] = pbox[k]; }
+    for (int k = 0; k < 3; ++k) {
+      so.lcb[k] = T.cmin[k]; so.lcb[3 + k] = T.cmax[k];
+      so.rcb[k] = T.cmin[k]; so.rcb[3 + k] = T.cmax[k];
+    }
+  }
   splits[t] = si;
   uint32_t id = atomicAdd(node_counter, 2u);
   uint32_t nl = si.nleft, nr = T.count - si.nleft;
@@ -681,7 +693,12 @@ __global__ void __launch_bounds__(32 * kSmallWarps) k_small(
   }
   sp = 1;
   __syncwarp();
+  uint32_t iterations = 0;
   while (sp > 0) {
+    if (++iterations > 4u * kSmall) {  // each iteration splits a node: at most n - 1 splits
+      if (lane == 0) atomicOr(err, 32u);
+      break;
+    }
     --sp;
     SmallShared::Entry E = S.stack[sp];
     __syncwarp();
@@ -717,6 +734,11 @@ __global__ void __launch_bounds__(32 * kSmallWarps) k_small(
     SplitOut so;
     warp_eval(S.cnt, S.blo, S.bhi, S.clo, S.chi, E.cmin, E.cmax, so);
     uint32_t nl;
+    if (so.axis >= 0 && (so.nl == 0 || so.nl >= E.lc)) {
+      // cannot happen with consistent binning; guarantees progress regardless
+      if (lane == 0) atomicOr(err, 16u);
+      so.axis = -1;
+    }
     if (so.axis < 0) {
       // median split in the current order; bounds by warp reduction
       nl = E.lc / 2;
@@ -1122,7 +1144,12 @@ int build_bvh(const float4* d_lo, const float4* d_hi, uint32_t n, bool want_bvh8
   }
   NR_TRY(cudaMemcpyAsync(counters, hc, sizeof(hc), cudaMemcpyHostToDevice, st));
 
+  int levels = 0;
   while (n_large > 0) {
+    if (++levels > 96) {
+      fprintf(stderr, "nectar_b200: BVH build did not converge\n");
+      return (int)cudaErrorUnknown;
+    }
     k_task_blocks<<<(n_large + 255) / 256, 256, 0, st>>>(large, n_large, blk_start);
     k_scan_single<<<1, 1024, 0, st>>>(blk_start, n_large, counters + 7);
     uint32_t total_blocks = 0;
@@ -1201,7 +1228,9 @@ int build_bvh(const float4* d_lo, const float4* d_hi, uint32_t n, bool want_bvh8
     uint32_t hz[3] = {1u, 0u, 0u};  // wide counter, prim counter, n_next
     NR_TRY(cudaMemcpyAsync(counters + 4, hz, sizeof(hz), cudaMemcpyHostToDevice, st));
     uint32_t n_cur = 1;
+    int wide_levels = 0;
     while (n_cur > 0) {
+      if (++wide_levels > 96) return (int)cudaErrorUnknown;
       NR_TRY(cudaMemsetAsync(counters + 6, 0, 4, st));
       k_collapse<<<(n_cur + 127) / 128, 128, 0, st>>>(nodes, order, wa, n_cur, wb, counters + 6,
                                                       counters + 4, counters + 5, out.d_bvh8,

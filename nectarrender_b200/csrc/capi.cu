@@ -572,6 +572,21 @@ int nr_scene_load_obj(nr_scene* s, const char* path, uint32_t* out_id) {
   return NR_OK;
 }
 
+int nr_scene_get_mesh(const nr_scene* s, uint32_t id, float* P, float* N, float* T, float* UV,
+                      uint32_t* tris, uint32_t* nv, uint32_t* nt) {
+  if (!s || !nv || !nt) return fail(NR_ERR_INVALID, "nr_scene_get_mesh: null argument");
+  if (id >= s->meshes.size()) return fail(NR_ERR_INVALID, "nr_scene_get_mesh: unknown mesh id");
+  const HostMesh& m = s->meshes[id];
+  *nv = (uint32_t)(m.positions.size() / 3);
+  *nt = (uint32_t)(m.triangles.size() / 3);
+  if (P) std::copy(m.positions.begin(), m.positions.end(), P);
+  if (N) std::copy(m.normals.begin(), m.normals.end(), N);
+  if (T) std::copy(m.tangents.begin(), m.tangents.end(), T);
+  if (UV) std::copy(m.uvs.begin(), m.uvs.end(), UV);
+  if (tris) std::copy(m.triangles.begin(), m.triangles.end(), tris);
+  return NR_OK;
+}
+
 int nr_scene_add_object(nr_scene* s, const nr_object_desc* d, uint32_t* out_id) {
   if (!s || !d) return fail(NR_ERR_INVALID, "nr_scene_add_object: null argument");
   if (s->objects.size() >= NR_MAX_OBJECTS)
@@ -925,11 +940,17 @@ struct nr_render {
   }
 };
 
-// Draw order of multi-draw constructor arguments in the reference's device
-// build; see DESIGN notes on argument evaluation order.
+// Order of the draws taken by multi-draw constructor arguments: the
+// reference's CUDA build evaluates them left to right (probed on sm_100a).
 static int g_device_rtl = 0;
 
 extern "C" {
+
+int nr_device_draw_order(void) { return g_device_rtl; }
+int nr_set_draw_order(int rtl) {
+  g_device_rtl = rtl ? 1 : 0;
+  return NR_OK;
+}
 
 int nr_render_config_default(nr_render_config* c) {
   if (!c) return fail(NR_ERR_INVALID, "null config");
@@ -1094,7 +1115,7 @@ static int run_kernel(nr_render* r, const KernelParams& P) {
   if (herr) {
     cudaMemset(r->err, 0, 4);
     return fail(NR_ERR_DEVICE, "integrator error word 0x" + std::to_string(herr) +
-                                   " (traversal stack overflow)");
+                                   " (1: traversal stack overflow, 8: traversal step bound)");
   }
   if (r->counters_on) {
     unsigned long long c[5];

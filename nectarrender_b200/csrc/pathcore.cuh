@@ -186,6 +186,10 @@ struct TraceStats {
 #ifndef NR_STACK
 #define NR_STACK 64
 #endif
+// Upper bound on traversal steps of one query; a well-formed tree needs far
+// fewer. Reaching it sets error bit 8 and ends the query, so a corrupted tree
+// can never keep a kernel spinning.
+constexpr uint32_t kMaxTraversalSteps = 1u << 20;
 
 // Closest triangle of a mesh in object space with Interval(tmin, tmax) and
 // inclusive acceptance (mesh.h:239-292): returns the leaf-order triangle slot.
@@ -201,7 +205,11 @@ __device__ __forceinline__ int mesh_closest_bvh2(const DevMesh& m, const Ray& r,
   int sp = 0;
   int cur = 0;
   if (m.n_bvh2 == 0) return -1;
-  while (true) {
+  for (uint32_t steps = 0;; ++steps) {
+    if (steps >= kMaxTraversalSteps || (uint32_t)cur >= m.n_bvh2) {
+      atomicOr(err, 8u);
+      break;
+    }
     const Bvh2Node* nd = m.bvh2 + cur;
     float4 A = __ldg(&nd->a), B = __ldg(&nd->b), C = __ldg(&nd->c);
     int4 D = __ldg(&nd->d);
@@ -329,7 +337,11 @@ __device__ __forceinline__ int mesh_closest_bvh8(const DevMesh& m, const Ray& r,
   // to node 0.
   uint2 ngroup = make_uint2(0u, 0x80000000u);
   const uint32_t oct_inv = 7u - oct;
-  while (true) {
+  for (uint32_t steps = 0;; ++steps) {
+    if (steps >= kMaxTraversalSteps) {
+      atomicOr(err, 8u);
+      break;
+    }
     if (ngroup.y > 0x00ffffffu) {
       uint32_t hits = ngroup.y;
       uint32_t child_bit = 31u - __clz(hits);
@@ -337,6 +349,10 @@ __device__ __forceinline__ int mesh_closest_bvh8(const DevMesh& m, const Ray& r,
       uint32_t slot = (child_bit - 24u) ^ oct_inv;
       uint32_t imask = hits & 0xffu;
       uint32_t node_index = ngroup.x + __popc(imask & ~(0xffffffffu << slot));
+      if (node_index >= m.n_bvh8) {
+        atomicOr(err, 8u);
+        break;
+      }
       if (ngroup.y > 0x00ffffffu) {
         if (sp < NR_STACK) stack[sp++] = ngroup;
         else atomicOr(err, 1u);
@@ -499,7 +515,11 @@ __device__ __forceinline__ bool scene_hit(const DevScene& sc, const Ray& wr, Hit
   uint32_t stack[NR_STACK];
   int sp = 0;
   int cur = 0;
-  while (true) {
+  for (uint32_t steps = 0;; ++steps) {
+    if (steps >= kMaxTraversalSteps || (uint32_t)cur >= sc.n_tlas2) {
+      atomicOr(err, 8u);
+      break;
+    }
     const Bvh2Node* nd = sc.tlas2 + cur;
     float4 A = __ldg(&nd->a), B = __ldg(&nd->b), C = __ldg(&nd->c);
     int4 D = __ldg(&nd->d);

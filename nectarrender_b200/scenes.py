@@ -30,7 +30,8 @@ from pathlib import Path
 
 import numpy as np
 
-ASSETS = Path(os.environ.get("NR_ASSET_DIR", Path(__file__).resolve().parent / "_assets"))
+# generated assets are cached outside the source tree
+ASSETS = Path(os.environ.get("NR_ASSET_DIR", "/tmp/nectarrender_b200_assets"))
 
 # nr_hittable / nr_material enums (include/nectar_b200.h)
 QUAD, SPHERE, CUBE, MESH, MEDIUM, LIGHT = 1, 2, 3, 4, 5, 6

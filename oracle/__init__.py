@@ -178,6 +178,10 @@ class _Lib:
             raise RuntimeError(f"{self.prefix}render failed ({rc})")
         return b, d, n, p, b64
 
+    def open_scene(self, spec: SceneSpec, draw_rtl: int = 1) -> "SceneHandle":
+        """Builds the checker's scene once (files parsed, BVH built on the host)."""
+        return SceneHandle(self, spec, draw_rtl)
+
     def mesh_sah(self, spec: SceneSpec, mesh: int = 0) -> tuple[float, int]:
         P, N, T, UV, tris = self.load_obj(spec.meshes[mesh])
         m = OrMesh(spec.meshes[mesh].encode(), _f(P), _f(N), _f(T), _f(UV), len(P) // 3,
@@ -192,6 +196,44 @@ class _Lib:
         return out
 
 
+class SceneHandle:
+    def __init__(self, lib: "_Lib", spec: SceneSpec, draw_rtl: int):
+        self.lib, self.spec = lib, spec
+        self.draw_rtl = draw_rtl
+        s = lib.or_scene(spec)
+        self._keep = lib._keep
+        create = getattr(lib.lib, lib.prefix + "scene_create")
+        create.restype = C.c_void_p
+        self.h = create(C.byref(s), draw_rtl)
+        if not self.h:
+            raise RuntimeError("scene_create failed")
+
+    def render(self, first: int, count: int = 1, mode: int = 1, rows=None, threads: int = 0,
+               fp64: bool = False, cfg: RenderConfig | None = None, spec: SceneSpec | None = None):
+        spec = spec or self.spec
+        cam = camera_desc(spec.camera)
+        cfg = cfg or render_config(spec)
+        H, W = int(spec.camera["resolution"][0]), int(spec.camera["resolution"][1])
+        b = np.zeros((3, H, W), np.float32)
+        d, n = np.zeros_like(b), np.zeros_like(b)
+        p = np.full((H, W), 0xffffffff, np.uint32)
+        b64 = np.zeros((3, H, W), np.float64) if fp64 else None
+        r0, r1 = rows or (0, H)
+        req = OrRequest(first, count, mode, self.draw_rtl, r0, r1, threads, _f(b), _f(d), _f(n),
+                        p.ctypes.data_as(C.POINTER(C.c_uint32)),
+                        b64.ctypes.data_as(C.POINTER(C.c_double)) if fp64 else None)
+        fn = getattr(self.lib.lib, self.lib.prefix + "scene_render")
+        rc = fn(C.c_void_p(self.h), C.byref(cam), C.byref(cfg), C.byref(req))
+        if rc != 0:
+            raise RuntimeError(f"scene_render failed ({rc})")
+        return b, d, n, p, b64
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            getattr(self.lib.lib, self.lib.prefix + "scene_destroy")(C.c_void_p(self.h))
+            self.h = None
+
+
 class Oracle(_Lib):
     prefix = "oracle_"
     path = ORACLE_SO
@@ -200,6 +242,17 @@ class Oracle(_Lib):
         out = np.zeros(2 * n, np.float32)
         self.lib.oracle_n_rooks(n, seed, draw_rtl, _f(out))
         return out.reshape(n, 2)
+
+
+def display(img: np.ndarray, cfg) -> tuple[np.ndarray, np.ndarray]:
+    """Oracle display transform of a (3, H, W) float image: (uint8, float)."""
+    lib = Oracle().lib
+    img = np.ascontiguousarray(img, dtype=np.float32)
+    hw = img.shape[1] * img.shape[2]
+    o8 = np.zeros(img.shape, np.uint8)
+    of = np.zeros(img.shape, np.float32)
+    lib.oracle_display(_f(img), hw, C.byref(cfg), o8.ctypes.data_as(C.POINTER(C.c_uint8)), _f(of))
+    return o8, of
 
 
 class RefCPU(_Lib):
@@ -215,3 +268,47 @@ class RefCPU(_Lib):
                cfg=None):
         # the reference's host build evaluates multi-draw arguments right to left
         return super().render(spec, first, count, mode, rows, threads, 1, fp64, cfg)
+
+
+class RefCUDA(_Lib):
+    """The reference's CUDA path (sm_100a build of trace.cu, data.cu, cuda.cu,
+    scene.cpp) driven through its own host API."""
+    prefix = "refcuda_"
+    path = REF_CUDA_SO
+
+    def __init__(self):
+        if not self.path.exists():
+            raise FileNotFoundError(f"{self.path} not built (oracle/Makefile)")
+        self.lib = C.CDLL(str(self.path))
+        self._keep = []
+        self.cpu = RefCPU()  # file readers for the scene description
+
+    def load_obj(self, path):
+        return self.cpu.load_obj(path)
+
+    def load_hdr(self, path):
+        return self.cpu.load_hdr(path)
+
+    def probe_draw_order(self) -> tuple[int, int]:
+        a, b = C.c_int(), C.c_int()
+        rc = self.lib.refcuda_probe_draw_order(C.byref(a), C.byref(b))
+        if rc != 0:
+            raise RuntimeError(f"draw-order probe failed ({rc})")
+        return a.value, b.value
+
+    def render(self, spec, first, count=1, mode=1, rows=None, threads=0, draw_rtl=1, fp64=False,
+               cfg=None):
+        """Returns (beauty, diffuse, normal, elapsed_ms) of the reference's
+        CUDA render loop over samples [first, first+count)."""
+        s = self.or_scene(spec)
+        cam = camera_desc(spec.camera)
+        cfg = cfg or render_config(spec)
+        H, W = int(spec.camera["resolution"][0]), int(spec.camera["resolution"][1])
+        b = np.zeros((3, H, W), np.float32)
+        d, n = np.zeros_like(b), np.zeros_like(b)
+        req = OrRequest(first, count, mode, 0, 0, H, 0, _f(b), _f(d), _f(n), None, None)
+        ms = C.c_double()
+        rc = self.lib.refcuda_render(C.byref(s), C.byref(cam), C.byref(cfg), C.byref(req), C.byref(ms))
+        if rc != 0:
+            raise RuntimeError(f"refcuda_render failed ({rc})")
+        return b, d, n, ms.value

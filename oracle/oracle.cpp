@@ -1188,6 +1188,54 @@ bool read_hdr(const char* path, std::vector<float>& chw, uint32_t& H, uint32_t& 
   return true;
 }
 
+
+// display transform (data/src/stream.cu:7-159): white balance, tonemap,
+// sqrt gamma, then NaN->0, clamp, *255 and truncation to uint8
+V kelvin_rgb(float kelvin) {
+  float temp = kelvin / 100.0f, r, g, b;
+  if (temp <= 66.0f) {
+    r = 255.0f;
+    g = 99.4708025861f * logf(temp) - 161.1195681661f;
+  } else {
+    r = 329.698727446f * powf(temp - 60.0f, -0.1332047592f);
+    g = 288.1221695283f * powf(temp - 60.0f, -0.0755148492f);
+  }
+  if (temp >= 66.0f) b = 255.0f;
+  else if (temp <= 19.0f) b = 0.0f;
+  else b = 138.5177312231f * logf(temp - 10.0f) - 305.0447927307f;
+  return V{fminf(1.0f, fmaxf(0.0f, r / 255.0f)), fminf(1.0f, fmaxf(0.0f, g / 255.0f)),
+           fminf(1.0f, fmaxf(0.0f, b / 255.0f))};
+}
+V display_pixel(V c, const nr_stream_config& cfg) {
+  if (cfg.apply_white_balance) {
+    V ref = kelvin_rgb(6500.0f);
+    V tgt = kelvin_rgb(fmaxf(1000.0f, fminf(cfg.wb_temperature, 40000.0f)));
+    V ratio{tgt.x / fmaxf(ref.x, 1e-4f), tgt.y / fmaxf(ref.y, 1e-4f), tgt.z / fmaxf(ref.z, 1e-4f)};
+    c = c * ratio;
+    float tint = cfg.wb_tint * 0.0025f;
+    c = V{c.x * (1.0f + tint * 0.5f), c.y * (1.0f - tint), c.z * (1.0f + tint * 0.5f)};
+  }
+  if (cfg.apply_tonemapping) {
+    V col = c;
+    if (cfg.tm_method == 1) {
+      float iw2 = 1.0f / (cfg.tm_white_point * cfg.tm_white_point);
+      V num = col * (V{1, 1, 1} + col * iw2);
+      col = num / (V{1, 1, 1} + col);
+    } else if (cfg.tm_method == 2) {
+      V num = col * (col * 2.51f + 0.03f);
+      V den = col * (col * 2.43f + 0.59f) + 0.14f;
+      col = V{fminf(1.0f, fmaxf(0.0f, num.x / den.x)), fminf(1.0f, fmaxf(0.0f, num.y / den.y)),
+              fminf(1.0f, fmaxf(0.0f, num.z / den.z))};
+    }
+    float a = cfg.tm_alpha;
+    c = ((1.0f - a) * c + a * col);
+    c = V{fminf(1.0f, fmaxf(0.0f, c.x)), fminf(1.0f, fmaxf(0.0f, c.y)), fminf(1.0f, fmaxf(0.0f, c.z))};
+  }
+  if (cfg.linear_to_gamma)
+    c = V{c.x > 0.0f ? sqrtf(c.x) : 0.0f, c.y > 0.0f ? sqrtf(c.y) : 0.0f, c.z > 0.0f ? sqrtf(c.z) : 0.0f};
+  return c;
+}
+
 // ---- integrator (engine/src/trace.cu:11-79, engine/src/brdf.cu:4-35) --------
 struct Sample {
   V beauty{0, 0, 0}, diffuse{0, 0, 0}, normal{0, 0, 0};
@@ -1371,11 +1419,26 @@ V running_mean(V avg, V s, uint32_t n) {  // data.cu:28-50
 
 extern "C" {
 
-int oracle_render(const or_scene* in, const nr_camera_desc* cam, const nr_render_config* cfg,
-                  const or_request* req) {
-  if (!in || !cam || !cfg || !req) return -1;
+struct OracleHandle {
   Scene S;
-  if (!build_scene(in, req->draw_rtl != 0, S)) return -2;
+};
+
+void* oracle_scene_create(const or_scene* in, int32_t draw_rtl) {
+  if (!in) return nullptr;
+  OracleHandle* h = new OracleHandle();
+  if (!build_scene(in, draw_rtl != 0, h->S)) {
+    delete h;
+    return nullptr;
+  }
+  return h;
+}
+
+void oracle_scene_destroy(void* h) { delete static_cast<OracleHandle*>(h); }
+
+int oracle_scene_render(void* handle, const nr_camera_desc* cam, const nr_render_config* cfg,
+                        const or_request* req) {
+  if (!handle || !cam || !cfg || !req) return -1;
+  const Scene& S = static_cast<OracleHandle*>(handle)->S;
   Cam c = make_cam(*cam, cfg->seed);
   uint32_t r0 = req->row_begin, r1 = std::min(req->row_end, c.H);
   size_t hw = (size_t)c.W * c.H;
@@ -1417,6 +1480,16 @@ int oracle_render(const or_scene* in, const nr_camera_desc* cam, const nr_render
   }
   for (auto& th : pool) th.join();
   return 0;
+}
+
+int oracle_render(const or_scene* in, const nr_camera_desc* cam, const nr_render_config* cfg,
+                  const or_request* req) {
+  if (!in || !req) return -1;
+  void* h = oracle_scene_create(in, req->draw_rtl);
+  if (!h) return -2;
+  int rc = oracle_scene_render(h, cam, cfg, req);
+  oracle_scene_destroy(h);
+  return rc;
 }
 
 double oracle_mesh_sah(const or_mesh* om, uint64_t* n_nodes) {
@@ -1478,6 +1551,25 @@ int oracle_load_hdr(const char* path, float* chw, uint32_t* C, uint32_t* H, uint
   *W = w;
   if (d.size() > cap) return 1;
   std::copy(d.begin(), d.end(), chw);
+  return 0;
+}
+
+int oracle_display(const float* chw, uint32_t hw, const nr_stream_config* cfg, uint8_t* out8,
+                   float* outf) {
+  for (size_t i = 0; i < hw; ++i) {
+    V c = display_pixel(V{chw[i], chw[hw + i], chw[2 * hw + i]}, *cfg);
+    if (outf) {
+      outf[i] = c.x;
+      outf[hw + i] = c.y;
+      outf[2 * hw + i] = c.z;
+    }
+    float v[3] = {c.x, c.y, c.z};
+    for (int k = 0; k < 3; ++k) {
+      float x = std::isnan(v[k]) ? 0.0f : v[k];
+      x = fmaxf(0.0f, fminf(1.0f, x)) * 255.0f;
+      if (out8) out8[k * (size_t)hw + i] = (uint8_t)x;
+    }
+  }
   return 0;
 }
 

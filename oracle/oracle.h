@@ -66,6 +66,11 @@ typedef struct or_request {
 
 int oracle_render(const or_scene* s, const nr_camera_desc* cam, const nr_render_config* cfg,
                   const or_request* req);
+/* the same with the scene built once: create, render any number of times, destroy */
+void* oracle_scene_create(const or_scene* s, int32_t draw_rtl);
+int oracle_scene_render(void* scene, const nr_camera_desc* cam, const nr_render_config* cfg,
+                        const or_request* req);
+void oracle_scene_destroy(void* scene);
 /* Binary-tree SAH cost C = sum_inner A/A_root + sum_leaf A/A_root * N of the
  * reference builder (bvh.h:35-320) over triangle boxes of a mesh. */
 double oracle_mesh_sah(const or_mesh* m, uint64_t* n_nodes);
@@ -82,9 +87,18 @@ int oracle_load_obj(const char* path, float* positions, float* normals, float* t
 int oracle_load_hdr(const char* path, float* chw, uint32_t* C, uint32_t* H, uint32_t* W,
                     uint64_t capacity);
 
+/* display transform of process_stream_kernel (data/src/stream.cu:146-159)
+ * over hw pixels of a planar 3-channel float image */
+int oracle_display(const float* chw, uint32_t hw, const nr_stream_config* cfg, uint8_t* out8,
+                   float* outf);
+
 /* same signatures in the reference builds */
 int refcpu_render(const or_scene* s, const nr_camera_desc* cam, const nr_render_config* cfg,
                   const or_request* req);
+void* refcpu_scene_create(const or_scene* s, int32_t draw_rtl);
+int refcpu_scene_render(void* scene, const nr_camera_desc* cam, const nr_render_config* cfg,
+                        const or_request* req);
+void refcpu_scene_destroy(void* scene);
 double refcpu_mesh_sah(const or_mesh* m, uint64_t* n_nodes);
 int refcpu_n_rooks(uint32_t n, uint32_t seed, float* out);
 int refcpu_uniforms(uint32_t seed, uint32_t subsequence, uint32_t count, float* out);

@@ -310,9 +310,13 @@ Out trace_pixel(RefScene& S, DeviceCamera& cam, const nr_render_config& cfg, int
 
 extern "C" {
 
-int refcpu_render(const or_scene* in, const nr_camera_desc* c, const nr_render_config* cfg,
-                  const or_request* req) {
-  std::unique_ptr<RefScene> S = build(in);
+void* refcpu_scene_create(const or_scene* in, int32_t) { return build(in).release(); }
+
+void refcpu_scene_destroy(void* h) { delete static_cast<RefScene*>(h); }
+
+int refcpu_scene_render(void* handle, const nr_camera_desc* c, const nr_render_config* cfg,
+                        const or_request* req) {
+  RefScene* S = static_cast<RefScene*>(handle);
   CameraParams params(Vector2(c->resolution[0], c->resolution[1]),
                       Vector3(c->position[0], c->position[1], c->position[2]),
                       Vector3(c->rotation[0], c->rotation[1], c->rotation[2]), c->samples_per_pixel,
@@ -365,6 +369,14 @@ int refcpu_render(const or_scene* in, const nr_camera_desc* c, const nr_render_c
     });
   for (auto& th : pool) th.join();
   return 0;
+}
+
+int refcpu_render(const or_scene* in, const nr_camera_desc* c, const nr_render_config* cfg,
+                  const or_request* req) {
+  void* h = refcpu_scene_create(in, 1);
+  int rc = refcpu_scene_render(h, c, cfg, req);
+  refcpu_scene_destroy(h);
+  return rc;
 }
 
 double refcpu_mesh_sah(const or_mesh* om, uint64_t* n_nodes) {

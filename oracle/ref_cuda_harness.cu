@@ -1,0 +1,179 @@
+// ref_cuda_harness.cu — drives the reference's CUDA path compiled for sm_100a
+// (TEST INFRASTRUCTURE, built by oracle/Makefile into oracle/_ref/).
+//
+// The scene is assembled through the reference's own host API (Hittable,
+// Material and Texture factories, Skylight::simple/hdri, Scene::build), the
+// camera through Camera::__construct, and each sample runs the reference's
+// trace_full launcher followed by RenderLayers::accumulate and clear, with a
+// device synchronisation per sample: the loop body of RenderEngine::render
+// (nectar_render/csrc/engine/src/engine.cpp:42-74) without its GUI polling.
+// The only addition is clearing freshly allocated AOV buffers, which the
+// reference leaves to whatever cudaMalloc returns (its fill kernel writes one
+// element, core/src/cuda.cu:64-74).
+#include <chrono>
+#include <cstring>
+#include <memory>
+#include <vector>
+#include <pybind11/functional.h>
+#include <pybind11/numpy.h>
+#include <pybind11/pybind11.h>
+
+#include "core/include/core.h"
+#include "engine/include/engine/trace.h"
+#include "engine/include/engine/camera.h"
+#include "scene/include/scene.h"
+#include "data/include/data.h"
+
+#include "oracle.h"
+
+namespace {
+
+std::shared_ptr<Texture> tex(const nr_texture_desc& t) {
+  return Texture::from_color(Color(t.rgb[0], t.rgb[1], t.rgb[2]));
+}
+
+Material material(const nr_material_desc& d) {
+  switch (d.type) {
+    case NR_MATERIAL_LAMBERTIAN: return Material::lambertian(tex(d.tex[0]));
+    case NR_MATERIAL_PBR:
+      return Material::pbr(tex(d.tex[0]), tex(d.tex[1]), tex(d.tex[2]), tex(d.tex[3]), tex(d.tex[4]));
+    case NR_MATERIAL_DIELECTRIC: return Material::dielectric(Color(d.tint[0], d.tint[1], d.tint[2]), d.ior);
+    case NR_MATERIAL_EMISSIVE: return Material::emissive(tex(d.tex[0]), d.brightness);
+    case NR_MATERIAL_ISOTROPIC: return Material::isotropic(tex(d.tex[0]));
+  }
+  return Material();
+}
+
+Hittable shape(int type, const nr_object_desc& d, const or_scene* s, Material m) {
+  Vector3 p(d.position[0], d.position[1], d.position[2]);
+  Vector3 r(d.rotation[0], d.rotation[1], d.rotation[2]);
+  Vector3 sc(d.scale[0], d.scale[1], d.scale[2]);
+  switch (type) {
+    case NR_HITTABLE_QUAD: return Hittable::quad(p, r, sc, std::move(m));
+    case NR_HITTABLE_CUBE: return Hittable::cube(p, r, sc, std::move(m));
+    case NR_HITTABLE_SPHERE: return Hittable::sphere(p, d.radius, std::move(m));
+    case NR_HITTABLE_MESH: return Hittable::mesh(s->meshes[d.mesh].obj_path, p, r, sc, std::move(m));
+  }
+  return Hittable();
+}
+
+__global__ void probe_kernel(float* out) {
+  Generator g(7u, 11u);
+  Vector3 v = Vector3::random(-1.0f, 1.0f, g);
+  out[0] = v.x(); out[1] = v.y(); out[2] = v.z();
+  Generator h(7u, 11u);
+  Quad q;
+  Transform xf;
+  Vector3 p = q.random(Vector3(0.0f), h, xf);
+  out[3] = p.x(); out[4] = p.y(); out[5] = p.z();
+  Generator k(7u, 11u);
+  for (int i = 0; i < 3; ++i) out[6 + i] = k.random_float(-1.0f, 1.0f);
+  Generator k2(7u, 11u);
+  for (int i = 0; i < 2; ++i) out[9 + i] = k2.random_float();
+}
+
+void clear(RenderLayers& L) {
+  for (DataObject* o : L.get_data())
+    if (o->is_enabled() && o->data_ptr()) cudaMemset(o->data_ptr(), 0, o->n_bytes());
+}
+
+void read3(DataObject& o, float* host) {
+  if (host) cudaMemcpy(host, o.data_ptr(), o.n_bytes(), cudaMemcpyDeviceToHost);
+}
+
+}  // namespace
+
+extern "C" {
+
+// Draw order of Vector3::random and Quad::random in device code:
+// 1 = right to left, 0 = left to right, -1 = neither.
+int refcuda_probe_draw_order(int* vec3_order, int* quad_order) {
+  float* d = nullptr;
+  if (cudaMalloc(&d, 16 * sizeof(float)) != cudaSuccess) return -1;
+  probe_kernel<<<1, 1>>>(d);
+  float h[16];
+  if (cudaMemcpy(h, d, sizeof(h), cudaMemcpyDeviceToHost) != cudaSuccess) return -2;
+  cudaFree(d);
+  *vec3_order = (h[0] == h[6] && h[2] == h[8]) ? 0 : ((h[0] == h[8] && h[2] == h[6]) ? 1 : -1);
+  float ra = h[3] + 0.5f;  // corner.x = -0.5, u = (1,0,0)
+  *quad_order = (ra == h[9]) ? 0 : ((ra == h[10]) ? 1 : -1);
+  return 0;
+}
+
+int refcuda_render(const or_scene* s, const nr_camera_desc* c, const nr_render_config* cfg,
+                   const or_request* req, double* elapsed_ms) {
+  cudaDeviceSetLimit(cudaLimitStackSize, CUDA_STACK_SIZE_LIMIT);
+  std::vector<std::unique_ptr<Hittable>> keep;
+  std::vector<Hittable*> hittables, lights;
+  for (uint32_t i = 0; i < s->n_objects; ++i) {
+    const nr_object_desc& d = s->objects[i];
+    const nr_material_desc& md = s->materials[d.material];
+    if (d.type == NR_HITTABLE_OBJECT_LIGHT || d.type == NR_HITTABLE_CONSTANT_MEDIUM) {
+      keep.emplace_back(new Hittable(shape(d.wrapped_type, d, s, Material())));
+      Hittable& bound = *keep.back();
+      if (d.type == NR_HITTABLE_OBJECT_LIGHT) {
+        keep.emplace_back(new Hittable(Hittable::object_light(bound, md.brightness, tex(md.tex[0]))));
+        lights.push_back(keep.back().get());
+      } else {
+        keep.emplace_back(new Hittable(Hittable::constant_medium(bound, d.density, tex(md.tex[0]))));
+        hittables.push_back(keep.back().get());
+      }
+    } else {
+      keep.emplace_back(new Hittable(shape(d.type, d, s, material(md))));
+      hittables.push_back(keep.back().get());
+    }
+  }
+  Skylight sky;
+  if (s->sky_type == NR_SKY_SIMPLE)
+    sky = Skylight::simple(Color(s->sky_start[0], s->sky_start[1], s->sky_start[2]),
+                           Color(s->sky_end[0], s->sky_end[1], s->sky_end[2]));
+  else if (s->sky_type == NR_SKY_HDRI) {
+    sky = Skylight::hdri(std::string(s->hdri_path));
+    sky.config_hdri().rotation = s->hdri_rotation;
+    sky.config_hdri().intensity = s->hdri_intensity;
+  }
+  auto scene = std::make_unique<Scene>(hittables, lights, std::move(sky));
+  scene->build();
+  CameraParams params(Vector2(c->resolution[0], c->resolution[1]),
+                      Vector3(c->position[0], c->position[1], c->position[2]),
+                      Vector3(c->rotation[0], c->rotation[1], c->rotation[2]), c->samples_per_pixel,
+                      c->focal_length, c->focus_distance, c->aperture, c->sensor_width, c->shutter_speed);
+  Camera cam(params);
+  cam.__construct(cfg->seed);
+  RenderLayers aovs(cam.resolution());
+  RenderLayers sample_aovs(&aovs);
+  clear(aovs);
+  clear(sample_aovs);
+  cudaDeviceSynchronize();
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0);
+  uint32_t last = req->first + (req->mode == 0 ? 1 : req->count);
+  for (uint32_t smp = req->first; smp < last; ++smp) {
+    TraceConfig tc{smp, cfg->ray_depth, cfg->seed, cfg->rr_enabled != 0, cfg->rr_start_bounce,
+                   cfg->rr_survival};
+    trace_full(cam, scene->graph, sample_aovs.aovs(), tc);
+    if (req->mode == 0) break;
+    aovs.accumulate(sample_aovs, smp);
+    sample_aovs.clear();
+    cudaDeviceSynchronize();
+  }
+  cudaEventRecord(e1);
+  cudaEventSynchronize(e1);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  if (elapsed_ms) *elapsed_ms = ms;
+  cudaError_t err = cudaGetLastError();
+  RenderLayers& src = req->mode == 0 ? sample_aovs : aovs;
+  read3(src.beauty, req->beauty);
+  read3(src.diffuse, req->diffuse);
+  read3(src.world_normal, req->normal);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  aovs.free_aovs();
+  sample_aovs.free_aovs();
+  return err == cudaSuccess ? 0 : (int)err;
+}
+
+}  // extern "C"
