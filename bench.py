@@ -35,7 +35,7 @@ sys.path.insert(0, str(HERE))
 
 import numpy as np
 
-from nectarrender_b200 import scenes
+from nectarrender_b200 import capi, scenes
 
 METRIC = "samples/s (pixel-samples per second, mesh-stress scene)"
 
@@ -52,6 +52,8 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-reference-cuda", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=12.0)
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--schedule", default="wavefront", choices=["wavefront", "megakernel"])
     return p.parse_args()
 
 
@@ -68,7 +70,8 @@ def config_json(args, h, w, spec, l2):
                         f"({20 * 4 ** args.levels} tris) + 256 spheres + 2048x1024 HDRI, "
                         f"{w}x{h}, depth {spec.ray_depth}",
             "width": w, "height": h, "ray_depth": spec.ray_depth,
-            "spp_per_step": args.spp_per_step, "integrator": "reference-compatible megakernel",
+            "spp_per_step": args.spp_per_step,
+            "integrator": f"reference-compatible, {args.schedule} schedule",
             "parallelism": f"sample-sharded x{args.gpus}", "l2": l2}
 
 
@@ -205,7 +208,7 @@ def run_ours(args):
     scene = capi.Scene(spec)
     build_wall = time.perf_counter() - t_build
     stats = scene.stats()
-    render = capi.Render(scene)
+    render = capi.Render(scene, schedule=1 if args.schedule == "wavefront" else 0)
     stream_handle = ctypes.c_uint64()
     lib.nr_render_stream(render.h, ctypes.byref(stream_handle))
     stream = torch.cuda.ExternalStream(stream_handle.value)
@@ -283,7 +286,7 @@ def run_ours(args):
 
     # end to end through the public API: render + display readback to host
     e2e = None
-    if rank == 0:
+    if rank == 0 and not args.no_e2e:
         pt = pathtracer()
         e2e = e2e_public_api(pt, spec, S, args)
 
@@ -306,7 +309,7 @@ def run_ours(args):
                 "config": config_json(args, h, w, spec, "flushed between timed steps (256 MiB write)"),
                 "clocks": clk.summary(),
                 "e2e": e2e,
-                "gpu_launches": args.steps,
+                "gpu_launches": args.steps * (render_launches_per_step(spec, args)),
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "traffic": traffic,
                              "peak_source": peak_src,
@@ -326,6 +329,17 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def render_launches_per_step(spec, args):
+    """Kernels of ours launched per step: the megakernel once; the wavefront
+    per wave generate + depth x (extend, shade, queue rotate) + accumulate."""
+    if args.schedule == "megakernel":
+        return 1
+    h, w = (int(x) for x in args.res.split("x"))
+    per_wave = max(1, min(8, (8 << 20) // (w * h)))
+    waves = -(-args.spp_per_step // per_wave)
+    return waves * (2 + 3 * spec.ray_depth)
+
+
 def e2e_public_api(pt, spec, S, args):
     """RenderEngine.render() for S samples + TransferStream.readback() (uint8
     CHW to host), timed per step with the host clock around the public calls
@@ -343,7 +357,7 @@ def e2e_public_api(pt, spec, S, args):
     times = []
     for i in range(args.warmup + args.steps):
         t0 = time.perf_counter()
-        eng.set_n_samples(S + 1)   # re-creates the render: camera + pattern H2D, layers cleared
+        eng.set_n_samples(S + 1)   # restart at sample 1 (RenderEngine.set_n_samples)
         eng.render()
         ptr = st.readback()
         dt = time.perf_counter() - t0
@@ -351,7 +365,11 @@ def e2e_public_api(pt, spec, S, args):
             times.append(dt)
     w, h = int(spec.camera["resolution"][1]), int(spec.camera["resolution"][0])
     v = w * h * S * len(times) / sum(times)
-    h2d = 56 + 8 * (S + 1) + 1024
+    # per step the host sends the camera, the render settings and the stream
+    # (display) settings; the scene stays resident like the reference's
+    import ctypes
+    h2d = (ctypes.sizeof(capi.CameraDesc) + ctypes.sizeof(capi.RenderConfig)
+           + ctypes.sizeof(capi.StreamConfig))
     return {"value": v, "unit": "samples/s", "h2d_bytes_per_step": h2d,
             "d2h_bytes_per_step": 3 * w * h,
             "path": "_pathtracer RenderEngine.render + TransferStream.readback (uint8 CHW)"}

@@ -166,6 +166,9 @@ typedef struct nr_render_config {
   int32_t schedule;         /* NR_SCHEDULE_*                                */
   int32_t fp64_accumulate;  /* also keep an FP64 sum of the beauty layer    */
   uint32_t layer_mask;      /* bit i enables LayerType i (default 0x13)      */
+  int32_t extend_variant;   /* wavefront traversal: CTAs per SM the register
+                               budget targets (4, 5, 6 or 8; 0 = default)   */
+  uint32_t samples_per_wave;/* wavefront: sample indices per wave (0 = ~8M paths) */
 } nr_render_config;
 
 /* StreamConfig display fields (nectar_render/csrc/data/include/data/stream.h:13-30). */
@@ -258,6 +261,9 @@ int nr_scene_set_sky_hdri(nr_scene* scene, const float* chw, uint32_t C, uint32_
 int nr_scene_load_hdr(nr_scene* scene, const char* path, float rotation_deg, float intensity);
 /* HDRISkylightConfig rotation/intensity (skylight.h:14-21) after creation. */
 int nr_scene_set_hdri_params(nr_scene* scene, float rotation_deg, float intensity);
+/* Leaf sizes of the 8-wide trees (1..3 primitives; defaults: meshes 3,
+ * top level 1). Takes effect at the next nr_scene_build. */
+int nr_scene_set_tuning(nr_scene* scene, uint32_t mesh_leaf_max, uint32_t tlas_leaf_max);
 /* Uploads the scene and builds every BVH on the GPU (Scene::build,
  * nectar_render/csrc/scene/src/scene.cpp:68-76). Must precede nr_render_create. */
 int nr_scene_build(nr_scene* scene);

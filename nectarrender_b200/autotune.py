@@ -1,0 +1,105 @@
+"""Launch-shape tuner for the wavefront integrator.
+
+Picks, by timing on the scene that will be rendered, the knobs that change
+speed but never the image:
+
+  * ``mesh_leaf`` / ``tlas_leaf`` - primitives per 8-wide BVH leaf (1..3) of
+    the mesh trees and of the top-level tree;
+  * ``extend_variant`` - CTAs per SM the traversal kernel's register budget
+    targets (4, 5, 6 or 8: 128, 96, 80 or 64 registers per thread);
+  * ``samples_per_wave`` - sample indices in flight per wave, i.e. the length
+    of the path queues (paths = W*H*samples_per_wave);
+  * ``schedule`` - wavefront or the per-pixel megakernel.
+
+Every candidate renders the same samples (the parity tests cover each knob),
+so the record only trades time. A record is keyed by the scene's signature
+and can be saved and reused with :func:`load` / :func:`save`.
+"""
+from __future__ import annotations
+
+import itertools
+import json
+from dataclasses import asdict, dataclass, field
+from pathlib import Path
+
+from . import capi
+from .scenes import SceneSpec
+
+VARIANTS = (4, 5, 6, 8)
+
+
+@dataclass
+class Tuning:
+    mesh_leaf: int = 3
+    tlas_leaf: int = 1
+    extend_variant: int = 5
+    samples_per_wave: int = 0
+    schedule: int = capi.SCHEDULE_WAVEFRONT
+    ms_per_sample: float = 0.0
+    table: list = field(default_factory=list)
+
+    def render_overrides(self) -> dict:
+        return {"extend_variant": self.extend_variant,
+                "samples_per_wave": self.samples_per_wave, "schedule": self.schedule}
+
+    def scene_overrides(self) -> dict:
+        return {"mesh_leaf": self.mesh_leaf, "tlas_leaf": self.tlas_leaf}
+
+
+def signature(spec: SceneSpec) -> str:
+    """Identifies the workload a record was tuned on."""
+    cam = spec.camera
+    return json.dumps({"res": [int(cam["resolution"][0]), int(cam["resolution"][1])],
+                       "depth": spec.ray_depth, "objects": len(spec.objects), "name": spec.name,
+                       "meshes": [Path(m).name for m in spec.meshes]}, sort_keys=True)
+
+
+def _time(scene: capi.Scene, spec: SceneSpec, over: dict, samples: int, reps: int) -> float:
+    r = capi.Render(scene, spec, **over)
+    r.samples(1, samples)  # warm-up: allocates the queues, loads the kernels
+    best = float("inf")
+    for _ in range(reps):
+        r.samples(1, samples)
+        best = min(best, r.last_ms())
+    return best / samples
+
+
+def tune(spec: SceneSpec, samples: int = 4, reps: int = 2, leaves=((3, 1), (2, 1), (1, 1), (3, 2)),
+         variants=VARIANTS, waves=(0, 2, 4), megakernel: bool = True) -> Tuning:
+    """Times every candidate on `spec` (device time of `samples` sample
+    indices, best of `reps`) and returns the fastest as a :class:`Tuning`."""
+    table = []
+    best = None
+    for mesh_leaf, tlas_leaf in leaves:
+        scene = capi.Scene(spec, mesh_leaf=mesh_leaf, tlas_leaf=tlas_leaf)
+        cands = [dict(extend_variant=v, samples_per_wave=w, schedule=capi.SCHEDULE_WAVEFRONT)
+                 for v, w in itertools.product(variants, waves)]
+        if megakernel:
+            cands.append(dict(extend_variant=0, samples_per_wave=0,
+                              schedule=capi.SCHEDULE_MEGAKERNEL))
+        for over in cands:
+            ms = _time(scene, spec, over, samples, reps)
+            row = dict(mesh_leaf=mesh_leaf, tlas_leaf=tlas_leaf, ms_per_sample=ms, **over)
+            table.append(row)
+            if best is None or ms < best["ms_per_sample"]:
+                best = row
+        del scene
+    t = Tuning(**{k: best[k] for k in ("mesh_leaf", "tlas_leaf", "extend_variant",
+                                       "samples_per_wave", "schedule", "ms_per_sample")})
+    t.table = table
+    return t
+
+
+def save(path: str | Path, spec: SceneSpec, t: Tuning) -> None:
+    p = Path(path)
+    records = json.loads(p.read_text()) if p.exists() else {}
+    records[signature(spec)] = asdict(t)
+    p.write_text(json.dumps(records, indent=1))
+
+
+def load(path: str | Path, spec: SceneSpec) -> Tuning | None:
+    p = Path(path)
+    if not p.exists():
+        return None
+    rec = json.loads(p.read_text()).get(signature(spec))
+    return Tuning(**rec) if rec else None

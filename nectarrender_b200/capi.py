@@ -43,7 +43,8 @@ class CameraDesc(C.Structure):
 class RenderConfig(C.Structure):
     _fields_ = [("ray_depth", C.c_uint32), ("seed", C.c_uint32), ("rr_enabled", C.c_int32),
                 ("rr_start_bounce", C.c_uint32), ("rr_survival", C.c_float), ("mode", C.c_int32),
-                ("schedule", C.c_int32), ("fp64_accumulate", C.c_int32), ("layer_mask", C.c_uint32)]
+                ("schedule", C.c_int32), ("fp64_accumulate", C.c_int32), ("layer_mask", C.c_uint32),
+                ("extend_variant", C.c_int32), ("samples_per_wave", C.c_uint32)]
 
 
 class StreamConfig(C.Structure):
@@ -66,13 +67,18 @@ class TraceCounters(C.Structure):
 
 
 # symbols declared in include/nectar_b200.h
+# nr_render_config.schedule
+SCHEDULE_MEGAKERNEL = 0
+SCHEDULE_WAVEFRONT = 1
+
 EXPORTS = [
     "nr_abi_version", "nr_last_error", "nr_device_count", "nr_device_draw_order",
     "nr_set_draw_order", "nr_scene_create", "nr_scene_destroy",
     "nr_scene_add_material", "nr_scene_add_image", "nr_scene_add_mesh", "nr_scene_get_mesh",
     "nr_scene_load_obj",
     "nr_scene_add_object", "nr_scene_set_sky_null", "nr_scene_set_sky_simple",
-    "nr_scene_set_sky_hdri", "nr_scene_load_hdr", "nr_scene_set_hdri_params", "nr_scene_build",
+    "nr_scene_set_sky_hdri", "nr_scene_load_hdr", "nr_scene_set_hdri_params",
+    "nr_scene_set_tuning", "nr_scene_build",
     "nr_scene_get_stats", "nr_scene_get_binary_bvh", "nr_render_config_default",
     "nr_render_create", "nr_render_destroy", "nr_render_reset", "nr_render_samples",
     "nr_render_sample_layers", "nr_render_layer_device_ptr", "nr_render_read_layer",
@@ -165,11 +171,12 @@ class Scene:
     """An nr_scene built from a SceneSpec (registry semantics of the
     reference: one material per hittable, lights after hittables)."""
 
-    def __init__(self, spec: SceneSpec, build: bool = True):
+    def __init__(self, spec: SceneSpec, build: bool = True, mesh_leaf: int = 3, tlas_leaf: int = 1):
         self.lib = library()
         self.spec = spec
         self.h = C.c_void_p()
         _check(self.lib.nr_scene_create(C.byref(self.h)), "nr_scene_create")
+        _check(self.lib.nr_scene_set_tuning(self.h, mesh_leaf, tlas_leaf), "nr_scene_set_tuning")
         for path in spec.meshes:
             mid = C.c_uint32()
             _check(self.lib.nr_scene_load_obj(self.h, path.encode(), C.byref(mid)), "nr_scene_load_obj")

@@ -35,7 +35,6 @@ constexpr uint32_t kSmall = 256;
 constexpr int kChunk = 2048;  // primitives per CTA in the large-node passes
 constexpr int kPassThreads = 256;
 constexpr float kEps = 1e-4f;  // reference EPS: axes with a smaller centroid extent are skipped
-constexpr int kWideLeafMax = 3;
 
 __device__ __forceinline__ uint32_t f2key(float f) {
   uint32_t u = __float_as_uint(f);
@@ -893,7 +892,7 @@ struct WideWork {
 __global__ void k_collapse(const BinNode* nodes, const uint32_t* order, const WideWork* cur,
                            uint32_t n_cur, WideWork* next, uint32_t* n_next,
                            uint32_t* wide_counter, uint32_t* prim_counter, Bvh8Node* wide,
-                           uint32_t* order8) {
+                           uint32_t* order8, uint32_t leaf_max) {
   uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= n_cur) return;
   WideWork item = cur[w];
@@ -910,7 +909,7 @@ __global__ void k_collapse(const BinNode* nodes, const uint32_t* order, const Wi
       float best_a = -1.0f;
       for (int i = 0; i < n; ++i) {
         const BinNode& c = nodes[ch[i]];
-        if (c.left < 0 || c.count <= (uint32_t)kWideLeafMax) continue;
+        if (c.left < 0 || c.count <= leaf_max) continue;
         float a = area6(c.lo[0], c.lo[1], c.lo[2], c.hi[0], c.hi[1], c.hi[2]);
         if (a > best_a) { best_a = a; best = i; }
       }
@@ -972,7 +971,7 @@ __global__ void k_collapse(const BinNode* nodes, const uint32_t* order, const Wi
     int i = child_in_slot[s];
     if (i < 0) continue;
     const BinNode& c = nodes[ch[i]];
-    if (c.left >= 0 && c.count > (uint32_t)kWideLeafMax) n_inner++;
+    if (c.left >= 0 && c.count > leaf_max) n_inner++;
     else n_prims += c.count;
   }
   uint32_t child_base = n_inner ? atomicAdd(wide_counter, n_inner) : 0u;
@@ -998,7 +997,7 @@ __global__ void k_collapse(const BinNode* nodes, const uint32_t* order, const Wi
       qlo[k][s] = (uint8_t)fminf(fmaxf(ql, 0.0f), 255.0f);
       qhi[k][s] = (uint8_t)fminf(fmaxf(qh, 0.0f), 255.0f);
     }
-    if (c.left >= 0 && c.count > (uint32_t)kWideLeafMax) {
+    if (c.left >= 0 && c.count > leaf_max) {
       meta[s] = (uint8_t)((1u << 5) | (24u + (uint32_t)s));
       imask |= 1u << s;
       next[next_base + inner_i] = WideWork{(uint32_t)ch[i], child_base + inner_i};
@@ -1047,7 +1046,9 @@ void free_build(BuildResult& r) {
 }
 
 int build_bvh(const float4* d_lo, const float4* d_hi, uint32_t n, bool want_bvh8,
-              BuildResult& out, cudaStream_t st) {
+              BuildResult& out, cudaStream_t st, uint32_t leaf_max) {
+  if (leaf_max < 1) leaf_max = 1;
+  if (leaf_max > 3) leaf_max = 3;
   out = BuildResult{};
   if (n == 0) return 0;
   cudaEvent_t ev0, ev1;
@@ -1234,7 +1235,7 @@ int build_bvh(const float4* d_lo, const float4* d_hi, uint32_t n, bool want_bvh8
       NR_TRY(cudaMemsetAsync(counters + 6, 0, 4, st));
       k_collapse<<<(n_cur + 127) / 128, 128, 0, st>>>(nodes, order, wa, n_cur, wb, counters + 6,
                                                       counters + 4, counters + 5, out.d_bvh8,
-                                                      out.d_order8);
+                                                      out.d_order8, leaf_max);
       NR_TRY(cudaGetLastError());
       NR_TRY(cudaMemcpyAsync(&n_cur, counters + 6, 4, cudaMemcpyDeviceToHost, st));
       NR_TRY(cudaStreamSynchronize(st));

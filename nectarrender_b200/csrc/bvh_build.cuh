@@ -30,9 +30,10 @@ struct BuildResult {
 
 // Builds the binary SAH tree over `n` primitive boxes given as device arrays
 // lo[i] = (x, y, z, _), hi[i] = (x, y, z, _) and derives the 2-wide and
-// 8-wide traversal layouts. Returns a cudaError_t value.
+// 8-wide traversal layouts; 8-wide leaves hold at most `leaf_max` (1..3)
+// primitives. Returns a cudaError_t value.
 int build_bvh(const float4* d_lo, const float4* d_hi, uint32_t n, bool want_bvh8,
-              BuildResult& out, cudaStream_t st);
+              BuildResult& out, cudaStream_t st, uint32_t leaf_max = 3);
 
 void free_build(BuildResult& r);
 

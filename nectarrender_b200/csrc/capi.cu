@@ -25,6 +25,7 @@
 #include "host_io.h"
 #include "image_ops.cuh"
 #include "integrator.cuh"
+#include "wavefront.cuh"
 
 using namespace nr;
 
@@ -372,11 +373,13 @@ struct nr_scene {
   DevObject* d_objects = nullptr;
   DevMesh* d_mesh_table = nullptr;
   float* d_hdri = nullptr;
+  CubeFace* d_cube_faces = nullptr;
   BuildResult tlas;
   DevScene dev{};
   nr_scene_stats stats{};
   std::vector<int32_t> ref_leaf_order;
   int32_t light = -1;
+  uint32_t mesh_leaf_max = 3, tlas_leaf_max = 1;
 
   void release_device() {
     for (auto p : d_images) cudaFree(p);
@@ -387,6 +390,8 @@ struct nr_scene {
     cudaFree(d_objects);
     cudaFree(d_mesh_table);
     cudaFree(d_hdri);
+    cudaFree(d_cube_faces);
+    d_cube_faces = nullptr;
     d_materials = nullptr;
     d_objects = nullptr;
     d_mesh_table = nullptr;
@@ -664,6 +669,15 @@ int nr_scene_set_hdri_params(nr_scene* s, float rotation, float intensity) {
   return NR_OK;
 }
 
+int nr_scene_set_tuning(nr_scene* s, uint32_t mesh_leaf_max, uint32_t tlas_leaf_max) {
+  if (!s || mesh_leaf_max < 1 || mesh_leaf_max > 3 || tlas_leaf_max < 1 || tlas_leaf_max > 3)
+    return fail(NR_ERR_INVALID, "nr_scene_set_tuning: leaf sizes must be 1..3");
+  s->mesh_leaf_max = mesh_leaf_max;
+  s->tlas_leaf_max = tlas_leaf_max;
+  s->built = false;
+  return NR_OK;
+}
+
 int nr_scene_build(nr_scene* s) {
   if (!s) return fail(NR_ERR_INVALID, "null scene");
   if (s->objects.empty()) return fail(NR_ERR_INVALID, "Hittables list cannot be empty.");
@@ -678,7 +692,8 @@ int nr_scene_build(nr_scene* s) {
 
   // device-built constants: cube faces and the HDRI rotation
   M3 hdri_rot;
-  CU(launch_init_constants(s->hdri_rotation, &hdri_rot, st), "init constants");
+  CU(cudaMalloc(&s->d_cube_faces, sizeof(CubeFace) * 6), "alloc cube faces");
+  CU(launch_init_constants(s->hdri_rotation, s->d_cube_faces, &hdri_rot, st), "init constants");
 
   // images and materials
   for (auto& im : s->images) {
@@ -717,7 +732,7 @@ int nr_scene_build(nr_scene* s) {
     CU(cudaMalloc(&lo, sizeof(float4) * nt), "alloc boxes");
     CU(cudaMalloc(&hi, sizeof(float4) * nt), "alloc boxes");
     k_tri_boxes<<<(nt + 255) / 256, 256, 0, st>>>(g.pos, g.vidx, nt, lo, hi);
-    int be = build_bvh(lo, hi, nt, true, g.bvh, st);
+    int be = build_bvh(lo, hi, nt, true, g.bvh, st, s->mesh_leaf_max);
     cudaFree(lo);
     cudaFree(hi);
     if (be != 0) return cuda_fail((cudaError_t)be, "mesh BVH build");
@@ -782,7 +797,7 @@ int nr_scene_build(nr_scene* s) {
   float4 *dlo = nullptr, *dhi = nullptr;
   CU(upload(dlo, blo.data(), blo.size(), st), "upload boxes");
   CU(upload(dhi, bhi.data(), bhi.size(), st), "upload boxes");
-  int be = build_bvh(dlo, dhi, (uint32_t)objs.size(), true, s->tlas, st);
+  int be = build_bvh(dlo, dhi, (uint32_t)objs.size(), true, s->tlas, st, s->tlas_leaf_max);
   cudaFree(dlo);
   cudaFree(dhi);
   if (be != 0) return cuda_fail((cudaError_t)be, "top-level BVH build");
@@ -828,10 +843,12 @@ int nr_scene_build(nr_scene* s) {
   ds.tlas2 = s->tlas.d_bvh2;
   ds.tlas8 = s->tlas.d_bvh8;
   ds.tlas_prims = s->tlas.d_order;
+  ds.tlas_prims8 = s->tlas.d_order8;
   ds.n_tlas2 = s->tlas.n_bvh2;
   ds.n_tlas8 = s->tlas.n_bvh8;
   ds.light = s->light;
   ds.use_bvh8 = 1;
+  ds.cube_faces = s->d_cube_faces;
   ds.sky = sky;
 
   CU(cudaEventRecord(e1, st), "event");
@@ -918,11 +935,14 @@ struct nr_render {
   float* dispf = nullptr;
   V3* wb_scratch = nullptr;
   DevCamera dcam{};
+  WfParams wf{};
+  uint32_t samples_per_wave = 0;
   int rtl = 0;
   bool counters_on = false;
   nr_trace_counters last{};
   double last_ms = 0.0;
   ~nr_render() {
+    if (wf.capacity) wf_free(wf);
     for (auto p : layer) cudaFree(p);
     cudaFree(beauty64);
     for (auto p : raw) cudaFree(p);
@@ -961,9 +981,11 @@ int nr_render_config_default(nr_render_config* c) {
   c->rr_start_bounce = 3;
   c->rr_survival = 0.95f;
   c->mode = NR_MODE_REFERENCE;
-  c->schedule = NR_SCHEDULE_MEGAKERNEL;
+  c->schedule = NR_SCHEDULE_WAVEFRONT;
   c->fp64_accumulate = 0;
   c->layer_mask = (1u << NR_LAYER_BEAUTY) | (1u << NR_LAYER_DIFFUSE) | (1u << NR_LAYER_WORLD_NORMAL);
+  c->extend_variant = 0;
+  c->samples_per_wave = 0;
   return NR_OK;
 }
 
@@ -1100,11 +1122,42 @@ static KernelParams make_params(nr_render* r, uint32_t first, uint32_t count, bo
   return P;
 }
 
+// Waves of the wavefront schedule hold up to ~8M paths (about 1 GB of state).
+static uint32_t waves_of(nr_render* r) {
+  if (r->cfg.samples_per_wave > 0) return std::min(16u, r->cfg.samples_per_wave);
+  uint32_t N = r->W * r->H;
+  uint32_t s = std::max(1u, std::min(8u, (8u << 20) / std::max(1u, N)));
+  return s;
+}
+
+static int launch(nr_render* r, const KernelParams& P) {
+  if (r->cfg.schedule != NR_SCHEDULE_WAVEFRONT) {
+    CU(cudaMemsetAsync(r->work, 0, 4, r->stream), "clear work counter");
+    CU(launch_megakernel(P, r->counters_on, r->stream), "launch integrator");
+    return NR_OK;
+  }
+  uint32_t N = r->W * r->H;
+  if (!r->wf.capacity) {
+    r->samples_per_wave = waves_of(r);
+    CU(wf_alloc(r->wf, r->samples_per_wave * N), "allocate wavefront state");
+  }
+  uint32_t per = P.write_raw ? 1u : r->samples_per_wave;
+  for (uint32_t s = 0; s < P.n_samples; s += per) {
+    WfParams W = r->wf;
+    W.kp = P;
+    W.extend_variant = r->cfg.extend_variant > 0 ? r->cfg.extend_variant : 5;
+    W.base = P.first_sample + s;
+    W.count = std::min(per, P.n_samples - s);
+    CU(wf_launch_wave(W, r->counters_on, r->stream), "launch wavefront");
+  }
+  return NR_OK;
+}
+
 static int run_kernel(nr_render* r, const KernelParams& P) {
-  CU(cudaMemsetAsync(r->work, 0, 4, r->stream), "clear work counter");
   if (r->counters_on) CU(cudaMemsetAsync(r->counters, 0, 8 * 5, r->stream), "clear counters");
   CU(cudaEventRecord(r->ev0, r->stream), "event");
-  CU(launch_megakernel(P, r->counters_on, r->stream), "launch integrator");
+  int rc = launch(r, P);
+  if (rc != NR_OK) return rc;
   CU(cudaEventRecord(r->ev1, r->stream), "event");
   CU(cudaEventSynchronize(r->ev1), "integrator");
   float ms = 0.f;
@@ -1124,7 +1177,9 @@ static int run_kernel(nr_render* r, const KernelParams& P) {
     r->last.node_visits = c[1];
     r->last.tri_tests = c[2];
     r->last.obj_tests = c[3];
-    r->last.paths = c[4];
+    r->last.paths = r->cfg.schedule == NR_SCHEDULE_WAVEFRONT
+                        ? (unsigned long long)P.n_samples * r->W * r->H
+                        : c[4];
   }
   return NR_OK;
 }

@@ -28,7 +28,8 @@ struct KernelParams {
   unsigned long long* counters;  // rays, nodes, tris, objects, paths
 };
 
-cudaError_t launch_init_constants(float hdri_rotation_deg, M3* host_hdri_rot, cudaStream_t st);
+cudaError_t launch_init_constants(float hdri_rotation_deg, CubeFace* d_faces, M3* host_hdri_rot,
+                                  cudaStream_t st);
 cudaError_t launch_megakernel(const KernelParams& P, bool counters, cudaStream_t st);
 int mega_grid_blocks();
 

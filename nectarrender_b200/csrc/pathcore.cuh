@@ -108,20 +108,16 @@ __device__ __forceinline__ bool sphere_hit(const Ray& r, float tmin, float tmax,
 
 // Cube = six quads with fixed face transforms (shapes.h:60-173). The face
 // transforms are built on the device exactly as the reference's device-side
-// Cube constructor does (see init_cube_faces in integrator.cu).
-struct CubeFace {
-  M3 R, invR;
-  V3 pos;
-};
-static __constant__ CubeFace c_cube_faces[6];
-
-__device__ __forceinline__ bool cube_hit(const Ray& r, float tmin, float tmax, Hit& h) {
+// Cube constructor does (init_device_constants in integrator.cu) and stored
+// once per scene (DevScene::cube_faces).
+__device__ __forceinline__ bool cube_hit(const CubeFace* faces, const Ray& r, float tmin,
+                                         float tmax, Hit& h) {
   bool any = false;
   int hit_face = -1;
   Ray hit_ray;
   const V3 one = V3{1.0f, 1.0f, 1.0f};
   for (int i = 0; i < 6; ++i) {
-    const CubeFace& f = c_cube_faces[i];
+    const CubeFace& f = faces[i];
     // to_object_space with unit scale (inv_s = 1/(1+FMIN+FMIN) = 1 in float)
     V3 o = mul(f.invR, r.o - f.pos) * one;
     V3 d = mul(f.invR, r.d) * one;
@@ -136,7 +132,7 @@ __device__ __forceinline__ bool cube_hit(const Ray& r, float tmin, float tmax, H
     }
   }
   if (any) {
-    const CubeFace& f = c_cube_faces[hit_face];
+    const CubeFace& f = faces[hit_face];
     to_world(h, f.R, f.pos, one, one, hit_ray, r, false);
   }
   return any;
@@ -423,27 +419,30 @@ __device__ __forceinline__ bool mesh_hit(const DevScene& sc, const DevObject& ob
 }
 
 // Hittable::hit dispatch on an object-space ray for the primitive kinds a
-// wrapper can hold (hittable.h:332-352).
-__device__ __forceinline__ bool shape_hit(const DevScene& sc, const DevObject& ob, int type,
-                                          const Ray& r, float tmin, float tmax, Hit& h,
-                                          bool ref_mode, TraceStats& st, uint32_t* err) {
+// wrapper can hold (hittable.h:332-352). `mesh_fn(ob, r, tmin, tmax, h)`
+// intersects the object's mesh; callers choose its traversal.
+template <typename MeshFn>
+__device__ __forceinline__ bool shape_hit_t(const CubeFace* faces, const DevObject& ob, int type,
+                                            const Ray& r, float tmin, float tmax, Hit& h,
+                                            MeshFn&& mesh_fn) {
   switch (type) {
     case 1: return quad_hit(r, tmin, tmax, h);
     case 2: return sphere_hit(r, tmin, tmax, ob.radius, ob.scale, h);
-    case 3: return cube_hit(r, tmin, tmax, h);
-    case 4: return mesh_hit(sc, ob, r, tmin, tmax, h, ref_mode, st, err);
+    case 3: return cube_hit(faces, r, tmin, tmax, h);
+    case 4: return mesh_fn(ob, r, tmin, tmax, h);
   }
   return false;
 }
 
 // ConstantMedium::hit (volumes.h:10-45): two boundary hits of the wrapped
 // shape, free flight from a hash of the object-space ray.
-__device__ __forceinline__ bool medium_hit(const DevScene& sc, const DevObject& ob, const Ray& r,
-                                           float tmin, float tmax, Hit& h, bool ref_mode,
-                                           TraceStats& st, uint32_t* err) {
+template <typename MeshFn>
+__device__ __forceinline__ bool medium_hit_t(const CubeFace* faces, const DevObject& ob,
+                                             const Ray& r, float tmin, float tmax, Hit& h,
+                                             MeshFn&& mesh_fn) {
   Hit h1, h2;
-  if (!shape_hit(sc, ob, ob.wrapped_type, r, -FMAX, FMAX, h1, ref_mode, st, err)) return false;
-  if (!shape_hit(sc, ob, ob.wrapped_type, r, h1.t + EPS, FMAX, h2, ref_mode, st, err)) return false;
+  if (!shape_hit_t(faces, ob, ob.wrapped_type, r, -FMAX, FMAX, h1, mesh_fn)) return false;
+  if (!shape_hit_t(faces, ob, ob.wrapped_type, r, h1.t + EPS, FMAX, h2, mesh_fn)) return false;
   if (h1.t < tmin) h1.t = tmin;
   if (h2.t > tmax) h2.t = tmax;
   if (h1.t >= h2.t) return false;
@@ -464,10 +463,10 @@ __device__ __forceinline__ bool medium_hit(const DevScene& sc, const DevObject& 
 }
 
 // Hittable::hit on an object-space ray (hittable.h:332-352).
-__device__ __forceinline__ bool object_hit_local(const DevScene& sc, const DevObject& ob,
-                                                 const Ray& r, float tmin, float tmax, Hit& h,
-                                                 bool ref_mode, TraceStats& st,
-                                                 uint32_t* err) {
+template <typename MeshFn>
+__device__ __forceinline__ bool object_hit_local_t(const CubeFace* faces, const DevObject& ob,
+                                                   const Ray& r, float tmin, float tmax, Hit& h,
+                                                   MeshFn&& mesh_fn) {
   h.prim = 0xffffffffu;
   h.uv = V2{0.0f, 0.0f};
   h.tangent = V3{0.0f, 0.0f, 0.0f};
@@ -476,12 +475,23 @@ __device__ __forceinline__ bool object_hit_local(const DevScene& sc, const DevOb
   h.t = 0.0f;
   switch (ob.type) {
     case 6:  // ObjectLight: wrapped->hit(ray, Interval(-FMAX, FMAX)) (lights.h:10-18)
-      return shape_hit(sc, ob, ob.wrapped_type, r, -FMAX, FMAX, h, ref_mode, st, err);
+      return shape_hit_t(faces, ob, ob.wrapped_type, r, -FMAX, FMAX, h, mesh_fn);
     case 5:
-      return medium_hit(sc, ob, r, tmin, tmax, h, ref_mode, st, err);
+      return medium_hit_t(faces, ob, r, tmin, tmax, h, mesh_fn);
     default:
-      return shape_hit(sc, ob, ob.type, r, tmin, tmax, h, ref_mode, st, err);
+      return shape_hit_t(faces, ob, ob.type, r, tmin, tmax, h, mesh_fn);
   }
+}
+
+// The same with the local-stack mesh traversal of the megakernel.
+__device__ __forceinline__ bool object_hit_local(const DevScene& sc, const DevObject& ob,
+                                                 const Ray& r, float tmin, float tmax, Hit& h,
+                                                 bool ref_mode, TraceStats& st,
+                                                 uint32_t* err) {
+  auto mesh_fn = [&](const DevObject& o, const Ray& rr, float t0, float t1, Hit& hh) {
+    return mesh_hit(sc, o, rr, t0, t1, hh, ref_mode, st, err);
+  };
+  return object_hit_local_t(sc.cube_faces, ob, r, tmin, tmax, h, mesh_fn);
 }
 
 // Hittable::hit_test (hittable.h:324-330): object space, Interval(EPS, FMAX),

@@ -1035,7 +1035,18 @@ PYBIND11_MODULE(_pathtracer, m) {
       .def("get_engine_type", [](EngineCore& e) { return e.type.load(); })
       .def("set_engine_type", [](EngineCore& e, EngineType t) { e.type = t; })
       .def("n_samples", [](EngineCore& e) { return e.cam.p.samples_per_pixel; })
-      .def("set_n_samples", [](EngineCore& e, uint32_t n) { e.cam.p.samples_per_pixel = n; e.make_render(); })
+      // RenderEngine::set_n_samples (engine.cpp:139-143) restarts at sample 1.
+      // The sample pattern is rebuilt when n changes; the reference keeps the
+      // pattern of the constructor's n and reads past it for larger n.
+      .def("set_n_samples",
+           [](EngineCore& e, uint32_t n) {
+             if (e.render && n == e.cam.p.samples_per_pixel) {
+               e.reset();
+             } else {
+               e.cam.p.samples_per_pixel = n;
+               e.make_render();
+             }
+           })
       .def("max_depth", [](EngineCore& e) { return e.ray_depth; })
       .def("set_max_depth", [](EngineCore& e, uint32_t d) { e.ray_depth = d; e.make_render(); })
       .def("update_streaming_layer", [](EngineCore& e, LayerType t) { e.stream.layer = (int)t; })

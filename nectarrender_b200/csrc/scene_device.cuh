@@ -53,6 +53,13 @@ struct alignas(16) TriRecord {
   float4 e2;  // v2 - v0
 };
 
+// One face of the reference's Cube (shapes.h:192-223): rotation, its
+// transpose and position; the scale is 1.
+struct CubeFace {
+  M3 R, invR;
+  V3 pos;
+};
+
 struct DevTexture {
   int32_t type;  // 0 constant, 1 image
   float r, g, b;
@@ -125,11 +132,13 @@ struct DevScene {
   uint32_t n_meshes;
   const Bvh2Node* tlas2;
   const Bvh8Node* tlas8;
-  const uint32_t* tlas_prims;  // top-level leaf slot -> object slot
+  const uint32_t* tlas_prims;  // 2-wide top-level leaf slot -> object slot
+  const uint32_t* tlas_prims8; // 8-wide top-level leaf slot -> object slot
   uint32_t n_tlas2;
   uint32_t n_tlas8;
   int32_t light;  // object slot of lights[0], -1 if the scene has no lights
   int32_t use_bvh8;
+  const CubeFace* cube_faces;  // 6 faces
   DevSky sky;
 };
 

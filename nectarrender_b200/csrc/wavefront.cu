@@ -1,0 +1,586 @@
+// wavefront.cu — wavefront path tracer: generate / extend / shade /
+// accumulate kernels over path state kept in HBM.
+//
+// A wave renders `count` consecutive sample indices of every pixel: path
+// p = k*N + pixel (N = W*H) carries sample index base + k. Each bounce runs
+//   extend  — persistent traversal kernel: warps take 32 queued paths at a
+//             time, walk the 8-wide top-level tree and, for mesh instances,
+//             the 8-wide bottom-level tree in object space, with per-thread
+//             stacks in shared memory; writes a 20-byte hit record;
+//   shade   — rebuilds the closest hit exactly as the reference's hit_test
+//             would return it, runs emission / scatter / BSDF sampling /
+//             Russian roulette (nectar_render/csrc/engine/src/trace.cu:11-79,
+//             brdf.cu:4-35) and appends surviving paths to the next queue
+//             with one atomic per warp;
+// and after the last bounce
+//   accumulate — folds the wave's samples of each pixel into the running mean
+//             in sample order (data.cu:28-50) and the FP64 sums.
+// Path state per path: ray origin+time, direction, throughput + draw counter,
+// beauty + primary id, diffuse + bounce, normal (six 16-byte records) plus
+// the hit record. Queue lengths live in device memory, so the sequence of
+// launches of a wave is fixed and is captured once as a CUDA graph.
+#include "pathstep.cuh"
+#include "wavefront.cuh"
+
+namespace nr {
+
+constexpr int kExtThreads = 128;
+constexpr int kTlasStack = 8;
+constexpr int kBlasStack = 24;
+constexpr int kShadeThreads = 128;
+
+enum : uint32_t {
+  CTR_N0 = 0,      // paths in queue 0
+  CTR_N1 = 1,      // paths in queue 1
+  CTR_WORK = 2,    // extend work counter
+  CTR_ERR = 3,
+};
+
+__device__ __forceinline__ float4 ld4(const float4* p) { return __ldg(p); }
+
+// ---------------------------------------------------------------------------
+// compressed 8-wide traversal with a shared-memory stack; `leaf(slot, tmax)`
+// is called for every primitive slot whose leaf box the ray enters.
+template <typename Leaf>
+__device__ __forceinline__ void cwbvh_trace(const Bvh8Node* __restrict__ nodes, uint32_t n_nodes,
+                                            const V3& o, const V3& d, const V3& inv, float tmin,
+                                            float& tmax, uint2* stk, uint32_t stride, int depth,
+                                            Leaf&& leaf, uint32_t& node_count, uint32_t* err) {
+  if (n_nodes == 0) return;
+  uint32_t oct = (d.x < 0.0f ? 4u : 0u) | (d.y < 0.0f ? 2u : 0u) | (d.z < 0.0f ? 1u : 0u);
+  const uint32_t oct_inv = 7u - oct;
+  const uint32_t oct_inv4 = oct_inv * 0x01010101u;
+  uint2 ngroup = make_uint2(0u, 0x80000000u);
+  int sp = 0;
+  for (uint32_t steps = 0;; ++steps) {
+    if (steps >= kMaxTraversalSteps) {
+      atomicOr(err, 8u);
+      return;
+    }
+    if (ngroup.y > 0x00ffffffu) {
+      uint32_t hits = ngroup.y;
+      uint32_t child_bit = 31u - __clz(hits);
+      ngroup.y &= ~(1u << child_bit);
+      uint32_t slot = (child_bit - 24u) ^ oct_inv;
+      uint32_t imask = hits & 0xffu;
+      uint32_t node_index = ngroup.x + __popc(imask & ~(0xffffffffu << slot));
+      if (node_index >= n_nodes) {
+        atomicOr(err, 8u);
+        return;
+      }
+      if (ngroup.y > 0x00ffffffu) {
+        if (sp < depth) stk[(sp++) * stride] = ngroup;
+        else atomicOr(err, 1u);
+      }
+      float4 n0;
+      uint4 n1;
+      uint32_t hm = bvh8_intersect(nodes + node_index, o, inv, oct_inv4, tmin, tmax, n0, n1);
+      node_count++;
+      ngroup = make_uint2(n1.x, (hm & 0xff000000u) | (__float_as_uint(n0.w) >> 24));
+      uint32_t tbits = hm & 0x00ffffffu;
+      while (tbits) {
+        uint32_t b = __ffs(tbits) - 1u;
+        tbits &= tbits - 1u;
+        leaf(n1.y + b, tmax);
+      }
+    }
+    if (ngroup.y <= 0x00ffffffu) {
+      if (sp == 0) return;
+      ngroup = stk[(--sp) * stride];
+    }
+  }
+}
+
+// World-space t of an object-space hit as HitRecord::to_world_space computes
+// it with the bias (hit_record.h:24-51), without the tangent frame.
+__device__ __forceinline__ float world_t(V3 p, V3 n, const DevObject& ob, const Ray& r_obj,
+                                         const Ray& wr) {
+  p = mul(ob.R, p * ob.scale) + ob.pos;
+  bool front = dot(r_obj.d, n) < 0.0f;
+  n = front ? n : -n;
+  n = normalize(mul(ob.R, n * ob.inv_s));
+  bool front2 = dot(wr.d, n) < 0.0f;
+  n = front2 ? n : -n;
+  p += n * EPS;
+  return dot(p - wr.o, wr.d) / length_squared(wr.d);
+}
+
+__device__ __forceinline__ V3 mesh_normal(const DevMesh& m, uint32_t tri, float u, float v) {
+  uint32_t i0 = __ldg(m.tri_vidx + 3 * tri), i1 = __ldg(m.tri_vidx + 3 * tri + 1),
+           i2 = __ldg(m.tri_vidx + 3 * tri + 2);
+  float w = 1.0f - u - v;
+  V3 n0 = V3{__ldg(m.vnormal + 3 * i0), __ldg(m.vnormal + 3 * i0 + 1), __ldg(m.vnormal + 3 * i0 + 2)};
+  V3 n1 = V3{__ldg(m.vnormal + 3 * i1), __ldg(m.vnormal + 3 * i1 + 1), __ldg(m.vnormal + 3 * i1 + 2)};
+  V3 n2 = V3{__ldg(m.vnormal + 3 * i2), __ldg(m.vnormal + 3 * i2 + 1), __ldg(m.vnormal + 3 * i2 + 2)};
+  return normalize(n0 * w + n1 * u + n2 * v);
+}
+
+// Mesh::hit + interpolate_hit (mesh.h:239-292, 367-383) with the 8-wide tree
+// and a shared-memory stack.
+__device__ __forceinline__ bool mesh_hit8(const DevScene& sc, const DevObject& ob, const Ray& r,
+                                          float tmin, float tmax, Hit& h, uint2* stk,
+                                          uint32_t stride, uint32_t* err) {
+  const DevMesh& m = sc.meshes[ob.mesh];
+  int best = -1;
+  float bu = 0.f, bv = 0.f;
+  uint32_t nodes = 0;
+  auto tri_leaf = [&](uint32_t ts, float& tm) {
+    const TriRecord* tr = m.tris8 + ts;
+    float4 p0 = ld4(&tr->v0), p1 = ld4(&tr->e1), p2 = ld4(&tr->e2);
+    if (__float_as_uint(p1.w) != 0u) return;
+    float t, u, v;
+    if (tri_hit(r, V3{p0.x, p0.y, p0.z}, V3{p1.x, p1.y, p1.z}, V3{p2.x, p2.y, p2.z}, tmin, tm, t,
+                u, v)) {
+      tm = t;
+      bu = u;
+      bv = v;
+      best = (int)ts;
+    }
+  };
+  cwbvh_trace(m.bvh8, m.n_bvh8, r.o, r.d, r.inv, tmin, tmax, stk, stride, kBlasStack, tri_leaf,
+              nodes, err);
+  if (best < 0) return false;
+  uint32_t tri = __float_as_uint(__ldg(&m.tris8[best].v0.w));
+  uint32_t i0 = __ldg(m.tri_vidx + 3 * tri), i1 = __ldg(m.tri_vidx + 3 * tri + 1),
+           i2 = __ldg(m.tri_vidx + 3 * tri + 2);
+  h.t = tmax;
+  h.p = ray_at(r, tmax);
+  float w = 1.0f - bu - bv;
+  V2 uv0 = V2{__ldg(m.vuv + 2 * i0), __ldg(m.vuv + 2 * i0 + 1)};
+  V2 uv1 = V2{__ldg(m.vuv + 2 * i1), __ldg(m.vuv + 2 * i1 + 1)};
+  V2 uv2 = V2{__ldg(m.vuv + 2 * i2), __ldg(m.vuv + 2 * i2 + 1)};
+  h.uv = V2{uv0.x * w + uv1.x * bu + uv2.x * bv, uv0.y * w + uv1.y * bu + uv2.y * bv};
+  h.n = mesh_normal(m, tri, bu, bv);
+  V3 t0 = V3{__ldg(m.vtangent + 3 * i0), __ldg(m.vtangent + 3 * i0 + 1), __ldg(m.vtangent + 3 * i0 + 2)};
+  V3 t1 = V3{__ldg(m.vtangent + 3 * i1), __ldg(m.vtangent + 3 * i1 + 1), __ldg(m.vtangent + 3 * i1 + 2)};
+  V3 t2 = V3{__ldg(m.vtangent + 3 * i2), __ldg(m.vtangent + 3 * i2 + 1), __ldg(m.vtangent + 3 * i2 + 2)};
+  h.tangent = normalize(t0 * w + t1 * bu + t2 * bv);
+  h.prim = tri;
+  return true;
+}
+
+// Closest hit of a world ray over the whole scene: the object with the
+// smallest biased world t in (EPS, best), as SceneGraph::hit selects it
+// (scene/include/graph.h:16-66). Returns obj = 0xffffffff on a miss.
+template <bool kCount>
+__device__ __forceinline__ void trace_closest(const DevScene& sc, const Ray& wr, uint2* tlas_stk,
+                                              uint2* blas_stk, uint32_t stride, uint32_t& out_obj,
+                                              uint32_t& out_slot, float& out_t, float& out_u,
+                                              float& out_v, TraceStats& st, uint32_t* err) {
+  float best = FMAX;
+  out_obj = 0xffffffffu;
+  out_slot = 0xffffffffu;
+  out_t = 0.0f;
+  out_u = out_v = 0.0f;
+  const float slack = (2.0f * EPS + 1e-4f * (fabsf(wr.o.x) + fabsf(wr.o.y) + fabsf(wr.o.z) + 1.0f)) /
+                      length(wr.d);
+  uint32_t nodes = 0;
+  auto object_leaf = [&](uint32_t slot, float& tlas_tmax) {
+    uint32_t oi = __ldg(sc.tlas_prims8 + slot);
+    const DevObject& ob = sc.objects[oi];
+    Ray r = to_object(ob, wr);
+    if (kCount) st.objs++;
+    if (ob.type == 4) {
+      const DevMesh& m = sc.meshes[ob.mesh];
+      float tmax = fminf(FMAX, best * 1.0011f + slack);
+      int best_slot = -1;
+      float bu = 0.f, bv = 0.f;
+      auto tri_leaf = [&](uint32_t ts, float& tm) {
+        const TriRecord* tr = m.tris8 + ts;
+        float4 p0 = ld4(&tr->v0), p1 = ld4(&tr->e1), p2 = ld4(&tr->e2);
+        if (kCount) st.tris++;
+        if (__float_as_uint(p1.w) != 0u) return;  // zero-extent box: never hit in the reference
+        float t, u, v;
+        if (tri_hit(r, V3{p0.x, p0.y, p0.z}, V3{p1.x, p1.y, p1.z}, V3{p2.x, p2.y, p2.z}, EPS, tm,
+                    t, u, v)) {
+          tm = t;
+          bu = u;
+          bv = v;
+          best_slot = (int)ts;
+        }
+      };
+      cwbvh_trace(m.bvh8, m.n_bvh8, r.o, r.d, r.inv, EPS, tmax, blas_stk, stride, kBlasStack,
+                  tri_leaf, nodes, err);
+      if (best_slot >= 0) {
+        uint32_t tri = __float_as_uint(__ldg(&m.tris8[best_slot].v0.w));
+        V3 p = ray_at(r, tmax);
+        V3 n = mesh_normal(m, tri, bu, bv);
+        float tw = world_t(p, n, ob, r, wr);
+        if (EPS < tw && tw < best) {
+          best = tw;
+          tlas_tmax = best;
+          out_obj = oi;
+          out_slot = (uint32_t)best_slot;
+          out_t = tmax;
+          out_u = bu;
+          out_v = bv;
+        }
+      }
+    } else {
+      Hit h;
+      auto mesh_fn = [&](const DevObject& o, const Ray& rr, float t0, float t1, Hit& hh) {
+        return mesh_hit8(sc, o, rr, t0, t1, hh, blas_stk, stride, err);
+      };
+      if (object_hit_local_t(sc.cube_faces, ob, r, EPS, FMAX, h, mesh_fn)) {
+        float tw = world_t(h.p, h.n, ob, r, wr);
+        if (EPS < tw && tw < best) {
+          best = tw;
+          tlas_tmax = best;
+          out_obj = oi;
+          out_slot = 0xffffffffu;
+          out_t = h.t;
+        }
+      }
+    }
+  };
+  float tlas_tmax = FMAX;
+  cwbvh_trace(sc.tlas8, sc.n_tlas8, wr.o, wr.d, wr.inv, EPS, tlas_tmax, tlas_stk, stride, kTlasStack,
+              object_leaf, nodes, err);
+  if (kCount) st.nodes += nodes;
+}
+
+// Rebuilds the hit record of the closest object (Hittable::hit_test).
+__device__ __forceinline__ void rebuild_hit(const DevScene& sc, uint32_t oi, uint32_t slot, float t,
+                                            float u, float v, const Ray& wr, Hit& h, uint2* stk,
+                                            uint32_t stride, uint32_t* err) {
+  const DevObject& ob = sc.objects[oi];
+  Ray r = to_object(ob, wr);
+  h.prim = 0xffffffffu;
+  if (ob.type == 4) {
+    const DevMesh& m = sc.meshes[ob.mesh];
+    uint32_t tri = __float_as_uint(__ldg(&m.tris8[slot].v0.w));
+    uint32_t i0 = __ldg(m.tri_vidx + 3 * tri), i1 = __ldg(m.tri_vidx + 3 * tri + 1),
+             i2 = __ldg(m.tri_vidx + 3 * tri + 2);
+    h.t = t;
+    h.p = ray_at(r, t);
+    float w = 1.0f - u - v;
+    V2 uv0 = V2{__ldg(m.vuv + 2 * i0), __ldg(m.vuv + 2 * i0 + 1)};
+    V2 uv1 = V2{__ldg(m.vuv + 2 * i1), __ldg(m.vuv + 2 * i1 + 1)};
+    V2 uv2 = V2{__ldg(m.vuv + 2 * i2), __ldg(m.vuv + 2 * i2 + 1)};
+    h.uv = V2{uv0.x * w + uv1.x * u + uv2.x * v, uv0.y * w + uv1.y * u + uv2.y * v};
+    h.n = mesh_normal(m, tri, u, v);
+    V3 t0 = V3{__ldg(m.vtangent + 3 * i0), __ldg(m.vtangent + 3 * i0 + 1), __ldg(m.vtangent + 3 * i0 + 2)};
+    V3 t1 = V3{__ldg(m.vtangent + 3 * i1), __ldg(m.vtangent + 3 * i1 + 1), __ldg(m.vtangent + 3 * i1 + 2)};
+    V3 t2 = V3{__ldg(m.vtangent + 3 * i2), __ldg(m.vtangent + 3 * i2 + 1), __ldg(m.vtangent + 3 * i2 + 2)};
+    h.tangent = normalize(t0 * w + t1 * u + t2 * v);
+    h.prim = tri;
+  } else {
+    auto mesh_fn = [&](const DevObject& o, const Ray& rr, float t0, float t1, Hit& hh) {
+      return mesh_hit8(sc, o, rr, t0, t1, hh, stk, stride, err);
+    };
+    object_hit_local_t(sc.cube_faces, ob, r, EPS, FMAX, h, mesh_fn);
+  }
+  to_world(h, ob.R, ob.pos, ob.scale, ob.inv_s, r, wr, true);
+  h.obj = oi;
+}
+
+// ---------------------------------------------------------------------------
+// kernels
+
+__global__ void k_wf_generate(WfParams W) {
+  const KernelParams& P = W.kp;
+  const uint32_t N = P.W * P.H;
+  uint32_t total = N * W.count;
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < total; p += gridDim.x * blockDim.x) {
+    uint32_t k = p / N, pix = p - k * N;
+    uint32_t x = pix % P.W, y = pix / P.W;
+    uint32_t sample = W.base + k;
+    Rng g;
+    g.init(P.seed, pix + sample * (P.W * P.H));
+    Ray r = camera_ray(P.cam, x, y, pix, sample, P.seed, g, P.rtl != 0);
+    W.ray_o[p] = make_float4(r.o.x, r.o.y, r.o.z, r.tm);
+    W.ray_d[p] = make_float4(r.d.x, r.d.y, r.d.z, __uint_as_float(0u));
+    W.atten[p] = make_float4(1.0f, 1.0f, 1.0f, __uint_as_float(g.draw));
+    W.acc_b[p] = make_float4(0.f, 0.f, 0.f, __uint_as_float(0xffffffffu));
+    W.acc_d[p] = make_float4(0.f, 0.f, 0.f, 0.f);
+    W.acc_n[p] = make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    W.ctr[CTR_N0] = total;
+    W.ctr[CTR_N1] = 0u;
+    W.ctr[CTR_WORK] = 0u;
+  }
+}
+
+// kMinBlocks bounds registers so that kMinBlocks CTAs of 128 threads fit per
+// SM (4: 128 registers, 5: 96, 6: 80, 8: 64); the autotuner picks the variant.
+template <bool kCount, int kMinBlocks>
+__global__ void __launch_bounds__(kExtThreads, kMinBlocks) k_wf_extend(WfParams W, int qsel,
+                                                                       int identity) {
+  extern __shared__ uint2 wf_smem[];
+  const KernelParams& P = W.kp;
+  const uint32_t n = W.ctr[qsel];
+  const uint32_t* queue = qsel == 0 ? W.queue0 : W.queue1;
+  const uint32_t lane = threadIdx.x & 31u;
+  uint2* tlas_stk = wf_smem + threadIdx.x;
+  uint2* blas_stk = wf_smem + kTlasStack * kExtThreads + threadIdx.x;
+  TraceStats st{0u, 0u, 0u};
+  uint32_t rays = 0;
+  while (true) {
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(&W.ctr[CTR_WORK], 32u);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base >= n) break;
+    uint32_t i = base + lane;
+    if (i < n) {
+      uint32_t p = identity ? i : __ldg(queue + i);
+      float4 o = ld4(W.ray_o + p), d = ld4(W.ray_d + p);
+      Ray r = make_ray(V3{o.x, o.y, o.z}, V3{d.x, d.y, d.z}, o.w);
+      uint32_t obj, slot;
+      float t, u, v;
+      trace_closest<kCount>(P.scene, r, tlas_stk, blas_stk, kExtThreads, obj, slot, t, u, v, st, P.err);
+      W.hit[p] = make_uint4(obj, slot, __float_as_uint(u), __float_as_uint(v));
+      W.hit_t[p] = t;
+      rays++;
+    }
+  }
+  if (kCount) {
+    unsigned long long vals[4] = {rays, st.nodes, st.tris, st.objs};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      unsigned long long a = vals[k];
+      for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
+      if (lane == 0) atomicAdd(P.counters + k, a);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kShadeThreads) k_wf_shade(WfParams W, int qsel, int identity) {
+  __shared__ uint2 shade_stk[kBlasStack * kShadeThreads];
+  const KernelParams& P = W.kp;
+  const DevScene& sc = P.scene;
+  const uint32_t n = W.ctr[qsel];
+  const uint32_t* queue = qsel == 0 ? W.queue0 : W.queue1;
+  uint32_t* next_queue = qsel == 0 ? W.queue1 : W.queue0;
+  uint32_t* next_n = &W.ctr[qsel == 0 ? CTR_N1 : CTR_N0];
+  const uint32_t N = P.W * P.H;
+  const uint32_t lane = threadIdx.x & 31u;
+  TraceStats st{0u, 0u, 0u};
+  // grid-stride loop with whole warps in every iteration (for the warp-aggregated append)
+  for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+    uint32_t i = base + threadIdx.x;
+    bool alive = false;
+    uint32_t p = 0;
+    if (i < n) {
+      p = identity ? i : __ldg(queue + i);
+      float4 o = W.ray_o[p], d = W.ray_d[p], at = W.atten[p], ab = W.acc_b[p];
+      uint32_t bounce = __float_as_uint(d.w);
+      PathState s;
+      s.ray = make_ray(V3{o.x, o.y, o.z}, V3{d.x, d.y, d.z}, o.w);
+      s.atten = V3{at.x, at.y, at.z};
+      s.beauty = V3{ab.x, ab.y, ab.z};
+      s.primary = __float_as_uint(ab.w);
+      s.bounce = bounce;
+      uint32_t k = p / N, pix = p - k * N;
+      Rng g;
+      g.init(P.seed, pix + (W.base + k) * (P.W * P.H), __float_as_uint(at.w));
+      uint4 hv = W.hit[p];
+      bool hit = hv.x != 0xffffffffu;
+      Hit rec;
+      if (hit) rebuild_hit(sc, hv.x, hv.y, W.hit_t[p], __uint_as_float(hv.z), __uint_as_float(hv.w),
+                           s.ray, rec, shade_stk + threadIdx.x, kShadeThreads, P.err);
+      if (bounce == 0u && hit) {
+        uint32_t oid = sc.objects[rec.obj].object_id;
+        s.primary = (oid << 22) | (rec.prim == 0xffffffffu ? 0u : ((rec.prim + 1u) & 0x3fffffu));
+      }
+      if (!hit) {
+        s.beauty += s.atten * sky_sample(sc.sky, s.ray);
+      } else {
+        const DevMaterial& m = sc.materials[sc.objects[rec.obj].material];
+        Ray r_in = s.ray;
+        s.beauty += s.atten * mat_emitted(m, rec);
+        Scatter sr;
+        bool cont = mat_scatter(m, rec, s.ray, sr, g);
+        if (cont) {
+          if (sr.skip_pdf) {
+            s.atten *= sr.atten;
+            s.ray = make_ray(rec.p, sr.skip_dir, s.ray.tm);
+          } else {
+            cont = sample_brdf(P, m, rec, sr, r_in, s, g, st);
+          }
+        }
+        if (cont) {
+          if (bounce == 0u) {
+            float4 ad = W.acc_d[p], an = W.acc_n[p];
+            W.acc_d[p] = make_float4(ad.x + s.atten.x, ad.y + s.atten.y, ad.z + s.atten.z, 0.f);
+            W.acc_n[p] = make_float4(an.x + rec.n.x, an.y + rec.n.y, an.z + rec.n.z, 0.f);
+          }
+          if (P.rr_enabled && bounce >= P.rr_start) {
+            float survival = fmaxf(s.atten.x, fmaxf(s.atten.y, s.atten.z));
+            survival = fminf(survival, P.rr_survival);
+            if (g.uniform() > survival) cont = false;
+            else s.atten *= v3(1.0f / survival);
+          }
+        }
+        if (cont && bounce + 1u < P.depth) {
+          alive = true;
+          W.ray_o[p] = make_float4(s.ray.o.x, s.ray.o.y, s.ray.o.z, s.ray.tm);
+          W.ray_d[p] = make_float4(s.ray.d.x, s.ray.d.y, s.ray.d.z, __uint_as_float(bounce + 1u));
+          W.atten[p] = make_float4(s.atten.x, s.atten.y, s.atten.z, __uint_as_float(g.draw));
+        }
+      }
+      W.acc_b[p] = make_float4(s.beauty.x, s.beauty.y, s.beauty.z, __uint_as_float(s.primary));
+    }
+    // warp-aggregated append of the surviving paths
+    uint32_t mask = __ballot_sync(0xffffffffu, alive);
+    if (mask) {
+      uint32_t leader = __ffs(mask) - 1u;
+      uint32_t off = 0;
+      if (lane == leader) off = atomicAdd(next_n, __popc(mask));
+      off = __shfl_sync(0xffffffffu, off, leader);
+      if (alive) next_queue[off + __popc(mask & ((1u << lane) - 1u))] = p;
+    }
+  }
+}
+
+// Clears the counters for the next bounce: the queue that was just consumed
+// becomes the output of the following shade, and the extend work counter
+// restarts.
+__global__ void k_wf_rotate(WfParams W, int consumed) {
+  if (threadIdx.x == 0) {
+    W.ctr[consumed] = 0u;
+    W.ctr[CTR_WORK] = 0u;
+  }
+}
+
+__global__ void k_wf_accumulate(WfParams W) {
+  const KernelParams& P = W.kp;
+  const uint32_t N = P.W * P.H;
+  const size_t hw = N;
+  for (uint32_t pix = blockIdx.x * blockDim.x + threadIdx.x; pix < N; pix += gridDim.x * blockDim.x) {
+    if (P.write_raw) {
+      float4 b = W.acc_b[pix], d = W.acc_d[pix], n = W.acc_n[pix];
+      if (P.beauty) store3(P.beauty, hw, pix, V3{b.x, b.y, b.z});
+      if (P.diffuse) store3(P.diffuse, hw, pix, V3{d.x, d.y, d.z});
+      if (P.normal) store3(P.normal, hw, pix, V3{n.x, n.y, n.z});
+      if (P.primary) P.primary[pix] = __float_as_uint(b.w);
+      continue;
+    }
+    V3 ab = P.beauty ? load3(P.beauty, hw, pix) : V3{0, 0, 0};
+    V3 ad = P.diffuse ? load3(P.diffuse, hw, pix) : V3{0, 0, 0};
+    V3 an = P.normal ? load3(P.normal, hw, pix) : V3{0, 0, 0};
+    double s64[3] = {0, 0, 0};
+    for (uint32_t k = 0; k < W.count; ++k) {
+      uint32_t p = k * N + pix, smp = W.base + k;
+      float4 b = W.acc_b[p], d = W.acc_d[p], n = W.acc_n[p];
+      ab = running_mean(ab, V3{b.x, b.y, b.z}, smp);
+      ad = running_mean(ad, V3{d.x, d.y, d.z}, smp);
+      an = running_mean(an, V3{n.x, n.y, n.z}, smp);
+      s64[0] += (double)b.x;
+      s64[1] += (double)b.y;
+      s64[2] += (double)b.z;
+    }
+    if (P.beauty) store3(P.beauty, hw, pix, ab);
+    if (P.diffuse) store3(P.diffuse, hw, pix, ad);
+    if (P.normal) store3(P.normal, hw, pix, an);
+    if (P.beauty64) {
+      P.beauty64[pix] += s64[0];
+      P.beauty64[hw + pix] += s64[1];
+      P.beauty64[2 * hw + pix] += s64[2];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+
+static int sm_count() {
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  }
+  return sms;
+}
+
+size_t wf_state_bytes(uint32_t n_paths) {
+  return (size_t)n_paths * (6 * sizeof(float4) + sizeof(uint4) + sizeof(float) + 2 * sizeof(uint32_t));
+}
+
+cudaError_t wf_alloc(WfParams& W, uint32_t n_paths) {
+  cudaError_t e;
+#define A(ptr, T) \
+  if ((e = cudaMalloc(&W.ptr, sizeof(T) * (size_t)n_paths)) != cudaSuccess) return e;
+  A(ray_o, float4);
+  A(ray_d, float4);
+  A(atten, float4);
+  A(acc_b, float4);
+  A(acc_d, float4);
+  A(acc_n, float4);
+  A(hit, uint4);
+  A(hit_t, float);
+  A(queue0, uint32_t);
+  A(queue1, uint32_t);
+#undef A
+  if ((e = cudaMalloc(&W.ctr, 16 * sizeof(uint32_t))) != cudaSuccess) return e;
+  W.capacity = n_paths;
+  return cudaMemset(W.ctr, 0, 16 * sizeof(uint32_t));
+}
+
+void wf_free(WfParams& W) {
+  cudaFree(W.ray_o);
+  cudaFree(W.ray_d);
+  cudaFree(W.atten);
+  cudaFree(W.acc_b);
+  cudaFree(W.acc_d);
+  cudaFree(W.acc_n);
+  cudaFree(W.hit);
+  cudaFree(W.hit_t);
+  cudaFree(W.queue0);
+  cudaFree(W.queue1);
+  cudaFree(W.ctr);
+  W = WfParams{};
+}
+
+using ExtendFn = void (*)(WfParams, int, int);
+static ExtendFn extend_fn(bool counters, int variant) {
+  switch (variant) {
+    case 5: return counters ? k_wf_extend<true, 5> : k_wf_extend<false, 5>;
+    case 6: return counters ? k_wf_extend<true, 6> : k_wf_extend<false, 6>;
+    case 8: return counters ? k_wf_extend<true, 8> : k_wf_extend<false, 8>;
+    default: return counters ? k_wf_extend<true, 4> : k_wf_extend<false, 4>;
+  }
+}
+
+static int extend_blocks(ExtendFn fn) {
+  static ExtendFn cached_fn[16] = {nullptr};
+  static int cached_blocks[16] = {0};
+  for (int i = 0; i < 16; ++i) {
+    if (cached_fn[i] == fn) return cached_blocks[i];
+    if (!cached_fn[i]) {
+      size_t smem = sizeof(uint2) * (kTlasStack + kBlasStack) * kExtThreads;
+      int per_sm = 0;
+      cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kExtThreads, smem);
+      cached_fn[i] = fn;
+      cached_blocks[i] = sm_count() * (per_sm > 0 ? per_sm : 1);
+      return cached_blocks[i];
+    }
+  }
+  return sm_count() * 4;
+}
+
+// Launch sequence of one wave (capturable: every size is read on the device).
+cudaError_t wf_launch_wave(const WfParams& W, bool counters, cudaStream_t st) {
+  const KernelParams& P = W.kp;
+  uint32_t total = P.W * P.H * W.count;
+  int gen_blocks = (int)std::min<uint32_t>((total + 255) / 256, (uint32_t)sm_count() * 16);
+  k_wf_generate<<<gen_blocks, 256, 0, st>>>(W);
+  size_t smem = sizeof(uint2) * (kTlasStack + kBlasStack) * kExtThreads;
+  ExtendFn ext = extend_fn(counters, W.extend_variant);
+  int eb = extend_blocks(ext);
+  int shade_blocks = (int)std::min<uint32_t>((total + kShadeThreads - 1) / kShadeThreads,
+                                             (uint32_t)sm_count() * 16);
+  for (uint32_t b = 0; b < P.depth; ++b) {
+    int q = (int)(b & 1u);
+    ext<<<eb, kExtThreads, smem, st>>>(W, q, b == 0 ? 1 : 0);
+    k_wf_shade<<<shade_blocks, kShadeThreads, 0, st>>>(W, q, b == 0 ? 1 : 0);
+    k_wf_rotate<<<1, 32, 0, st>>>(W, q);
+  }
+  int acc_blocks = (int)std::min<uint32_t>((P.W * P.H + 255) / 256, (uint32_t)sm_count() * 16);
+  k_wf_accumulate<<<acc_blocks, 256, 0, st>>>(W);
+  return cudaGetLastError();
+}
+
+}  // namespace nr

@@ -1,0 +1,31 @@
+// wavefront.cuh — launch interface of the wavefront integrator.
+#pragma once
+#include "integrator.cuh"
+
+namespace nr {
+
+struct WfParams {
+  KernelParams kp;
+  uint32_t base;   // first sample index of the wave
+  uint32_t count;  // sample indices in the wave
+  uint32_t capacity;
+  int32_t extend_variant;  // 4, 5, 6 or 8 CTAs per SM
+  float4* ray_o;
+  float4* ray_d;
+  float4* atten;
+  float4* acc_b;
+  float4* acc_d;
+  float4* acc_n;
+  uint4* hit;
+  float* hit_t;
+  uint32_t* queue0;
+  uint32_t* queue1;
+  uint32_t* ctr;
+};
+
+size_t wf_state_bytes(uint32_t n_paths);
+cudaError_t wf_alloc(WfParams& W, uint32_t n_paths);
+void wf_free(WfParams& W);
+cudaError_t wf_launch_wave(const WfParams& W, bool counters, cudaStream_t st);
+
+}  // namespace nr

@@ -91,6 +91,29 @@ def test_mesh_hdri_samples(mesh_scene, orc, refcuda, s):
     assert (p == op).mean() >= 0.999
 
 
+@pytest.mark.parametrize("variant,mesh_leaf,tlas_leaf,spw,schedule", [
+    (4, 3, 1, 0, capi.SCHEDULE_WAVEFRONT),
+    (6, 1, 2, 1, capi.SCHEDULE_WAVEFRONT),
+    (8, 2, 3, 3, capi.SCHEDULE_WAVEFRONT),
+    (5, 1, 1, 0, capi.SCHEDULE_MEGAKERNEL),
+])
+def test_tuning_knobs_do_not_change_samples(mesh_scene, refcuda, variant, mesh_leaf, tlas_leaf,
+                                            spw, schedule):
+    """Every traversal variant, leaf size, wave size and schedule the tuner
+    may pick renders the same per-sample images."""
+    spec, _, _ = mesh_scene
+    sc = capi.Scene(spec, mesh_leaf=mesh_leaf, tlas_leaf=tlas_leaf)
+    r = capi.Render(sc, extend_variant=variant, samples_per_wave=spw, schedule=schedule)
+    r.samples(1, 3)
+    acc = r.layer(0)
+    rb, *_ = refcuda.render(spec, 1, count=3, mode=1)
+    assert frac_close(acc, rb) >= 0.99
+    b, d, n, p = r.sample_layers(2)
+    rb2, _, rn2, _ = refcuda.render(spec, 2, mode=0)
+    assert frac_close(b, rb2) >= 0.99
+    assert frac_close(n, rn2) >= 0.999
+
+
 def test_participating_medium_samples(orc, refcuda):
     spec = scenes.mesh_stress(levels=3, res_h=48, res_w=48, spp=2, depth=32, n_spheres=8,
                               hdri_size=(128, 64), scene_seed=2)
