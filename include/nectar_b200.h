@@ -261,7 +261,7 @@ int nr_scene_set_sky_hdri(nr_scene* scene, const float* chw, uint32_t C, uint32_
 int nr_scene_load_hdr(nr_scene* scene, const char* path, float rotation_deg, float intensity);
 /* HDRISkylightConfig rotation/intensity (skylight.h:14-21) after creation. */
 int nr_scene_set_hdri_params(nr_scene* scene, float rotation_deg, float intensity);
-/* Leaf sizes of the 8-wide trees (1..3 primitives; defaults: meshes 3,
+/* Leaf sizes of the 8-wide trees (1..3 primitives; defaults: meshes 1,
  * top level 1). Takes effect at the next nr_scene_build. */
 int nr_scene_set_tuning(nr_scene* scene, uint32_t mesh_leaf_max, uint32_t tlas_leaf_max);
 /* Uploads the scene and builds every BVH on the GPU (Scene::build,

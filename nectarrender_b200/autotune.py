@@ -30,7 +30,7 @@ VARIANTS = (4, 5, 6, 8)
 
 @dataclass
 class Tuning:
-    mesh_leaf: int = 3
+    mesh_leaf: int = 1
     tlas_leaf: int = 1
     extend_variant: int = 5
     samples_per_wave: int = 0
@@ -64,8 +64,8 @@ def _time(scene: capi.Scene, spec: SceneSpec, over: dict, samples: int, reps: in
     return best / samples
 
 
-def tune(spec: SceneSpec, samples: int = 4, reps: int = 2, leaves=((3, 1), (2, 1), (1, 1), (3, 2)),
-         variants=VARIANTS, waves=(0, 2, 4), megakernel: bool = True) -> Tuning:
+def tune(spec: SceneSpec, samples: int = 4, reps: int = 2, leaves=((1, 1), (2, 1), (3, 1), (1, 2)),
+         variants=VARIANTS, waves=(0, 2, 4, 8), megakernel: bool = True) -> Tuning:
     """Times every candidate on `spec` (device time of `samples` sample
     indices, best of `reps`) and returns the fastest as a :class:`Tuning`."""
     table = []

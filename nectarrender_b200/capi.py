@@ -171,7 +171,7 @@ class Scene:
     """An nr_scene built from a SceneSpec (registry semantics of the
     reference: one material per hittable, lights after hittables)."""
 
-    def __init__(self, spec: SceneSpec, build: bool = True, mesh_leaf: int = 3, tlas_leaf: int = 1):
+    def __init__(self, spec: SceneSpec, build: bool = True, mesh_leaf: int = 1, tlas_leaf: int = 1):
         self.lib = library()
         self.spec = spec
         self.h = C.c_void_p()

@@ -379,7 +379,7 @@ struct nr_scene {
   nr_scene_stats stats{};
   std::vector<int32_t> ref_leaf_order;
   int32_t light = -1;
-  uint32_t mesh_leaf_max = 3, tlas_leaf_max = 1;
+  uint32_t mesh_leaf_max = 1, tlas_leaf_max = 1;
 
   void release_device() {
     for (auto p : d_images) cudaFree(p);

@@ -37,9 +37,13 @@ def test_band_matches_oracle(full):
     ob, od, on, op, _ = h.render(3, 1, mode=0, rows=(500, 540))
     band = slice(500, 540)
     assert (p[band] == op[band]).mean() >= 0.999
-    # unit normals: components near zero get an absolute bar of 2e-5
-    # (host sqrt versus device fast-math normalisation of interpolated normals)
-    assert frac_close(n[:, band], on[:, band], rtol=1e-4, floor=0.2) >= 0.99
+    # Unit normals, absolute bar. Grazing sphere hits amplify the device's
+    # fused multiply-adds in the quadratic's discriminant (the oracle is host
+    # code without contraction) into ~1e-4 moves of the hit point; the
+    # ulp-level bar is against the reference's CUDA build in the parity tests.
+    dn = np.abs(n[:, band] - on[:, band])
+    assert (dn <= 2e-4).mean() >= 0.99
+    assert float(np.median(dn)) <= 1e-6
     # host libm (oracle) versus device fast-math moves HDRI lookups by ulps;
     # the tight per-sample bar is against the reference's CUDA build
     assert frac_close(b[:, band], ob[:, band], rtol=1e-3) >= 0.97
