@@ -289,6 +289,35 @@ int nr_render_reset(nr_render* render);
  * mean avg*(n-1)/n + s/n with n = sample index (data.cu:28-50). The reference
  * render() loop is first = 1, count = samples_per_pixel - 1 (engine.cpp:43). */
 int nr_render_samples(nr_render* render, uint32_t first, uint32_t count);
+
+/* nr_render_samples_static: no counterpart in the reference.
+ * Renders exactly like nr_render_samples (same sample indices, same layers,
+ * same results; always the wavefront schedule) but allocates no device memory
+ * during the call. nr_render_samples allocates its wave state (W*H*samples
+ * per wave paths of ~124 B, about 1 GB at 1920x1080) on its first call; this
+ * entry point carves that state out of a fixed library-owned device buffer of
+ * NR_STATIC_WAVE_BYTES instead. It is for callers that cannot allocate while
+ * rendering: a process whose free device memory is already reserved by
+ * another allocator (e.g. a framework's caching allocator), or an interactive
+ * caller that cannot take the device-wide synchronisation cudaMalloc and
+ * cudaFree imply. Everything else the call uses was allocated by
+ * nr_render_create.
+ *  - Limit: W*H <= NR_STATIC_WAVE_PATHS pixels (e.g. 512x512); larger renders
+ *    fail with NR_ERR_LIMIT before any work. A wave holds
+ *    NR_STATIC_WAVE_PATHS / (W*H) sample indices (at most the render's
+ *    samples_per_wave setting).
+ *  - Setup: the first call on each device looks up the buffer's address
+ *    (cudaGetSymbolAddress, with the render's device current). Make that
+ *    first call before any stream capture on that device.
+ *  - Nothing in the buffer has to start at zero: the first kernel of every
+ *    wave resets the queue counters the later kernels read.
+ *  - There is one buffer per device per process. Calls that overlap in time
+ *    (several host threads, several renders on the same device) race on it
+ *    and corrupt each other's paths: serialise them. The call returns when
+ *    its work is complete, so calls from one thread never overlap. */
+#define NR_STATIC_WAVE_BYTES (32u << 20)
+#define NR_STATIC_WAVE_PATHS 270528u
+int nr_render_samples_static(nr_render* render, uint32_t first, uint32_t count);
 /* Renders one sample index and writes its raw per-sample layers (the
  * reference's sample_aovs before accumulation) to host float CHW buffers;
  * any pointer may be NULL. Used for per-sample parity. */

@@ -32,7 +32,8 @@ NVCC_FLAGS = ARCH + [
     "-Xcompiler", "-fPIC,-O2", "-Xptxas", "-O3",
     f"-I{CSRC}", f"-I{INCLUDE}",
 ]
-CU_SOURCES = ["capi.cu", "integrator.cu", "wavefront.cu", "bvh_build.cu", "image_ops.cu"]
+CU_SOURCES = ["capi.cu", "integrator.cu", "wavefront.cu", "bvh_build.cu", "image_ops.cu",
+              "static_wave.cu"]
 CPP_SOURCES = ["host_io.cpp"]
 LIB = HERE / "libnectar_b200.so"
 

@@ -81,6 +81,7 @@ EXPORTS = [
     "nr_scene_set_tuning", "nr_scene_build",
     "nr_scene_get_stats", "nr_scene_get_binary_bvh", "nr_render_config_default",
     "nr_render_create", "nr_render_destroy", "nr_render_reset", "nr_render_samples",
+    "nr_render_samples_static",
     "nr_render_sample_layers", "nr_render_layer_device_ptr", "nr_render_read_layer",
     "nr_render_read_beauty_fp64", "nr_render_readback", "nr_render_display_float",
     "nr_render_dims", "nr_render_set_counters", "nr_render_get_counters", "nr_render_last_ms",

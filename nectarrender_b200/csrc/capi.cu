@@ -10,6 +10,7 @@
 // leaf order that decides lights[0]) are computed here with the same host
 // arithmetic; values it computes on the device (cube face transforms, the
 // HDRI rotation, white-balance gains) are computed by device kernels.
+#include <atomic>
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -1194,6 +1195,71 @@ int nr_render_samples(nr_render* r, uint32_t first, uint32_t count) {
   int rc = run_kernel(r, P);
   if (rc == NR_OK) r->n64 = first + count - 1;
   return rc;
+}
+
+// nr_render_samples_static: the wave state lives in static_wave.cu's
+// file-scope device buffer, looked up once per device.
+static std::atomic<uintptr_t> g_static_wave_addr[64];
+
+int nr_render_samples_static(nr_render* r, uint32_t first, uint32_t count) {
+  if (!r) return fail(NR_ERR_INVALID, "null render");
+  if (count == 0) return NR_OK;
+  if (first == 0) return fail(NR_ERR_INVALID, "sample indices start at 1");
+  if ((uint64_t)first + count > r->cam.samples_per_pixel)
+    return fail(NR_ERR_INVALID, "sample index beyond samples_per_pixel");
+  const uint32_t N = r->W * r->H;
+  if ((uint64_t)r->W * r->H > NR_STATIC_WAVE_PATHS)
+    return fail(NR_ERR_LIMIT, "nr_render_samples_static: " + std::to_string(r->W) + "x" +
+                                  std::to_string(r->H) + " = " + std::to_string(N) +
+                                  " pixels exceeds the static wave buffer's " +
+                                  std::to_string(NR_STATIC_WAVE_PATHS) + " paths");
+  int dev = 0;
+  CU(cudaGetDevice(&dev), "cudaGetDevice");
+  if (dev < 0 || dev >= 64) return fail(NR_ERR_LIMIT, "device ordinal beyond 63");
+  uintptr_t addr = g_static_wave_addr[dev].load(std::memory_order_acquire);
+  if (!addr) {
+    void* p = nullptr;
+    CU(static_wave_address(&p), "cudaGetSymbolAddress(static wave buffer)");
+    addr = (uintptr_t)p;
+    g_static_wave_addr[dev].store(addr, std::memory_order_release);
+  }
+  WfParams W{};
+  static_wave_carve((void*)addr, W);
+  KernelParams P = make_params(r, first, count, false);
+  uint32_t per = std::max(1u, std::min(waves_of(r), NR_STATIC_WAVE_PATHS / N));
+
+  if (r->counters_on) CU(cudaMemsetAsync(r->counters, 0, 8 * 5, r->stream), "clear counters");
+  CU(cudaEventRecord(r->ev0, r->stream), "event");
+  for (uint32_t s = 0; s < count; s += per) {
+    WfParams w = W;
+    w.kp = P;
+    w.extend_variant = r->cfg.extend_variant > 0 ? r->cfg.extend_variant : 5;
+    w.base = first + s;
+    w.count = std::min(per, count - s);
+    CU(wf_launch_wave(w, r->counters_on, r->stream), "launch wavefront");
+  }
+  CU(cudaEventRecord(r->ev1, r->stream), "event");
+  CU(cudaEventSynchronize(r->ev1), "integrator");
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, r->ev0, r->ev1);
+  r->last_ms = ms;
+  uint32_t herr = 0;
+  CU(cudaMemcpy(&herr, r->err, 4, cudaMemcpyDeviceToHost), "read error word");
+  if (herr) {
+    cudaMemset(r->err, 0, 4);
+    return fail(NR_ERR_DEVICE, "integrator error word 0x" + std::to_string(herr));
+  }
+  if (r->counters_on) {
+    unsigned long long c[5];
+    CU(cudaMemcpy(c, r->counters, sizeof(c), cudaMemcpyDeviceToHost), "read counters");
+    r->last.rays = c[0];
+    r->last.node_visits = c[1];
+    r->last.tri_tests = c[2];
+    r->last.obj_tests = c[3];
+    r->last.paths = (unsigned long long)count * N;
+  }
+  r->n64 = first + count - 1;
+  return NR_OK;
 }
 
 int nr_render_sample_layers(nr_render* r, uint32_t sample_idx, float* beauty, float* diffuse,

@@ -26,6 +26,11 @@ struct WfParams {
 size_t wf_state_bytes(uint32_t n_paths);
 cudaError_t wf_alloc(WfParams& W, uint32_t n_paths);
 void wf_free(WfParams& W);
+// static_wave.cu: address of the library-owned wave buffer on the current
+// device, and its division into the wave's arrays (capacity
+// NR_STATIC_WAVE_PATHS paths).
+cudaError_t static_wave_address(void** out);
+void static_wave_carve(void* base, WfParams& W);
 cudaError_t wf_launch_wave(const WfParams& W, bool counters, cudaStream_t st);
 
 }  // namespace nr
