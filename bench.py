@@ -232,6 +232,11 @@ def run_ours(args):
     torch.cuda.synchronize()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
           for _ in range(args.steps)]
+    # per-kernel device time: events between consecutive launches on the
+    # render stream, recorded inside the timed steps
+    render.profiling(True)
+    kernel_ms = {k: 0.0 for k in capi.KERNEL_CLASSES}
+    kernel_launches = {k: 0 for k in capi.KERNEL_CLASSES}
     with Clocks(local) as clk:
         for k in range(args.steps):
             l2_flush.zero_()  # evict the scene from L2 between timed steps
@@ -239,7 +244,11 @@ def run_ours(args):
             ev[k][0].record(stream)
             render.samples(first_index(args.warmup + 1 + k), S)
             ev[k][1].record(stream)
+            for name, (ms, n) in render.last_profile().items():
+                kernel_ms[name] += ms
+                kernel_launches[name] += n
         torch.cuda.synchronize()
+    render.profiling(False)
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
@@ -262,25 +271,35 @@ def run_ours(args):
         torch.cuda.synchronize()
         combine_ms = 1e3 * (time.perf_counter() - t0)
 
-    # roofline of the integrator kernel from counted record fetches
-    # wide nodes 80 B, triangle records 48 B, object records 128 B, and the
-    # running-mean load+store of 3 layers x 3 channels x 4 B per pixel
-    per_launch_bytes = (counts["node_visits"] * 80 + counts["tri_tests"] * 48 +
-                        counts["obj_tests"] * 128 + w * h * 72)
-    kernel_ms = t_ms / args.steps
-    achieved = per_launch_bytes / (kernel_ms * 1e-3) / 1e9
+    # Roofline of the dominant kernel from counted record fetches. Per ray
+    # query: wide nodes 80 B, triangle records 48 B, object records 128 B,
+    # plus the ray (origin + direction 32 B) and queue slot (4 B) read and
+    # the hit record (20 B) written. The megakernel schedule also folds the
+    # running mean (3 layers x 3 channels x 4 B read + write per pixel).
+    trav_bytes = (counts["node_visits"] * 80 + counts["tri_tests"] * 48 +
+                  counts["obj_tests"] * 128 + counts["rays"] * 56)
+    if args.schedule == "megakernel":
+        dom, dom_bytes = "megakernel", trav_bytes + w * h * 72
+    else:
+        dom, dom_bytes = "extend", trav_bytes
+    dom_ms = kernel_ms[dom] / args.steps            # per step
+    dom_launches = max(1, kernel_launches[dom] // args.steps)
+    achieved = dom_bytes / (dom_ms * 1e-3) / 1e9
     peaks = {}
     try:
         peaks = json.loads((HERE / "MEASURED_PEAKS.json").read_text())
         peak, peak_src = float(peaks["hbm_gbs"]), "measured"
     except (OSError, KeyError, ValueError):
         peak, peak_src = 6650.0, "fallback"
+    # DRAM bytes of the dominant kernel per launch, from an ncu capture of
+    # this workload (dram__bytes_read.sum + dram__bytes_write.sum summed
+    # over one step's launches, divided by the launches)
     traffic = None
-    tp = HERE / "profiles" / "megakernel_traffic.json"
+    tp = HERE / "profiles" / f"{dom}_traffic.json"
     if tp.exists():
         try:
             t = json.loads(tp.read_text())
-            traffic = t["dram_bytes_per_sample"] * w * h * S
+            traffic = t["dram_bytes_per_step"] / max(1, t["launches_per_step"])
         except (OSError, KeyError, ValueError):
             traffic = None
 
@@ -309,12 +328,17 @@ def run_ours(args):
                 "config": config_json(args, h, w, spec, "flushed between timed steps (256 MiB write)"),
                 "clocks": clk.summary(),
                 "e2e": e2e,
-                "gpu_launches": args.steps * (render_launches_per_step(spec, args)),
+                "gpu_launches": sum(kernel_launches.values()),
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "traffic": traffic,
-                             "peak_source": peak_src,
-                             "algorithmic_bytes_per_launch": per_launch_bytes,
-                             "counts_per_launch": counts},
+                             "kernel": dom, "peak_source": peak_src,
+                             "algorithmic_bytes_per_launch": dom_bytes / dom_launches,
+                             "launch_ms": dom_ms / dom_launches,
+                             "counts_per_step": counts},
+                "kernels": {k: {"ms_per_step": kernel_ms[k] / args.steps,
+                                "launches_per_step": kernel_launches[k] / args.steps,
+                                "share": kernel_ms[k] / max(1e-9, sum(kernel_ms.values()))}
+                            for k in capi.KERNEL_CLASSES if kernel_launches[k]},
                 "cpu_baseline": cpu,
                 "reference_cuda": ref_cuda,
                 "scene": {"build_ms_device": stats["build_ms"], "build_wall_s": build_wall,
@@ -327,17 +351,6 @@ def run_ours(args):
     if dist:
         dist.barrier()
         dist.destroy_process_group()
-
-
-def render_launches_per_step(spec, args):
-    """Kernels of ours launched per step: the megakernel once; the wavefront
-    per wave generate + depth x (extend, shade, queue rotate) + accumulate."""
-    if args.schedule == "megakernel":
-        return 1
-    h, w = (int(x) for x in args.res.split("x"))
-    per_wave = max(1, min(8, (8 << 20) // (w * h)))
-    waves = -(-args.spp_per_step // per_wave)
-    return waves * (2 + 3 * spec.ray_depth)
 
 
 def e2e_public_api(pt, spec, S, args):

@@ -205,6 +205,23 @@ typedef struct nr_trace_counters {
   uint64_t paths;       /* pixel-samples completed                           */
 } nr_trace_counters;
 
+/* Device time per kernel class of the last nr_render_samples call, from CUDA
+ * events recorded between consecutive launches on the render stream (filled
+ * when profiling is enabled). Index: NR_KERNEL_*. */
+enum {
+  NR_KERNEL_GENERATE = 0,   /* camera rays of a wave                         */
+  NR_KERNEL_EXTEND = 1,     /* closest-hit traversal of a queue              */
+  NR_KERNEL_SHADE = 2,      /* materials, sky, RR, next queue                */
+  NR_KERNEL_ROTATE = 3,     /* queue swap                                    */
+  NR_KERNEL_ACCUMULATE = 4, /* running mean into the layers                  */
+  NR_KERNEL_MEGAKERNEL = 5, /* per-pixel schedule                            */
+  NR_KERNEL_CLASSES = 6
+};
+typedef struct nr_kernel_profile {
+  double ms[NR_KERNEL_CLASSES];
+  uint32_t launches[NR_KERNEL_CLASSES];
+} nr_kernel_profile;
+
 typedef struct nr_scene nr_scene;
 typedef struct nr_render nr_render;
 
@@ -341,6 +358,9 @@ int nr_render_dims(const nr_render* render, uint32_t* C, uint32_t* H, uint32_t* 
 /* Counters of the last nr_render_samples call when enabled. */
 int nr_render_set_counters(nr_render* render, int32_t enabled);
 int nr_render_get_counters(const nr_render* render, nr_trace_counters* out);
+/* Per-kernel device time of the last nr_render_samples call when enabled. */
+int nr_render_set_profiling(nr_render* render, int32_t enabled);
+int nr_render_get_profile(const nr_render* render, nr_kernel_profile* out);
 /* Device time in milliseconds of the last nr_render_samples call (CUDA events
  * on the render stream). */
 int nr_render_last_ms(const nr_render* render, double* out_ms);

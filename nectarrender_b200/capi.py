@@ -61,6 +61,13 @@ class SceneStats(C.Structure):
                 ("build_ms", C.c_double), ("device_bytes", C.c_uint64)]
 
 
+KERNEL_CLASSES = ("generate", "extend", "shade", "rotate", "accumulate", "megakernel")
+
+
+class KernelProfile(C.Structure):
+    _fields_ = [("ms", C.c_double * 6), ("launches", C.c_uint32 * 6)]
+
+
 class TraceCounters(C.Structure):
     _fields_ = [("rays", C.c_uint64), ("node_visits", C.c_uint64), ("tri_tests", C.c_uint64),
                 ("obj_tests", C.c_uint64), ("paths", C.c_uint64)]
@@ -81,7 +88,7 @@ EXPORTS = [
     "nr_scene_set_tuning", "nr_scene_build",
     "nr_scene_get_stats", "nr_scene_get_binary_bvh", "nr_render_config_default",
     "nr_render_create", "nr_render_destroy", "nr_render_reset", "nr_render_samples",
-    "nr_render_samples_static",
+    "nr_render_samples_static", "nr_render_set_profiling", "nr_render_get_profile",
     "nr_render_sample_layers", "nr_render_layer_device_ptr", "nr_render_read_layer",
     "nr_render_read_beauty_fp64", "nr_render_readback", "nr_render_display_float",
     "nr_render_dims", "nr_render_set_counters", "nr_render_get_counters", "nr_render_last_ms",
@@ -303,6 +310,15 @@ class Render:
         c = TraceCounters()
         self.lib.nr_render_get_counters(self.h, C.byref(c))
         return {k: getattr(c, k) for k, _ in TraceCounters._fields_}
+
+    def profiling(self, on: bool = True) -> None:
+        _check(self.lib.nr_render_set_profiling(self.h, int(on)), "nr_render_set_profiling")
+
+    def last_profile(self) -> dict:
+        """{kernel class: (device ms, launches)} of the last samples() call."""
+        p = KernelProfile()
+        _check(self.lib.nr_render_get_profile(self.h, C.byref(p)), "nr_render_get_profile")
+        return {k: (p.ms[i], p.launches[i]) for i, k in enumerate(KERNEL_CLASSES)}
 
     def last_ms(self) -> float:
         v = C.c_double()

@@ -940,6 +940,10 @@ struct nr_render {
   uint32_t samples_per_wave = 0;
   int rtl = 0;
   bool counters_on = false;
+  bool profile_on = false;
+  std::vector<cudaEvent_t> pev;  // profiling: one event per launch boundary
+  std::vector<uint8_t> pkind;
+  nr_kernel_profile prof{};
   nr_trace_counters last{};
   double last_ms = 0.0;
   ~nr_render() {
@@ -955,6 +959,7 @@ struct nr_render {
     cudaFree(disp8);
     cudaFree(dispf);
     cudaFree(wb_scratch);
+    for (auto e : pev) cudaEventDestroy(e);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (stream) cudaStreamDestroy(stream);
@@ -1131,10 +1136,11 @@ static uint32_t waves_of(nr_render* r) {
   return s;
 }
 
-static int launch(nr_render* r, const KernelParams& P) {
+static int launch(nr_render* r, const KernelParams& P, WaveTimer* tm) {
   if (r->cfg.schedule != NR_SCHEDULE_WAVEFRONT) {
     CU(cudaMemsetAsync(r->work, 0, 4, r->stream), "clear work counter");
     CU(launch_megakernel(P, r->counters_on, r->stream), "launch integrator");
+    if (tm) tm->mark(NR_KERNEL_MEGAKERNEL, r->stream);
     return NR_OK;
   }
   uint32_t N = r->W * r->H;
@@ -1149,7 +1155,7 @@ static int launch(nr_render* r, const KernelParams& P) {
     W.extend_variant = r->cfg.extend_variant > 0 ? r->cfg.extend_variant : 5;
     W.base = P.first_sample + s;
     W.count = std::min(per, P.n_samples - s);
-    CU(wf_launch_wave(W, r->counters_on, r->stream), "launch wavefront");
+    CU(wf_launch_wave(W, r->counters_on, r->stream, tm), "launch wavefront");
   }
   return NR_OK;
 }
@@ -1157,13 +1163,29 @@ static int launch(nr_render* r, const KernelParams& P) {
 static int run_kernel(nr_render* r, const KernelParams& P) {
   if (r->counters_on) CU(cudaMemsetAsync(r->counters, 0, 8 * 5, r->stream), "clear counters");
   CU(cudaEventRecord(r->ev0, r->stream), "event");
-  int rc = launch(r, P);
+  WaveTimer tm;
+  if (r->profile_on) {
+    CU(cudaEventRecord(r->pev[0], r->stream), "event");
+    tm.ev = r->pev.data() + 1;
+    tm.kind = r->pkind.data() + 1;
+    tm.cap = (int)r->pev.size() - 1;
+  }
+  int rc = launch(r, P, r->profile_on ? &tm : nullptr);
   if (rc != NR_OK) return rc;
   CU(cudaEventRecord(r->ev1, r->stream), "event");
   CU(cudaEventSynchronize(r->ev1), "integrator");
   float ms = 0.f;
   cudaEventElapsedTime(&ms, r->ev0, r->ev1);
   r->last_ms = ms;
+  if (r->profile_on) {
+    r->prof = nr_kernel_profile{};
+    for (int i = 0; i < tm.n; ++i) {
+      float d = 0.f;
+      cudaEventElapsedTime(&d, i ? tm.ev[i - 1] : r->pev[0], tm.ev[i]);
+      r->prof.ms[tm.kind[i]] += d;
+      r->prof.launches[tm.kind[i]] += 1;
+    }
+  }
   uint32_t herr = 0;
   CU(cudaMemcpy(&herr, r->err, 4, cudaMemcpyDeviceToHost), "read error word");
   if (herr) {
@@ -1351,6 +1373,24 @@ int nr_render_dims(const nr_render* r, uint32_t* C, uint32_t* H, uint32_t* W) {
 int nr_render_set_counters(nr_render* r, int32_t on) {
   if (!r) return fail(NR_ERR_INVALID, "null render");
   r->counters_on = on != 0;
+  return NR_OK;
+}
+
+int nr_render_set_profiling(nr_render* r, int32_t on) {
+  if (!r) return fail(NR_ERR_INVALID, "null render");
+  if (on && r->pev.empty()) {
+    // up to 4095 launches per call are timed (a wave is 2 + 3 * depth launches)
+    r->pev.resize(4096, nullptr);
+    r->pkind.resize(4096, 0);
+    for (auto& e : r->pev) CU(cudaEventCreate(&e), "event");
+  }
+  r->profile_on = on != 0;
+  return NR_OK;
+}
+
+int nr_render_get_profile(const nr_render* r, nr_kernel_profile* out) {
+  if (!r || !out) return fail(NR_ERR_INVALID, "null argument");
+  *out = r->prof;
   return NR_OK;
 }
 

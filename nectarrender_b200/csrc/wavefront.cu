@@ -562,11 +562,12 @@ static int extend_blocks(ExtendFn fn) {
 }
 
 // Launch sequence of one wave (capturable: every size is read on the device).
-cudaError_t wf_launch_wave(const WfParams& W, bool counters, cudaStream_t st) {
+cudaError_t wf_launch_wave(const WfParams& W, bool counters, cudaStream_t st, WaveTimer* tm) {
   const KernelParams& P = W.kp;
   uint32_t total = P.W * P.H * W.count;
   int gen_blocks = (int)std::min<uint32_t>((total + 255) / 256, (uint32_t)sm_count() * 16);
   k_wf_generate<<<gen_blocks, 256, 0, st>>>(W);
+  if (tm) tm->mark(NR_KERNEL_GENERATE, st);
   size_t smem = sizeof(uint2) * (kTlasStack + kBlasStack) * kExtThreads;
   ExtendFn ext = extend_fn(counters, W.extend_variant);
   int eb = extend_blocks(ext);
@@ -575,11 +576,15 @@ cudaError_t wf_launch_wave(const WfParams& W, bool counters, cudaStream_t st) {
   for (uint32_t b = 0; b < P.depth; ++b) {
     int q = (int)(b & 1u);
     ext<<<eb, kExtThreads, smem, st>>>(W, q, b == 0 ? 1 : 0);
+    if (tm) tm->mark(NR_KERNEL_EXTEND, st);
     k_wf_shade<<<shade_blocks, kShadeThreads, 0, st>>>(W, q, b == 0 ? 1 : 0);
+    if (tm) tm->mark(NR_KERNEL_SHADE, st);
     k_wf_rotate<<<1, 32, 0, st>>>(W, q);
+    if (tm) tm->mark(NR_KERNEL_ROTATE, st);
   }
   int acc_blocks = (int)std::min<uint32_t>((P.W * P.H + 255) / 256, (uint32_t)sm_count() * 16);
   k_wf_accumulate<<<acc_blocks, 256, 0, st>>>(W);
+  if (tm) tm->mark(NR_KERNEL_ACCUMULATE, st);
   return cudaGetLastError();
 }
 

@@ -1,6 +1,7 @@
 // wavefront.cuh — launch interface of the wavefront integrator.
 #pragma once
 #include "integrator.cuh"
+#include "../../include/nectar_b200.h"
 
 namespace nr {
 
@@ -31,6 +32,23 @@ void wf_free(WfParams& W);
 // NR_STATIC_WAVE_PATHS paths).
 cudaError_t static_wave_address(void** out);
 void static_wave_carve(void* base, WfParams& W);
-cudaError_t wf_launch_wave(const WfParams& W, bool counters, cudaStream_t st);
+// Optional timing of a wave: an event is recorded after every launch and
+// tagged with the launch's kernel class (NR_KERNEL_*); the host attributes
+// the time between consecutive events to the later launch.
+struct WaveTimer {
+  cudaEvent_t* ev = nullptr;
+  uint8_t* kind = nullptr;
+  int cap = 0;
+  int n = 0;
+  void mark(int k, cudaStream_t st) {
+    if (n < cap) {
+      cudaEventRecord(ev[n], st);
+      kind[n++] = (uint8_t)k;
+    }
+  }
+};
+
+cudaError_t wf_launch_wave(const WfParams& W, bool counters, cudaStream_t st,
+                           WaveTimer* timer = nullptr);
 
 }  // namespace nr
