@@ -43,7 +43,7 @@ METRIC = "samples/s (pixel-samples per second, mesh-stress scene)"
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--steps", type=int, default=60)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--spp-per-step", type=int, default=4)
@@ -232,11 +232,6 @@ def run_ours(args):
     torch.cuda.synchronize()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
           for _ in range(args.steps)]
-    # per-kernel device time: events between consecutive launches on the
-    # render stream, recorded inside the timed steps
-    render.profiling(True)
-    kernel_ms = {k: 0.0 for k in capi.KERNEL_CLASSES}
-    kernel_launches = {k: 0 for k in capi.KERNEL_CLASSES}
     with Clocks(local) as clk:
         for k in range(args.steps):
             l2_flush.zero_()  # evict the scene from L2 between timed steps
@@ -244,10 +239,23 @@ def run_ours(args):
             ev[k][0].record(stream)
             render.samples(first_index(args.warmup + 1 + k), S)
             ev[k][1].record(stream)
-            for name, (ms, n) in render.last_profile().items():
-                kernel_ms[name] += ms
-                kernel_launches[name] += n
         torch.cuda.synchronize()
+    graphs = render.graph_stats()
+    # Per-kernel device time: the same steps again with an event recorded
+    # after every launch on the render stream (direct launches instead of
+    # the wave graphs, so that each kernel is bracketed by events).
+    render.profiling(True)
+    kernel_ms = {k: 0.0 for k in capi.KERNEL_CLASSES}
+    kernel_launches = {k: 0 for k in capi.KERNEL_CLASSES}
+    prof_step_ms = []
+    for k in range(args.steps):
+        l2_flush.zero_()
+        torch.cuda.synchronize()
+        render.samples(first_index(args.warmup + 1 + k), S)
+        prof_step_ms.append(render.last_ms())
+        for name, (ms, n) in render.last_profile().items():
+            kernel_ms[name] += ms
+            kernel_launches[name] += n
     render.profiling(False)
     if dist:
         dist.barrier()
@@ -329,6 +337,8 @@ def run_ours(args):
                 "clocks": clk.summary(),
                 "e2e": e2e,
                 "gpu_launches": sum(kernel_launches.values()),
+                "wave_graphs": {"captured": graphs[0], "replays": graphs[1]},
+                "ms_per_step_profiled": sum(prof_step_ms) / len(prof_step_ms),
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "traffic": traffic,
                              "kernel": dom, "peak_source": peak_src,

@@ -169,6 +169,7 @@ typedef struct nr_render_config {
   int32_t extend_variant;   /* wavefront traversal: CTAs per SM the register
                                budget targets (4, 5, 6 or 8; 0 = default)   */
   uint32_t samples_per_wave;/* wavefront: sample indices per wave (0 = ~8M paths) */
+  int32_t use_graphs;       /* wavefront: replay each wave as a CUDA graph (1) */
 } nr_render_config;
 
 /* StreamConfig display fields (nectar_render/csrc/data/include/data/stream.h:13-30). */
@@ -212,7 +213,7 @@ enum {
   NR_KERNEL_GENERATE = 0,   /* camera rays of a wave                         */
   NR_KERNEL_EXTEND = 1,     /* closest-hit traversal of a queue              */
   NR_KERNEL_SHADE = 2,      /* materials, sky, RR, next queue                */
-  NR_KERNEL_ROTATE = 3,     /* queue swap                                    */
+  NR_KERNEL_ROTATE = 3,     /* queue swap and wave bookkeeping               */
   NR_KERNEL_ACCUMULATE = 4, /* running mean into the layers                  */
   NR_KERNEL_MEGAKERNEL = 5, /* per-pixel schedule                            */
   NR_KERNEL_CLASSES = 6
@@ -361,6 +362,8 @@ int nr_render_get_counters(const nr_render* render, nr_trace_counters* out);
 /* Per-kernel device time of the last nr_render_samples call when enabled. */
 int nr_render_set_profiling(nr_render* render, int32_t enabled);
 int nr_render_get_profile(const nr_render* render, nr_kernel_profile* out);
+/* Wave graphs captured and replayed by this render so far (use_graphs). */
+int nr_render_graph_stats(const nr_render* render, uint32_t* captured, uint64_t* replays);
 /* Device time in milliseconds of the last nr_render_samples call (CUDA events
  * on the render stream). */
 int nr_render_last_ms(const nr_render* render, double* out_ms);

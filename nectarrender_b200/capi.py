@@ -44,7 +44,8 @@ class RenderConfig(C.Structure):
     _fields_ = [("ray_depth", C.c_uint32), ("seed", C.c_uint32), ("rr_enabled", C.c_int32),
                 ("rr_start_bounce", C.c_uint32), ("rr_survival", C.c_float), ("mode", C.c_int32),
                 ("schedule", C.c_int32), ("fp64_accumulate", C.c_int32), ("layer_mask", C.c_uint32),
-                ("extend_variant", C.c_int32), ("samples_per_wave", C.c_uint32)]
+                ("extend_variant", C.c_int32), ("samples_per_wave", C.c_uint32),
+                ("use_graphs", C.c_int32)]
 
 
 class StreamConfig(C.Structure):
@@ -89,6 +90,7 @@ EXPORTS = [
     "nr_scene_get_stats", "nr_scene_get_binary_bvh", "nr_render_config_default",
     "nr_render_create", "nr_render_destroy", "nr_render_reset", "nr_render_samples",
     "nr_render_samples_static", "nr_render_set_profiling", "nr_render_get_profile",
+    "nr_render_graph_stats",
     "nr_render_sample_layers", "nr_render_layer_device_ptr", "nr_render_read_layer",
     "nr_render_read_beauty_fp64", "nr_render_readback", "nr_render_display_float",
     "nr_render_dims", "nr_render_set_counters", "nr_render_get_counters", "nr_render_last_ms",
@@ -319,6 +321,12 @@ class Render:
         p = KernelProfile()
         _check(self.lib.nr_render_get_profile(self.h, C.byref(p)), "nr_render_get_profile")
         return {k: (p.ms[i], p.launches[i]) for i, k in enumerate(KERNEL_CLASSES)}
+
+    def graph_stats(self) -> tuple[int, int]:
+        """(wave graphs captured, graph replays) of this render so far."""
+        cap, rep = C.c_uint32(), C.c_uint64()
+        _check(self.lib.nr_render_graph_stats(self.h, C.byref(cap), C.byref(rep)), "graph_stats")
+        return cap.value, rep.value
 
     def last_ms(self) -> float:
         v = C.c_double()

@@ -944,6 +944,15 @@ struct nr_render {
   std::vector<cudaEvent_t> pev;  // profiling: one event per launch boundary
   std::vector<uint8_t> pkind;
   nr_kernel_profile prof{};
+  // captured waves: the wave's launches with everything but its first sample
+  // index baked in (that one is read from device memory)
+  struct WaveGraph {
+    WfParams key;
+    cudaGraphExec_t exec = nullptr;
+  };
+  std::vector<WaveGraph> graphs;
+  uint32_t graphs_captured = 0;
+  uint64_t graph_replays = 0;
   nr_trace_counters last{};
   double last_ms = 0.0;
   ~nr_render() {
@@ -959,6 +968,8 @@ struct nr_render {
     cudaFree(disp8);
     cudaFree(dispf);
     cudaFree(wb_scratch);
+    for (auto& g : graphs)
+      if (g.exec) cudaGraphExecDestroy(g.exec);
     for (auto e : pev) cudaEventDestroy(e);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
@@ -992,6 +1003,7 @@ int nr_render_config_default(nr_render_config* c) {
   c->layer_mask = (1u << NR_LAYER_BEAUTY) | (1u << NR_LAYER_DIFFUSE) | (1u << NR_LAYER_WORLD_NORMAL);
   c->extend_variant = 0;
   c->samples_per_wave = 0;
+  c->use_graphs = 1;
   return NR_OK;
 }
 
@@ -1136,6 +1148,51 @@ static uint32_t waves_of(nr_render* r) {
   return s;
 }
 
+// Launches one wave through a CUDA graph. A wave configuration (all launch
+// parameters except the first sample index) is launched directly the first
+// time it is seen, captured the second time and replayed from then on.
+static cudaError_t launch_wave_graph(nr_render* r, const WfParams& W) {
+  WfParams key;
+  memcpy(&key, &W, sizeof(key));
+  key.base = 0;
+  key.kp.first_sample = 0;
+  key.kp.n_samples = 0;
+  for (auto& g : r->graphs) {
+    if (memcmp(&g.key, &key, sizeof(key)) != 0) continue;
+    if (g.exec) {
+      r->graph_replays++;
+      return cudaGraphLaunch(g.exec, r->stream);
+    }
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(r->stream, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return e;
+    cudaError_t el = wf_launch_wave(W, false, r->stream, nullptr);
+    e = cudaStreamEndCapture(r->stream, &graph);
+    if (el != cudaSuccess || e != cudaSuccess) {
+      if (graph) cudaGraphDestroy(graph);
+      return el != cudaSuccess ? el : e;
+    }
+    e = cudaGraphInstantiate(&g.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+      g.exec = nullptr;
+      return e;
+    }
+    r->graphs_captured++;
+    r->graph_replays++;
+    return cudaGraphLaunch(g.exec, r->stream);
+  }
+  if (r->graphs.size() >= 8) {
+    if (r->graphs.front().exec) cudaGraphExecDestroy(r->graphs.front().exec);
+    r->graphs.erase(r->graphs.begin());
+  }
+  nr_render::WaveGraph g;
+  memset(&g.key, 0, sizeof(g.key));
+  g.key = key;
+  r->graphs.push_back(g);
+  return wf_launch_wave(W, false, r->stream, nullptr);
+}
+
 static int launch(nr_render* r, const KernelParams& P, WaveTimer* tm) {
   if (r->cfg.schedule != NR_SCHEDULE_WAVEFRONT) {
     CU(cudaMemsetAsync(r->work, 0, 4, r->stream), "clear work counter");
@@ -1149,13 +1206,18 @@ static int launch(nr_render* r, const KernelParams& P, WaveTimer* tm) {
     CU(wf_alloc(r->wf, r->samples_per_wave * N), "allocate wavefront state");
   }
   uint32_t per = P.write_raw ? 1u : r->samples_per_wave;
+  WfParams W = r->wf;
+  W.kp = P;
+  W.extend_variant = r->cfg.extend_variant > 0 ? r->cfg.extend_variant : 5;
+  CU(wf_set_base(W, P.first_sample, r->stream), "set wave base");
+  if (tm) tm->mark(NR_KERNEL_ROTATE, r->stream);
   for (uint32_t s = 0; s < P.n_samples; s += per) {
-    WfParams W = r->wf;
-    W.kp = P;
-    W.extend_variant = r->cfg.extend_variant > 0 ? r->cfg.extend_variant : 5;
     W.base = P.first_sample + s;
     W.count = std::min(per, P.n_samples - s);
-    CU(wf_launch_wave(W, r->counters_on, r->stream, tm), "launch wavefront");
+    if (!r->counters_on && !tm && r->cfg.use_graphs)
+      CU(launch_wave_graph(r, W), "launch wavefront graph");
+    else
+      CU(wf_launch_wave(W, r->counters_on, r->stream, tm), "launch wavefront");
   }
   return NR_OK;
 }
@@ -1252,6 +1314,7 @@ int nr_render_samples_static(nr_render* r, uint32_t first, uint32_t count) {
 
   if (r->counters_on) CU(cudaMemsetAsync(r->counters, 0, 8 * 5, r->stream), "clear counters");
   CU(cudaEventRecord(r->ev0, r->stream), "event");
+  CU(wf_set_base(W, first, r->stream), "set wave base");
   for (uint32_t s = 0; s < count; s += per) {
     WfParams w = W;
     w.kp = P;
@@ -1385,6 +1448,13 @@ int nr_render_set_profiling(nr_render* r, int32_t on) {
     for (auto& e : r->pev) CU(cudaEventCreate(&e), "event");
   }
   r->profile_on = on != 0;
+  return NR_OK;
+}
+
+int nr_render_graph_stats(const nr_render* r, uint32_t* captured, uint64_t* replays) {
+  if (!r) return fail(NR_ERR_INVALID, "null render");
+  if (captured) *captured = r->graphs_captured;
+  if (replays) *replays = r->graph_replays;
   return NR_OK;
 }
 

@@ -34,7 +34,13 @@ enum : uint32_t {
   CTR_N1 = 1,      // paths in queue 1
   CTR_WORK = 2,    // extend work counter
   CTR_ERR = 3,
+  CTR_BASE = 4,    // first sample index of the current wave
 };
+
+// The wave's first sample index is read from device memory, so that the
+// launches of a wave do not depend on it and one captured graph serves every
+// wave of the same size.
+__device__ __forceinline__ uint32_t wave_base(const WfParams& W) { return W.ctr[CTR_BASE]; }
 
 __device__ __forceinline__ float4 ld4(const float4* p) { return __ldg(p); }
 
@@ -281,10 +287,11 @@ __global__ void k_wf_generate(WfParams W) {
   const KernelParams& P = W.kp;
   const uint32_t N = P.W * P.H;
   uint32_t total = N * W.count;
+  const uint32_t base = wave_base(W);
   for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < total; p += gridDim.x * blockDim.x) {
     uint32_t k = p / N, pix = p - k * N;
     uint32_t x = pix % P.W, y = pix / P.W;
-    uint32_t sample = W.base + k;
+    uint32_t sample = base + k;
     Rng g;
     g.init(P.seed, pix + sample * (P.W * P.H));
     Ray r = camera_ray(P.cam, x, y, pix, sample, P.seed, g, P.rtl != 0);
@@ -355,6 +362,7 @@ __global__ void __launch_bounds__(kShadeThreads) k_wf_shade(WfParams W, int qsel
   uint32_t* next_n = &W.ctr[qsel == 0 ? CTR_N1 : CTR_N0];
   const uint32_t N = P.W * P.H;
   const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t wbase = wave_base(W);
   TraceStats st{0u, 0u, 0u};
   // grid-stride loop with whole warps in every iteration (for the warp-aggregated append)
   for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
@@ -373,7 +381,7 @@ __global__ void __launch_bounds__(kShadeThreads) k_wf_shade(WfParams W, int qsel
       s.bounce = bounce;
       uint32_t k = p / N, pix = p - k * N;
       Rng g;
-      g.init(P.seed, pix + (W.base + k) * (P.W * P.H), __float_as_uint(at.w));
+      g.init(P.seed, pix + (wbase + k) * (P.W * P.H), __float_as_uint(at.w));
       uint4 hv = W.hit[p];
       bool hit = hv.x != 0xffffffffu;
       Hit rec;
@@ -447,6 +455,7 @@ __global__ void k_wf_accumulate(WfParams W) {
   const KernelParams& P = W.kp;
   const uint32_t N = P.W * P.H;
   const size_t hw = N;
+  const uint32_t base = wave_base(W);
   for (uint32_t pix = blockIdx.x * blockDim.x + threadIdx.x; pix < N; pix += gridDim.x * blockDim.x) {
     if (P.write_raw) {
       float4 b = W.acc_b[pix], d = W.acc_d[pix], n = W.acc_n[pix];
@@ -461,7 +470,7 @@ __global__ void k_wf_accumulate(WfParams W) {
     V3 an = P.normal ? load3(P.normal, hw, pix) : V3{0, 0, 0};
     double s64[3] = {0, 0, 0};
     for (uint32_t k = 0; k < W.count; ++k) {
-      uint32_t p = k * N + pix, smp = W.base + k;
+      uint32_t p = k * N + pix, smp = base + k;
       float4 b = W.acc_b[p], d = W.acc_d[p], n = W.acc_n[p];
       ab = running_mean(ab, V3{b.x, b.y, b.z}, smp);
       ad = running_mean(ad, V3{d.x, d.y, d.z}, smp);
@@ -481,6 +490,15 @@ __global__ void k_wf_accumulate(WfParams W) {
   }
 }
 
+__global__ void k_wf_set_base(uint32_t* ctr, uint32_t base) {
+  if (threadIdx.x == 0) ctr[CTR_BASE] = base;
+}
+
+// Last launch of a wave: the next wave starts `count` sample indices later.
+__global__ void k_wf_advance(WfParams W) {
+  if (threadIdx.x == 0) W.ctr[CTR_BASE] += W.count;
+}
+
 // ---------------------------------------------------------------------------
 // host side
 
@@ -492,6 +510,11 @@ static int sm_count() {
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   }
   return sms;
+}
+
+cudaError_t wf_set_base(const WfParams& W, uint32_t first_sample, cudaStream_t st) {
+  k_wf_set_base<<<1, 32, 0, st>>>(W.ctr, first_sample);
+  return cudaGetLastError();
 }
 
 size_t wf_state_bytes(uint32_t n_paths) {
@@ -585,6 +608,8 @@ cudaError_t wf_launch_wave(const WfParams& W, bool counters, cudaStream_t st, Wa
   int acc_blocks = (int)std::min<uint32_t>((P.W * P.H + 255) / 256, (uint32_t)sm_count() * 16);
   k_wf_accumulate<<<acc_blocks, 256, 0, st>>>(W);
   if (tm) tm->mark(NR_KERNEL_ACCUMULATE, st);
+  k_wf_advance<<<1, 32, 0, st>>>(W);
+  if (tm) tm->mark(NR_KERNEL_ROTATE, st);
   return cudaGetLastError();
 }
 

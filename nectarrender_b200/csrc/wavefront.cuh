@@ -7,7 +7,9 @@ namespace nr {
 
 struct WfParams {
   KernelParams kp;
-  uint32_t base;   // first sample index of the wave
+  uint32_t base;   // first sample index of the wave (host side; the kernels
+                   // read it from ctr, set by wf_set_base and advanced by
+                   // each wave's last launch)
   uint32_t count;  // sample indices in the wave
   uint32_t capacity;
   int32_t extend_variant;  // 4, 5, 6 or 8 CTAs per SM
@@ -48,7 +50,11 @@ struct WaveTimer {
   }
 };
 
+// Launches one wave: generate, depth x (extend, shade, rotate), accumulate,
+// advance. The wave's first sample index must have been set on the stream by
+// wf_set_base (for the first wave of a run; each wave advances it).
 cudaError_t wf_launch_wave(const WfParams& W, bool counters, cudaStream_t st,
                            WaveTimer* timer = nullptr);
+cudaError_t wf_set_base(const WfParams& W, uint32_t first_sample, cudaStream_t st);
 
 }  // namespace nr

@@ -114,6 +114,23 @@ def test_tuning_knobs_do_not_change_samples(mesh_scene, refcuda, variant, mesh_l
     assert frac_close(n, rn2) >= 0.999
 
 
+def test_wave_graphs_replay_the_same_samples(mesh_scene):
+    """Waves replayed from captured CUDA graphs read their first sample index
+    from device memory; three calls in a row (direct, capture, replay) equal
+    direct launches."""
+    spec, sc, _ = mesh_scene
+    g = capi.Render(sc, samples_per_wave=1)
+    d = capi.Render(sc, samples_per_wave=1, use_graphs=0)
+    for first in (1, 2, 3):
+        g.samples(first, 1)
+        d.samples(first, 1)
+        for layer in (0, 1, 4):
+            np.testing.assert_array_equal(g.layer(layer), d.layer(layer))
+    captured, replays = g.graph_stats()
+    assert captured == 1 and replays == 2
+    assert d.graph_stats() == (0, 0)
+
+
 def test_participating_medium_samples(orc, refcuda):
     spec = scenes.mesh_stress(levels=3, res_h=48, res_w=48, spp=2, depth=32, n_spheres=8,
                               hdri_size=(128, 64), scene_seed=2)
