@@ -54,6 +54,9 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=12.0)
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--schedule", default="wavefront", choices=["wavefront", "megakernel"])
+    p.add_argument("--extend-variant", type=int, default=0,
+                   help="traversal kernel variant (0: library default; see autotune.py)")
+    p.add_argument("--mesh-leaf", type=int, default=1)
     return p.parse_args()
 
 
@@ -72,6 +75,7 @@ def config_json(args, h, w, spec, l2):
             "width": w, "height": h, "ray_depth": spec.ray_depth,
             "spp_per_step": args.spp_per_step,
             "integrator": f"reference-compatible, {args.schedule} schedule",
+            "extend_variant": args.extend_variant or "default", "mesh_leaf": args.mesh_leaf,
             "parallelism": f"sample-sharded x{args.gpus}", "l2": l2}
 
 
@@ -205,10 +209,11 @@ def run_ours(args):
     spec, h, w = workload(args)
     lib = library()
     t_build = time.perf_counter()
-    scene = capi.Scene(spec)
+    scene = capi.Scene(spec, mesh_leaf=args.mesh_leaf)
     build_wall = time.perf_counter() - t_build
     stats = scene.stats()
-    render = capi.Render(scene, schedule=1 if args.schedule == "wavefront" else 0)
+    render = capi.Render(scene, schedule=1 if args.schedule == "wavefront" else 0,
+                         extend_variant=args.extend_variant)
     stream_handle = ctypes.c_uint64()
     lib.nr_render_stream(render.h, ctypes.byref(stream_handle))
     stream = torch.cuda.ExternalStream(stream_handle.value)

@@ -166,8 +166,11 @@ typedef struct nr_render_config {
   int32_t schedule;         /* NR_SCHEDULE_*                                */
   int32_t fp64_accumulate;  /* also keep an FP64 sum of the beauty layer    */
   uint32_t layer_mask;      /* bit i enables LayerType i (default 0x13)      */
-  int32_t extend_variant;   /* wavefront traversal: CTAs per SM the register
-                               budget targets (4, 5, 6 or 8; 0 = default)   */
+  int32_t extend_variant;   /* wavefront traversal kernel: 4, 5, 6, 8 = nested
+                               two-level traversal with that many CTAs per
+                               SM; 14..18 = flattened traversal with lane
+                               refill; 100*a + b = a for bounce 0, b after;
+                               0 = default (514)                            */
   uint32_t samples_per_wave;/* wavefront: sample indices per wave (0 = ~8M paths) */
   int32_t use_graphs;       /* wavefront: replay each wave as a CUDA graph (1) */
 } nr_render_config;

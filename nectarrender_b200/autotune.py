@@ -5,8 +5,11 @@ speed but never the image:
 
   * ``mesh_leaf`` / ``tlas_leaf`` - primitives per 8-wide BVH leaf (1..3) of
     the mesh trees and of the top-level tree;
-  * ``extend_variant`` - CTAs per SM the traversal kernel's register budget
-    targets (4, 5, 6 or 8: 128, 96, 80 or 64 registers per thread);
+  * ``extend_variant`` - traversal kernel and the CTAs per SM its register
+    budget targets: 4, 5, 6, 8 (nested two-level traversal; 128, 96, 80 or
+    64 registers per thread) and 14, 15, 16, 18 (flattened traversal with lane
+    refill, same budgets); 100 * a + b runs a for the camera rays of bounce
+    0 and b for the later bounces;
   * ``samples_per_wave`` - sample indices in flight per wave, i.e. the length
     of the path queues (paths = W*H*samples_per_wave);
   * ``schedule`` - wavefront or the per-pixel megakernel.
@@ -25,14 +28,14 @@ from pathlib import Path
 from . import capi
 from .scenes import SceneSpec
 
-VARIANTS = (4, 5, 6, 8)
+VARIANTS = (5, 14, 514, 515, 414, 614)
 
 
 @dataclass
 class Tuning:
     mesh_leaf: int = 1
     tlas_leaf: int = 1
-    extend_variant: int = 5
+    extend_variant: int = 514
     samples_per_wave: int = 0
     schedule: int = capi.SCHEDULE_WAVEFRONT
     ms_per_sample: float = 0.0

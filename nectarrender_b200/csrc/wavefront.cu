@@ -352,6 +352,290 @@ __global__ void __launch_bounds__(kExtThreads, kMinBlocks) k_wf_extend(WfParams 
   }
 }
 
+// ---------------------------------------------------------------------------
+// Flattened two-level traversal with lane refill.
+//
+// One loop iteration does one unit of work per lane: a primitive of the
+// current leaf group, a wide node, a stack pop, a switch between the top-level
+// tree and a mesh tree, or the end of a ray. Lanes whose ray has ended take
+// new rays from the queue whenever at least kRefill lanes of the warp are idle,
+// so a warp no longer waits for its slowest ray. The order in which nodes and
+// primitives are visited per ray is the one of trace_closest, so the closest
+// hit (ties included) is the same.
+constexpr uint32_t kRefill = 12;
+
+__device__ __forceinline__ uint32_t octant_inv4(const V3& d) {
+  uint32_t oct = (d.x < 0.0f ? 4u : 0u) | (d.y < 0.0f ? 2u : 0u) | (d.z < 0.0f ? 1u : 0u);
+  return (7u - oct) * 0x01010101u;
+}
+
+// Per-thread state the flat loop touches only when a ray starts, enters or
+// leaves a mesh, or records a hit lives in shared memory (one word per field
+// per thread, field-major), which keeps the loop within 96 registers.
+enum : uint32_t {
+  FS_WO = 0,        // world origin x, y, z
+  FS_WD = 3,        // world direction x, y, z
+  FS_WTM = 6,       // ray time
+  FS_SLACK = 7,     // world-t slack of the instance prune
+  FS_OUT_OBJ = 8,   // closest object so far
+  FS_OUT_SLOT = 9,  // its triangle slot (meshes)
+  FS_OUT_T = 10,    // its object-space t
+  FS_OUT_U = 11,
+  FS_OUT_V = 12,
+  FS_TL_NG = 13,    // saved top-level node group (2 words)
+  FS_TL_TG = 15,    // saved top-level leaf group (2 words)
+  FS_TL_SP = 17,    // saved top-level stack depth
+  FS_TL_TMAX = 18,  // saved top-level t bound
+  FS_MESH_OI = 19,  // mesh instance being traversed
+  FS_PATH = 20,     // path index of the ray
+  FS_COUNT = 21
+};
+constexpr size_t kExtStackBytes = sizeof(uint2) * (kTlasStack + kBlasStack) * kExtThreads;
+constexpr size_t kFlatSmemBytes = kExtStackBytes + sizeof(uint32_t) * FS_COUNT * kExtThreads;
+
+template <bool kCount, int kMinBlocks>
+__global__ void __launch_bounds__(kExtThreads, kMinBlocks) k_wf_extend_flat(WfParams W, int qsel,
+                                                                            int identity) {
+  extern __shared__ uint2 wf_smem[];
+  const KernelParams& P = W.kp;
+  const DevScene& sc = P.scene;
+  const uint32_t n = W.ctr[qsel];
+  const uint32_t* queue = qsel == 0 ? W.queue0 : W.queue1;
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t lt_mask = (1u << lane) - 1u;
+  uint2* const tstk = wf_smem + threadIdx.x;
+  uint2* const bstk = wf_smem + kTlasStack * kExtThreads + threadIdx.x;
+  uint32_t* const cold = reinterpret_cast<uint32_t*>(wf_smem + (kTlasStack + kBlasStack) * kExtThreads) +
+                         threadIdx.x;
+  auto cf = [&](uint32_t f) -> float& { return reinterpret_cast<float*>(cold)[f * kExtThreads]; };
+  auto cu = [&](uint32_t f) -> uint32_t& { return cold[f * kExtThreads]; };
+  uint32_t rays = 0, nodes = 0, tris = 0, objs = 0;
+
+  bool active = false, exhausted = false, in_mesh = false;
+  uint32_t steps = 0, oct4 = 0, cur_n = 0;
+  V3 o{0, 0, 0}, d{0, 0, 1}, inv{0, 0, 1};
+  float tmax = FMAX, best = FMAX, bu = 0.f, bv = 0.f;
+  uint2 ng = make_uint2(0u, 0u), tg = make_uint2(0u, 0u);
+  int sp = 0, best_slot = -1;
+  const Bvh8Node* cur_nodes = sc.tlas8;
+  const TriRecord* cur_tris = nullptr;
+
+  while (true) {
+    if (!exhausted) {
+      const uint32_t idle = __ballot_sync(0xffffffffu, !active);
+      const uint32_t nidle = __popc(idle);
+      if (nidle >= kRefill || nidle == 32u) {
+        const uint32_t leader = __ffs(idle) - 1u;
+        uint32_t base = 0;
+        if (lane == leader) base = atomicAdd(&W.ctr[CTR_WORK], nidle);
+        base = __shfl_sync(0xffffffffu, base, leader);
+        if (base + nidle >= n) exhausted = true;
+        if (!active) {
+          const uint32_t i = base + __popc(idle & lt_mask);
+          if (i < n) {
+            const uint32_t p = identity ? i : __ldg(queue + i);
+            const float4 ro = ld4(W.ray_o + p), rd = ld4(W.ray_d + p);
+            o = V3{ro.x, ro.y, ro.z};
+            d = V3{rd.x, rd.y, rd.z};
+            inv = V3{1.0f / d.x, 1.0f / d.y, 1.0f / d.z};
+            oct4 = octant_inv4(d);
+            cf(FS_WO) = o.x;
+            cf(FS_WO + 1) = o.y;
+            cf(FS_WO + 2) = o.z;
+            cf(FS_WD) = d.x;
+            cf(FS_WD + 1) = d.y;
+            cf(FS_WD + 2) = d.z;
+            cf(FS_WTM) = ro.w;
+            cf(FS_SLACK) = (2.0f * EPS + 1e-4f * (fabsf(o.x) + fabsf(o.y) + fabsf(o.z) + 1.0f)) /
+                           length(d);
+            cu(FS_OUT_OBJ) = 0xffffffffu;
+            cu(FS_OUT_SLOT) = 0xffffffffu;
+            cf(FS_OUT_T) = 0.f;
+            cf(FS_OUT_U) = 0.f;
+            cf(FS_OUT_V) = 0.f;
+            cu(FS_PATH) = p;
+            best = FMAX;
+            tmax = FMAX;
+            ng = make_uint2(0u, sc.n_tlas8 ? 0x80000000u : 0u);
+            tg = make_uint2(0u, 0u);
+            sp = 0;
+            in_mesh = false;
+            cur_nodes = sc.tlas8;
+            cur_n = sc.n_tlas8;
+            steps = 0;
+            active = true;
+            rays++;
+          }
+        }
+      }
+    }
+    if (__ballot_sync(0xffffffffu, active) == 0u) break;
+    if (!active) continue;
+
+    if (++steps > kMaxTraversalSteps) {
+      atomicOr(P.err, 8u);
+      tg.y = 0u;
+      ng.y = 0u;
+      sp = 0;
+      in_mesh = false;
+    }
+    if (tg.y != 0u) {
+      // one primitive of the current leaf group
+      const uint32_t b = __ffs(tg.y) - 1u;
+      tg.y &= tg.y - 1u;
+      const uint32_t slot = tg.x + b;
+      if (in_mesh) {
+        const TriRecord* tr = cur_tris + slot;
+        const float4 p0 = ld4(&tr->v0), p1 = ld4(&tr->e1), p2 = ld4(&tr->e2);
+        if (kCount) tris++;
+        if (__float_as_uint(p1.w) == 0u) {  // zero-extent box: never hit in the reference
+          Ray r;
+          r.o = o;
+          r.d = d;
+          r.inv = inv;
+          r.tm = 0.f;
+          float t, u, v;
+          if (tri_hit(r, V3{p0.x, p0.y, p0.z}, V3{p1.x, p1.y, p1.z}, V3{p2.x, p2.y, p2.z}, EPS,
+                      tmax, t, u, v)) {
+            tmax = t;
+            bu = u;
+            bv = v;
+            best_slot = (int)slot;
+          }
+        }
+      } else {
+        const uint32_t oi = __ldg(sc.tlas_prims8 + slot);
+        const DevObject& ob = sc.objects[oi];
+        if (kCount) objs++;
+        const Ray wr = make_ray(o, d, cf(FS_WTM));  // at the top level the ray is the world ray
+        if (ob.type == 4) {
+          const DevMesh& m = sc.meshes[ob.mesh];
+          if (m.n_bvh8 > 0) {
+            // enter the mesh tree in object space
+            cu(FS_TL_NG) = ng.x;
+            cu(FS_TL_NG + 1) = ng.y;
+            cu(FS_TL_TG) = tg.x;
+            cu(FS_TL_TG + 1) = tg.y;
+            cu(FS_TL_SP) = (uint32_t)sp;
+            cf(FS_TL_TMAX) = tmax;
+            cu(FS_MESH_OI) = oi;
+            const Ray r = to_object(ob, wr);
+            o = r.o;
+            d = r.d;
+            inv = r.inv;
+            oct4 = octant_inv4(d);
+            tmax = fminf(FMAX, best * 1.0011f + cf(FS_SLACK));
+            ng = make_uint2(0u, 0x80000000u);
+            tg = make_uint2(0u, 0u);
+            sp = 0;
+            in_mesh = true;
+            best_slot = -1;
+            cur_nodes = m.bvh8;
+            cur_n = m.n_bvh8;
+            cur_tris = m.tris8;
+          }
+        } else {
+          const Ray r = to_object(ob, wr);
+          Hit h;
+          auto mesh_fn = [&](const DevObject& mo, const Ray& rr, float t0, float t1, Hit& hh) {
+            return mesh_hit8(sc, mo, rr, t0, t1, hh, bstk, kExtThreads, P.err);
+          };
+          if (object_hit_local_t(sc.cube_faces, ob, r, EPS, FMAX, h, mesh_fn)) {
+            const float tw = world_t(h.p, h.n, ob, r, wr);
+            if (EPS < tw && tw < best) {
+              best = tw;
+              tmax = best;
+              cu(FS_OUT_OBJ) = oi;
+              cu(FS_OUT_SLOT) = 0xffffffffu;
+              cf(FS_OUT_T) = h.t;
+            }
+          }
+        }
+      }
+    } else if (ng.y > 0x00ffffffu) {
+      // one wide node
+      const uint32_t hits = ng.y;
+      const uint32_t child_bit = 31u - __clz(hits);
+      ng.y &= ~(1u << child_bit);
+      const uint32_t cslot = (child_bit - 24u) ^ (oct4 & 7u);
+      const uint32_t node_index = ng.x + __popc((hits & 0xffu) & ~(0xffffffffu << cslot));
+      if (node_index >= cur_n) {
+        atomicOr(P.err, 8u);
+        ng.y = 0u;
+        sp = 0;
+      } else {
+        if (ng.y > 0x00ffffffu) {
+          const int depth = in_mesh ? kBlasStack : kTlasStack;
+          uint2* stk = in_mesh ? bstk : tstk;
+          if (sp < depth) stk[(sp++) * kExtThreads] = ng;
+          else atomicOr(P.err, 1u);
+        }
+        float4 n0;
+        uint4 n1;
+        const uint32_t hm = bvh8_intersect(cur_nodes + node_index, o, inv, oct4, EPS, tmax, n0, n1);
+        if (kCount) nodes++;
+        ng = make_uint2(n1.x, (hm & 0xff000000u) | (__float_as_uint(n0.w) >> 24));
+        tg = make_uint2(n1.y, hm & 0x00ffffffu);
+      }
+    } else if (sp > 0) {
+      uint2* stk = in_mesh ? bstk : tstk;
+      ng = stk[(--sp) * kExtThreads];
+    } else if (in_mesh) {
+      // leave the mesh tree: the candidate competes in world space
+      const V3 wo{cf(FS_WO), cf(FS_WO + 1), cf(FS_WO + 2)};
+      const V3 wd{cf(FS_WD), cf(FS_WD + 1), cf(FS_WD + 2)};
+      float tl_tmax = cf(FS_TL_TMAX);
+      if (best_slot >= 0) {
+        const uint32_t oi = cu(FS_MESH_OI);
+        const DevObject& ob = sc.objects[oi];
+        const DevMesh& m = sc.meshes[ob.mesh];
+        const uint32_t tri = __float_as_uint(__ldg(&m.tris8[best_slot].v0.w));
+        Ray r;
+        r.o = o;
+        r.d = d;
+        r.inv = inv;
+        r.tm = 0.f;
+        const Ray wr = make_ray(wo, wd, 0.f);
+        const float tw = world_t(ray_at(r, tmax), mesh_normal(m, tri, bu, bv), ob, r, wr);
+        if (EPS < tw && tw < best) {
+          best = tw;
+          tl_tmax = best;
+          cu(FS_OUT_OBJ) = oi;
+          cu(FS_OUT_SLOT) = (uint32_t)best_slot;
+          cf(FS_OUT_T) = tmax;
+          cf(FS_OUT_U) = bu;
+          cf(FS_OUT_V) = bv;
+        }
+      }
+      ng = make_uint2(cu(FS_TL_NG), cu(FS_TL_NG + 1));
+      tg = make_uint2(cu(FS_TL_TG), cu(FS_TL_TG + 1));
+      sp = (int)cu(FS_TL_SP);
+      tmax = tl_tmax;
+      o = wo;
+      d = wd;
+      inv = V3{1.0f / d.x, 1.0f / d.y, 1.0f / d.z};
+      oct4 = octant_inv4(d);
+      in_mesh = false;
+      cur_nodes = sc.tlas8;
+      cur_n = sc.n_tlas8;
+    } else {
+      const uint32_t p = cu(FS_PATH);
+      W.hit[p] = make_uint4(cu(FS_OUT_OBJ), cu(FS_OUT_SLOT), cu(FS_OUT_U), cu(FS_OUT_V));
+      W.hit_t[p] = cf(FS_OUT_T);
+      active = false;
+    }
+  }
+  if (kCount) {
+    unsigned long long vals[4] = {rays, nodes, tris, objs};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      unsigned long long a = vals[k];
+      for (int off = 16; off > 0; off >>= 1) a += __shfl_down_sync(0xffffffffu, a, off);
+      if (lane == 0) atomicAdd(P.counters + k, a);
+    }
+  }
+}
+
 __global__ void __launch_bounds__(kShadeThreads) k_wf_shade(WfParams W, int qsel, int identity) {
   __shared__ uint2 shade_stk[kBlasStack * kShadeThreads];
   const KernelParams& P = W.kp;
@@ -557,22 +841,32 @@ void wf_free(WfParams& W) {
 }
 
 using ExtendFn = void (*)(WfParams, int, int);
+// Variants: 4, 5, 6, 8 = nested traversal with that many CTAs per SM;
+// 14, 15, 16, 18 = flattened traversal with lane refill, 4..8 CTAs per SM.
 static ExtendFn extend_fn(bool counters, int variant) {
   switch (variant) {
     case 5: return counters ? k_wf_extend<true, 5> : k_wf_extend<false, 5>;
     case 6: return counters ? k_wf_extend<true, 6> : k_wf_extend<false, 6>;
     case 8: return counters ? k_wf_extend<true, 8> : k_wf_extend<false, 8>;
+    case 14: return counters ? k_wf_extend_flat<true, 4> : k_wf_extend_flat<false, 4>;
+    case 15: return counters ? k_wf_extend_flat<true, 5> : k_wf_extend_flat<false, 5>;
+    case 16: return counters ? k_wf_extend_flat<true, 6> : k_wf_extend_flat<false, 6>;
+    case 18: return counters ? k_wf_extend_flat<true, 8> : k_wf_extend_flat<false, 8>;
     default: return counters ? k_wf_extend<true, 4> : k_wf_extend<false, 4>;
   }
 }
 
-static int extend_blocks(ExtendFn fn) {
-  static ExtendFn cached_fn[16] = {nullptr};
-  static int cached_blocks[16] = {0};
-  for (int i = 0; i < 16; ++i) {
+static bool extend_is_flat(int variant) { return variant >= 14; }
+static size_t extend_smem(int variant) {
+  return extend_is_flat(variant) ? kFlatSmemBytes : kExtStackBytes;
+}
+
+static int extend_blocks(ExtendFn fn, size_t smem) {
+  static ExtendFn cached_fn[32] = {nullptr};
+  static int cached_blocks[32] = {0};
+  for (int i = 0; i < 32; ++i) {
     if (cached_fn[i] == fn) return cached_blocks[i];
     if (!cached_fn[i]) {
-      size_t smem = sizeof(uint2) * (kTlasStack + kBlasStack) * kExtThreads;
       int per_sm = 0;
       cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kExtThreads, smem);
@@ -591,14 +885,20 @@ cudaError_t wf_launch_wave(const WfParams& W, bool counters, cudaStream_t st, Wa
   int gen_blocks = (int)std::min<uint32_t>((total + 255) / 256, (uint32_t)sm_count() * 16);
   k_wf_generate<<<gen_blocks, 256, 0, st>>>(W);
   if (tm) tm->mark(NR_KERNEL_GENERATE, st);
-  size_t smem = sizeof(uint2) * (kTlasStack + kBlasStack) * kExtThreads;
-  ExtendFn ext = extend_fn(counters, W.extend_variant);
-  int eb = extend_blocks(ext);
+  // extend_variant v, or 100 * v0 + v: variant v0 for the camera rays of
+  // bounce 0 and v for the later bounces
+  const int v_rest = W.extend_variant % 100;
+  const int v_first = W.extend_variant >= 100 ? W.extend_variant / 100 : v_rest;
+  ExtendFn ext = extend_fn(counters, v_rest);
+  ExtendFn ext0 = extend_fn(counters, v_first);
+  const size_t smem = extend_smem(v_rest), smem0 = extend_smem(v_first);
+  int eb = extend_blocks(ext, smem), eb0 = extend_blocks(ext0, smem0);
   int shade_blocks = (int)std::min<uint32_t>((total + kShadeThreads - 1) / kShadeThreads,
                                              (uint32_t)sm_count() * 16);
   for (uint32_t b = 0; b < P.depth; ++b) {
     int q = (int)(b & 1u);
-    ext<<<eb, kExtThreads, smem, st>>>(W, q, b == 0 ? 1 : 0);
+    if (b == 0) ext0<<<eb0, kExtThreads, smem0, st>>>(W, q, 1);
+    else ext<<<eb, kExtThreads, smem, st>>>(W, q, 0);
     if (tm) tm->mark(NR_KERNEL_EXTEND, st);
     k_wf_shade<<<shade_blocks, kShadeThreads, 0, st>>>(W, q, b == 0 ? 1 : 0);
     if (tm) tm->mark(NR_KERNEL_SHADE, st);

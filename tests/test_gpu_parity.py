@@ -96,6 +96,10 @@ def test_mesh_hdri_samples(mesh_scene, orc, refcuda, s):
     (6, 1, 2, 1, capi.SCHEDULE_WAVEFRONT),
     (8, 2, 3, 3, capi.SCHEDULE_WAVEFRONT),
     (5, 1, 1, 0, capi.SCHEDULE_MEGAKERNEL),
+    (14, 1, 1, 0, capi.SCHEDULE_WAVEFRONT),
+    (15, 3, 2, 2, capi.SCHEDULE_WAVEFRONT),
+    (16, 2, 1, 0, capi.SCHEDULE_WAVEFRONT),
+    (515, 1, 1, 0, capi.SCHEDULE_WAVEFRONT),
 ])
 def test_tuning_knobs_do_not_change_samples(mesh_scene, refcuda, variant, mesh_leaf, tlas_leaf,
                                             spw, schedule):
