@@ -78,6 +78,9 @@ class TraceCounters(C.Structure):
 # nr_render_config.schedule
 SCHEDULE_MEGAKERNEL = 0
 SCHEDULE_WAVEFRONT = 1
+# nr_render_config.mode
+MODE_REFERENCE = 0
+MODE_PERF = 1
 
 EXPORTS = [
     "nr_abi_version", "nr_last_error", "nr_device_count", "nr_device_draw_order",

@@ -374,6 +374,9 @@ struct nr_scene {
   DevObject* d_objects = nullptr;
   DevMesh* d_mesh_table = nullptr;
   float* d_hdri = nullptr;
+  float* d_alias_prob = nullptr;    // HDRI importance sampling (perf mode)
+  uint32_t* d_alias_idx = nullptr;
+  float* d_texel_pdf = nullptr;
   CubeFace* d_cube_faces = nullptr;
   BuildResult tlas;
   DevScene dev{};
@@ -391,12 +394,18 @@ struct nr_scene {
     cudaFree(d_objects);
     cudaFree(d_mesh_table);
     cudaFree(d_hdri);
+    cudaFree(d_alias_prob);
+    cudaFree(d_alias_idx);
+    cudaFree(d_texel_pdf);
     cudaFree(d_cube_faces);
     d_cube_faces = nullptr;
     d_materials = nullptr;
     d_objects = nullptr;
     d_mesh_table = nullptr;
     d_hdri = nullptr;
+    d_alias_prob = nullptr;
+    d_alias_idx = nullptr;
+    d_texel_pdf = nullptr;
     free_build(tlas);
     built = false;
   }
@@ -670,6 +679,65 @@ int nr_scene_set_hdri_params(nr_scene* s, float rotation, float intensity) {
   return NR_OK;
 }
 
+// Sampling table of an equirectangular HDRI for NR_MODE_PERF: texel weight =
+// the largest luminance in the texel's 3x3 neighbourhood (the bilinear lookup
+// spreads a bright texel into its neighbours, so their density must not be
+// small) x sin(theta) (the solid angle of the texel row); a Walker alias
+// table built with Vose's method (IEEE TSE 17(9), 1991) and the normalised
+// texel probabilities. Returns false when the image carries no energy.
+static bool build_sky_alias(const HostImageF& im, std::vector<float>& prob,
+                            std::vector<uint32_t>& alias, std::vector<float>& texel_pdf) {
+  const size_t W = im.W, H = im.H, n = W * H, hw = n;
+  std::vector<double> lum(n), w(n);
+  for (size_t i = 0; i < n; ++i)
+    lum[i] = std::max(0.0, 0.2126 * im.chw[i] + 0.7152 * im.chw[hw + i] + 0.0722 * im.chw[2 * hw + i]);
+  double sum = 0.0;
+  for (size_t y = 0; y < H; ++y) {
+    const double st = std::sin(M_PI * ((double)y + 0.5) / (double)H);
+    for (size_t x = 0; x < W; ++x) {
+      double m = 0.0;
+      for (int dy = -1; dy <= 1; ++dy) {
+        const size_t yy = (size_t)std::min<long>((long)H - 1, std::max<long>(0, (long)y + dy));
+        for (int dx = -1; dx <= 1; ++dx) {
+          const size_t xx = (x + W + dx) % W;
+          m = std::max(m, lum[yy * W + xx]);
+        }
+      }
+      const size_t i = y * W + x;
+      w[i] = m * st;
+      sum += w[i];
+    }
+  }
+  if (!(sum > 0.0)) return false;
+  prob.assign(n, 1.0f);
+  alias.resize(n);
+  texel_pdf.resize(n);
+  std::vector<double> q(n);
+  std::vector<uint32_t> small, large;
+  small.reserve(n);
+  large.reserve(n);
+  for (size_t i = 0; i < n; ++i) {
+    texel_pdf[i] = (float)(w[i] / sum);
+    q[i] = w[i] * (double)n / sum;
+    alias[i] = (uint32_t)i;
+    (q[i] < 1.0 ? small : large).push_back((uint32_t)i);
+  }
+  while (!small.empty() && !large.empty()) {
+    const uint32_t l = small.back(), g = large.back();
+    small.pop_back();
+    prob[l] = (float)q[l];
+    alias[l] = g;
+    q[g] = (q[g] + q[l]) - 1.0;
+    if (q[g] < 1.0) {
+      large.pop_back();
+      small.push_back(g);
+    }
+  }
+  for (uint32_t i : large) prob[i] = 1.0f;
+  for (uint32_t i : small) prob[i] = 1.0f;  // round-off leftovers
+  return true;
+}
+
 int nr_scene_set_tuning(nr_scene* s, uint32_t mesh_leaf_max, uint32_t tlas_leaf_max) {
   if (!s || mesh_leaf_max < 1 || mesh_leaf_max > 3 || tlas_leaf_max < 1 || tlas_leaf_max > 3)
     return fail(NR_ERR_INVALID, "nr_scene_set_tuning: leaf sizes must be 1..3");
@@ -831,6 +899,17 @@ int nr_scene_build(nr_scene* s) {
     sky.H = (int)s->hdri.H;
     sky.W = (int)s->hdri.W;
     dev_bytes += s->hdri.chw.size() * 4;
+    std::vector<float> prob, tpdf;
+    std::vector<uint32_t> alias;
+    if (build_sky_alias(s->hdri, prob, alias, tpdf)) {
+      CU(upload(s->d_alias_prob, prob.data(), prob.size(), st), "upload sky table");
+      CU(upload(s->d_alias_idx, alias.data(), alias.size(), st), "upload sky table");
+      CU(upload(s->d_texel_pdf, tpdf.data(), tpdf.size(), st), "upload sky table");
+      sky.alias_prob = s->d_alias_prob;
+      sky.alias_idx = s->d_alias_idx;
+      sky.texel_pdf = s->d_texel_pdf;
+      dev_bytes += prob.size() * 12;
+    }
   }
 
   DevScene& ds = s->dev;
@@ -1200,7 +1279,8 @@ static cudaError_t launch_wave_graph(nr_render* r, const WfParams& W) {
 }
 
 static int launch(nr_render* r, const KernelParams& P, WaveTimer* tm) {
-  if (r->cfg.schedule != NR_SCHEDULE_WAVEFRONT) {
+  // NR_MODE_PERF runs on the wavefront schedule only
+  if (r->cfg.schedule != NR_SCHEDULE_WAVEFRONT && r->cfg.mode != NR_MODE_PERF) {
     CU(cudaMemsetAsync(r->work, 0, 4, r->stream), "clear work counter");
     CU(launch_megakernel(P, r->counters_on, r->stream), "launch integrator");
     if (tm) tm->mark(NR_KERNEL_MEGAKERNEL, r->stream);
@@ -1209,7 +1289,8 @@ static int launch(nr_render* r, const KernelParams& P, WaveTimer* tm) {
   uint32_t N = r->W * r->H;
   if (!r->wf.capacity) {
     r->samples_per_wave = waves_of(r);
-    CU(wf_alloc(r->wf, r->samples_per_wave * N), "allocate wavefront state");
+    CU(wf_alloc(r->wf, r->samples_per_wave * N, r->cfg.mode == NR_MODE_PERF),
+       "allocate wavefront state");
   }
   uint32_t per = P.write_raw ? 1u : r->samples_per_wave;
   WfParams W = r->wf;
@@ -1298,6 +1379,8 @@ int nr_render_samples_static(nr_render* r, uint32_t first, uint32_t count) {
   if ((uint64_t)first + count > r->cam.samples_per_pixel)
     return fail(NR_ERR_INVALID, "sample index beyond samples_per_pixel");
   const uint32_t N = r->W * r->H;
+  if (r->cfg.mode != NR_MODE_REFERENCE)
+    return fail(NR_ERR_STATE, "nr_render_samples_static renders NR_MODE_REFERENCE only");
   if ((uint64_t)r->W * r->H > NR_STATIC_WAVE_PATHS)
     return fail(NR_ERR_LIMIT, "nr_render_samples_static: " + std::to_string(r->W) + "x" +
                                   std::to_string(r->H) + " = " + std::to_string(N) +

@@ -35,6 +35,8 @@ enum : uint32_t {
   CTR_WORK = 2,    // extend work counter
   CTR_ERR = 3,
   CTR_BASE = 4,    // first sample index of the current wave
+  CTR_SH = 5,      // shadow rays queued by this bounce's shade (perf mode)
+  CTR_SHWORK = 6,  // shadow kernel work counter
 };
 
 // The wave's first sample index is read from device memory, so that the
@@ -172,8 +174,9 @@ template <bool kCount>
 __device__ __forceinline__ void trace_closest(const DevScene& sc, const Ray& wr, uint2* tlas_stk,
                                               uint2* blas_stk, uint32_t stride, uint32_t& out_obj,
                                               uint32_t& out_slot, float& out_t, float& out_u,
-                                              float& out_v, TraceStats& st, uint32_t* err) {
-  float best = FMAX;
+                                              float& out_v, TraceStats& st, uint32_t* err,
+                                              float best0 = FMAX) {
+  float best = best0;
   out_obj = 0xffffffffu;
   out_slot = 0xffffffffu;
   out_t = 0.0f;
@@ -239,7 +242,7 @@ __device__ __forceinline__ void trace_closest(const DevScene& sc, const Ray& wr,
       }
     }
   };
-  float tlas_tmax = FMAX;
+  float tlas_tmax = best0;
   cwbvh_trace(sc.tlas8, sc.n_tlas8, wr.o, wr.d, wr.inv, EPS, tlas_tmax, tlas_stk, stride, kTlasStack,
               object_leaf, nodes, err);
   if (kCount) st.nodes += nodes;
@@ -301,11 +304,14 @@ __global__ void k_wf_generate(WfParams W) {
     W.acc_b[p] = make_float4(0.f, 0.f, 0.f, __uint_as_float(0xffffffffu));
     W.acc_d[p] = make_float4(0.f, 0.f, 0.f, 0.f);
     W.acc_n[p] = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (W.mis_pdf) W.mis_pdf[p] = 0.0f;  // camera rays: emission is not MIS-weighted
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     W.ctr[CTR_N0] = total;
     W.ctr[CTR_N1] = 0u;
     W.ctr[CTR_WORK] = 0u;
+    W.ctr[CTR_SH] = 0u;
+    W.ctr[CTR_SHWORK] = 0u;
   }
 }
 
@@ -636,6 +642,9 @@ __global__ void __launch_bounds__(kExtThreads, kMinBlocks) k_wf_extend_flat(WfPa
   }
 }
 
+// kPerf: NR_MODE_PERF (next-event estimation + MIS); otherwise the
+// reference's estimator draw for draw.
+template <bool kPerf>
 __global__ void __launch_bounds__(kShadeThreads) k_wf_shade(WfParams W, int qsel, int identity) {
   __shared__ uint2 shade_stk[kBlasStack * kShadeThreads];
   const KernelParams& P = W.kp;
@@ -647,11 +656,18 @@ __global__ void __launch_bounds__(kShadeThreads) k_wf_shade(WfParams W, int qsel
   const uint32_t N = P.W * P.H;
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t wbase = wave_base(W);
+  uint2* const my_stk = shade_stk + threadIdx.x;
+  auto mesh_fn = [&](const DevObject& mo, const Ray& rr, float t0, float t1, Hit& hh) {
+    return mesh_hit8(sc, mo, rr, t0, t1, hh, my_stk, kShadeThreads, P.err);
+  };
+  const bool nee_light = kPerf && light_nee_ready(sc);
+  const bool nee_sky = kPerf && sky_nee_ready(sc.sky);
+  const float sel = (nee_light && nee_sky) ? 0.5f : 1.0f;
   TraceStats st{0u, 0u, 0u};
   // grid-stride loop with whole warps in every iteration (for the warp-aggregated append)
   for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
     uint32_t i = base + threadIdx.x;
-    bool alive = false;
+    bool alive = false, shadow = false;
     uint32_t p = 0;
     if (i < n) {
       p = identity ? i : __ldg(queue + i);
@@ -663,6 +679,7 @@ __global__ void __launch_bounds__(kShadeThreads) k_wf_shade(WfParams W, int qsel
       s.beauty = V3{ab.x, ab.y, ab.z};
       s.primary = __float_as_uint(ab.w);
       s.bounce = bounce;
+      const float pdf_prev = kPerf ? W.mis_pdf[p] : 0.0f;
       uint32_t k = p / N, pix = p - k * N;
       Rng g;
       g.init(P.seed, pix + (wbase + k) * (P.W * P.H), __float_as_uint(at.w));
@@ -670,25 +687,75 @@ __global__ void __launch_bounds__(kShadeThreads) k_wf_shade(WfParams W, int qsel
       bool hit = hv.x != 0xffffffffu;
       Hit rec;
       if (hit) rebuild_hit(sc, hv.x, hv.y, W.hit_t[p], __uint_as_float(hv.z), __uint_as_float(hv.w),
-                           s.ray, rec, shade_stk + threadIdx.x, kShadeThreads, P.err);
+                           s.ray, rec, my_stk, kShadeThreads, P.err);
       if (bounce == 0u && hit) {
         uint32_t oid = sc.objects[rec.obj].object_id;
         s.primary = (oid << 22) | (rec.prim == 0xffffffffu ? 0u : ((rec.prim + 1u) & 0x3fffffu));
       }
       if (!hit) {
-        s.beauty += s.atten * sky_sample(sc.sky, s.ray);
+        float w = 1.0f;
+        if (kPerf && nee_sky && pdf_prev > 0.0f)
+          w = power_heuristic(pdf_prev, sel * sky_dir_pdf(sc.sky, s.ray.d));
+        s.beauty += s.atten * sky_sample(sc.sky, s.ray) * w;
       } else {
         const DevMaterial& m = sc.materials[sc.objects[rec.obj].material];
         Ray r_in = s.ray;
-        s.beauty += s.atten * mat_emitted(m, rec);
+        {
+          float w = 1.0f;
+          if (kPerf && nee_light && pdf_prev > 0.0f && (int32_t)rec.obj == sc.light)
+            w = power_heuristic(pdf_prev, sel * light_pdf_value(sc, r_in.o, r_in.d, st, P.err));
+          s.beauty += s.atten * mat_emitted(m, rec) * w;
+        }
         Scatter sr;
         bool cont = mat_scatter(m, rec, s.ray, sr, g);
+        float pdf_next = 0.0f;
         if (cont) {
           if (sr.skip_pdf) {
             s.atten *= sr.atten;
             s.ray = make_ray(rec.p, sr.skip_dir, s.ray.tm);
-          } else {
+          } else if (!kPerf) {
             cont = sample_brdf(P, m, rec, sr, r_in, s, g, st);
+          } else {
+            const V3 view = normalize(-r_in.d);
+            // next-event estimation: one emitter sample
+            if (nee_light || nee_sky) {
+              bool use_light = nee_light && (!nee_sky || g.random_float() < 0.5f);
+              V3 ldir, Le;
+              float lpdf = 0.0f, dist = FMAX;
+              bool ok;
+              if (use_light) {
+                ok = light_sample_nee(sc, rec.p, g, P.rtl != 0, ldir, dist, lpdf, Le, st, P.err,
+                                      mesh_fn);
+                dist = dist * 0.999f - 2.0f * EPS;
+              } else {
+                ldir = normalize(sky_sample_dir(sc.sky, g, lpdf));
+                Le = sky_sample(sc.sky, make_ray(rec.p, ldir, 0.0f));
+                ok = lpdf > 0.0f;
+                dist = FMAX;
+              }
+              if (ok && dist > 0.0f) {
+                const V3 f = perf_bsdf_eval(m, rec, view, ldir);
+                if (f.x > 0.0f || f.y > 0.0f || f.z > 0.0f) {
+                  const float pl = sel * lpdf;
+                  const float wl = power_heuristic(pl, perf_bsdf_pdf(sr.pdf, ldir));
+                  const V3 c = s.atten * f * Le * (wl / pl);
+                  W.sh_o[p] = make_float4(rec.p.x, rec.p.y, rec.p.z, dist);
+                  W.sh_d[p] = make_float4(ldir.x, ldir.y, ldir.z, 0.0f);
+                  W.sh_c[p] = make_float4(c.x, c.y, c.z, 0.0f);
+                  shadow = true;
+                }
+              }
+            }
+            // continue with the material's own sampler
+            const V3 dir = pdf_generate(sr.pdf, g, P.rtl != 0);
+            const float pb = perf_bsdf_pdf(sr.pdf, dir);
+            if (pb > 0.0f) {
+              s.atten *= perf_bsdf_eval(m, rec, view, dir) / pb;
+              s.ray = make_ray(rec.p, dir, r_in.tm);
+              pdf_next = pb;
+            } else {
+              cont = false;
+            }
           }
         }
         if (cont) {
@@ -709,11 +776,13 @@ __global__ void __launch_bounds__(kShadeThreads) k_wf_shade(WfParams W, int qsel
           W.ray_o[p] = make_float4(s.ray.o.x, s.ray.o.y, s.ray.o.z, s.ray.tm);
           W.ray_d[p] = make_float4(s.ray.d.x, s.ray.d.y, s.ray.d.z, __uint_as_float(bounce + 1u));
           W.atten[p] = make_float4(s.atten.x, s.atten.y, s.atten.z, __uint_as_float(g.draw));
+          if (kPerf) W.mis_pdf[p] = pdf_next;
         }
       }
       W.acc_b[p] = make_float4(s.beauty.x, s.beauty.y, s.beauty.z, __uint_as_float(s.primary));
     }
-    // warp-aggregated append of the surviving paths
+    // warp-aggregated append of the surviving paths (and, in perf mode, of
+    // the shadow rays)
     uint32_t mask = __ballot_sync(0xffffffffu, alive);
     if (mask) {
       uint32_t leader = __ffs(mask) - 1u;
@@ -721,6 +790,52 @@ __global__ void __launch_bounds__(kShadeThreads) k_wf_shade(WfParams W, int qsel
       if (lane == leader) off = atomicAdd(next_n, __popc(mask));
       off = __shfl_sync(0xffffffffu, off, leader);
       if (alive) next_queue[off + __popc(mask & ((1u << lane) - 1u))] = p;
+    }
+    if (kPerf) {
+      uint32_t smask = __ballot_sync(0xffffffffu, shadow);
+      if (smask) {
+        uint32_t leader = __ffs(smask) - 1u;
+        uint32_t off = 0;
+        if (lane == leader) off = atomicAdd(&W.ctr[CTR_SH], __popc(smask));
+        off = __shfl_sync(0xffffffffu, off, leader);
+        if (shadow) W.sh_queue[off + __popc(smask & ((1u << lane) - 1u))] = p;
+      }
+    }
+  }
+}
+
+// Shadow rays of one bounce (perf mode): an unoccluded ray adds its
+// precomputed contribution to the path's beauty.
+__global__ void __launch_bounds__(kExtThreads) k_wf_shadow(WfParams W) {
+  extern __shared__ uint2 wf_smem[];
+  const KernelParams& P = W.kp;
+  const uint32_t n = W.ctr[CTR_SH];
+  const uint32_t lane = threadIdx.x & 31u;
+  uint2* tlas_stk = wf_smem + threadIdx.x;
+  uint2* blas_stk = wf_smem + kTlasStack * kExtThreads + threadIdx.x;
+  TraceStats st{0u, 0u, 0u};
+  while (true) {
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(&W.ctr[CTR_SHWORK], 32u);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base >= n) break;
+    const uint32_t i = base + lane;
+    if (i < n) {
+      const uint32_t p = __ldg(W.sh_queue + i);
+      const float4 o = W.sh_o[p], d = W.sh_d[p];
+      const Ray r = make_ray(V3{o.x, o.y, o.z}, V3{d.x, d.y, d.z}, 0.0f);
+      uint32_t obj, slot;
+      float t, u, v;
+      trace_closest<false>(P.scene, r, tlas_stk, blas_stk, kExtThreads, obj, slot, t, u, v, st,
+                           P.err, o.w);
+      if (obj == 0xffffffffu) {
+        const float4 c = W.sh_c[p];
+        float4 b = W.acc_b[p];
+        b.x += c.x;
+        b.y += c.y;
+        b.z += c.z;
+        W.acc_b[p] = b;
+      }
     }
   }
 }
@@ -732,6 +847,8 @@ __global__ void k_wf_rotate(WfParams W, int consumed) {
   if (threadIdx.x == 0) {
     W.ctr[consumed] = 0u;
     W.ctr[CTR_WORK] = 0u;
+    W.ctr[CTR_SH] = 0u;
+    W.ctr[CTR_SHWORK] = 0u;
   }
 }
 
@@ -801,11 +918,13 @@ cudaError_t wf_set_base(const WfParams& W, uint32_t first_sample, cudaStream_t s
   return cudaGetLastError();
 }
 
-size_t wf_state_bytes(uint32_t n_paths) {
-  return (size_t)n_paths * (6 * sizeof(float4) + sizeof(uint4) + sizeof(float) + 2 * sizeof(uint32_t));
+size_t wf_state_bytes(uint32_t n_paths, bool perf) {
+  size_t per = 6 * sizeof(float4) + sizeof(uint4) + sizeof(float) + 2 * sizeof(uint32_t);
+  if (perf) per += sizeof(float) + 3 * sizeof(float4) + sizeof(uint32_t);
+  return (size_t)n_paths * per;
 }
 
-cudaError_t wf_alloc(WfParams& W, uint32_t n_paths) {
+cudaError_t wf_alloc(WfParams& W, uint32_t n_paths, bool perf) {
   cudaError_t e;
 #define A(ptr, T) \
   if ((e = cudaMalloc(&W.ptr, sizeof(T) * (size_t)n_paths)) != cudaSuccess) return e;
@@ -819,6 +938,13 @@ cudaError_t wf_alloc(WfParams& W, uint32_t n_paths) {
   A(hit_t, float);
   A(queue0, uint32_t);
   A(queue1, uint32_t);
+  if (perf) {
+    A(mis_pdf, float);
+    A(sh_o, float4);
+    A(sh_d, float4);
+    A(sh_c, float4);
+    A(sh_queue, uint32_t);
+  }
 #undef A
   if ((e = cudaMalloc(&W.ctr, 16 * sizeof(uint32_t))) != cudaSuccess) return e;
   W.capacity = n_paths;
@@ -836,6 +962,11 @@ void wf_free(WfParams& W) {
   cudaFree(W.hit_t);
   cudaFree(W.queue0);
   cudaFree(W.queue1);
+  cudaFree(W.mis_pdf);
+  cudaFree(W.sh_o);
+  cudaFree(W.sh_d);
+  cudaFree(W.sh_c);
+  cudaFree(W.sh_queue);
   cudaFree(W.ctr);
   W = WfParams{};
 }
@@ -900,8 +1031,15 @@ cudaError_t wf_launch_wave(const WfParams& W, bool counters, cudaStream_t st, Wa
     if (b == 0) ext0<<<eb0, kExtThreads, smem0, st>>>(W, q, 1);
     else ext<<<eb, kExtThreads, smem, st>>>(W, q, 0);
     if (tm) tm->mark(NR_KERNEL_EXTEND, st);
-    k_wf_shade<<<shade_blocks, kShadeThreads, 0, st>>>(W, q, b == 0 ? 1 : 0);
-    if (tm) tm->mark(NR_KERNEL_SHADE, st);
+    if (W.mis_pdf) {
+      k_wf_shade<true><<<shade_blocks, kShadeThreads, 0, st>>>(W, q, b == 0 ? 1 : 0);
+      if (tm) tm->mark(NR_KERNEL_SHADE, st);
+      k_wf_shadow<<<sm_count() * 4, kExtThreads, kExtStackBytes, st>>>(W);
+      if (tm) tm->mark(NR_KERNEL_EXTEND, st);
+    } else {
+      k_wf_shade<false><<<shade_blocks, kShadeThreads, 0, st>>>(W, q, b == 0 ? 1 : 0);
+      if (tm) tm->mark(NR_KERNEL_SHADE, st);
+    }
     k_wf_rotate<<<1, 32, 0, st>>>(W, q);
     if (tm) tm->mark(NR_KERNEL_ROTATE, st);
   }

@@ -24,10 +24,18 @@ struct WfParams {
   uint32_t* queue0;
   uint32_t* queue1;
   uint32_t* ctr;
+  // NR_MODE_PERF only (null otherwise): BSDF pdf of each path's current
+  // direction, and one shadow ray per path per bounce (origin + max t,
+  // direction, contribution) with its queue
+  float* mis_pdf;
+  float4* sh_o;
+  float4* sh_d;
+  float4* sh_c;
+  uint32_t* sh_queue;
 };
 
-size_t wf_state_bytes(uint32_t n_paths);
-cudaError_t wf_alloc(WfParams& W, uint32_t n_paths);
+size_t wf_state_bytes(uint32_t n_paths, bool perf = false);
+cudaError_t wf_alloc(WfParams& W, uint32_t n_paths, bool perf = false);
 void wf_free(WfParams& W);
 // static_wave.cu: address of the library-owned wave buffer on the current
 // device, and its division into the wave's arrays (capacity
