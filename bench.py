@@ -57,6 +57,8 @@ def parse():
     p.add_argument("--extend-variant", type=int, default=0,
                    help="traversal kernel variant (0: library default; see autotune.py)")
     p.add_argument("--mesh-leaf", type=int, default=1)
+    p.add_argument("--no-rmse", action="store_true", help="skip the time-to-RMSE measurement")
+    p.add_argument("--rmse-oracle-spp", type=int, default=8192)
     return p.parse_args()
 
 
@@ -326,6 +328,10 @@ def run_ours(args):
     if rank == 0 and not args.no_reference_cuda:
         ref_cuda = reference_cuda_rate(spec, w, h)
 
+    rmse = None
+    if rank == 0 and world == 1 and not args.no_rmse:
+        rmse = time_to_rmse(args)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         done, secs, kind, cores = cpu_reference_rate(spec, h, w, args.cpu_seconds)
@@ -356,6 +362,7 @@ def run_ours(args):
                             for k in capi.KERNEL_CLASSES if kernel_launches[k]},
                 "cpu_baseline": cpu,
                 "reference_cuda": ref_cuda,
+                "time_to_rmse": rmse,
                 "scene": {"build_ms_device": stats["build_ms"], "build_wall_s": build_wall,
                           "triangles": stats["n_triangles"], "wide_nodes": stats["wide_nodes"],
                           "sah_cost_binary": stats["sah_cost_binary"]},
@@ -401,6 +408,52 @@ def e2e_public_api(pt, spec, S, args):
     return {"value": v, "unit": "samples/s", "h2d_bytes_per_step": h2d,
             "d2h_bytes_per_step": 3 * w * h,
             "path": "_pathtracer RenderEngine.render + TransferStream.readback (uint8 CHW)"}
+
+
+def time_to_rmse(args, target=0.01):
+    """Device time until the display-referred image sqrt(clamp(x, 0, 1)) is
+    within `target` RMSE (all pixels x 3 channels) of an FP64-accumulated
+    high-sample render of the same scene, for perf mode and for the
+    reference estimator. The oracle is rendered in perf mode with another
+    seed: under the HDRI's sun the reference estimator's own high-sample
+    render is still far from converged (its RMSE is reported). Sample counts
+    double between checks, so the reported time is that of the first power
+    of two that reaches the target. The scene is the mesh-stress scene at
+    320x180."""
+    from nectarrender_b200 import capi
+    h, w = 180, 320
+    n_or = args.rmse_oracle_spp
+    spec = scenes.mesh_stress(levels=args.levels, res_h=h, res_w=w, spp=n_or + 1)
+    sc = capi.Scene(spec, mesh_leaf=args.mesh_leaf)
+    orc = capi.Render(sc, mode=capi.MODE_PERF, fp64_accumulate=1, seed=spec.seed + 1000)
+    t0 = time.perf_counter()
+    orc.samples(1, n_or)
+    oracle_s = time.perf_counter() - t0
+    disp_o = np.sqrt(np.clip(orc.beauty_fp64(), 0.0, 1.0))
+    del orc
+    out = {"target_rmse": target, "domain": "sqrt(clamp(x,0,1)), all pixels x 3 channels",
+           "workload": f"mesh_stress {w}x{h}, depth {spec.ray_depth}", "oracle_spp": n_or,
+           "oracle_wall_s": oracle_s}
+    for name, mode in (("perf_mode", capi.MODE_PERF), ("reference_estimator", capi.MODE_REFERENCE)):
+        r = capi.Render(sc, mode=mode, fp64_accumulate=1, seed=spec.seed)
+        done, n, t_ms, rmse = 0, 1, 0.0, float("inf")
+        curve = []
+        while done + n <= n_or // 2:
+            r.samples(done + 1, n)
+            t_ms += r.last_ms()
+            done += n
+            img = np.sqrt(np.clip(r.beauty_fp64(), 0.0, 1.0))
+            rmse = float(np.sqrt(np.mean((img - disp_o) ** 2)))
+            curve.append([done, round(t_ms, 3), round(rmse, 5)])
+            if rmse <= target:
+                break
+            n = done
+        out[name] = {"spp": done, "device_ms": t_ms, "rmse": rmse, "reached": rmse <= target,
+                     "curve_spp_ms_rmse": curve}
+    a, b = out["reference_estimator"], out["perf_mode"]
+    if a["reached"] and b["reached"] and b["device_ms"] > 0:
+        out["speedup_perf_vs_reference_estimator"] = a["device_ms"] / b["device_ms"]
+    return out
 
 
 def reference_cuda_rate(spec, w, h):
