@@ -373,6 +373,32 @@ int nr_render_last_ms(const nr_render* render, double* out_ms);
 /* Opaque cudaStream_t of the render (for callers that time or order work). */
 int nr_render_stream(const nr_render* render, uint64_t* out_stream);
 
+/* viewport ----------------------------------------------------------------- */
+/* Shaded preview into the beauty / diffuse / world-normal layers (overwrites
+ * them): headlight + directional shading of the material's viewport colour,
+ * sky (optionally under the axis grid) on a miss; one centre ray per pixel
+ * (RenderEngine::viewport -> trace_viewport_kernel,
+ * nectar_render/csrc/engine/src/engine.cpp:77-95, trace.cu:100-162). */
+int nr_render_viewport(nr_render* render, int32_t show_axis_grid);
+/* Closest hit of the screen-space ray through (u, v) in [0,1]^2
+ * (hit_test_ray_kernel, trace.cu:168-188; SceneInterface::query_scene). */
+typedef struct nr_pick_result {
+  int32_t hit;
+  uint32_t object_id;    /* HitRecord::object_id                            */
+  uint32_t material_id;  /* HitRecord::material_id                          */
+  float t;
+  float p[3];
+  float n[3];
+  float uv[2];
+  int32_t front_face;
+} nr_pick_result;
+int nr_render_pick(nr_render* render, float u, float v, nr_pick_result* out);
+/* Outline mask (H x W uint8, 255 on the outline) of the pixels whose centre
+ * ray hits `object_id` (selection_mask, nectar_render/csrc/scene/src/
+ * scene_interface.cu:54-81). */
+int nr_render_selection_mask(nr_render* render, uint32_t object_id, int32_t outline_radius,
+                             uint8_t* host_hw);
+
 /* device-pointer level (callers that own their buffers) -------------------- */
 /* Fused running-mean accumulate of one sample layer into an average layer on
  * the given stream: avg = avg*(n-1)/n + s/n (accumulate_samples_kernel,

@@ -69,6 +69,12 @@ class KernelProfile(C.Structure):
     _fields_ = [("ms", C.c_double * 6), ("launches", C.c_uint32 * 6)]
 
 
+class PickResult(C.Structure):
+    _fields_ = [("hit", C.c_int32), ("object_id", C.c_uint32), ("material_id", C.c_uint32),
+                ("t", C.c_float), ("p", c_float3), ("n", c_float3), ("uv", C.c_float * 2),
+                ("front_face", C.c_int32)]
+
+
 class TraceCounters(C.Structure):
     _fields_ = [("rays", C.c_uint64), ("node_visits", C.c_uint64), ("tri_tests", C.c_uint64),
                 ("obj_tests", C.c_uint64), ("paths", C.c_uint64)]
@@ -93,7 +99,7 @@ EXPORTS = [
     "nr_scene_get_stats", "nr_scene_get_binary_bvh", "nr_render_config_default",
     "nr_render_create", "nr_render_destroy", "nr_render_reset", "nr_render_samples",
     "nr_render_samples_static", "nr_render_set_profiling", "nr_render_get_profile",
-    "nr_render_graph_stats",
+    "nr_render_graph_stats", "nr_render_viewport", "nr_render_pick", "nr_render_selection_mask",
     "nr_render_sample_layers", "nr_render_layer_device_ptr", "nr_render_read_layer",
     "nr_render_read_beauty_fp64", "nr_render_readback", "nr_render_display_float",
     "nr_render_dims", "nr_render_set_counters", "nr_render_get_counters", "nr_render_last_ms",
@@ -324,6 +330,24 @@ class Render:
         p = KernelProfile()
         _check(self.lib.nr_render_get_profile(self.h, C.byref(p)), "nr_render_get_profile")
         return {k: (p.ms[i], p.launches[i]) for i, k in enumerate(KERNEL_CLASSES)}
+
+    def viewport(self, show_axis_grid: bool = True) -> None:
+        _check(self.lib.nr_render_viewport(self.h, int(show_axis_grid)), "nr_render_viewport")
+
+    def pick(self, u: float, v: float) -> dict:
+        r = PickResult()
+        _check(self.lib.nr_render_pick(self.h, C.c_float(u), C.c_float(v), C.byref(r)),
+               "nr_render_pick")
+        return {"hit": bool(r.hit), "object_id": r.object_id, "material_id": r.material_id,
+                "t": r.t, "p": tuple(r.p), "n": tuple(r.n), "uv": tuple(r.uv),
+                "front_face": bool(r.front_face)}
+
+    def selection_mask(self, object_id: int, outline_radius: int = 2) -> np.ndarray:
+        out = np.zeros((self.H, self.W), np.uint8)
+        _check(self.lib.nr_render_selection_mask(self.h, object_id, outline_radius,
+                                                 out.ctypes.data_as(C.POINTER(C.c_uint8))),
+               "nr_render_selection_mask")
+        return out
 
     def graph_stats(self) -> tuple[int, int]:
         """(wave graphs captured, graph replays) of this render so far."""

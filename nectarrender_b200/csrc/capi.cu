@@ -27,6 +27,7 @@
 #include "image_ops.cuh"
 #include "integrator.cuh"
 #include "wavefront.cuh"
+#include "viewport.cuh"
 
 using namespace nr;
 
@@ -1030,6 +1031,8 @@ struct nr_render {
     cudaGraphExec_t exec = nullptr;
   };
   std::vector<WaveGraph> graphs;
+  PickOut* d_pick = nullptr;        // viewport queries (allocated on first use)
+  uint8_t* d_mask = nullptr;        // 2 x W*H selection masks
   uint32_t graphs_captured = 0;
   uint64_t graph_replays = 0;
   nr_trace_counters last{};
@@ -1050,6 +1053,8 @@ struct nr_render {
     for (auto& g : graphs)
       if (g.exec) cudaGraphExecDestroy(g.exec);
     for (auto e : pev) cudaEventDestroy(e);
+    cudaFree(d_pick);
+    cudaFree(d_mask);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (stream) cudaStreamDestroy(stream);
@@ -1433,6 +1438,48 @@ int nr_render_samples_static(nr_render* r, uint32_t first, uint32_t count) {
     r->last.paths = (unsigned long long)count * N;
   }
   r->n64 = first + count - 1;
+  return NR_OK;
+}
+
+int nr_render_viewport(nr_render* r, int32_t show_axis_grid) {
+  if (!r) return fail(NR_ERR_INVALID, "null render");
+  KernelParams P = make_params(r, 0, 0, false);
+  P.beauty64 = nullptr;
+  CU(launch_viewport(P, show_axis_grid, r->stream), "viewport");
+  CU(cudaStreamSynchronize(r->stream), "viewport");
+  uint32_t herr = 0;
+  CU(cudaMemcpy(&herr, r->err, 4, cudaMemcpyDeviceToHost), "read error word");
+  if (herr) {
+    cudaMemset(r->err, 0, 4);
+    return fail(NR_ERR_DEVICE, "viewport error word 0x" + std::to_string(herr));
+  }
+  return NR_OK;
+}
+
+int nr_render_pick(nr_render* r, float u, float v, nr_pick_result* out) {
+  if (!r || !out) return fail(NR_ERR_INVALID, "null argument");
+  if (!r->d_pick) CU(cudaMalloc(&r->d_pick, sizeof(PickOut)), "alloc pick");
+  KernelParams P = make_params(r, 0, 0, false);
+  CU(launch_pick(P, u, v, r->d_pick, r->stream), "pick");
+  PickOut h;
+  CU(cudaMemcpyAsync(&h, r->d_pick, sizeof(h), cudaMemcpyDeviceToHost, r->stream), "read pick");
+  CU(cudaStreamSynchronize(r->stream), "pick");
+  static_assert(sizeof(PickOut) == sizeof(nr_pick_result), "pick result layout");
+  memcpy(out, &h, sizeof(h));
+  return NR_OK;
+}
+
+int nr_render_selection_mask(nr_render* r, uint32_t object_id, int32_t outline_radius,
+                             uint8_t* host_hw) {
+  if (!r || !host_hw || outline_radius < 0 || outline_radius > 64)
+    return fail(NR_ERR_INVALID, "bad argument (outline radius 0..64)");
+  size_t hw = (size_t)r->W * r->H;
+  if (!r->d_mask) CU(cudaMalloc(&r->d_mask, 2 * hw), "alloc mask");
+  KernelParams P = make_params(r, 0, 0, false);
+  CU(launch_selection_mask(P, object_id, outline_radius, r->d_mask, r->d_mask + hw, r->stream),
+     "selection mask");
+  CU(cudaMemcpyAsync(host_hw, r->d_mask + hw, hw, cudaMemcpyDeviceToHost, r->stream), "read mask");
+  CU(cudaStreamSynchronize(r->stream), "selection mask");
   return NR_OK;
 }
 

@@ -392,6 +392,29 @@ struct EnginePollResponse {
   CameraParams camera_params;
 };
 
+// HitRecord (hittable/include/hittable/hit_record.h:9-22) as a picking query
+// returns it.
+struct HitRecord {
+  size_t object_id = 0;
+  size_t material_id = 0;
+  Vector3 p, n, tangent;
+  Vector2 uv;
+  float t = 0.f;
+  bool front_face = false;
+  bool hit = false;
+};
+
+// SceneInterface's picking and selection (scene/include/interface.h:60-71,
+// 193-199): query_scene(u, v) casts the screen-space ray and keeps the hit.
+struct SceneInterface {
+  EngineCore* eng = nullptr;
+  HitRecord rec;
+  std::atomic<bool> enabled{false};
+  int outline_radius = 2;
+  void query_scene(float u, float v);
+  py::array selection_mask() const;
+};
+
 struct EngineCore {
   Camera cam;
   uint32_t ray_depth, seed;
@@ -403,6 +426,8 @@ struct EngineCore {
   EngineRequests requests;
   std::atomic<EngineState> state{EngineState::IDLE};
   std::atomic<EngineType> type{EngineType::PATHTRACER};
+  std::atomic<bool> show_axis_grid{true};
+  SceneInterface scene_interface;
   int mode = NR_MODE_REFERENCE;
   bool hooks_set = false;
   std::function<void()> on_render_started = [] {}, on_render_finished = [] {}, on_stopped = [] {},
@@ -412,6 +437,7 @@ struct EngineCore {
 
   EngineCore(const Camera& c, uint32_t depth, uint32_t sd) : cam(c), ray_depth(depth), seed(sd) {
     stream.eng = this;
+    scene_interface.eng = this;
     wire_layers(false);
   }
   ~EngineCore() {
@@ -451,11 +477,31 @@ struct EngineCore {
     check(nr_render_create(scene, &d, &cfg, &render), "RenderEngine");
     sample_idx = 1;
   }
+  // RenderEngine::reset (engine.cpp:216-220): the next sample is 1, whose
+  // running mean overwrites the layers; they are not cleared (a viewport
+  // frame or a stopped render stays visible until then).
   void reset() {
     sample_idx = 1;
-    if (render) check(nr_render_reset(render), "RenderEngine.reset");
     py::gil_scoped_acquire gil;
     on_reset();
+  }
+  // RenderEngine::viewport (engine.cpp:77-95): one preview frame into the
+  // layers; returns 3 (waiting for the next refresh), 1 stopped, 2 restarted.
+  int run_viewport() {
+    if (!render) throw std::runtime_error("RenderEngine.render() called before set_scene()");
+    EnginePollResponse resp;
+    {
+      py::gil_scoped_acquire gil;
+      resp = poll_updates();
+    }
+    if (requests.stop_.exchange(false)) return 1;
+    if (resp.should_update_camera) {
+      cam.p = resp.camera_params;
+      make_render();
+    }
+    check(nr_render_viewport(render, show_axis_grid.load() ? 1 : 0), "RenderEngine.viewport");
+    if (requests.restart_.exchange(false)) return 2;
+    return 3;
   }
   // RenderEngine::render (engine.cpp:42-74): samples sample_idx .. n-1
   int run() {
@@ -490,6 +536,33 @@ struct EngineCore {
     return 0;
   }
 };
+
+void SceneInterface::query_scene(float u, float v) {
+  if (!eng || !eng->render) throw std::runtime_error("query_scene() before set_scene()");
+  nr_pick_result r;
+  check(nr_render_pick(eng->render, u, v, &r), "SceneInterface.query_scene");
+  rec = HitRecord{};
+  rec.hit = r.hit != 0;
+  if (rec.hit) {
+    rec.object_id = r.object_id;
+    rec.material_id = r.material_id;
+    rec.p = Vector3(r.p[0], r.p[1], r.p[2]);
+    rec.n = Vector3(r.n[0], r.n[1], r.n[2]);
+    rec.uv = Vector2(r.uv[0], r.uv[1]);
+    rec.t = r.t;
+    rec.front_face = r.front_face != 0;
+    enabled = true;
+  }
+}
+
+py::array SceneInterface::selection_mask() const {
+  if (!eng || !eng->render) throw std::runtime_error("selection mask before set_scene()");
+  py::array_t<uint8_t> out({(size_t)eng->H(), (size_t)eng->W()});
+  check(nr_render_selection_mask(eng->render, (uint32_t)rec.object_id, outline_radius,
+                                 out.mutable_data()),
+        "SceneInterface.get_scene_outline");
+  return std::move(out);
+}
 
 uintptr_t DataObject::device_ptr() const {
   if (!eng || !eng->render || !enabled) return 0;
@@ -695,6 +768,16 @@ PYBIND11_MODULE(_pathtracer, m) {
 
   // ---- hittable
   auto m_hit = m.def_submodule("hittable", "Hittable module.");
+  py::class_<HitRecord>(m_hit, "HitRecord")
+      .def(py::init<>())
+      .def_readonly("object_id", &HitRecord::object_id)
+      .def_readonly("material_id", &HitRecord::material_id)
+      .def_readonly("p", &HitRecord::p)
+      .def_readonly("n", &HitRecord::n)
+      .def_readonly("tangent", &HitRecord::tangent)
+      .def_readonly("uv", &HitRecord::uv)
+      .def_readonly("t", &HitRecord::t)
+      .def_readonly("front_face", &HitRecord::front_face);
   auto default_mat = []() { return make_lambertian(Texture::from_color(Color::purple())); };
   py::class_<Hittable>(m_hit, "Hittable")
       .def(py::init<>())
@@ -824,6 +907,16 @@ PYBIND11_MODULE(_pathtracer, m) {
            }),
            py::arg("hittables"), py::arg("lights"), py::arg("skylight"), py::keep_alive<1, 2>(),
            py::keep_alive<1, 3>());
+
+  py::class_<SceneInterface>(m_scene, "SceneInterface")
+      .def("query_scene", &SceneInterface::query_scene, py::arg("u"), py::arg("v"))
+      .def("get_hit_record", [](SceneInterface& si) -> HitRecord& { return si.rec; },
+           py::return_value_policy::reference_internal)
+      .def("enable", [](SceneInterface& si) { si.enabled = true; })
+      .def("disable", [](SceneInterface& si) { si.enabled = false; })
+      .def("is_enabled", [](SceneInterface& si) { return si.enabled.load(); })
+      .def("is_disabled", [](SceneInterface& si) { return !si.enabled.load(); })
+      .def("get_scene_outline", &SceneInterface::selection_mask);
 
   // ---- data
   auto m_data = m.def_submodule("data", "Data module.");
@@ -1004,7 +1097,12 @@ PYBIND11_MODULE(_pathtracer, m) {
                  e.reset();
                  e.state = EngineState::RENDERING;
                  { py::gil_scoped_acquire gil; e.on_render_started(); }
-                 int rs = e.run();
+                 int rs = e.type.load() == EngineType::VIEWPORT ? e.run_viewport() : e.run();
+                 if (rs == 3) {  // WAITING: refresh the viewport again
+                   e.requests.start();
+                   std::this_thread::sleep_for(std::chrono::milliseconds(16));
+                   continue;
+                 }
                  e.state = EngineState::IDLE;
                  py::gil_scoped_acquire gil;
                  if (rs == 0) e.on_render_finished();
@@ -1032,6 +1130,9 @@ PYBIND11_MODULE(_pathtracer, m) {
       .def("get_state", [](EngineCore& e) { return e.state.load(); })
       .def("is_idle", [](EngineCore& e) { return e.state == EngineState::IDLE; })
       .def("is_rendering", [](EngineCore& e) { return e.state == EngineState::RENDERING; })
+      .def("set_axis_grid_visible", [](EngineCore& e, bool v) { e.show_axis_grid = v; })
+      .def("get_scene_interface", [](EngineCore& e) -> SceneInterface& { return e.scene_interface; },
+           py::return_value_policy::reference_internal)
       .def("get_engine_type", [](EngineCore& e) { return e.type.load(); })
       .def("set_engine_type", [](EngineCore& e, EngineType t) { e.type = t; })
       .def("n_samples", [](EngineCore& e) { return e.cam.p.samples_per_pixel; })

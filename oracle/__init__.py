@@ -208,6 +208,46 @@ class SceneHandle:
         if not self.h:
             raise RuntimeError("scene_create failed")
 
+    def viewport(self, show_axis_grid: bool = True, seed: int | None = None):
+        """(beauty, diffuse, normal) of the viewport preview (oracle only)."""
+        spec = self.spec
+        cam = camera_desc(spec.camera)
+        H, W = int(spec.camera["resolution"][0]), int(spec.camera["resolution"][1])
+        b = np.zeros((3, H, W), np.float32)
+        d, n = np.zeros_like(b), np.zeros_like(b)
+        rc = getattr(self.lib.lib, self.lib.prefix + "scene_viewport")(C.c_void_p(self.h), C.byref(cam),
+                                                spec.seed if seed is None else seed,
+                                                int(show_axis_grid), _f(b), _f(d), _f(n))
+        if rc != 0:
+            raise RuntimeError(f"oracle_scene_viewport failed ({rc})")
+        return b, d, n
+
+    def pick(self, u: float, v: float, seed: int | None = None) -> dict:
+        from nectarrender_b200.capi import PickResult
+        r = PickResult()
+        cam = camera_desc(self.spec.camera)
+        rc = getattr(self.lib.lib, self.lib.prefix + "scene_pick")(C.c_void_p(self.h), C.byref(cam),
+                                            self.spec.seed if seed is None else seed,
+                                            C.c_float(u), C.c_float(v), C.byref(r))
+        if rc != 0:
+            raise RuntimeError(f"oracle_scene_pick failed ({rc})")
+        return {"hit": bool(r.hit), "object_id": r.object_id, "material_id": r.material_id,
+                "t": r.t, "p": tuple(r.p), "n": tuple(r.n), "uv": tuple(r.uv),
+                "front_face": bool(r.front_face)}
+
+    def selection_mask(self, object_id: int, radius: int = 2, seed: int | None = None):
+        spec = self.spec
+        cam = camera_desc(spec.camera)
+        H, W = int(spec.camera["resolution"][0]), int(spec.camera["resolution"][1])
+        out = np.zeros((H, W), np.uint8)
+        rc = getattr(self.lib.lib, self.lib.prefix + "scene_selection_mask")(C.c_void_p(self.h), C.byref(cam),
+                                                      spec.seed if seed is None else seed,
+                                                      int(object_id), int(radius),
+                                                      out.ctypes.data_as(C.POINTER(C.c_uint8)))
+        if rc != 0:
+            raise RuntimeError(f"oracle_scene_selection_mask failed ({rc})")
+        return out
+
     def render(self, first: int, count: int = 1, mode: int = 1, rows=None, threads: int = 0,
                fp64: bool = False, cfg: RenderConfig | None = None, spec: SceneSpec | None = None):
         spec = spec or self.spec

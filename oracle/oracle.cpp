@@ -1417,6 +1417,69 @@ V running_mean(V avg, V s, uint32_t n) {  // data.cu:28-50
 
 }  // namespace
 
+// ---- viewport (engine/src/trace.cu:100-188, engine/src/axis_grid.cu,
+// scene/src/scene_interface.cu:3-81) ---------------------------------------
+float vp_saturate(float x) { return fminf(fmaxf(x, 0.0f), 1.0f); }
+float vp_smoothstep(float a, float b, float x) {  // core/cg_std.h:98-103
+  float t = vp_saturate((x - a) / (b - a));
+  return t * t * (3.0f - (2.0f * t));
+}
+V vp_lerp(V x, V y, float w) { return x + w * (y - x); }  // core/cg_std.h:91-93
+float vp_comp(V v, int a) { return a == 0 ? v.x : (a == 1 ? v.y : v.z); }
+float vp_grid_mask(float u, float v, float spacing, float width) {  // axis_grid.cu:4-9
+  float du = fabsf(fmodf(u + spacing * 0.5f, spacing) - spacing * 0.5f);
+  float dv = fabsf(fmodf(v + spacing * 0.5f, spacing) - spacing * 0.5f);
+  return 1.0f - vp_smoothstep(0.0f, width, fminf(du, dv));
+}
+bool vp_axis_grid(const Ray& r, float max_t, int axis, V major, V& color, float& alpha) {
+  float da = vp_comp(r.d, axis);  // axis_grid.cu:11-53
+  if (fabsf(da) < 1e-6f) return false;
+  float t = -vp_comp(r.o, axis) / da;
+  if (t <= 0.0f || t >= max_t) return false;
+  V p = r.o + t * r.d;
+  p = V{fabsf(p.x), fabsf(p.y), fabsf(p.z)};
+  float u = vp_comp(p, (axis + 1) % 3), v = vp_comp(p, (axis + 2) % 3);
+  float pixel_size = 1e-3f * t;
+  float level = fmaxf(log10f(fmaxf(pixel_size, 1e-5f)) + 1.0f, 0.0f);
+  float level0 = floorf(level);
+  float blend = level - level0;
+  float s0 = powf(10.0f, level0), s1 = s0 * 10.0f;
+  float width = pixel_size * 1.5f;
+  float g0 = vp_grid_mask(u, v, s0, width), g1 = vp_grid_mask(u, v, s1, width);
+  float mask = fmaxf(g0 * (1.0f - blend), g1);
+  if (mask < 0.01f) return false;
+  float fade = fmaxf(0.0f, 1.0f - t / 100.0f);
+  color = vp_lerp(V{0.35f, 0.35f, 0.35f}, major, vp_smoothstep(0.0f, 1.0f, g1));
+  alpha = mask * fade;
+  return true;
+}
+bool vp_triplanar(const Ray& r, V& color, float& alpha) {  // axis_grid.cu:55-72
+  return vp_axis_grid(r, FMAX, 0, V{1.0f, 0.3f, 0.3f}, color, alpha) ||
+         vp_axis_grid(r, FMAX, 1, V{0.3f, 1.0f, 0.3f}, color, alpha) ||
+         vp_axis_grid(r, FMAX, 2, V{0.3f, 0.3f, 1.0f}, color, alpha);
+}
+V vp_color(const Mat& m) {  // material.h viewport_color
+  if (m.type == NR_MATERIAL_DIELECTRIC) return m.tint;
+  if (m.type >= 1 && m.type <= 5) return tex(m.tex[0]);
+  return V{0, 0, 0};
+}
+Ray vp_center_ray(const Cam& c, uint32_t x, uint32_t y) {  // camera.h:181-184
+  V2 base = c.pattern[0];
+  V2 shift = pcg_vector2(0.0f, 0u);
+  V2 off{fmodf(base.x + shift.x, 1.0f) - 0.5f, fmodf(base.y + shift.y, 1.0f) - 0.5f};
+  float u = ((float)x + off.x - (c.rx - 1.0f) * 0.5f) * (c.uvw_x / c.rx);
+  float v = ((float)y + off.y - (c.ry - 1.0f) * 0.5f) * (c.uvw_y / c.ry);
+  V center = mul(c.R, V{u, v, -c.focal});
+  V focus_point = c.pos + center * (c.focus / c.focal);
+  return mkray(c.pos, normalize(focus_point - c.pos));
+}
+Ray vp_screen_ray(const Cam& c, float su, float sv) {  // camera.h:215-227
+  float x = su * c.rx, y = sv * c.ry;
+  float u = (x - (c.rx - 1.0f) * 0.5f) * (c.uvw_x / c.rx);
+  float v = (y - (c.ry - 1.0f) * 0.5f) * (c.uvw_y / c.ry);
+  return mkray(c.pos, normalize(mul(c.R, V{u, v, -c.focal})));
+}
+
 extern "C" {
 
 struct OracleHandle {
@@ -1479,6 +1542,102 @@ int oracle_scene_render(void* handle, const nr_camera_desc* cam, const nr_render
     });
   }
   for (auto& th : pool) th.join();
+  return 0;
+}
+
+// trace_viewport_kernel (trace.cu:100-162) into float CHW layers.
+int oracle_scene_viewport(void* handle, const nr_camera_desc* cam, uint32_t seed,
+                          int32_t show_axis_grid, float* beauty, float* diffuse, float* normal) {
+  if (!handle || !cam) return -1;
+  const Scene& S = static_cast<OracleHandle*>(handle)->S;
+  Cam c = make_cam(*cam, seed);
+  size_t hw = (size_t)c.W * c.H;
+  for (uint32_t y = 0; y < c.H; ++y)
+    for (uint32_t x = 0; x < c.W; ++x) {
+      size_t i = (size_t)y * c.W + x;
+      Ray ray = vp_center_ray(c, x, y);
+      Hit rec;
+      V b{0, 0, 0}, d{0, 0, 0}, n{0, 0, 0};
+      if (!scene_hit(S, ray, rec)) {
+        V sk = sky(S, ray), gc;
+        float ga;
+        b = (show_axis_grid && vp_triplanar(ray, gc, ga)) ? vp_lerp(sk, gc, ga) : sk;
+      } else {
+        V lv = c.pos - rec.p;
+        float ld = len(lv);
+        float head = dot(normalize(lv), rec.n) * 0.5f + 0.5f;
+        head *= 1.0f / (ld * ld);
+        head = fminf(0.75f, head);
+        float dir = (dot(V{1.0f, 1.0f, 1.0f}, rec.n) + 1.0f) * 0.5f;
+        dir = fmaxf(0.1f, dir);
+        V col = vp_color(S.mats[S.objs[rec.obj].mat]);
+        b = col * fmaxf(head, dir);
+        d = col;
+        n = rec.n;
+      }
+      if (beauty) store(beauty, hw, i, b);
+      if (diffuse) store(diffuse, hw, i, d);
+      if (normal) store(normal, hw, i, n);
+    }
+  return 0;
+}
+
+// hit_test_ray_kernel (trace.cu:168-188)
+int oracle_scene_pick(void* handle, const nr_camera_desc* cam, uint32_t seed, float u, float v,
+                      nr_pick_result* out) {
+  if (!handle || !cam || !out) return -1;
+  const Scene& S = static_cast<OracleHandle*>(handle)->S;
+  Cam c = make_cam(*cam, seed);
+  Hit rec;
+  memset(out, 0, sizeof(*out));
+  out->hit = scene_hit(S, vp_screen_ray(c, u, v), rec) ? 1 : 0;
+  if (out->hit) {
+    out->object_id = (uint32_t)S.objs[rec.obj].id;
+    out->material_id = (uint32_t)S.objs[rec.obj].mat;
+    out->t = rec.t;
+    out->p[0] = rec.p.x;
+    out->p[1] = rec.p.y;
+    out->p[2] = rec.p.z;
+    out->n[0] = rec.n.x;
+    out->n[1] = rec.n.y;
+    out->n[2] = rec.n.z;
+    out->uv[0] = rec.uv.x;
+    out->uv[1] = rec.uv.y;
+    out->front_face = rec.front_face ? 1 : 0;
+  }
+  return 0;
+}
+
+// mask_selected_kernel + build_outline_kernel (scene_interface.cu:3-52)
+int oracle_scene_selection_mask(void* handle, const nr_camera_desc* cam, uint32_t seed,
+                                uint32_t object_id, int32_t radius, uint8_t* out) {
+  if (!handle || !cam || !out) return -1;
+  const Scene& S = static_cast<OracleHandle*>(handle)->S;
+  Cam c = make_cam(*cam, seed);
+  const int W = (int)c.W, H = (int)c.H;
+  std::vector<uint8_t> base((size_t)W * H);
+  for (int y = 0; y < H; ++y)
+    for (int x = 0; x < W; ++x) {
+      Hit rec;
+      float su = ((float)x + 0.5f) / (float)W, sv = ((float)y + 0.5f) / (float)H;
+      bool hit = scene_hit(S, vp_screen_ray(c, su, sv), rec);
+      base[(size_t)y * W + x] = (hit && (uint32_t)S.objs[rec.obj].id == object_id) ? 255u : 0u;
+    }
+  for (int y = 0; y < H; ++y)
+    for (int x = 0; x < W; ++x) {
+      uint8_t v = 0;
+      if (base[(size_t)y * W + x] == 0)
+        for (int dy = -radius; dy <= radius && !v; ++dy)
+          for (int dx = -radius; dx <= radius; ++dx) {
+            int nx = x + dx, ny = y + dy;
+            if (nx < 0 || ny < 0 || nx >= W || ny >= H) continue;
+            if (base[(size_t)ny * W + nx]) {
+              v = 255u;
+              break;
+            }
+          }
+      out[(size_t)y * W + x] = v;
+    }
   return 0;
 }
 

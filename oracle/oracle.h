@@ -71,6 +71,19 @@ void* oracle_scene_create(const or_scene* s, int32_t draw_rtl);
 int oracle_scene_render(void* scene, const nr_camera_desc* cam, const nr_render_config* cfg,
                         const or_request* req);
 void oracle_scene_destroy(void* scene);
+/* viewport preview, picking ray and selection outline on a scene handle */
+int oracle_scene_viewport(void* scene, const nr_camera_desc* cam, uint32_t seed,
+                          int32_t show_axis_grid, float* beauty, float* diffuse, float* normal);
+int oracle_scene_pick(void* scene, const nr_camera_desc* cam, uint32_t seed, float u, float v,
+                      nr_pick_result* out);
+int oracle_scene_selection_mask(void* scene, const nr_camera_desc* cam, uint32_t seed,
+                                uint32_t object_id, int32_t radius, uint8_t* out);
+int refcpu_scene_viewport(void* scene, const nr_camera_desc* cam, uint32_t seed,
+                          int32_t show_axis_grid, float* beauty, float* diffuse, float* normal);
+int refcpu_scene_pick(void* scene, const nr_camera_desc* cam, uint32_t seed, float u, float v,
+                      nr_pick_result* out);
+int refcpu_scene_selection_mask(void* scene, const nr_camera_desc* cam, uint32_t seed,
+                                uint32_t object_id, int32_t radius, uint8_t* out);
 /* Binary-tree SAH cost C = sum_inner A/A_root + sum_leaf A/A_root * N of the
  * reference builder (bvh.h:35-320) over triangle boxes of a mesh. */
 double oracle_mesh_sah(const or_mesh* m, uint64_t* n_nodes);

@@ -14,7 +14,12 @@
 //    with the AOV writes kept in registers;
 //  * a traversal of the reference's mesh BVH that reports which triangle the
 //    closest hit came from (Mesh::hit does not record it), for primary-hit
-//    primitive ids.
+//    primitive ids;
+//  * the per-pixel bodies of trace_viewport_kernel and hit_test_ray_kernel
+//    (engine/src/trace.cu:100-188) and of mask_selected_kernel and
+//    build_outline_kernel (scene/src/scene_interface.cu:3-52), around the
+//    reference's own camera rays, scene traversal, viewport colours, sky and
+//    axis grid.
 // Access to private members is opened with a macro after all standard and
 // pybind11 headers are included.
 #include <algorithm>
@@ -45,6 +50,7 @@
 #include "scene/include/graph.h"
 #include "engine/include/engine/camera.h"
 #include "engine/src/brdf.cu"
+#include "engine/src/axis_grid.cu"
 #undef private
 
 #include "oracle.h"
@@ -368,6 +374,128 @@ int refcpu_scene_render(void* handle, const nr_camera_desc* c, const nr_render_c
         }
     });
   for (auto& th : pool) th.join();
+  return 0;
+}
+
+static CameraParams ref_params(const nr_camera_desc* c) {
+  return CameraParams(Vector2(c->resolution[0], c->resolution[1]),
+                      Vector3(c->position[0], c->position[1], c->position[2]),
+                      Vector3(c->rotation[0], c->rotation[1], c->rotation[2]), c->samples_per_pixel,
+                      c->focal_length, c->focus_distance, c->aperture, c->sensor_width,
+                      c->shutter_speed);
+}
+
+int refcpu_scene_viewport(void* handle, const nr_camera_desc* c, uint32_t seed,
+                          int32_t show_axis_grid, float* beauty, float* diffuse, float* normal) {
+  RefScene* S = static_cast<RefScene*>(handle);
+  CameraParams params = ref_params(c);
+  SampleGenerator sg;
+  std::vector<Vector2> pattern = sg.generate_n_rooks(c->samples_per_pixel, seed);
+  DeviceCamera cam(params, pattern.data());
+  SceneGraph* scene = &S->graph;
+  size_t H = cam.H, W = cam.W, hw = H * W;
+  for (size_t y = 0; y < H; ++y)
+    for (size_t x = 0; x < W; ++x) {
+      size_t i = y * W + x;
+      Color b(0.0f), d(0.0f), n(0.0f);
+      HitRecord rec;
+      Ray ray = cam.get_ray_center((uint32_t)x, (uint32_t)y);
+      bool hit = scene->hit(ray, Interval(EPS, FMAX), rec);
+      if (!hit) {
+        Color grid_color;
+        float grid_alpha;
+        if (show_axis_grid && triplanar_grid(ray, FMAX, grid_color, grid_alpha))
+          b = CG::lerp(scene->skylight->sample(ray), grid_color, grid_alpha);
+        else
+          b = scene->skylight->sample(ray);
+      } else {
+        Vector3 light_vector = cam.p.position - rec.p;
+        float light_dist = light_vector.length();
+        Vector3 headlight_dir = normalize(light_vector);
+        float headlight = dot(headlight_dir, rec.n) * 0.5f + 0.5f;
+        headlight *= 1.0f / (light_dist * light_dist);
+        headlight = fminf(0.75f, headlight);
+        Vector3 directional_light_dir = Vector3(1.0f, 1.0f, 1.0f);
+        float directional = (dot(directional_light_dir, rec.n) + 1.0f) * 0.5f;
+        directional = fmaxf(0.1f, directional);
+        Color col = rec.mat->viewport_color(rec);
+        b = col * fmaxf(headlight, directional);
+        d = col;
+        n = Color(rec.n);
+      }
+      auto put = [&](float* buf, const Color& v) {
+        if (!buf) return;
+        buf[i] = v.r();
+        buf[hw + i] = v.g();
+        buf[2 * hw + i] = v.b();
+      };
+      put(beauty, b);
+      put(diffuse, d);
+      put(normal, n);
+    }
+  return 0;
+}
+
+int refcpu_scene_pick(void* handle, const nr_camera_desc* c, uint32_t seed, float u, float v,
+                      nr_pick_result* out) {
+  RefScene* S = static_cast<RefScene*>(handle);
+  CameraParams params = ref_params(c);
+  SampleGenerator sg;
+  std::vector<Vector2> pattern = sg.generate_n_rooks(c->samples_per_pixel, seed);
+  DeviceCamera cam(params, pattern.data());
+  HitRecord rec;
+  Ray ray = cam.screen_space_ray(u, v);
+  bool hit = S->graph.hit(ray, Interval(EPS, FMAX), rec);
+  memset(out, 0, sizeof(*out));
+  out->hit = hit ? 1 : 0;
+  if (hit) {
+    out->object_id = (uint32_t)rec.object_id;
+    out->material_id = (uint32_t)rec.material_id;
+    out->t = rec.t;
+    for (int k = 0; k < 3; ++k) {
+      out->p[k] = rec.p[k];
+      out->n[k] = rec.n[k];
+    }
+    out->uv[0] = rec.uv.x();
+    out->uv[1] = rec.uv.y();
+    out->front_face = rec.front_face ? 1 : 0;
+  }
+  return 0;
+}
+
+int refcpu_scene_selection_mask(void* handle, const nr_camera_desc* c, uint32_t seed,
+                                uint32_t object_id, int32_t radius, uint8_t* out) {
+  RefScene* S = static_cast<RefScene*>(handle);
+  CameraParams params = ref_params(c);
+  SampleGenerator sg;
+  std::vector<Vector2> pattern = sg.generate_n_rooks(c->samples_per_pixel, seed);
+  DeviceCamera cam(params, pattern.data());
+  const int H = (int)cam.H, W = (int)cam.W;
+  std::vector<uint8_t> base((size_t)H * W);
+  for (int y = 0; y < H; ++y)
+    for (int x = 0; x < W; ++x) {
+      float su = (x + 0.5f) / (float)W;
+      float sv = (y + 0.5f) / (float)H;
+      Ray ray = cam.screen_space_ray(su, sv);
+      HitRecord rec;
+      bool hit = S->graph.hit(ray, Interval(EPS, FMAX), rec);
+      base[(size_t)y * W + x] = (hit && rec.object_id == object_id) ? 255u : 0u;
+    }
+  for (int y = 0; y < H; ++y)
+    for (int x = 0; x < W; ++x) {
+      size_t idx = (size_t)y * W + x;
+      out[idx] = 0u;
+      if (base[idx] != 0) continue;
+      for (int dy = -radius; dy <= radius && !out[idx]; dy++)
+        for (int dx = -radius; dx <= radius; dx++) {
+          int nx = x + dx, ny = y + dy;
+          if (nx < 0 || ny < 0 || nx >= W || ny >= H) continue;
+          if (base[(size_t)ny * W + nx] != 0) {
+            out[idx] = 255u;
+            break;
+          }
+        }
+    }
   return 0;
 }
 

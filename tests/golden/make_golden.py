@@ -13,6 +13,9 @@ Fixtures:
                     HDRI at 20x20: raw layers of sample 1, running mean of
                     samples 1..2, parsed OBJ arrays, HDR floats, SAH cost
   icosphere_l2.obj, sky_32x16.hdr   the input files of mesh_small
+  viewport24.npz    Cornell scene 24x24: viewport preview layers with and
+                    without the axis grid, 8 picking rays, the selection
+                    outline (radius 2) of the object under the centre
 """
 from __future__ import annotations
 
@@ -47,8 +50,28 @@ def local_mesh_spec():
     return spec
 
 
+def viewport_fixture(ref):
+    spec = cornell_spec()
+    h = ref.open_scene(spec, draw_rtl=1)
+    out = {}
+    for grid in (0, 1):
+        b, d, n = h.viewport(bool(grid))
+        out[f"beauty_grid{grid}"], out[f"diffuse_grid{grid}"], out[f"normal_grid{grid}"] = b, d, n
+    uv = np.random.default_rng(1).uniform(0.02, 0.98, size=(8, 2)).astype(np.float32)
+    picks = [h.pick(float(u), float(v)) for u, v in uv]
+    out["pick_uv"] = uv
+    out["pick_hit"] = np.array([int(p["hit"]) for p in picks], np.int32)
+    out["pick_obj"] = np.array([p["object_id"] for p in picks], np.int32)
+    out["pick_t"] = np.array([p["t"] for p in picks], np.float32)
+    oid = h.pick(0.5, 0.5)["object_id"]
+    out["mask_object"] = np.array(oid)
+    out["mask_r2"] = h.selection_mask(oid, 2)
+    np.savez_compressed(HERE / "viewport24.npz", **out)
+
+
 def main():
     ref = oracle.RefCPU()
+    viewport_fixture(ref)
     spec = cornell_spec()
     out = {}
     for s in (1, 2):
