@@ -399,6 +399,25 @@ int nr_render_pick(nr_render* render, float u, float v, nr_pick_result* out);
 int nr_render_selection_mask(nr_render* render, uint32_t object_id, int32_t outline_radius,
                              uint8_t* host_hw);
 
+/* learned denoiser building blocks (no reference counterpart: they replace
+ * the OIDN stage, nectar_render/csrc/data/include/data/denoise.h:21-104) -- */
+/* 3x3 convolution, stride 1, zero padding 1, over NHWC BF16 tensors of B
+ * images of H x W pixels (B*H*W a multiple of 128): y[p, y_off + co] =
+ * act(bias[co] + sum_{tap, ci} x[p + off(tap), x_off + ci] * w[tap][co][ci]),
+ * FP32 accumulation on the tcgen05 tensor cores; act = ReLU when relu != 0.
+ * cin, cout: multiples of 16 up to 256; strides and offsets in channels,
+ * multiples of 8. Device pointers; runs on `stream`. */
+int nr_conv3x3_forward_device(const void* x, int32_t x_stride, int32_t x_off, const void* w,
+                              const float* bias, void* y, int32_t y_stride, int32_t y_off,
+                              int32_t cin, int32_t cout, int32_t B, int32_t H, int32_t W,
+                              int32_t relu, uint64_t stream);
+/* Weight gradient of the same convolution, accumulated into FP32
+ * dw[tap][co][ci] += sum_p dy[p, dy_off + co] * x[p + off(tap), x_off + ci]
+ * (cout <= 128). */
+int nr_conv3x3_wgrad_device(const void* dy, int32_t dy_stride, int32_t dy_off, const void* x,
+                            int32_t x_stride, int32_t x_off, float* dw, int32_t cin,
+                            int32_t cout, int32_t B, int32_t H, int32_t W, uint64_t stream);
+
 /* device-pointer level (callers that own their buffers) -------------------- */
 /* Fused running-mean accumulate of one sample layer into an average layer on
  * the given stream: avg = avg*(n-1)/n + s/n (accumulate_samples_kernel,

@@ -28,6 +28,7 @@
 #include "integrator.cuh"
 #include "wavefront.cuh"
 #include "viewport.cuh"
+#include "conv_tc.cuh"
 
 using namespace nr;
 
@@ -1615,6 +1616,52 @@ int nr_render_last_ms(const nr_render* r, double* out) {
 int nr_render_stream(const nr_render* r, uint64_t* out) {
   if (!r || !out) return fail(NR_ERR_INVALID, "null argument");
   *out = (uint64_t)(uintptr_t)r->stream;
+  return NR_OK;
+}
+
+static uint32_t* conv_err_word() {
+  static uint32_t* d = nullptr;
+  if (!d && cudaMalloc(&d, 4) == cudaSuccess) cudaMemset(d, 0, 4);
+  return d;
+}
+
+int nr_conv3x3_forward_device(const void* x, int32_t x_stride, int32_t x_off, const void* w,
+                              const float* bias, void* y, int32_t y_stride, int32_t y_off,
+                              int32_t cin, int32_t cout, int32_t B, int32_t H, int32_t W,
+                              int32_t relu, uint64_t stream) {
+  if (!x || !w || !y || B < 1 || H < 1 || W < 1) return fail(NR_ERR_INVALID, "bad argument");
+  ConvFwdArgs a{static_cast<const __nv_bfloat16*>(x), x_stride, x_off,
+                static_cast<const __nv_bfloat16*>(w), bias, static_cast<__nv_bfloat16*>(y),
+                y_stride, y_off, cin, cout, B, H, W, relu, conv_err_word()};
+  if (!a.err) return fail(NR_ERR_CUDA, "alloc error word");
+  cudaError_t e = launch_conv_fwd(a, (cudaStream_t)(uintptr_t)stream);
+  if (e == cudaErrorInvalidValue)
+    return fail(NR_ERR_INVALID, "conv3x3: channels must be multiples of 16 (<= 256), strides and "
+                                "offsets multiples of 8");
+  CU(e, "conv3x3 forward");
+  return NR_OK;
+}
+
+int nr_conv3x3_wgrad_device(const void* dy, int32_t dy_stride, int32_t dy_off, const void* x,
+                            int32_t x_stride, int32_t x_off, float* dw, int32_t cin,
+                            int32_t cout, int32_t B, int32_t H, int32_t W, uint64_t stream) {
+  if (!dy || !x || !dw || B < 1 || H < 1 || W < 1) return fail(NR_ERR_INVALID, "bad argument");
+  const int P = B * H * W;
+  const int chunks = (P + 127) / 128;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  // about two CTAs per SM over the 9 taps
+  int per = std::max(1, (chunks * 9 + 2 * sms - 1) / (2 * sms));
+  ConvWgradArgs a{static_cast<const __nv_bfloat16*>(dy), dy_stride, dy_off,
+                  static_cast<const __nv_bfloat16*>(x), x_stride, x_off, dw, cin, cout, B, H, W,
+                  per, conv_err_word()};
+  if (!a.err) return fail(NR_ERR_CUDA, "alloc error word");
+  cudaError_t e = launch_conv_wgrad(a, (cudaStream_t)(uintptr_t)stream);
+  if (e == cudaErrorInvalidValue)
+    return fail(NR_ERR_INVALID, "conv3x3 wgrad: cin multiple of 16 (<= 256), cout multiple of 16 "
+                                "(<= 128), strides and offsets multiples of 8");
+  CU(e, "conv3x3 wgrad");
   return NR_OK;
 }
 

@@ -1,0 +1,298 @@
+// conv_tc.cu — tcgen05 implicit-GEMM 3x3 convolutions (see conv_tc.cuh).
+//
+// Forward / backward-data: one CTA of 128 threads computes a 128-pixel x cout
+// tile. The K loop runs over the 9 taps; per tap the 128 shifted input rows
+// (zero outside the image) and the tap's cout x cin weights are copied into
+// shared memory with cp.async (16-byte chunks, zero-fill at the borders) in
+// the K-major no-swizzle canonical layout, and one thread issues cin / 16
+// MMAs (M = 128, N = cout, K = 16) into a tensor-memory accumulator. Two
+// shared-memory stages alternate: the copy of tap t overlaps the MMAs of tap
+// t - 1; a stage is refilled after the tcgen05.commit of its previous MMAs
+// has arrived on that stage's mbarrier. The epilogue loads the accumulator
+// (tcgen05.ld, one pixel row per thread), adds the bias, applies ReLU and
+// stores BF16.
+//
+// Backward-weights: CTA (g, tap) reduces chunks of 128 pixels: D[co, ci] +=
+// dY^T[co, p] * Xshift^T[ci, p] with both operands MN-major in shared memory
+// (cout rows padded to the M = 128 tile with zeros), then adds its FP32
+// partial sums to dW with atomics.
+#include "conv_tc.cuh"
+#include "tcgen05.cuh"
+
+namespace nr {
+
+namespace {
+
+constexpr int kThreads = 128;
+constexpr uint32_t kWaitLimit = 1u << 26;
+
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, bool valid) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" :: "r"(dst), "l"(src),
+               "r"(valid ? 16u : 0u) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+
+__host__ __device__ inline uint32_t tmem_cols(int n) {
+  return n <= 32 ? 32u : (n <= 64 ? 64u : (n <= 128 ? 128u : 256u));
+}
+
+__device__ __forceinline__ uint4 pack_bf16x8(const float (&v)[8]) {
+  uint4 r;
+  __nv_bfloat162 a = __floats2bfloat162_rn(v[0], v[1]);
+  __nv_bfloat162 b = __floats2bfloat162_rn(v[2], v[3]);
+  __nv_bfloat162 c = __floats2bfloat162_rn(v[4], v[5]);
+  __nv_bfloat162 d = __floats2bfloat162_rn(v[6], v[7]);
+  r.x = *reinterpret_cast<uint32_t*>(&a);
+  r.y = *reinterpret_cast<uint32_t*>(&b);
+  r.z = *reinterpret_cast<uint32_t*>(&c);
+  r.w = *reinterpret_cast<uint32_t*>(&d);
+  return r;
+}
+
+__global__ void __launch_bounds__(kThreads) k_conv_fwd(ConvFwdArgs a) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  __shared__ __align__(8) uint64_t bar[2];
+  __shared__ uint32_t tmem_base;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int cin = a.cin, cout = a.cout;
+  const int P = a.B * a.H * a.W;
+  const int p0 = blockIdx.x * 128;
+  const uint32_t a_bytes = 128u * cin * 2u, b_bytes = (uint32_t)cout * cin * 2u;
+  const uint32_t stage_bytes = a_bytes + b_bytes;
+  const uint32_t base = tc::smem_u32(smem);
+  const uint32_t lbo_a = 128u * 16u, lbo_b = (uint32_t)cout * 16u;
+  const uint32_t ncols = tmem_cols(cout);
+
+  if (tid == 0) {
+    tc::mbar_init(&bar[0], 1);
+    tc::mbar_init(&bar[1], 1);
+  }
+  if (warp == 0) tc::tmem_alloc(&tmem_base, ncols);
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tmem = tmem_base;
+  const uint32_t idesc = tc::idesc_bf16(128, (uint32_t)cout, false, false);
+
+  // this thread's pixel rows (fixed over the taps)
+  bool ok = true;
+  for (int t = 0; t < 9 && ok; ++t) {
+    const int s = t & 1;
+    if (t >= 2) {
+      // CTA-uniform: every thread polls, all agree before any of them leaves
+      const bool w = tc::mbar_wait(&bar[s], (uint32_t)((t >> 1) - 1) & 1u, kWaitLimit);
+      if (!__syncthreads_and(w)) {
+        ok = false;
+        break;
+      }
+    }
+    const uint32_t sa = base + s * stage_bytes, sb = sa + a_bytes;
+    const int dy = t / 3 - 1, dx = t % 3 - 1;
+    const int kg_n = cin >> 3;
+    for (int i = tid; i < 128 * kg_n; i += kThreads) {
+      const int r = i & 127, kg = i >> 7;
+      const int p = p0 + r;
+      bool valid = p < P;
+      const __nv_bfloat16* src = a.x;
+      if (valid) {
+        const int xw = p % a.W, rest = p / a.W;
+        const int yh = rest % a.H, b = rest / a.H;
+        const int sy = yh + dy, sx = xw + dx;
+        valid = sy >= 0 && sy < a.H && sx >= 0 && sx < a.W;
+        if (valid)
+          src = a.x + ((size_t)(b * a.H + sy) * a.W + sx) * a.x_stride + a.x_off + kg * 8;
+      }
+      cp_async16(sa + (uint32_t)r * 16u + (uint32_t)kg * lbo_a, src, valid);
+    }
+    const __nv_bfloat16* wt = a.w + (size_t)t * cout * cin;
+    for (int i = tid; i < cout * kg_n; i += kThreads) {
+      const int n = i % cout, kg = i / cout;
+      cp_async16(sb + (uint32_t)n * 16u + (uint32_t)kg * lbo_b, wt + (size_t)n * cin + kg * 8, true);
+    }
+    cp_async_wait_all();
+    tc::fence_smem_to_async();
+    __syncthreads();
+    if (tid == 0) {
+      tc::fence_after_sync();
+      for (int kk = 0; kk < (cin >> 4); ++kk) {
+        const uint64_t da = tc::smem_desc(sa + 2u * kk * lbo_a, lbo_a, 128u);
+        const uint64_t db = tc::smem_desc(sb + 2u * kk * lbo_b, lbo_b, 128u);
+        tc::mma_bf16(tmem, da, db, idesc, (t > 0 || kk > 0) ? 1u : 0u);
+      }
+      tc::mma_commit(&bar[s]);
+    }
+  }
+  // tap 8 used stage 0 for the fifth time: wait for that phase (parity 0)
+  if (ok) ok = __syncthreads_and(tc::mbar_wait(&bar[0], 0u, kWaitLimit));
+  if (!ok && tid == 0) atomicOr(a.err, 2u);
+  tc::fence_after_sync();
+  __syncthreads();
+  if (ok) {
+    const int p = p0 + warp * 32 + lane;
+    for (int c = 0; c < (cout >> 3); ++c) {
+      float v[8];
+      tc::tmem_ld8(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(c * 8), v);
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        if (a.bias) v[j] += a.bias[c * 8 + j];
+        if (a.relu) v[j] = fmaxf(v[j], 0.0f);
+      }
+      if (p < P)
+        *reinterpret_cast<uint4*>(a.y + (size_t)p * a.y_stride + a.y_off + c * 8) = pack_bf16x8(v);
+    }
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) tc::tmem_dealloc(tmem, ncols);
+}
+
+__global__ void __launch_bounds__(kThreads) k_conv_wgrad(ConvWgradArgs a) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  __shared__ __align__(8) uint64_t bar[2];
+  __shared__ uint32_t tmem_base;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int cin = a.cin, cout = a.cout;
+  const int P = a.B * a.H * a.W;
+  const int n_chunks = (P + 127) / 128;
+  const int tap = blockIdx.y;
+  const int dy = tap / 3 - 1, dx = tap % 3 - 1;
+  const int c0 = blockIdx.x * a.chunks_per_cta;
+  const int c1 = min(n_chunks, c0 + a.chunks_per_cta);
+  const uint32_t lbo = 128u, sbo = 2048u;  // MN-major: 8 pixels x 16 B per K group
+  const uint32_t a_bytes = 16u * sbo;      // 128 (padded) output channels
+  const uint32_t b_bytes = (uint32_t)(cin >> 3) * sbo;
+  const uint32_t stage_bytes = a_bytes + b_bytes;
+  const uint32_t base = tc::smem_u32(smem);
+  const uint32_t ncols = tmem_cols(cin);
+
+  // zero both stages once: rows >= cout of the A tiles stay zero
+  for (uint32_t i = tid * 16u; i < 2u * stage_bytes; i += kThreads * 16u)
+    *reinterpret_cast<uint4*>(smem + i) = make_uint4(0u, 0u, 0u, 0u);
+  if (tid == 0) {
+    tc::mbar_init(&bar[0], 1);
+    tc::mbar_init(&bar[1], 1);
+  }
+  if (warp == 0) tc::tmem_alloc(&tmem_base, ncols);
+  tc::fence_smem_to_async();
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tmem = tmem_base;
+  const uint32_t idesc = tc::idesc_bf16(128, (uint32_t)cin, true, true);
+
+  bool ok = true;
+  int uses[2] = {0, 0};
+  for (int c = c0; c < c1 && ok; ++c) {
+    const int j = c - c0, s = j & 1;
+    if (j >= 2) {
+      const bool w = tc::mbar_wait(&bar[s], (uint32_t)(uses[s] - 1) & 1u, kWaitLimit);
+      if (!__syncthreads_and(w)) {
+        ok = false;
+        break;
+      }
+    }
+    const uint32_t sa = base + s * stage_bytes, sb = sa + a_bytes;
+    const int pbase = c * 128;
+    for (int i = tid; i < (cout >> 3) * 128; i += kThreads) {
+      const int pl = i & 127, cg = i >> 7;
+      const int p = pbase + pl;
+      const bool valid = p < P;
+      const __nv_bfloat16* src = valid ? a.dy + (size_t)p * a.dy_stride + a.dy_off + cg * 8 : a.dy;
+      cp_async16(sa + (uint32_t)cg * sbo + (uint32_t)(pl >> 3) * lbo + (uint32_t)(pl & 7) * 16u,
+                 src, valid);
+    }
+    for (int i = tid; i < (cin >> 3) * 128; i += kThreads) {
+      const int pl = i & 127, cg = i >> 7;
+      const int p = pbase + pl;
+      bool valid = p < P;
+      const __nv_bfloat16* src = a.x;
+      if (valid) {
+        const int xw = p % a.W, rest = p / a.W;
+        const int yh = rest % a.H, b = rest / a.H;
+        const int sy = yh + dy, sx = xw + dx;
+        valid = sy >= 0 && sy < a.H && sx >= 0 && sx < a.W;
+        if (valid)
+          src = a.x + ((size_t)(b * a.H + sy) * a.W + sx) * a.x_stride + a.x_off + cg * 8;
+      }
+      cp_async16(sb + (uint32_t)cg * sbo + (uint32_t)(pl >> 3) * lbo + (uint32_t)(pl & 7) * 16u,
+                 src, valid);
+    }
+    cp_async_wait_all();
+    tc::fence_smem_to_async();
+    __syncthreads();
+    if (tid == 0) {
+      tc::fence_after_sync();
+      for (int kk = 0; kk < 8; ++kk) {
+        const uint64_t da = tc::smem_desc(sa + 2u * kk * lbo, lbo, sbo);
+        const uint64_t db = tc::smem_desc(sb + 2u * kk * lbo, lbo, sbo);
+        tc::mma_bf16(tmem, da, db, idesc, (j > 0 || kk > 0) ? 1u : 0u);
+      }
+      tc::mma_commit(&bar[s]);
+    }
+    uses[s]++;
+  }
+  const int n_local = c1 - c0;
+  if (ok && n_local > 0) {
+    const int s_last = (n_local - 1) & 1;
+    ok = __syncthreads_and(tc::mbar_wait(&bar[s_last], (uint32_t)(uses[s_last] - 1) & 1u, kWaitLimit));
+  }
+  if (!ok && tid == 0) atomicOr(a.err, 2u);
+  tc::fence_after_sync();
+  __syncthreads();
+  if (ok && n_local > 0) {
+    const int co = warp * 32 + lane;
+    for (int cg = 0; cg < (cin >> 3); ++cg) {
+      float v[8];
+      tc::tmem_ld8(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(cg * 8), v);
+      if (co < cout) {
+        float* dst = a.dw + ((size_t)tap * cout + co) * cin + cg * 8;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) atomicAdd(dst + q, v[q]);
+      }
+    }
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) tc::tmem_dealloc(tmem, ncols);
+}
+
+}  // namespace
+
+size_t conv_fwd_smem_bytes(int cin, int cout) {
+  return 2u * (128u * cin * 2u + (size_t)cout * cin * 2u);
+}
+size_t conv_wgrad_smem_bytes(int cin) { return 2u * (16u * 2048u + (size_t)(cin >> 3) * 2048u); }
+
+cudaError_t launch_conv_fwd(const ConvFwdArgs& a, cudaStream_t st) {
+  if (a.cin % 16 || a.cout % 16 || a.cin < 16 || a.cout < 16 || a.cin > 256 || a.cout > 256 ||
+      a.x_stride % 8 || a.x_off % 8 || a.y_stride % 8 || a.y_off % 8)
+    return cudaErrorInvalidValue;
+  const size_t smem = conv_fwd_smem_bytes(a.cin, a.cout);
+  if (smem > 200u * 1024u) return cudaErrorInvalidValue;
+  cudaError_t e = cudaFuncSetAttribute(k_conv_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
+  if (e != cudaSuccess) return e;
+  const int P = a.B * a.H * a.W;
+  k_conv_fwd<<<(P + 127) / 128, kThreads, smem, st>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_conv_wgrad(const ConvWgradArgs& a, cudaStream_t st) {
+  if (a.cin % 16 || a.cout % 16 || a.cin < 16 || a.cout < 16 || a.cin > 256 || a.cout > 128 ||
+      a.x_stride % 8 || a.x_off % 8 || a.dy_stride % 8 || a.dy_off % 8 || a.chunks_per_cta < 1)
+    return cudaErrorInvalidValue;
+  const size_t smem = conv_wgrad_smem_bytes(a.cin);
+  if (smem > 200u * 1024u) return cudaErrorInvalidValue;
+  cudaError_t e = cudaFuncSetAttribute(k_conv_wgrad, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
+  if (e != cudaSuccess) return e;
+  const int P = a.B * a.H * a.W;
+  const int n_chunks = (P + 127) / 128;
+  dim3 grid((n_chunks + a.chunks_per_cta - 1) / a.chunks_per_cta, 9);
+  k_conv_wgrad<<<grid, kThreads, smem, st>>>(a);
+  return cudaGetLastError();
+}
+
+}  // namespace nr
