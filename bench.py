@@ -59,6 +59,8 @@ def parse():
     p.add_argument("--mesh-leaf", type=int, default=1)
     p.add_argument("--no-rmse", action="store_true", help="skip the time-to-RMSE measurement")
     p.add_argument("--rmse-oracle-spp", type=int, default=8192)
+    p.add_argument("--no-denoiser", action="store_true", help="skip training the learned denoiser")
+    p.add_argument("--denoiser-seconds", type=float, default=40.0)
     return p.parse_args()
 
 
@@ -410,18 +412,54 @@ def e2e_public_api(pt, spec, S, args):
             "path": "_pathtracer RenderEngine.render + TransferStream.readback (uint8 CHW)"}
 
 
+def _layer_ptr(render, layer):
+    import ctypes
+    v = ctypes.c_uint64()
+    render.lib.nr_render_layer_device_ptr(render.h, layer, ctypes.byref(v))
+    return v.value
+
+
+def train_denoiser(args, log=None):
+    """Trains the U-Net denoiser on mesh-stress scenes other than the
+    evaluated one (scene seeds 21-23, 256x256): inputs are perf-mode renders
+    at 2, 4 and 8 samples, targets 512-sample renders. Returns (denoiser,
+    info)."""
+    import torch
+    from nectarrender_b200 import capi, denoise
+    t0 = time.perf_counter()
+    pairs = []
+    for ss in (21, 22, 23):
+        spec = scenes.mesh_stress(levels=args.levels, res_h=256, res_w=256, spp=513, depth=12,
+                                  scene_seed=ss)
+        sc = capi.Scene(spec, mesh_leaf=args.mesh_leaf)
+        tgt = capi.Render(sc, mode=capi.MODE_PERF, seed=1000 + ss)
+        tgt.samples(1, 512)
+        target = denoise.render_layers(tgt)[0]
+        for n in (2, 4, 8):
+            r = capi.Render(sc, mode=capi.MODE_PERF, seed=ss)
+            r.samples(1, n)
+            pairs.append((denoise.render_layers(r), target))
+    data_s = time.perf_counter() - t0
+    den = denoise.Denoiser(max_pixels=max(192 * 320, 8 * 128 * 128), seed=7)
+    steps, train_s, loss = denoise.train(den, pairs, seconds=args.denoiser_seconds, crop=128,
+                                         batch=8, log=log)
+    return den, {"training_scenes": 3, "pairs": len(pairs), "data_wall_s": data_s,
+                 "train_steps": steps, "train_wall_s": train_s, "final_loss": loss}
+
+
 def time_to_rmse(args, target=0.01):
     """Device time until the display-referred image sqrt(clamp(x, 0, 1)) is
     within `target` RMSE (all pixels x 3 channels) of an FP64-accumulated
-    high-sample render of the same scene, for perf mode and for the
-    reference estimator. The oracle is rendered in perf mode with another
-    seed: under the HDRI's sun the reference estimator's own high-sample
-    render is still far from converged (its RMSE is reported). Sample counts
-    double between checks, so the reported time is that of the first power
-    of two that reaches the target. The scene is the mesh-stress scene at
-    320x180."""
+    high-sample render of the same scene, for perf mode, the reference
+    estimator and perf mode followed by the learned denoiser. The oracle is
+    rendered in perf mode with another seed: under the HDRI's sun the
+    reference estimator's own high-sample render is still far from
+    converged. Sample counts double between checks; each curve point is
+    (samples, device ms, RMSE), the denoiser's time included. The scene is
+    the mesh-stress scene at 320x192."""
+    import torch
     from nectarrender_b200 import capi
-    h, w = 180, 320
+    h, w = 192, 320
     n_or = args.rmse_oracle_spp
     spec = scenes.mesh_stress(levels=args.levels, res_h=h, res_w=w, spp=n_or + 1)
     sc = capi.Scene(spec, mesh_leaf=args.mesh_leaf)
@@ -434,6 +472,7 @@ def time_to_rmse(args, target=0.01):
     out = {"target_rmse": target, "domain": "sqrt(clamp(x,0,1)), all pixels x 3 channels",
            "workload": f"mesh_stress {w}x{h}, depth {spec.ray_depth}", "oracle_spp": n_or,
            "oracle_wall_s": oracle_s}
+    rmse_of = lambda img: float(np.sqrt(np.mean((np.sqrt(np.clip(img, 0.0, 1.0)) - disp_o) ** 2)))
     for name, mode in (("perf_mode", capi.MODE_PERF), ("reference_estimator", capi.MODE_REFERENCE)):
         r = capi.Render(sc, mode=mode, fp64_accumulate=1, seed=spec.seed)
         done, n, t_ms, rmse = 0, 1, 0.0, float("inf")
@@ -442,8 +481,7 @@ def time_to_rmse(args, target=0.01):
             r.samples(done + 1, n)
             t_ms += r.last_ms()
             done += n
-            img = np.sqrt(np.clip(r.beauty_fp64(), 0.0, 1.0))
-            rmse = float(np.sqrt(np.mean((img - disp_o) ** 2)))
+            rmse = rmse_of(r.beauty_fp64())
             curve.append([done, round(t_ms, 3), round(rmse, 5)])
             if rmse <= target:
                 break
@@ -453,6 +491,43 @@ def time_to_rmse(args, target=0.01):
     a, b = out["reference_estimator"], out["perf_mode"]
     if a["reached"] and b["reached"] and b["device_ms"] > 0:
         out["speedup_perf_vs_reference_estimator"] = a["device_ms"] / b["device_ms"]
+    if not args.no_denoiser:
+        den, info = train_denoiser(args)
+        r = capi.Render(sc, mode=capi.MODE_PERF, seed=spec.seed)
+        dst = torch.empty((1, 3, h, w), dtype=torch.float32, device="cuda")
+        ptrs = [_layer_ptr(r, l) for l in (0, 1, 4)]
+        done, n, t_ms = 0, 1, 0.0
+        curve = []
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        while done + n <= 256:
+            r.samples(done + 1, n)
+            t_ms += r.last_ms()
+            done += n
+            e0.record()
+            den.infer_device(ptrs[0], ptrs[1], ptrs[2], dst.data_ptr(), 1, h, w)
+            e1.record()
+            torch.cuda.synchronize()
+            d_ms = e0.elapsed_time(e1)
+            curve.append([done, round(t_ms + d_ms, 3), round(rmse_of(dst[0].cpu().numpy()), 5)])
+            n = done
+        info["curve_spp_ms_rmse"] = curve
+        info["denoise_ms"] = d_ms
+        # speed-up at equal error against the plain perf-mode curve
+        plain = out["perf_mode"]["curve_spp_ms_rmse"]
+        best = None
+        for spp_d, ms_d, r_d in curve:
+            hit = next((ms for _, ms, rr in plain if rr <= r_d), None)
+            if hit is not None and (best is None or hit / ms_d > best[0]):
+                best = (hit / ms_d, r_d, spp_d)
+        if best:
+            info["speedup_vs_perf_at_equal_rmse"] = {"speedup": best[0], "rmse": best[1],
+                                                     "denoised_spp": best[2]}
+        else:
+            info["speedup_vs_perf_at_equal_rmse"] = (
+                "plain perf mode does not reach the denoised error within "
+                f"{plain[-1][0]} samples")
+        info["reached_target"] = any(rr <= target for _, _, rr in curve)
+        out["learned_denoiser"] = info
     return out
 
 

@@ -418,6 +418,32 @@ int nr_conv3x3_wgrad_device(const void* dy, int32_t dy_stride, int32_t dy_off, c
                             int32_t x_stride, int32_t x_off, float* dw, int32_t cin,
                             int32_t cout, int32_t B, int32_t H, int32_t W, uint64_t stream);
 
+/* Learned denoiser: a five-level U-Net on the beauty, diffuse and
+ * world-normal layers (the inputs the reference hands to OIDN,
+ * nectar_render/csrc/data/include/data/stream.h:160-170), convolutions on
+ * the tcgen05 tensor cores, trained on the GPU. Images are device float
+ * planar CHW, B images of H x W stacked ([B][3][H][W]); H and W multiples of
+ * 16; B*H*W at most the max_pixels given at creation. */
+typedef struct nr_denoiser nr_denoiser;
+int nr_denoiser_create(uint32_t max_pixels, uint32_t seed, nr_denoiser** out);
+int nr_denoiser_destroy(nr_denoiser* d);
+/* One training step toward `target`: forward, L1 loss in log space,
+ * backward and (lr > 0) an Adam update; lr <= 0 only computes gradients.
+ * *loss = mean |log(1+out) - log(1+target)| before the update. */
+int nr_denoiser_train_step(nr_denoiser* d, const float* beauty, const float* diffuse,
+                           const float* normal, const float* target, int32_t B, int32_t H,
+                           int32_t W, float lr, double* loss, uint64_t stream);
+int nr_denoiser_infer(nr_denoiser* d, const float* beauty, const float* diffuse,
+                      const float* normal, float* out, int32_t B, int32_t H, int32_t W,
+                      uint64_t stream);
+/* Parameters (what = 0) or the last step's gradients (what = 1) as host
+ * float arrays, layer by layer: weights [9][cout][cin] then bias [cout]. */
+int nr_denoiser_param_count(const nr_denoiser* d, uint64_t* out);
+int nr_denoiser_get_params(const nr_denoiser* d, int32_t what, float* host);
+int nr_denoiser_set_params(nr_denoiser* d, const float* host);
+/* Layer count and (cin, cout) pairs in parameter order. */
+int nr_denoiser_layers(const nr_denoiser* d, int32_t* count, int32_t* cin_cout);
+
 /* device-pointer level (callers that own their buffers) -------------------- */
 /* Fused running-mean accumulate of one sample layer into an average layer on
  * the given stream: avg = avg*(n-1)/n + s/n (accumulate_samples_kernel,

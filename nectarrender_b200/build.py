@@ -33,7 +33,8 @@ NVCC_FLAGS = ARCH + [
     f"-I{CSRC}", f"-I{INCLUDE}",
 ]
 CU_SOURCES = ["capi.cu", "integrator.cu", "wavefront.cu", "bvh_build.cu", "image_ops.cu",
-              "static_wave.cu", "viewport.cu", "conv_tc.cu"]
+              "static_wave.cu", "viewport.cu", "conv_tc.cu",
+              "denoiser.cu"]
 CPP_SOURCES = ["host_io.cpp"]
 LIB = HERE / "libnectar_b200.so"
 

@@ -29,6 +29,7 @@
 #include "wavefront.cuh"
 #include "viewport.cuh"
 #include "conv_tc.cuh"
+#include "denoiser.cuh"
 
 using namespace nr;
 
@@ -1662,6 +1663,81 @@ int nr_conv3x3_wgrad_device(const void* dy, int32_t dy_stride, int32_t dy_off, c
     return fail(NR_ERR_INVALID, "conv3x3 wgrad: cin multiple of 16 (<= 256), cout multiple of 16 "
                                 "(<= 128), strides and offsets multiples of 8");
   CU(e, "conv3x3 wgrad");
+  return NR_OK;
+}
+
+}  // extern "C"
+
+struct nr_denoiser {
+  Denoiser d;
+};
+
+extern "C" {
+
+int nr_denoiser_create(uint32_t max_pixels, uint32_t seed, nr_denoiser** out) {
+  if (!out) return fail(NR_ERR_INVALID, "null argument");
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return fail(NR_ERR_NO_DEVICE, "no CUDA device");
+  auto d = std::make_unique<nr_denoiser>();
+  std::string e = denoiser_create(d->d, max_pixels, seed);
+  if (!e.empty()) return fail(e.find("must") != std::string::npos ? NR_ERR_INVALID : NR_ERR_CUDA, e);
+  *out = d.release();
+  return NR_OK;
+}
+
+int nr_denoiser_destroy(nr_denoiser* d) {
+  delete d;
+  return NR_OK;
+}
+
+static int den_status(const std::string& e) {
+  if (e.empty()) return NR_OK;
+  if (e.find("must") != std::string::npos || e.find("exceeds") != std::string::npos)
+    return fail(NR_ERR_INVALID, e);
+  if (e.find("timed out") != std::string::npos) return fail(NR_ERR_DEVICE, e);
+  return fail(NR_ERR_CUDA, e);
+}
+
+int nr_denoiser_train_step(nr_denoiser* d, const float* beauty, const float* diffuse,
+                           const float* normal, const float* target, int32_t B, int32_t H,
+                           int32_t W, float lr, double* loss, uint64_t stream) {
+  if (!d || !beauty || !target) return fail(NR_ERR_INVALID, "null argument");
+  cudaStream_t st = (cudaStream_t)(uintptr_t)stream;
+  int rc = den_status(denoiser_forward_backward(d->d, beauty, diffuse, normal, target, B, H, W,
+                                                loss, st));
+  if (rc != NR_OK || lr <= 0.0f) return rc;
+  return den_status(denoiser_adam(d->d, lr, st));
+}
+
+int nr_denoiser_infer(nr_denoiser* d, const float* beauty, const float* diffuse,
+                      const float* normal, float* out, int32_t B, int32_t H, int32_t W,
+                      uint64_t stream) {
+  if (!d || !beauty || !out) return fail(NR_ERR_INVALID, "null argument");
+  return den_status(denoiser_infer(d->d, beauty, diffuse, normal, out, B, H, W,
+                                   (cudaStream_t)(uintptr_t)stream));
+}
+
+int nr_denoiser_param_count(const nr_denoiser* d, uint64_t* out) {
+  if (!d || !out) return fail(NR_ERR_INVALID, "null argument");
+  *out = denoiser_param_count(d->d);
+  return NR_OK;
+}
+
+int nr_denoiser_get_params(const nr_denoiser* d, int32_t what, float* host) {
+  if (!d || !host || what < 0 || what > 1) return fail(NR_ERR_INVALID, "bad argument");
+  return den_status(denoiser_get(d->d, what, host));
+}
+
+int nr_denoiser_set_params(nr_denoiser* d, const float* host) {
+  if (!d || !host) return fail(NR_ERR_INVALID, "null argument");
+  return den_status(denoiser_set_weights(d->d, host));
+}
+
+int nr_denoiser_layers(const nr_denoiser* d, int32_t* count, int32_t* cin_cout) {
+  if (!d || !count) return fail(NR_ERR_INVALID, "null argument");
+  *count = denoiser_layer_count(d->d);
+  if (cin_cout)
+    for (int i = 0; i < *count; ++i) denoiser_layer_shape(d->d, i, cin_cout + 2 * i, cin_cout + 2 * i + 1);
   return NR_OK;
 }
 
