@@ -421,21 +421,22 @@ def _layer_ptr(render, layer):
 
 def train_denoiser(args, log=None):
     """Trains the U-Net denoiser on mesh-stress scenes other than the
-    evaluated one (scene seeds 21-23, 256x256): inputs are perf-mode renders
-    at 2, 4 and 8 samples, targets 512-sample renders. Returns (denoiser,
-    info)."""
+    evaluated one (scene seeds 21-28, icosphere level 6, 256x256): inputs are
+    perf-mode renders at 1 to 16 samples, targets 1024-sample renders.
+    Returns (denoiser, info)."""
     import torch
     from nectarrender_b200 import capi, denoise
     t0 = time.perf_counter()
     pairs = []
-    for ss in (21, 22, 23):
-        spec = scenes.mesh_stress(levels=args.levels, res_h=256, res_w=256, spp=513, depth=12,
+    seeds = range(21, 29)
+    for ss in seeds:
+        spec = scenes.mesh_stress(levels=6, res_h=256, res_w=256, spp=1025, depth=12,
                                   scene_seed=ss)
         sc = capi.Scene(spec, mesh_leaf=args.mesh_leaf)
         tgt = capi.Render(sc, mode=capi.MODE_PERF, seed=1000 + ss)
-        tgt.samples(1, 512)
+        tgt.samples(1, 1024)
         target = denoise.render_layers(tgt)[0]
-        for n in (2, 4, 8):
+        for n in (1, 2, 4, 8, 16):
             r = capi.Render(sc, mode=capi.MODE_PERF, seed=ss)
             r.samples(1, n)
             pairs.append((denoise.render_layers(r), target))
@@ -443,7 +444,7 @@ def train_denoiser(args, log=None):
     den = denoise.Denoiser(max_pixels=max(192 * 320, 8 * 128 * 128), seed=7)
     steps, train_s, loss = denoise.train(den, pairs, seconds=args.denoiser_seconds, crop=128,
                                          batch=8, log=log)
-    return den, {"training_scenes": 3, "pairs": len(pairs), "data_wall_s": data_s,
+    return den, {"training_scenes": len(seeds), "pairs": len(pairs), "data_wall_s": data_s,
                  "train_steps": steps, "train_wall_s": train_s, "final_loss": loss}
 
 
@@ -475,6 +476,8 @@ def time_to_rmse(args, target=0.01):
     rmse_of = lambda img: float(np.sqrt(np.mean((np.sqrt(np.clip(img, 0.0, 1.0)) - disp_o) ** 2)))
     for name, mode in (("perf_mode", capi.MODE_PERF), ("reference_estimator", capi.MODE_REFERENCE)):
         r = capi.Render(sc, mode=mode, fp64_accumulate=1, seed=spec.seed)
+        r.samples(1, 1)  # first call allocates the wave state: not part of the curve
+        r.reset()
         done, n, t_ms, rmse = 0, 1, 0.0, float("inf")
         curve = []
         while done + n <= n_or // 2:
@@ -494,8 +497,11 @@ def time_to_rmse(args, target=0.01):
     if not args.no_denoiser:
         den, info = train_denoiser(args)
         r = capi.Render(sc, mode=capi.MODE_PERF, seed=spec.seed)
+        r.samples(1, 1)  # first call allocates the wave state: not part of the curve
+        r.reset()
         dst = torch.empty((1, 3, h, w), dtype=torch.float32, device="cuda")
         ptrs = [_layer_ptr(r, l) for l in (0, 1, 4)]
+        den.infer_device(ptrs[0], ptrs[1], ptrs[2], dst.data_ptr(), 1, h, w)  # warm-up
         done, n, t_ms = 0, 1, 0.0
         curve = []
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

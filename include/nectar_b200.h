@@ -427,9 +427,10 @@ int nr_conv3x3_wgrad_device(const void* dy, int32_t dy_stride, int32_t dy_off, c
 typedef struct nr_denoiser nr_denoiser;
 int nr_denoiser_create(uint32_t max_pixels, uint32_t seed, nr_denoiser** out);
 int nr_denoiser_destroy(nr_denoiser* d);
-/* One training step toward `target`: forward, L1 loss in log space,
- * backward and (lr > 0) an Adam update; lr <= 0 only computes gradients.
- * *loss = mean |log(1+out) - log(1+target)| before the update. */
+/* One training step toward `target`: forward, squared-error loss in log
+ * space, backward and (lr > 0) an Adam update; lr <= 0 only computes
+ * gradients. *loss = mean 0.5 (log(1+out) - log(1+target))^2 before the
+ * update. */
 int nr_denoiser_train_step(nr_denoiser* d, const float* beauty, const float* diffuse,
                            const float* normal, const float* target, int32_t B, int32_t H,
                            int32_t W, float lr, double* loss, uint64_t stream);

@@ -52,9 +52,12 @@ __global__ void k_prep(const float* beauty, const float* diffuse, const float* n
   }
 }
 
-// L1 loss in log space; d(loss)/d(pred) = sign(pred - log(1 + target)) on the
-// first three output channels (Adam is invariant to the gradient scale, so
-// the 1/N of the mean is left out), zero on the others.
+// Squared error in log space, 0.5 * (pred - log(1 + target))^2 on the first
+// three output channels; d(loss)/d(pred) = pred - log(1 + target) (Adam is
+// invariant to the gradient scale, so the 1/N of the mean is left out), zero
+// on the others. A squared error estimates the conditional mean of the noisy
+// targets (an absolute error would estimate their median, which sits below
+// the mean under the heavy-tailed noise of path tracing).
 __global__ void k_loss(View out, const float* target, View dout, int B, int H, int W,
                        double* loss) {
   const size_t hw = (size_t)H * W, P = (size_t)B * hw;
@@ -64,8 +67,8 @@ __global__ void k_loss(View out, const float* target, View dout, int B, int H, i
     for (int c = 0; c < 3; ++c) {
       const float t = log1pf(fmaxf(target[b * 3 * hw + c * hw + i], 0.0f));
       const float d = ld(out, p, c) - t;
-      local += fabs((double)d);
-      st(dout, p, c, d > 0.0f ? 1.0f : (d < 0.0f ? -1.0f : 0.0f));
+      local += 0.5 * (double)d * (double)d;
+      st(dout, p, c, d);
     }
     for (int c = 3; c < dout.ch; ++c) st(dout, p, c, 0.0f);
   }

@@ -10,7 +10,7 @@
 //   encoder  32, 48, 64, 80, 96 (two convolutions per level)
 //   decoder  80, 64, 48, 32 (two convolutions per level, after concat)
 //   output   16 (first 3 = log(1 + beauty), no activation)
-// Loss: L1 in log space; Adam.
+// Loss: squared error in log space; Adam.
 #pragma once
 #include <cuda_bf16.h>
 #include <cstdint>

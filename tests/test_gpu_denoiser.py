@@ -76,9 +76,9 @@ def unet_grads(params, x0, target):
         below = b
     out = conv(below, *P[i]); acts[i] = (below, out)
     d = out[..., :3] - target
-    loss = np.abs(d).mean()
+    loss = (0.5 * d * d).mean()
     g_out = np.zeros_like(out)
-    g_out[..., :3] = np.sign(d)
+    g_out[..., :3] = d
     grads = [None] * len(P)
     dskip = {}
     dw, db, dx = conv_bwd(g_out, acts[i][0], P[i][0]); grads[i] = (dw, db)
