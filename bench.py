@@ -333,6 +333,9 @@ def run_ours(args):
     rmse = None
     if rank == 0 and world == 1 and not args.no_rmse:
         rmse = time_to_rmse(args)
+    learned = None
+    if rank == 0 and world == 1 and not args.no_denoiser:
+        learned = learned_kernels(peaks)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -365,6 +368,7 @@ def run_ours(args):
                 "cpu_baseline": cpu,
                 "reference_cuda": ref_cuda,
                 "time_to_rmse": rmse,
+                "learned_kernels": learned,
                 "scene": {"build_ms_device": stats["build_ms"], "build_wall_s": build_wall,
                           "triangles": stats["n_triangles"], "wide_nodes": stats["wide_nodes"],
                           "sah_cost_binary": stats["sah_cost_binary"]},
@@ -410,6 +414,58 @@ def e2e_public_api(pt, spec, S, args):
     return {"value": v, "unit": "samples/s", "h2d_bytes_per_step": h2d,
             "d2h_bytes_per_step": 3 * w * h,
             "path": "_pathtracer RenderEngine.render + TransferStream.readback (uint8 CHW)"}
+
+
+def learned_kernels(peaks):
+    """Tensor-core throughput of the denoiser's convolutions on one large
+    layer (4 x 256 x 256 pixels, 96 -> 96 channels: 43.5 GFLOP per pass),
+    timed with CUDA events, and the denoiser's inference time on a full
+    1920 x 1088 frame."""
+    import ctypes as C
+    import torch
+    from nectarrender_b200 import capi, denoise
+    lib = capi.library()
+    B, H, W, ci, co = 4, 256, 256, 96, 96
+    P = B * H * W
+    flops = 2.0 * P * 9 * ci * co
+    x = torch.randn(P, ci, device="cuda").to(torch.bfloat16)
+    w = (torch.randn(9, co, ci, device="cuda") * 0.05).to(torch.bfloat16)
+    y = torch.empty(P, co, device="cuda", dtype=torch.bfloat16)
+    dw = torch.zeros(9, co, ci, device="cuda")
+    s = C.c_uint64(torch.cuda.current_stream().cuda_stream)
+    vp = lambda t: C.c_void_p(t.data_ptr())
+    fwd = lambda: lib.nr_conv3x3_forward_device(vp(x), ci, 0, vp(w), None, vp(y), co, 0, ci, co, B, H,
+                                                W, 1, s)
+    wg = lambda: lib.nr_conv3x3_wgrad_device(vp(y), co, 0, vp(x), ci, 0,
+                                             C.cast(dw.data_ptr(), C.POINTER(C.c_float)), ci, co, B,
+                                             H, W, s)
+    out = {}
+    peak = float(peaks.get("bf16_tflops", 1590.0))
+    for name, fn in (("conv3x3_forward", fwd), ("conv3x3_weight_gradient", wg)):
+        for _ in range(3):
+            assert fn() == 0, capi.library().nr_last_error()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(10):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / 10
+        tf = flops / (ms * 1e-3) / 1e12
+        out[name] = {"shape": f"{B}x{H}x{W}, {ci}->{co}", "ms": ms, "tflops": tf, "bound": "tensor",
+                     "peak_tflops": peak, "frac": tf / peak}
+    den = denoise.Denoiser(max_pixels=1920 * 1088, seed=0)
+    img = [torch.rand(1, 3, 1088, 1920, device="cuda") for _ in range(3)]
+    o = torch.empty_like(img[0])
+    den.infer(*img, out=o)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(5):
+        den.infer(*img, out=o)
+    e1.record()
+    torch.cuda.synchronize()
+    out["denoiser_infer_1920x1088_ms"] = e0.elapsed_time(e1) / 5
+    return out
 
 
 def _layer_ptr(render, layer):
