@@ -173,6 +173,10 @@ typedef struct nr_render_config {
                                0 = default (514)                            */
   uint32_t samples_per_wave;/* wavefront: sample indices per wave (0 = ~8M paths) */
   int32_t use_graphs;       /* wavefront: replay each wave as a CUDA graph (1) */
+  uint32_t tail_max_paths;  /* wavefront, reference mode: from bounce 4 on, a
+                               queue of at most this many paths is finished
+                               by one per-path launch (0 = 131072,
+                               0xFFFFFFFF = never)                          */
 } nr_render_config;
 
 /* StreamConfig display fields (nectar_render/csrc/data/include/data/stream.h:13-30). */

@@ -1232,6 +1232,9 @@ static KernelParams make_params(nr_render* r, uint32_t first, uint32_t count, bo
 // (4 CTAs per SM) for the later bounces; 12% faster per sample than either
 // alone on the 1.31 M-triangle mesh scene at 1920x1080.
 constexpr int32_t kDefaultExtendVariant = 514;
+// Queue length below which the last bounces of a wave run as one per-path
+// launch (wavefront.cu, k_wf_tail).
+constexpr uint32_t kDefaultTailPaths = 131072;
 
 static uint32_t waves_of(nr_render* r) {
   if (r->cfg.samples_per_wave > 0) return std::min(16u, r->cfg.samples_per_wave);
@@ -1303,6 +1306,8 @@ static int launch(nr_render* r, const KernelParams& P, WaveTimer* tm) {
   WfParams W = r->wf;
   W.kp = P;
   W.extend_variant = r->cfg.extend_variant > 0 ? r->cfg.extend_variant : kDefaultExtendVariant;
+  W.tail_max_paths = r->cfg.tail_max_paths == 0 ? kDefaultTailPaths
+                     : (r->cfg.tail_max_paths == UINT32_MAX ? 0u : r->cfg.tail_max_paths);
   CU(wf_set_base(W, P.first_sample, r->stream), "set wave base");
   if (tm) tm->mark(NR_KERNEL_ROTATE, r->stream);
   for (uint32_t s = 0; s < P.n_samples; s += per) {
@@ -1415,6 +1420,8 @@ int nr_render_samples_static(nr_render* r, uint32_t first, uint32_t count) {
     WfParams w = W;
     w.kp = P;
     w.extend_variant = r->cfg.extend_variant > 0 ? r->cfg.extend_variant : kDefaultExtendVariant;
+    w.tail_max_paths = 0;  // the tail kernel's per-thread stack could make the driver grow its
+                           // local-memory reservation, an allocation this entry point avoids
     w.base = first + s;
     w.count = std::min(per, count - s);
     CU(wf_launch_wave(w, r->counters_on, r->stream), "launch wavefront");

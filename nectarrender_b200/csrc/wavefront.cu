@@ -37,7 +37,16 @@ enum : uint32_t {
   CTR_BASE = 4,    // first sample index of the current wave
   CTR_SH = 5,      // shadow rays queued by this bounce's shade (perf mode)
   CTR_SHWORK = 6,  // shadow kernel work counter
+  CTR_TAIL = 7,    // set once the tail kernel has finished the wave's paths
 };
+
+// Tail hand-off (reference mode): once a wave's queue has shrunk to at most
+// kTailMaxPaths paths after bounce kTailFrom or later, one launch finishes
+// every remaining path to its end, one path per thread, instead of one
+// extend and one shade launch per remaining bounce. The last bounces carry
+// few, long paths (glass and mirror chains): as separate launches each costs
+// the latency of its slowest ray; in one launch those latencies overlap.
+constexpr uint32_t kTailFrom = 3;
 
 // The wave's first sample index is read from device memory, so that the
 // launches of a wave do not depend on it and one captured graph serves every
@@ -312,6 +321,7 @@ __global__ void k_wf_generate(WfParams W) {
     W.ctr[CTR_WORK] = 0u;
     W.ctr[CTR_SH] = 0u;
     W.ctr[CTR_SHWORK] = 0u;
+    W.ctr[CTR_TAIL] = 0u;
   }
 }
 
@@ -320,6 +330,7 @@ __global__ void k_wf_generate(WfParams W) {
 template <bool kCount, int kMinBlocks>
 __global__ void __launch_bounds__(kExtThreads, kMinBlocks) k_wf_extend(WfParams W, int qsel,
                                                                        int identity) {
+  if (W.ctr[CTR_TAIL]) return;
   extern __shared__ uint2 wf_smem[];
   const KernelParams& P = W.kp;
   const uint32_t n = W.ctr[qsel];
@@ -402,6 +413,7 @@ constexpr size_t kFlatSmemBytes = kExtStackBytes + sizeof(uint32_t) * FS_COUNT *
 template <bool kCount, int kMinBlocks>
 __global__ void __launch_bounds__(kExtThreads, kMinBlocks) k_wf_extend_flat(WfParams W, int qsel,
                                                                             int identity) {
+  if (W.ctr[CTR_TAIL]) return;
   extern __shared__ uint2 wf_smem[];
   const KernelParams& P = W.kp;
   const DevScene& sc = P.scene;
@@ -646,6 +658,7 @@ __global__ void __launch_bounds__(kExtThreads, kMinBlocks) k_wf_extend_flat(WfPa
 // reference's estimator draw for draw.
 template <bool kPerf>
 __global__ void __launch_bounds__(kShadeThreads) k_wf_shade(WfParams W, int qsel, int identity) {
+  if (W.ctr[CTR_TAIL]) return;
   __shared__ uint2 shade_stk[kBlasStack * kShadeThreads];
   const KernelParams& P = W.kp;
   const DevScene& sc = P.scene;
@@ -806,6 +819,49 @@ __global__ void __launch_bounds__(kShadeThreads) k_wf_shade(WfParams W, int qsel
 
 // Shadow rays of one bounce (perf mode): an unoccluded ray adds its
 // precomputed contribution to the path's beauty.
+// Finishes every path of queue `qsel` with the per-path loop of the
+// megakernel (bounce_ref: the same estimator and draws as k_wf_shade), when
+// there are at most `max_paths` of them and the tail has not run yet.
+__global__ void __launch_bounds__(128) k_wf_tail(WfParams W, int qsel, uint32_t max_paths) {
+  if (W.ctr[CTR_TAIL]) return;
+  const uint32_t n = W.ctr[qsel];
+  if (n == 0u || n > max_paths) return;
+  const KernelParams& P = W.kp;
+  const uint32_t* queue = qsel == 0 ? W.queue0 : W.queue1;
+  const uint32_t N = P.W * P.H;
+  const uint32_t wbase = wave_base(W);
+  TraceStats st{0u, 0u, 0u};
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint32_t p = __ldg(queue + i);
+    const float4 o = W.ray_o[p], d = W.ray_d[p], at = W.atten[p], ab = W.acc_b[p], ad = W.acc_d[p],
+                 an = W.acc_n[p];
+    PathState s;
+    s.ray = make_ray(V3{o.x, o.y, o.z}, V3{d.x, d.y, d.z}, o.w);
+    s.atten = V3{at.x, at.y, at.z};
+    s.beauty = V3{ab.x, ab.y, ab.z};
+    s.diffuse = V3{ad.x, ad.y, ad.z};
+    s.normal = V3{an.x, an.y, an.z};
+    s.primary = __float_as_uint(ab.w);
+    s.bounce = __float_as_uint(d.w);
+    const uint32_t k = p / N, pix = p - k * N;
+    Rng g;
+    g.init(P.seed, pix + (wbase + k) * N, __float_as_uint(at.w));
+    while (bounce_ref(P, s, g, st)) {
+    }
+    W.acc_b[p] = make_float4(s.beauty.x, s.beauty.y, s.beauty.z, __uint_as_float(s.primary));
+    W.acc_d[p] = make_float4(s.diffuse.x, s.diffuse.y, s.diffuse.z, 0.f);
+    W.acc_n[p] = make_float4(s.normal.x, s.normal.y, s.normal.z, 0.f);
+  }
+}
+
+// Marks the wave finished when k_wf_tail took its queue (a separate launch,
+// so that no CTA of the tail kernel can see the mark before its own work).
+__global__ void k_wf_tail_mark(WfParams W, int qsel, uint32_t max_paths) {
+  if (threadIdx.x != 0 || W.ctr[CTR_TAIL]) return;
+  const uint32_t n = W.ctr[qsel];
+  if (n > 0u && n <= max_paths) W.ctr[CTR_TAIL] = 1u;
+}
+
 __global__ void __launch_bounds__(kExtThreads) k_wf_shadow(WfParams W) {
   extern __shared__ uint2 wf_smem[];
   const KernelParams& P = W.kp;
@@ -1042,6 +1098,14 @@ cudaError_t wf_launch_wave(const WfParams& W, bool counters, cudaStream_t st, Wa
     }
     k_wf_rotate<<<1, 32, 0, st>>>(W, q);
     if (tm) tm->mark(NR_KERNEL_ROTATE, st);
+    if (!W.mis_pdf && !counters && W.tail_max_paths > 0 && b >= kTailFrom && b + 1 < P.depth) {
+      const int tail_blocks = (int)std::min<uint32_t>((W.tail_max_paths + 127) / 128,
+                                                      (uint32_t)sm_count() * 8);
+      k_wf_tail<<<tail_blocks, 128, 0, st>>>(W, 1 - q, W.tail_max_paths);
+      if (tm) tm->mark(NR_KERNEL_EXTEND, st);
+      k_wf_tail_mark<<<1, 32, 0, st>>>(W, 1 - q, W.tail_max_paths);
+      if (tm) tm->mark(NR_KERNEL_ROTATE, st);
+    }
   }
   int acc_blocks = (int)std::min<uint32_t>((P.W * P.H + 255) / 256, (uint32_t)sm_count() * 16);
   k_wf_accumulate<<<acc_blocks, 256, 0, st>>>(W);

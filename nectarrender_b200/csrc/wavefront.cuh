@@ -12,7 +12,8 @@ struct WfParams {
                    // each wave's last launch)
   uint32_t count;  // sample indices in the wave
   uint32_t capacity;
-  int32_t extend_variant;  // 4, 5, 6 or 8 CTAs per SM
+  int32_t extend_variant;  // traversal kernel (see extend_fn)
+  uint32_t tail_max_paths; // tail hand-off bound (0: none)
   float4* ray_o;
   float4* ray_d;
   float4* atten;
