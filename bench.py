@@ -57,6 +57,8 @@ def parse():
     p.add_argument("--extend-variant", type=int, default=0,
                    help="traversal kernel variant (0: library default; see autotune.py)")
     p.add_argument("--mesh-leaf", type=int, default=1)
+    p.add_argument("--shade-variant", type=int, default=0,
+                   help="shading kernel register budget (0: library default)")
     p.add_argument("--no-rmse", action="store_true", help="skip the time-to-RMSE measurement")
     p.add_argument("--rmse-oracle-spp", type=int, default=8192)
     p.add_argument("--no-denoiser", action="store_true", help="skip training the learned denoiser")
@@ -217,7 +219,7 @@ def run_ours(args):
     build_wall = time.perf_counter() - t_build
     stats = scene.stats()
     render = capi.Render(scene, schedule=1 if args.schedule == "wavefront" else 0,
-                         extend_variant=args.extend_variant)
+                         extend_variant=args.extend_variant, shade_variant=args.shade_variant)
     stream_handle = ctypes.c_uint64()
     lib.nr_render_stream(render.h, ctypes.byref(stream_handle))
     stream = torch.cuda.ExternalStream(stream_handle.value)

@@ -177,6 +177,9 @@ typedef struct nr_render_config {
                                queue of at most this many paths is finished
                                by one per-path launch (0 = 131072,
                                0xFFFFFFFF = never)                          */
+  int32_t shade_variant;    /* wavefront shading kernel register budget: 5 or
+                               6 CTAs of 128 threads per SM, any other value
+                               128 registers; 0 = default (6)               */
 } nr_render_config;
 
 /* StreamConfig display fields (nectar_render/csrc/data/include/data/stream.h:13-30). */

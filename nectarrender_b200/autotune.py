@@ -12,6 +12,8 @@ speed but never the image:
     0 and b for the later bounces;
   * ``samples_per_wave`` - sample indices in flight per wave, i.e. the length
     of the path queues (paths = W*H*samples_per_wave);
+  * ``shade_variant`` - register budget of the shading kernel (5 or 6 CTAs
+    per SM, or 128 registers);
   * ``schedule`` - wavefront or the per-pixel megakernel.
 
 Every candidate renders the same samples (the parity tests cover each knob),
@@ -37,13 +39,14 @@ class Tuning:
     tlas_leaf: int = 1
     extend_variant: int = 514
     samples_per_wave: int = 0
+    shade_variant: int = 6
     schedule: int = capi.SCHEDULE_WAVEFRONT
     ms_per_sample: float = 0.0
     table: list = field(default_factory=list)
 
     def render_overrides(self) -> dict:
-        return {"extend_variant": self.extend_variant,
-                "samples_per_wave": self.samples_per_wave, "schedule": self.schedule}
+        return {"extend_variant": self.extend_variant, "samples_per_wave": self.samples_per_wave,
+                "shade_variant": self.shade_variant, "schedule": self.schedule}
 
     def scene_overrides(self) -> dict:
         return {"mesh_leaf": self.mesh_leaf, "tlas_leaf": self.tlas_leaf}
@@ -68,17 +71,18 @@ def _time(scene: capi.Scene, spec: SceneSpec, over: dict, samples: int, reps: in
 
 
 def tune(spec: SceneSpec, samples: int = 4, reps: int = 2, leaves=((1, 1), (2, 1), (3, 1), (1, 2)),
-         variants=VARIANTS, waves=(0, 2, 4, 8), megakernel: bool = True) -> Tuning:
+         variants=VARIANTS, waves=(0, 2, 4, 8), shades=(5, 6), megakernel: bool = True) -> Tuning:
     """Times every candidate on `spec` (device time of `samples` sample
     indices, best of `reps`) and returns the fastest as a :class:`Tuning`."""
     table = []
     best = None
     for mesh_leaf, tlas_leaf in leaves:
         scene = capi.Scene(spec, mesh_leaf=mesh_leaf, tlas_leaf=tlas_leaf)
-        cands = [dict(extend_variant=v, samples_per_wave=w, schedule=capi.SCHEDULE_WAVEFRONT)
-                 for v, w in itertools.product(variants, waves)]
+        cands = [dict(extend_variant=v, samples_per_wave=w, shade_variant=sv,
+                      schedule=capi.SCHEDULE_WAVEFRONT)
+                 for v, w, sv in itertools.product(variants, waves, shades)]
         if megakernel:
-            cands.append(dict(extend_variant=0, samples_per_wave=0,
+            cands.append(dict(extend_variant=0, samples_per_wave=0, shade_variant=0,
                               schedule=capi.SCHEDULE_MEGAKERNEL))
         for over in cands:
             ms = _time(scene, spec, over, samples, reps)
@@ -88,7 +92,8 @@ def tune(spec: SceneSpec, samples: int = 4, reps: int = 2, leaves=((1, 1), (2, 1
                 best = row
         del scene
     t = Tuning(**{k: best[k] for k in ("mesh_leaf", "tlas_leaf", "extend_variant",
-                                       "samples_per_wave", "schedule", "ms_per_sample")})
+                                       "samples_per_wave", "shade_variant", "schedule",
+                                       "ms_per_sample")})
     t.table = table
     return t
 

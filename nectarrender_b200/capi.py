@@ -45,7 +45,8 @@ class RenderConfig(C.Structure):
                 ("rr_start_bounce", C.c_uint32), ("rr_survival", C.c_float), ("mode", C.c_int32),
                 ("schedule", C.c_int32), ("fp64_accumulate", C.c_int32), ("layer_mask", C.c_uint32),
                 ("extend_variant", C.c_int32), ("samples_per_wave", C.c_uint32),
-                ("use_graphs", C.c_int32), ("tail_max_paths", C.c_uint32)]
+                ("use_graphs", C.c_int32), ("tail_max_paths", C.c_uint32),
+                ("shade_variant", C.c_int32)]
 
 
 class StreamConfig(C.Structure):

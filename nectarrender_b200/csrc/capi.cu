@@ -1235,6 +1235,10 @@ constexpr int32_t kDefaultExtendVariant = 514;
 // Queue length below which the last bounces of a wave run as one per-path
 // launch (wavefront.cu, k_wf_tail).
 constexpr uint32_t kDefaultTailPaths = 131072;
+// Shading kernel register budget for 6 CTAs of 128 threads per SM: spills a
+// little, but the occupancy gain hides more memory latency (9% less time per
+// sample than 128 registers on the 1.31 M-triangle scene).
+constexpr int32_t kDefaultShadeVariant = 6;
 
 static uint32_t waves_of(nr_render* r) {
   if (r->cfg.samples_per_wave > 0) return std::min(16u, r->cfg.samples_per_wave);
@@ -1306,6 +1310,7 @@ static int launch(nr_render* r, const KernelParams& P, WaveTimer* tm) {
   WfParams W = r->wf;
   W.kp = P;
   W.extend_variant = r->cfg.extend_variant > 0 ? r->cfg.extend_variant : kDefaultExtendVariant;
+  W.shade_variant = r->cfg.shade_variant > 0 ? r->cfg.shade_variant : kDefaultShadeVariant;
   W.tail_max_paths = r->cfg.tail_max_paths == 0 ? kDefaultTailPaths
                      : (r->cfg.tail_max_paths == UINT32_MAX ? 0u : r->cfg.tail_max_paths);
   CU(wf_set_base(W, P.first_sample, r->stream), "set wave base");
@@ -1420,6 +1425,7 @@ int nr_render_samples_static(nr_render* r, uint32_t first, uint32_t count) {
     WfParams w = W;
     w.kp = P;
     w.extend_variant = r->cfg.extend_variant > 0 ? r->cfg.extend_variant : kDefaultExtendVariant;
+    w.shade_variant = r->cfg.shade_variant > 0 ? r->cfg.shade_variant : kDefaultShadeVariant;
     w.tail_max_paths = 0;  // the tail kernel's per-thread stack could make the driver grow its
                            // local-memory reservation, an allocation this entry point avoids
     w.base = first + s;

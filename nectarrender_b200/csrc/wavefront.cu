@@ -656,8 +656,9 @@ __global__ void __launch_bounds__(kExtThreads, kMinBlocks) k_wf_extend_flat(WfPa
 
 // kPerf: NR_MODE_PERF (next-event estimation + MIS); otherwise the
 // reference's estimator draw for draw.
-template <bool kPerf>
-__global__ void __launch_bounds__(kShadeThreads) k_wf_shade(WfParams W, int qsel, int identity) {
+template <bool kPerf, int kMinBlocks>
+__global__ void __launch_bounds__(kShadeThreads, kMinBlocks) k_wf_shade(WfParams W, int qsel,
+                                                                      int identity) {
   if (W.ctr[CTR_TAIL]) return;
   __shared__ uint2 shade_stk[kBlasStack * kShadeThreads];
   const KernelParams& P = W.kp;
@@ -1088,12 +1089,17 @@ cudaError_t wf_launch_wave(const WfParams& W, bool counters, cudaStream_t st, Wa
     else ext<<<eb, kExtThreads, smem, st>>>(W, q, 0);
     if (tm) tm->mark(NR_KERNEL_EXTEND, st);
     if (W.mis_pdf) {
-      k_wf_shade<true><<<shade_blocks, kShadeThreads, 0, st>>>(W, q, b == 0 ? 1 : 0);
+      k_wf_shade<true, 1><<<shade_blocks, kShadeThreads, 0, st>>>(W, q, b == 0 ? 1 : 0);
       if (tm) tm->mark(NR_KERNEL_SHADE, st);
       k_wf_shadow<<<sm_count() * 4, kExtThreads, kExtStackBytes, st>>>(W);
       if (tm) tm->mark(NR_KERNEL_EXTEND, st);
     } else {
-      k_wf_shade<false><<<shade_blocks, kShadeThreads, 0, st>>>(W, q, b == 0 ? 1 : 0);
+      if (W.shade_variant == 5)
+        k_wf_shade<false, 5><<<shade_blocks, kShadeThreads, 0, st>>>(W, q, b == 0 ? 1 : 0);
+      else if (W.shade_variant == 6)
+        k_wf_shade<false, 6><<<shade_blocks, kShadeThreads, 0, st>>>(W, q, b == 0 ? 1 : 0);
+      else
+        k_wf_shade<false, 1><<<shade_blocks, kShadeThreads, 0, st>>>(W, q, b == 0 ? 1 : 0);
       if (tm) tm->mark(NR_KERNEL_SHADE, st);
     }
     k_wf_rotate<<<1, 32, 0, st>>>(W, q);

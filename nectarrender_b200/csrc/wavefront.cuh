@@ -14,6 +14,7 @@ struct WfParams {
   uint32_t capacity;
   int32_t extend_variant;  // traversal kernel (see extend_fn)
   uint32_t tail_max_paths; // tail hand-off bound (0: none)
+  int32_t shade_variant;   // 5 or 6: register budget for that many CTAs per SM; else none
   float4* ray_o;
   float4* ray_d;
   float4* atten;

@@ -93,6 +93,7 @@ def test_mesh_hdri_samples(mesh_scene, orc, refcuda, s):
 
 @pytest.mark.parametrize("variant,mesh_leaf,tlas_leaf,spw,schedule", [
     (4, 3, 1, 0, capi.SCHEDULE_WAVEFRONT),
+    (1004, 1, 1, 0, capi.SCHEDULE_WAVEFRONT),   # 128-register shading kernel, tail off
     (6, 1, 2, 1, capi.SCHEDULE_WAVEFRONT),
     (8, 2, 3, 3, capi.SCHEDULE_WAVEFRONT),
     (5, 1, 1, 0, capi.SCHEDULE_MEGAKERNEL),
@@ -107,7 +108,10 @@ def test_tuning_knobs_do_not_change_samples(mesh_scene, refcuda, variant, mesh_l
     may pick renders the same per-sample images."""
     spec, _, _ = mesh_scene
     sc = capi.Scene(spec, mesh_leaf=mesh_leaf, tlas_leaf=tlas_leaf)
-    r = capi.Render(sc, extend_variant=variant, samples_per_wave=spw, schedule=schedule)
+    extra = {}
+    if variant >= 1000:  # other shading kernel and no tail hand-off
+        variant, extra = variant - 1000, {"shade_variant": 4, "tail_max_paths": 0xFFFFFFFF}
+    r = capi.Render(sc, extend_variant=variant, samples_per_wave=spw, schedule=schedule, **extra)
     r.samples(1, 3)
     acc = r.layer(0)
     rb, *_ = refcuda.render(spec, 1, count=3, mode=1)
