@@ -148,6 +148,116 @@ __global__ void __launch_bounds__(kThreads) k_conv_fwd(ConvFwdArgs a) {
   if (warp == 0) tc::tmem_dealloc(tmem, ncols);
 }
 
+// Halo-tile forward: the CTA's 128 output pixels are an 8 x 16 block of one
+// image. Its 10 x 18 halo (zero outside the image) is copied into shared
+// memory once, K-major with 8-pixel core rows: halo pixel h = hy * 10 + hx at
+// byte h * 16 within each 8-channel group, groups 180 * 16 bytes apart. The
+// operand of tap (dy, dx) is then the same region seen from start address
+// (dy * 10 + dx) * 16 with a row-group stride (SBO) of one halo row, 160
+// bytes: no per-tap gather. Only the tap's weights are streamed, through two
+// stages.
+constexpr int kTileW = 8, kTileH = 16;
+constexpr int kHaloW = kTileW + 2, kHaloH = kTileH + 2, kHalo = kHaloW * kHaloH;
+
+__global__ void __launch_bounds__(kThreads) k_conv_fwd_halo(ConvFwdArgs a) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  __shared__ __align__(8) uint64_t bar[2];
+  __shared__ uint32_t tmem_base;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int cin = a.cin, cout = a.cout;
+  const int x0 = blockIdx.x * kTileW, y0 = blockIdx.y * kTileH, b = blockIdx.z;
+  const uint32_t lbo_a = (uint32_t)kHalo * 16u, sbo_a = (uint32_t)kHaloW * 16u;
+  const uint32_t a_bytes = (uint32_t)(cin >> 3) * lbo_a;
+  const uint32_t b_bytes = (uint32_t)cout * cin * 2u, lbo_b = (uint32_t)cout * 16u;
+  const uint32_t base = tc::smem_u32(smem);
+  const uint32_t sa = base, sb0 = base + a_bytes;
+  const uint32_t ncols = tmem_cols(cout);
+  const int kg_n = cin >> 3;
+
+  if (tid == 0) {
+    tc::mbar_init(&bar[0], 1);
+    tc::mbar_init(&bar[1], 1);
+  }
+  if (warp == 0) tc::tmem_alloc(&tmem_base, ncols);
+  // halo and the weights of tap 0
+  for (int i = tid; i < kHalo * kg_n; i += kThreads) {
+    const int h = i % kHalo, kg = i / kHalo;
+    const int yy = y0 - 1 + h / kHaloW, xx = x0 - 1 + h % kHaloW;
+    const bool valid = yy >= 0 && yy < a.H && xx >= 0 && xx < a.W;
+    const __nv_bfloat16* src =
+        valid ? a.x + ((size_t)(b * a.H + yy) * a.W + xx) * a.x_stride + a.x_off + kg * 8 : a.x;
+    cp_async16(sa + (uint32_t)kg * lbo_a + (uint32_t)h * 16u, src, valid);
+  }
+  for (int i = tid; i < cout * kg_n; i += kThreads) {
+    const int n = i % cout, kg = i / cout;
+    cp_async16(sb0 + (uint32_t)n * 16u + (uint32_t)kg * lbo_b, a.w + (size_t)n * cin + kg * 8, true);
+  }
+  cp_async_wait_all();
+  tc::fence_smem_to_async();
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tmem = tmem_base;
+  const uint32_t idesc = tc::idesc_bf16(128, (uint32_t)cout, false, false);
+
+  bool ok = true;
+  for (int t = 0; t < 9; ++t) {
+    const int s = t & 1;
+    const uint32_t sb = sb0 + s * b_bytes;
+    if (tid == 0) {
+      tc::fence_after_sync();
+      const uint32_t tap_off = (uint32_t)((t / 3) * kHaloW + (t % 3)) * 16u;
+      for (int kk = 0; kk < (cin >> 4); ++kk) {
+        const uint64_t da = tc::smem_desc(sa + tap_off + 2u * kk * lbo_a, lbo_a, sbo_a);
+        const uint64_t db = tc::smem_desc(sb + 2u * kk * lbo_b, lbo_b, 128u);
+        tc::mma_bf16(tmem, da, db, idesc, (t > 0 || kk > 0) ? 1u : 0u);
+      }
+      tc::mma_commit(&bar[s]);
+    }
+    if (t + 1 < 9) {
+      const int s1 = (t + 1) & 1;
+      if (t + 1 >= 2) {
+        // stage s1 last held tap t - 1: wait for its MMAs
+        const bool w = tc::mbar_wait(&bar[s1], (uint32_t)((t - 1) >> 1) & 1u, kWaitLimit);
+        if (!__syncthreads_and(w)) {
+          ok = false;
+          break;
+        }
+      }
+      const uint32_t sbn = sb0 + s1 * b_bytes;
+      const __nv_bfloat16* wt = a.w + (size_t)(t + 1) * cout * cin;
+      for (int i = tid; i < cout * kg_n; i += kThreads) {
+        const int n = i % cout, kg = i / cout;
+        cp_async16(sbn + (uint32_t)n * 16u + (uint32_t)kg * lbo_b, wt + (size_t)n * cin + kg * 8, true);
+      }
+      cp_async_wait_all();
+      tc::fence_smem_to_async();
+      __syncthreads();
+    }
+  }
+  if (ok) ok = __syncthreads_and(tc::mbar_wait(&bar[0], 0u, kWaitLimit));
+  if (!ok && tid == 0) atomicOr(a.err, 2u);
+  tc::fence_after_sync();
+  __syncthreads();
+  if (ok) {
+    const int r = warp * 32 + lane;
+    const size_t p = (size_t)(b * a.H + y0 + r / kTileW) * a.W + x0 + r % kTileW;
+    for (int c = 0; c < (cout >> 3); ++c) {
+      float v[8];
+      tc::tmem_ld8(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(c * 8), v);
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        if (a.bias) v[j] += a.bias[c * 8 + j];
+        if (a.relu) v[j] = fmaxf(v[j], 0.0f);
+      }
+      *reinterpret_cast<uint4*>(a.y + p * a.y_stride + a.y_off + c * 8) = pack_bf16x8(v);
+    }
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) tc::tmem_dealloc(tmem, ncols);
+}
+
 __global__ void __launch_bounds__(kThreads) k_conv_wgrad(ConvWgradArgs a) {
   extern __shared__ __align__(1024) unsigned char smem[];
   __shared__ __align__(8) uint64_t bar[2];
@@ -269,6 +379,15 @@ cudaError_t launch_conv_fwd(const ConvFwdArgs& a, cudaStream_t st) {
   if (a.cin % 16 || a.cout % 16 || a.cin < 16 || a.cout < 16 || a.cin > 256 || a.cout > 256 ||
       a.x_stride % 8 || a.x_off % 8 || a.y_stride % 8 || a.y_off % 8)
     return cudaErrorInvalidValue;
+  const size_t halo_smem = (size_t)(a.cin >> 3) * kHalo * 16u + 2u * (size_t)a.cout * a.cin * 2u;
+  if (a.W % kTileW == 0 && a.H % kTileH == 0 && halo_smem <= 200u * 1024u) {
+    cudaError_t e = cudaFuncSetAttribute(k_conv_fwd_halo,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)halo_smem);
+    if (e != cudaSuccess) return e;
+    dim3 grid(a.W / kTileW, a.H / kTileH, a.B);
+    k_conv_fwd_halo<<<grid, kThreads, halo_smem, st>>>(a);
+    return cudaGetLastError();
+  }
   const size_t smem = conv_fwd_smem_bytes(a.cin, a.cout);
   if (smem > 200u * 1024u) return cudaErrorInvalidValue;
   cudaError_t e = cudaFuncSetAttribute(k_conv_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize,
