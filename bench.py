@@ -62,6 +62,7 @@ def parse():
     p.add_argument("--no-rmse", action="store_true", help="skip the time-to-RMSE measurement")
     p.add_argument("--rmse-oracle-spp", type=int, default=8192)
     p.add_argument("--no-denoiser", action="store_true", help="skip training the learned denoiser")
+    p.add_argument("--no-multi", action="store_true", help="skip the multi-scene measurement")
     p.add_argument("--denoiser-seconds", type=float, default=40.0)
     return p.parse_args()
 
@@ -335,6 +336,9 @@ def run_ours(args):
     rmse = None
     if rank == 0 and world == 1 and not args.no_rmse:
         rmse = time_to_rmse(args)
+    multi = None
+    if rank == 0 and world == 1 and not args.no_multi:
+        multi = multi_scene(args)
     learned = None
     if rank == 0 and world == 1 and not args.no_denoiser:
         learned = learned_kernels(peaks)
@@ -371,6 +375,7 @@ def run_ours(args):
                 "reference_cuda": ref_cuda,
                 "time_to_rmse": rmse,
                 "learned_kernels": learned,
+                "multi_scene": multi,
                 "scene": {"build_ms_device": stats["build_ms"], "build_wall_s": build_wall,
                           "triangles": stats["n_triangles"], "wide_nodes": stats["wide_nodes"],
                           "sah_cost_binary": stats["sah_cost_binary"]},
@@ -416,6 +421,50 @@ def e2e_public_api(pt, spec, S, args):
     return {"value": v, "unit": "samples/s", "h2d_bytes_per_step": h2d,
             "d2h_bytes_per_step": 3 * w * h,
             "path": "_pathtracer RenderEngine.render + TransferStream.readback (uint8 CHW)"}
+
+
+def multi_scene(args):
+    """A set of 16 small scenes (scenes.scene_set: Cornell boxes and
+    mesh-stress scenes, 256-512 pixels a side, 16-64 samples, depth 4-16):
+    all samples of every scene rendered one scene after another, as the
+    reference does with one RenderEngine per scene, and in one
+    nr_render_samples_batch call; host wall time around each (both block
+    until the renders are done)."""
+    from nectarrender_b200 import capi
+    specs = scenes.scene_set(16, seed=0)
+    scs = [capi.Scene(s, mesh_leaf=args.mesh_leaf) for s in specs]
+    counts = [s.camera["samples_per_pixel"] - 1 for s in specs]
+    px = [int(s.camera["resolution"][0]) * int(s.camera["resolution"][1]) for s in specs]
+    total = float(sum(p * c for p, c in zip(px, counts)))
+    out = {"scenes": len(specs), "pixel_samples": total}
+    for mode in ("sequential", "batched"):
+        best = None
+        for _ in range(3):
+            rs = [capi.Render(sc) for sc in scs]
+            for r in rs:  # first call allocates: keep it out of the timing
+                r.samples(1, 1)
+                r.reset()
+            t0 = time.perf_counter()
+            if mode == "sequential":
+                for r, c in zip(rs, counts):
+                    r.samples(1, c)
+            else:
+                capi.render_batch(rs, [1] * len(rs), counts)
+            dt = time.perf_counter() - t0
+            best = dt if best is None else min(best, dt)
+        out[mode] = {"wall_s": best, "samples_per_s": total / best}
+    out["speedup"] = out["sequential"]["wall_s"] / out["batched"]["wall_s"]
+    if not args.no_reference_cuda:
+        try:
+            import oracle
+            rc = oracle.RefCUDA()
+            ms = sum(rc.render(s, 1, count=c, mode=1)[3] for s, c in zip(specs, counts))
+            out["reference_cuda"] = {"device_s": ms * 1e-3, "samples_per_s": total / (ms * 1e-3),
+                                     "note": "reference render loop per scene (sm_100a build), "
+                                             "CUDA events, scene builds excluded"}
+        except Exception as e:  # noqa: BLE001 - reported, not fatal
+            out["reference_cuda"] = {"unavailable": repr(e)[:200]}
+    return out
 
 
 def learned_kernels(peaks):

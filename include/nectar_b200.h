@@ -318,6 +318,15 @@ int nr_render_reset(nr_render* render);
  * render() loop is first = 1, count = samples_per_pixel - 1 (engine.cpp:43). */
 int nr_render_samples(nr_render* render, uint32_t first, uint32_t count);
 
+/* Renders several scenes at once: renders[i] gets sample indices
+ * [first[i], first[i] + count[i]) as nr_render_samples would, but every
+ * render's launches are queued on its own stream before any is waited for,
+ * so small scenes share the GPU instead of running one after another (the
+ * reference renders a scene set with one RenderEngine at a time). A render
+ * may appear once per batch. */
+int nr_render_samples_batch(nr_render* const* renders, uint32_t n, const uint32_t* first,
+                            const uint32_t* count);
+
 /* nr_render_samples_static: no counterpart in the reference.
  * Renders exactly like nr_render_samples (same sample indices, same layers,
  * same results; always the wavefront schedule) but allocates no device memory

@@ -99,7 +99,8 @@ EXPORTS = [
     "nr_scene_set_tuning", "nr_scene_build",
     "nr_scene_get_stats", "nr_scene_get_binary_bvh", "nr_render_config_default",
     "nr_render_create", "nr_render_destroy", "nr_render_reset", "nr_render_samples",
-    "nr_render_samples_static", "nr_render_set_profiling", "nr_render_get_profile",
+    "nr_render_samples_static", "nr_render_samples_batch", "nr_render_set_profiling",
+    "nr_render_get_profile",
     "nr_render_graph_stats", "nr_render_viewport", "nr_render_pick", "nr_render_selection_mask",
     "nr_conv3x3_forward_device", "nr_conv3x3_wgrad_device",
     "nr_denoiser_create", "nr_denoiser_destroy", "nr_denoiser_train_step", "nr_denoiser_infer",
@@ -261,6 +262,15 @@ class Scene:
 
 def _fptr(a: np.ndarray | None):
     return None if a is None else a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def render_batch(renders, first, count) -> None:
+    """nr_render_samples_batch over Render objects (first/count: lists)."""
+    n = len(renders)
+    hs = (C.c_void_p * n)(*[r.h.value for r in renders])
+    fa = (C.c_uint32 * n)(*first)
+    ca = (C.c_uint32 * n)(*count)
+    _check(library().nr_render_samples_batch(hs, n, fa, ca), "nr_render_samples_batch")
 
 
 class Render:

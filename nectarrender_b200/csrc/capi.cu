@@ -1326,10 +1326,10 @@ static int launch(nr_render* r, const KernelParams& P, WaveTimer* tm) {
   return NR_OK;
 }
 
-static int run_kernel(nr_render* r, const KernelParams& P) {
+// Enqueues a render call on the render's stream (events around it).
+static int enqueue_kernel(nr_render* r, const KernelParams& P, WaveTimer& tm) {
   if (r->counters_on) CU(cudaMemsetAsync(r->counters, 0, 8 * 5, r->stream), "clear counters");
   CU(cudaEventRecord(r->ev0, r->stream), "event");
-  WaveTimer tm;
   if (r->profile_on) {
     CU(cudaEventRecord(r->pev[0], r->stream), "event");
     tm.ev = r->pev.data() + 1;
@@ -1339,6 +1339,11 @@ static int run_kernel(nr_render* r, const KernelParams& P) {
   int rc = launch(r, P, r->profile_on ? &tm : nullptr);
   if (rc != NR_OK) return rc;
   CU(cudaEventRecord(r->ev1, r->stream), "event");
+  return NR_OK;
+}
+
+// Waits for an enqueued call and reads its timing, error word and counters.
+static int finish_kernel(nr_render* r, const KernelParams& P, const WaveTimer& tm) {
   CU(cudaEventSynchronize(r->ev1), "integrator");
   float ms = 0.f;
   cudaEventElapsedTime(&ms, r->ev0, r->ev1);
@@ -1373,6 +1378,13 @@ static int run_kernel(nr_render* r, const KernelParams& P) {
   return NR_OK;
 }
 
+static int run_kernel(nr_render* r, const KernelParams& P) {
+  WaveTimer tm;
+  int rc = enqueue_kernel(r, P, tm);
+  if (rc != NR_OK) return rc;
+  return finish_kernel(r, P, tm);
+}
+
 int nr_render_samples(nr_render* r, uint32_t first, uint32_t count) {
   if (!r) return fail(NR_ERR_INVALID, "null render");
   if (count == 0) return NR_OK;
@@ -1382,6 +1394,37 @@ int nr_render_samples(nr_render* r, uint32_t first, uint32_t count) {
   KernelParams P = make_params(r, first, count, false);
   int rc = run_kernel(r, P);
   if (rc == NR_OK) r->n64 = first + count - 1;
+  return rc;
+}
+
+int nr_render_samples_batch(nr_render* const* renders, uint32_t n, const uint32_t* first,
+                            const uint32_t* count) {
+  if (!renders || (n && (!first || !count))) return fail(NR_ERR_INVALID, "null argument");
+  for (uint32_t i = 0; i < n; ++i) {
+    nr_render* r = renders[i];
+    if (!r) return fail(NR_ERR_INVALID, "null render in batch");
+    if (first[i] == 0) return fail(NR_ERR_INVALID, "sample indices start at 1");
+    if ((uint64_t)first[i] + count[i] > r->cam.samples_per_pixel)
+      return fail(NR_ERR_INVALID, "sample index beyond samples_per_pixel");
+    for (uint32_t j = 0; j < i; ++j)
+      if (renders[j] == r) return fail(NR_ERR_INVALID, "a render appears twice in the batch");
+  }
+  std::vector<KernelParams> ps(n);
+  std::vector<WaveTimer> tms(n);
+  int rc = NR_OK;
+  uint32_t queued = 0;
+  for (; queued < n && rc == NR_OK; ++queued) {
+    if (count[queued] == 0) continue;
+    ps[queued] = make_params(renders[queued], first[queued], count[queued], false);
+    rc = enqueue_kernel(renders[queued], ps[queued], tms[queued]);
+  }
+  // every enqueued call is waited for, also after a failure
+  for (uint32_t i = 0; i < queued; ++i) {
+    if (count[i] == 0) continue;
+    int ri = finish_kernel(renders[i], ps[i], tms[i]);
+    if (ri == NR_OK) renders[i]->n64 = first[i] + count[i] - 1;
+    else if (rc == NR_OK) rc = ri;
+  }
   return rc;
 }
 

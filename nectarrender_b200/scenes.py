@@ -377,3 +377,26 @@ def to_pathtracer(spec: SceneSpec, pt=None):
         c["sensor_width"], c["shutter_speed"])
     cam = pt.engine.camera.Camera(params)
     return scene, cam, (hittables, lights, sky)
+
+
+def scene_set(n: int = 16, seed: int = 0, max_level: int = 6) -> list[SceneSpec]:
+    """A seeded set of small scenes of mixed size for the multi-scene
+    workload: Cornell boxes and mesh-stress scenes (icosphere levels 3 to
+    max_level), resolutions 256 to 512 in steps of 16, 16 to 64 samples,
+    depth 4 to 16."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        res = int(rng.integers(16, 33)) * 16
+        spp = int(rng.choice([16, 32, 64]))
+        depth = int(rng.integers(4, 17))
+        if i % 4 == 0:
+            s = cornell(res=res, spp=spp, depth=depth, seed=int(rng.integers(1 << 16)))
+        else:
+            s = mesh_stress(levels=int(rng.integers(3, max_level + 1)), res_h=res,
+                            res_w=int(rng.integers(16, 33)) * 16, spp=spp, depth=depth,
+                            n_spheres=int(rng.integers(8, 65)), hdri_size=(256, 128),
+                            scene_seed=100 + i)
+        s.name = f"set{seed}_{i}"
+        out.append(s)
+    return out
