@@ -379,7 +379,7 @@ __global__ void __launch_bounds__(kExtThreads, kMinBlocks) k_wf_extend(WfParams 
 // so a warp no longer waits for its slowest ray. The order in which nodes and
 // primitives are visited per ray is the one of trace_closest, so the closest
 // hit (ties included) is the same.
-constexpr uint32_t kRefill = 12;
+// (kRefill: a template parameter of the kernel, 12 by default.)
 
 __device__ __forceinline__ uint32_t octant_inv4(const V3& d) {
   uint32_t oct = (d.x < 0.0f ? 4u : 0u) | (d.y < 0.0f ? 2u : 0u) | (d.z < 0.0f ? 1u : 0u);
@@ -410,7 +410,7 @@ enum : uint32_t {
 constexpr size_t kExtStackBytes = sizeof(uint2) * (kTlasStack + kBlasStack) * kExtThreads;
 constexpr size_t kFlatSmemBytes = kExtStackBytes + sizeof(uint32_t) * FS_COUNT * kExtThreads;
 
-template <bool kCount, int kMinBlocks>
+template <bool kCount, int kMinBlocks, uint32_t kRefill = 12>
 __global__ void __launch_bounds__(kExtThreads, kMinBlocks) k_wf_extend_flat(WfParams W, int qsel,
                                                                             int identity) {
   if (W.ctr[CTR_TAIL]) return;
@@ -1040,6 +1040,10 @@ static ExtendFn extend_fn(bool counters, int variant) {
     case 15: return counters ? k_wf_extend_flat<true, 5> : k_wf_extend_flat<false, 5>;
     case 16: return counters ? k_wf_extend_flat<true, 6> : k_wf_extend_flat<false, 6>;
     case 18: return counters ? k_wf_extend_flat<true, 8> : k_wf_extend_flat<false, 8>;
+    // 24 / 34 / 44: as 14 with lanes refilled once 8 / 16 / 24 of them are idle
+    case 24: return counters ? k_wf_extend_flat<true, 4, 8> : k_wf_extend_flat<false, 4, 8>;
+    case 34: return counters ? k_wf_extend_flat<true, 4, 16> : k_wf_extend_flat<false, 4, 16>;
+    case 44: return counters ? k_wf_extend_flat<true, 4, 24> : k_wf_extend_flat<false, 4, 24>;
     default: return counters ? k_wf_extend<true, 4> : k_wf_extend<false, 4>;
   }
 }
