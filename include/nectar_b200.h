@@ -461,6 +461,31 @@ int nr_denoiser_set_params(nr_denoiser* d, const float* host);
 /* Layer count and (cin, cout) pairs in parameter order. */
 int nr_denoiser_layers(const nr_denoiser* d, int32_t* count, int32_t* cin_cout);
 
+/* Neural radiance cache (no reference counterpart): a multiresolution
+ * hash-grid encoding of position (16 levels x 2 features, 2^19 entries per
+ * level, resolutions 16..2048 inside [lo, hi]) plus direction, normal,
+ * roughness and albedo, into a 64-wide, 4-layer MLP whose GEMMs run on the
+ * tcgen05 tensor cores; trained online with a relative squared error.
+ * Queries are device float [count][16]: position, roughness, outgoing
+ * direction (unit, away from the surface), -, normal, -, diffuse albedo, -.
+ * Radiance in and out: device float [count][3]. */
+typedef struct nr_nrc nr_nrc;
+int nr_nrc_create(uint32_t max_queries, const float lo[3], const float hi[3], uint32_t seed,
+                  nr_nrc** out);
+int nr_nrc_destroy(nr_nrc* n);
+int nr_nrc_infer(nr_nrc* n, const float* queries, uint32_t count, float* radiance,
+                 uint64_t stream);
+/* One Adam step (lr <= 0: gradients only); *loss (if not null) = mean
+ * relative squared error before the step. */
+int nr_nrc_train(nr_nrc* n, const float* queries, const float* target, uint32_t count,
+                 float lr, double* loss, uint64_t stream);
+/* Host copies: what = 0 MLP weights ([64][64] x 3 then [16][64], out x in),
+ * 1 their gradients, 2 grid values, 3 grid gradients, 4 the encoded inputs
+ * of the last train call ([count][64]). */
+int nr_nrc_count(const nr_nrc* n, int32_t what, uint64_t* out);
+int nr_nrc_get(const nr_nrc* n, int32_t what, float* host);
+int nr_nrc_set(nr_nrc* n, const float* mlp, const float* grid);
+
 /* device-pointer level (callers that own their buffers) -------------------- */
 /* Fused running-mean accumulate of one sample layer into an average layer on
  * the given stream: avg = avg*(n-1)/n + s/n (accumulate_samples_kernel,

@@ -105,7 +105,8 @@ EXPORTS = [
     "nr_conv3x3_forward_device", "nr_conv3x3_wgrad_device",
     "nr_denoiser_create", "nr_denoiser_destroy", "nr_denoiser_train_step", "nr_denoiser_infer",
     "nr_denoiser_param_count", "nr_denoiser_get_params", "nr_denoiser_set_params",
-    "nr_denoiser_layers",
+    "nr_denoiser_layers", "nr_nrc_create", "nr_nrc_destroy", "nr_nrc_infer", "nr_nrc_train",
+    "nr_nrc_count", "nr_nrc_get", "nr_nrc_set",
     "nr_render_sample_layers", "nr_render_layer_device_ptr", "nr_render_read_layer",
     "nr_render_read_beauty_fp64", "nr_render_readback", "nr_render_display_float",
     "nr_render_dims", "nr_render_set_counters", "nr_render_get_counters", "nr_render_last_ms",

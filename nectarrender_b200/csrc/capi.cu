@@ -30,6 +30,7 @@
 #include "viewport.cuh"
 #include "conv_tc.cuh"
 #include "denoiser.cuh"
+#include "nrc.cuh"
 
 using namespace nr;
 
@@ -1728,6 +1729,10 @@ struct nr_denoiser {
   Denoiser d;
 };
 
+struct nr_nrc {
+  Nrc n;
+};
+
 extern "C" {
 
 int nr_denoiser_create(uint32_t max_pixels, uint32_t seed, nr_denoiser** out) {
@@ -1748,7 +1753,8 @@ int nr_denoiser_destroy(nr_denoiser* d) {
 
 static int den_status(const std::string& e) {
   if (e.empty()) return NR_OK;
-  if (e.find("must") != std::string::npos || e.find("exceeds") != std::string::npos)
+  if (e.find("must") != std::string::npos || e.find("exceeds") != std::string::npos ||
+      e.find("more queries") != std::string::npos)
     return fail(NR_ERR_INVALID, e);
   if (e.find("timed out") != std::string::npos) return fail(NR_ERR_DEVICE, e);
   return fail(NR_ERR_CUDA, e);
@@ -1795,6 +1801,53 @@ int nr_denoiser_layers(const nr_denoiser* d, int32_t* count, int32_t* cin_cout) 
   if (cin_cout)
     for (int i = 0; i < *count; ++i) denoiser_layer_shape(d->d, i, cin_cout + 2 * i, cin_cout + 2 * i + 1);
   return NR_OK;
+}
+
+int nr_nrc_create(uint32_t max_queries, const float lo[3], const float hi[3], uint32_t seed,
+                  nr_nrc** out) {
+  if (!out || !lo || !hi) return fail(NR_ERR_INVALID, "null argument");
+  int nd = 0;
+  if (cudaGetDeviceCount(&nd) != cudaSuccess || nd == 0) return fail(NR_ERR_NO_DEVICE, "no CUDA device");
+  auto n = std::make_unique<nr_nrc>();
+  std::string e = nrc_create(n->n, max_queries, lo, hi, seed);
+  if (!e.empty()) return fail(e.find("must") != std::string::npos ? NR_ERR_INVALID : NR_ERR_CUDA, e);
+  *out = n.release();
+  return NR_OK;
+}
+
+int nr_nrc_destroy(nr_nrc* n) {
+  delete n;
+  return NR_OK;
+}
+
+int nr_nrc_infer(nr_nrc* n, const float* queries, uint32_t count, float* radiance,
+                 uint64_t stream) {
+  if (!n || (count && (!queries || !radiance))) return fail(NR_ERR_INVALID, "null argument");
+  return den_status(nrc_infer(n->n, reinterpret_cast<const NrcQuery*>(queries), count, radiance,
+                              (cudaStream_t)(uintptr_t)stream));
+}
+
+int nr_nrc_train(nr_nrc* n, const float* queries, const float* target, uint32_t count,
+                 float lr, double* loss, uint64_t stream) {
+  if (!n || (count && (!queries || !target))) return fail(NR_ERR_INVALID, "null argument");
+  return den_status(nrc_train(n->n, reinterpret_cast<const NrcQuery*>(queries), target, count, lr,
+                              loss, (cudaStream_t)(uintptr_t)stream));
+}
+
+int nr_nrc_count(const nr_nrc* n, int32_t what, uint64_t* out) {
+  if (!n || !out || what < 0 || what > 4) return fail(NR_ERR_INVALID, "bad argument");
+  *out = nrc_count(n->n, what);
+  return NR_OK;
+}
+
+int nr_nrc_get(const nr_nrc* n, int32_t what, float* host) {
+  if (!n || !host || what < 0 || what > 4) return fail(NR_ERR_INVALID, "bad argument");
+  return den_status(nrc_get(n->n, what, host));
+}
+
+int nr_nrc_set(nr_nrc* n, const float* mlp, const float* grid) {
+  if (!n) return fail(NR_ERR_INVALID, "null argument");
+  return den_status(nrc_set_weights(n->n, mlp, grid));
 }
 
 int nr_accumulate_device(float* avg, const float* smp, uint32_t C, uint32_t H, uint32_t W,

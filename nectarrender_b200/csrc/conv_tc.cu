@@ -78,7 +78,8 @@ __global__ void __launch_bounds__(kThreads) k_conv_fwd(ConvFwdArgs a) {
 
   // this thread's pixel rows (fixed over the taps)
   bool ok = true;
-  for (int t = 0; t < 9 && ok; ++t) {
+  const int ntaps = a.taps == 1 ? 1 : 9;
+  for (int t = 0; t < ntaps && ok; ++t) {
     const int s = t & 1;
     if (t >= 2) {
       // CTA-uniform: every thread polls, all agree before any of them leaves
@@ -89,7 +90,7 @@ __global__ void __launch_bounds__(kThreads) k_conv_fwd(ConvFwdArgs a) {
       }
     }
     const uint32_t sa = base + s * stage_bytes, sb = sa + a_bytes;
-    const int dy = t / 3 - 1, dx = t % 3 - 1;
+    const int dy = ntaps == 1 ? 0 : t / 3 - 1, dx = ntaps == 1 ? 0 : t % 3 - 1;
     const int kg_n = cin >> 3;
     for (int i = tid; i < 128 * kg_n; i += kThreads) {
       const int r = i & 127, kg = i >> 7;
@@ -124,8 +125,10 @@ __global__ void __launch_bounds__(kThreads) k_conv_fwd(ConvFwdArgs a) {
       tc::mma_commit(&bar[s]);
     }
   }
-  // tap 8 used stage 0 for the fifth time: wait for that phase (parity 0)
-  if (ok) ok = __syncthreads_and(tc::mbar_wait(&bar[0], 0u, kWaitLimit));
+  // the last tap used stage (ntaps - 1) & 1 for the ((ntaps - 1) >> 1)-th time
+  if (ok)
+    ok = __syncthreads_and(tc::mbar_wait(&bar[(ntaps - 1) & 1], (uint32_t)((ntaps - 1) >> 1) & 1u,
+                                         kWaitLimit));
   if (!ok && tid == 0) atomicOr(a.err, 2u);
   tc::fence_after_sync();
   __syncthreads();
@@ -267,7 +270,8 @@ __global__ void __launch_bounds__(kThreads) k_conv_wgrad(ConvWgradArgs a) {
   const int P = a.B * a.H * a.W;
   const int n_chunks = (P + 127) / 128;
   const int tap = blockIdx.y;
-  const int dy = tap / 3 - 1, dx = tap % 3 - 1;
+  const bool one = a.taps == 1;
+  const int dy = one ? 0 : tap / 3 - 1, dx = one ? 0 : tap % 3 - 1;
   const int c0 = blockIdx.x * a.chunks_per_cta;
   const int c1 = min(n_chunks, c0 + a.chunks_per_cta);
   const uint32_t lbo = 128u, sbo = 2048u;  // MN-major: 8 pixels x 16 B per K group
@@ -380,7 +384,7 @@ cudaError_t launch_conv_fwd(const ConvFwdArgs& a, cudaStream_t st) {
       a.x_stride % 8 || a.x_off % 8 || a.y_stride % 8 || a.y_off % 8)
     return cudaErrorInvalidValue;
   const size_t halo_smem = (size_t)(a.cin >> 3) * kHalo * 16u + 2u * (size_t)a.cout * a.cin * 2u;
-  if (a.W % kTileW == 0 && a.H % kTileH == 0 && halo_smem <= 200u * 1024u) {
+  if (a.taps != 1 && a.W % kTileW == 0 && a.H % kTileH == 0 && halo_smem <= 200u * 1024u) {
     cudaError_t e = cudaFuncSetAttribute(k_conv_fwd_halo,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)halo_smem);
     if (e != cudaSuccess) return e;
@@ -409,7 +413,7 @@ cudaError_t launch_conv_wgrad(const ConvWgradArgs& a, cudaStream_t st) {
   if (e != cudaSuccess) return e;
   const int P = a.B * a.H * a.W;
   const int n_chunks = (P + 127) / 128;
-  dim3 grid((n_chunks + a.chunks_per_cta - 1) / a.chunks_per_cta, 9);
+  dim3 grid((n_chunks + a.chunks_per_cta - 1) / a.chunks_per_cta, a.taps == 1 ? 1 : 9);
   k_conv_wgrad<<<grid, kThreads, smem, st>>>(a);
   return cudaGetLastError();
 }

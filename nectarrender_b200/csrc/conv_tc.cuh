@@ -25,6 +25,8 @@ struct ConvFwdArgs {
   int32_t B, H, W;         // images of H x W pixels; P = B * H * W, a multiple of 128
   int32_t relu;
   uint32_t* err;           // bit 1: a tensor-core wait timed out
+  int32_t taps;            // 9: 3x3 convolution; 1: centre tap only, i.e. the
+                           // GEMM y[p] = W x[p] (w is then [1][cout][cin])
 };
 
 struct ConvWgradArgs {
@@ -37,6 +39,7 @@ struct ConvWgradArgs {
   int32_t B, H, W;
   int32_t chunks_per_cta;   // 128-pixel chunks reduced by one CTA
   uint32_t* err;
+  int32_t taps;             // 9, or 1: dw[0] += dy^T x (a GEMM over pixels)
 };
 
 size_t conv_fwd_smem_bytes(int cin, int cout);
