@@ -296,6 +296,10 @@ int nr_scene_set_tuning(nr_scene* scene, uint32_t mesh_leaf_max, uint32_t tlas_l
  * nectar_render/csrc/scene/src/scene.cpp:68-76). Must precede nr_render_create. */
 int nr_scene_build(nr_scene* scene);
 int nr_scene_get_stats(const nr_scene* scene, nr_scene_stats* out);
+/* World-space box around every object of a built scene (the union of the
+ * top-level leaf boxes); the radiance cache's grid spans it. No counterpart
+ * in the reference. */
+int nr_scene_get_bounds(const nr_scene* scene, float lo[3], float hi[3]);
 /* Binary SAH tree of mesh `mesh_id` as built on the GPU, for checks:
  * nodes as float[8] {lo.xyz, hi.xyz, left|prim, right|count} bit patterns
  * (int32 stored in the float slots). Pass NULL to query the count. */
@@ -485,6 +489,18 @@ int nr_nrc_train(nr_nrc* n, const float* queries, const float* target, uint32_t 
 int nr_nrc_count(const nr_nrc* n, int32_t what, uint64_t* out);
 int nr_nrc_get(const nr_nrc* n, int32_t what, float* host);
 int nr_nrc_set(nr_nrc* n, const float* mlp, const float* grid);
+
+/* Attaches a radiance cache to a render in NR_MODE_PERF (cache = NULL
+ * detaches it). Paths stop at hit index terminate_bounce and add the
+ * cache's radiance times their throughput; one path in train_one_in runs to
+ * full depth and, when lr > 0, trains the cache after every wave on the
+ * radiance measured behind each of its hits. The cache must have been
+ * created for at least as many queries as a wave holds paths to train on all
+ * records of a wave at once. */
+int nr_render_set_nrc(nr_render* render, nr_nrc* cache, uint32_t terminate_bounce,
+                      uint32_t train_one_in, float lr);
+/* Cache queries answered and training records used since attached. */
+int nr_render_nrc_stats(const nr_render* render, uint64_t* queries, uint64_t* records);
 
 /* device-pointer level (callers that own their buffers) -------------------- */
 /* Fused running-mean accumulate of one sample layer into an average layer on

@@ -97,7 +97,7 @@ EXPORTS = [
     "nr_scene_add_object", "nr_scene_set_sky_null", "nr_scene_set_sky_simple",
     "nr_scene_set_sky_hdri", "nr_scene_load_hdr", "nr_scene_set_hdri_params",
     "nr_scene_set_tuning", "nr_scene_build",
-    "nr_scene_get_stats", "nr_scene_get_binary_bvh", "nr_render_config_default",
+    "nr_scene_get_stats", "nr_scene_get_bounds", "nr_scene_get_binary_bvh", "nr_render_config_default",
     "nr_render_create", "nr_render_destroy", "nr_render_reset", "nr_render_samples",
     "nr_render_samples_static", "nr_render_samples_batch", "nr_render_set_profiling",
     "nr_render_get_profile",
@@ -106,7 +106,7 @@ EXPORTS = [
     "nr_denoiser_create", "nr_denoiser_destroy", "nr_denoiser_train_step", "nr_denoiser_infer",
     "nr_denoiser_param_count", "nr_denoiser_get_params", "nr_denoiser_set_params",
     "nr_denoiser_layers", "nr_nrc_create", "nr_nrc_destroy", "nr_nrc_infer", "nr_nrc_train",
-    "nr_nrc_count", "nr_nrc_get", "nr_nrc_set",
+    "nr_nrc_count", "nr_nrc_get", "nr_nrc_set", "nr_render_set_nrc", "nr_render_nrc_stats",
     "nr_render_sample_layers", "nr_render_layer_device_ptr", "nr_render_read_layer",
     "nr_render_read_beauty_fp64", "nr_render_readback", "nr_render_display_float",
     "nr_render_dims", "nr_render_set_counters", "nr_render_get_counters", "nr_render_last_ms",
@@ -231,6 +231,12 @@ class Scene:
         _check(self.lib.nr_scene_get_stats(self.h, C.byref(s)), "nr_scene_get_stats")
         return {k: getattr(s, k) for k, _ in SceneStats._fields_}
 
+    def bounds(self) -> tuple[np.ndarray, np.ndarray]:
+        """World-space box around every object (lo, hi)."""
+        lo, hi = np.zeros(3, np.float32), np.zeros(3, np.float32)
+        _check(self.lib.nr_scene_get_bounds(self.h, _fptr(lo), _fptr(hi)), "nr_scene_get_bounds")
+        return lo, hi
+
     def mesh(self, mesh_id: int = 0):
         """(positions, normals, tangents, uvs, triangles) as stored after parsing."""
         nv, nt = C.c_uint32(), C.c_uint32()
@@ -258,7 +264,7 @@ class Scene:
     def __del__(self):
         if getattr(self, "h", None) and self.h.value:
             self.lib.nr_scene_destroy(self.h)
-            self.h = C.c_void_p()
+            self.h = None  # module globals may already be gone at exit
 
 
 def _fptr(a: np.ndarray | None):
@@ -365,6 +371,18 @@ class Render:
                "nr_render_selection_mask")
         return out
 
+    def set_nrc(self, cache, terminate_bounce: int = 2, train_one_in: int = 32,
+                lr: float = 5e-3) -> None:
+        """Attach a nectarrender_b200.nrc.RadianceCache (None detaches)."""
+        self._nrc = cache  # keep it alive while attached
+        _check(self.lib.nr_render_set_nrc(self.h, cache.h if cache else None, terminate_bounce,
+                                          train_one_in, C.c_float(lr)), "nr_render_set_nrc")
+
+    def nrc_stats(self) -> tuple[int, int]:
+        q, t = C.c_uint64(), C.c_uint64()
+        _check(self.lib.nr_render_nrc_stats(self.h, C.byref(q), C.byref(t)), "nr_render_nrc_stats")
+        return q.value, t.value
+
     def graph_stats(self) -> tuple[int, int]:
         """(wave graphs captured, graph replays) of this render so far."""
         cap, rep = C.c_uint32(), C.c_uint64()
@@ -382,4 +400,4 @@ class Render:
     def __del__(self):
         if getattr(self, "h", None) and self.h.value:
             self.lib.nr_render_destroy(self.h)
-            self.h = C.c_void_p()
+            self.h = None  # module globals may already be gone at exit

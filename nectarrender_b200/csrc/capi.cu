@@ -386,6 +386,7 @@ struct nr_scene {
   DevScene dev{};
   nr_scene_stats stats{};
   std::vector<int32_t> ref_leaf_order;
+  float world_lo[3] = {0.f, 0.f, 0.f}, world_hi[3] = {0.f, 0.f, 0.f};  // union of object boxes
   int32_t light = -1;
   uint32_t mesh_leaf_max = 1, tlas_leaf_max = 1;
 
@@ -865,6 +866,10 @@ int nr_scene_build(nr_scene* s) {
     boxes[i] = h_transformed(object_local_box(s, o), x);
     blo[i] = make_float4(boxes[i].lo[0], boxes[i].lo[1], boxes[i].lo[2], 0.f);
     bhi[i] = make_float4(boxes[i].hi[0], boxes[i].hi[1], boxes[i].hi[2], 0.f);
+    for (int k = 0; k < 3; ++k) {
+      s->world_lo[k] = i ? std::min(s->world_lo[k], boxes[i].lo[k]) : boxes[i].lo[k];
+      s->world_hi[k] = i ? std::max(s->world_hi[k], boxes[i].hi[k]) : boxes[i].hi[k];
+    }
   }
   CU(upload(s->d_objects, objs.data(), objs.size(), st), "upload objects");
   float4 *dlo = nullptr, *dhi = nullptr;
@@ -956,6 +961,16 @@ int nr_scene_build(nr_scene* s) {
   return NR_OK;
 }
 
+int nr_scene_get_bounds(const nr_scene* s, float lo[3], float hi[3]) {
+  if (!s || !lo || !hi) return fail(NR_ERR_INVALID, "nr_scene_get_bounds: null argument");
+  if (!s->built) return fail(NR_ERR_STATE, "nr_scene_get_bounds: scene not built");
+  for (int k = 0; k < 3; ++k) {
+    lo[k] = s->world_lo[k];
+    hi[k] = s->world_hi[k];
+  }
+  return NR_OK;
+}
+
 int nr_scene_get_stats(const nr_scene* s, nr_scene_stats* out) {
   if (!s || !out) return fail(NR_ERR_INVALID, "null argument");
   if (!s->built) return fail(NR_ERR_STATE, "scene is not built");
@@ -1034,6 +1049,16 @@ struct nr_render {
     cudaGraphExec_t exec = nullptr;
   };
   std::vector<WaveGraph> graphs;
+  // radiance cache attached with nr_render_set_nrc (perf mode)
+  nr_nrc* nrc = nullptr;
+  uint32_t nrc_bounce = 2, nrc_one_in = 32;
+  float nrc_lr = 0.0f;
+  float4 *nrc_q = nullptr, *nrc_q_beta = nullptr, *nrc_t = nullptr, *nrc_t_beta = nullptr,
+         *nrc_t_before = nullptr;
+  float *nrc_radiance = nullptr, *nrc_target = nullptr;
+  uint32_t nrc_cap = 0;
+  uint64_t nrc_queries = 0, nrc_records = 0;  // totals since attached
+  std::string nrc_error;                       // set by the wave hook
   PickOut* d_pick = nullptr;        // viewport queries (allocated on first use)
   uint8_t* d_mask = nullptr;        // 2 x W*H selection masks
   uint32_t graphs_captured = 0;
@@ -1058,6 +1083,9 @@ struct nr_render {
     for (auto e : pev) cudaEventDestroy(e);
     cudaFree(d_pick);
     cudaFree(d_mask);
+    for (void* q : {(void*)nrc_q, (void*)nrc_q_beta, (void*)nrc_t, (void*)nrc_t_beta,
+                    (void*)nrc_t_before, (void*)nrc_radiance, (void*)nrc_target})
+      cudaFree(q);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (stream) cudaStreamDestroy(stream);
@@ -1293,6 +1321,43 @@ static cudaError_t launch_wave_graph(nr_render* r, const WfParams& W) {
   return wf_launch_wave(W, false, r->stream, nullptr);
 }
 
+struct nr_nrc {
+  Nrc n;
+};
+
+// After the bounces of a wave: the cache answers the queries of the paths
+// that stopped at the cache bounce, then trains on the training paths.
+static cudaError_t nrc_hook(void* ctx, const WfParams& W, cudaStream_t st) {
+  nr_render* r = static_cast<nr_render*>(ctx);
+  uint32_t n_q = 0, n_t = 0;
+  cudaError_t e = wf_nrc_counts(W, &n_q, &n_t, st);  // synchronises the stream
+  if (e != cudaSuccess) return e;
+  Nrc& cache = r->nrc->n;
+  std::string msg = nrc_poll_error(cache, st);  // waits of the previous wave's cache launches
+  const uint32_t chunk = std::max(1u, nrc_max_queries(cache));
+  for (uint32_t o = 0; o < n_q && msg.empty(); o += chunk) {
+    const uint32_t c = std::min(chunk, n_q - o);
+    WfParams Wo = W;
+    Wo.nrc_q_beta = W.nrc_q_beta + o;
+    msg = nrc_infer(cache, reinterpret_cast<const NrcQuery*>(W.nrc_q + 4 * (size_t)o), c,
+                    r->nrc_radiance, st);
+    if (msg.empty() && (e = wf_nrc_apply(Wo, r->nrc_radiance, c, st)) != cudaSuccess) return e;
+  }
+  r->nrc_queries += n_q;
+  if (msg.empty() && n_t && r->nrc_lr > 0.0f) {
+    if ((e = wf_nrc_targets(W, r->nrc_target, n_t, st)) != cudaSuccess) return e;
+    const uint32_t c = std::min(n_t, chunk);
+    msg = nrc_train(cache, reinterpret_cast<const NrcQuery*>(W.nrc_t), r->nrc_target, c,
+                    r->nrc_lr, nullptr, st);
+    r->nrc_records += c;
+  }
+  if (!msg.empty()) {
+    r->nrc_error = msg;
+    return cudaErrorUnknown;
+  }
+  return cudaSuccess;
+}
+
 static int launch(nr_render* r, const KernelParams& P, WaveTimer* tm) {
   // NR_MODE_PERF runs on the wavefront schedule only
   if (r->cfg.schedule != NR_SCHEDULE_WAVEFRONT && r->cfg.mode != NR_MODE_PERF) {
@@ -1314,15 +1379,54 @@ static int launch(nr_render* r, const KernelParams& P, WaveTimer* tm) {
   W.shade_variant = r->cfg.shade_variant > 0 ? r->cfg.shade_variant : kDefaultShadeVariant;
   W.tail_max_paths = r->cfg.tail_max_paths == 0 ? kDefaultTailPaths
                      : (r->cfg.tail_max_paths == UINT32_MAX ? 0u : r->cfg.tail_max_paths);
+  WaveHook hook;
+  const bool nrc = r->nrc && r->cfg.mode == NR_MODE_PERF && !P.write_raw;
+  if (nrc) {
+    const uint32_t cap = r->wf.capacity;
+    if (r->nrc_cap < cap) {
+      for (void* q : {(void*)r->nrc_q, (void*)r->nrc_q_beta, (void*)r->nrc_t, (void*)r->nrc_t_beta,
+                      (void*)r->nrc_t_before, (void*)r->nrc_radiance, (void*)r->nrc_target})
+        cudaFree(q);
+      CU(cudaMalloc(&r->nrc_q, sizeof(float4) * 4 * (size_t)cap), "alloc cache queries");
+      CU(cudaMalloc(&r->nrc_q_beta, sizeof(float4) * (size_t)cap), "alloc cache queries");
+      CU(cudaMalloc(&r->nrc_t, sizeof(float4) * 4 * (size_t)cap), "alloc cache records");
+      CU(cudaMalloc(&r->nrc_t_beta, sizeof(float4) * (size_t)cap), "alloc cache records");
+      CU(cudaMalloc(&r->nrc_t_before, sizeof(float4) * (size_t)cap), "alloc cache records");
+      CU(cudaMalloc(&r->nrc_radiance, sizeof(float) * 3 * (size_t)cap), "alloc cache output");
+      CU(cudaMalloc(&r->nrc_target, sizeof(float) * 3 * (size_t)cap), "alloc cache targets");
+      r->nrc_cap = cap;
+    }
+    W.nrc_bounce = r->nrc_bounce;
+    W.nrc_train_one_in = r->nrc_one_in;
+    W.nrc_q_cap = W.nrc_t_cap = r->nrc_cap;
+    W.nrc_q = r->nrc_q;
+    W.nrc_q_beta = r->nrc_q_beta;
+    W.nrc_t = r->nrc_t;
+    W.nrc_t_beta = r->nrc_t_beta;
+    W.nrc_t_before = r->nrc_t_before;
+    hook.fn = nrc_hook;
+    hook.ctx = r;
+  }
   CU(wf_set_base(W, P.first_sample, r->stream), "set wave base");
   if (tm) tm->mark(NR_KERNEL_ROTATE, r->stream);
   for (uint32_t s = 0; s < P.n_samples; s += per) {
     W.base = P.first_sample + s;
     W.count = std::min(per, P.n_samples - s);
-    if (!r->counters_on && !tm && r->cfg.use_graphs)
+    if (!r->counters_on && !tm && r->cfg.use_graphs && !nrc)
       CU(launch_wave_graph(r, W), "launch wavefront graph");
-    else
-      CU(wf_launch_wave(W, r->counters_on, r->stream, tm), "launch wavefront");
+    else {
+      cudaError_t e = wf_launch_wave(W, r->counters_on, r->stream, tm, nrc ? &hook : nullptr);
+      if (!r->nrc_error.empty()) {
+        const std::string m = r->nrc_error;
+        r->nrc_error.clear();
+        return fail(m.find("timed out") != std::string::npos ? NR_ERR_DEVICE : NR_ERR_CUDA, m);
+      }
+      CU(e, "launch wavefront");
+    }
+  }
+  if (nrc) {
+    const std::string m = nrc_poll_error(r->nrc->n, r->stream);  // the last wave's cache launches
+    if (!m.empty()) return fail(NR_ERR_DEVICE, m);
   }
   return NR_OK;
 }
@@ -1542,6 +1646,27 @@ int nr_render_selection_mask(nr_render* r, uint32_t object_id, int32_t outline_r
   return NR_OK;
 }
 
+int nr_render_set_nrc(nr_render* r, nr_nrc* cache, uint32_t terminate_bounce,
+                      uint32_t train_one_in, float lr) {
+  if (!r) return fail(NR_ERR_INVALID, "null render");
+  if (cache && r->cfg.mode != NR_MODE_PERF)
+    return fail(NR_ERR_STATE, "the radiance cache needs NR_MODE_PERF");
+  if (cache && (terminate_bounce < 1 || terminate_bounce >= r->cfg.ray_depth))
+    return fail(NR_ERR_INVALID, "terminate_bounce must be in [1, ray_depth)");
+  r->nrc = cache;
+  r->nrc_bounce = terminate_bounce;
+  r->nrc_one_in = std::max(1u, train_one_in);
+  r->nrc_lr = lr;
+  return NR_OK;
+}
+
+int nr_render_nrc_stats(const nr_render* r, uint64_t* queries, uint64_t* records) {
+  if (!r) return fail(NR_ERR_INVALID, "null render");
+  if (queries) *queries = r->nrc_queries;
+  if (records) *records = r->nrc_records;
+  return NR_OK;
+}
+
 int nr_render_sample_layers(nr_render* r, uint32_t sample_idx, float* beauty, float* diffuse,
                             float* normal, uint32_t* primary) {
   if (!r) return fail(NR_ERR_INVALID, "null render");
@@ -1727,10 +1852,6 @@ int nr_conv3x3_wgrad_device(const void* dy, int32_t dy_stride, int32_t dy_off, c
 
 struct nr_denoiser {
   Denoiser d;
-};
-
-struct nr_nrc {
-  Nrc n;
 };
 
 extern "C" {

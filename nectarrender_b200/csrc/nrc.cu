@@ -413,6 +413,21 @@ std::string nrc_train(Nrc& c, const NrcQuery* q, const float* target, uint32_t c
   return {};
 }
 
+uint32_t nrc_max_queries(const Nrc& c) { return c.net ? c.net->max_q : 0u; }
+
+std::string nrc_poll_error(Nrc& c, cudaStream_t st) {
+  if (!c.net) return "nrc: not created";
+  uint32_t err = 0;
+  cudaError_t e = cudaStreamSynchronize(st);
+  if (e == cudaSuccess) e = cudaMemcpy(&err, c.net->d_err, 4, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_msg(e, "nrc");
+  if (err) {
+    cudaMemset(c.net->d_err, 0, 4);
+    return "nrc: a tensor-core wait timed out";
+  }
+  return {};
+}
+
 size_t nrc_count(const Nrc& c, int what) {
   if (!c.net) return 0;
   if (what <= 1) {

@@ -40,6 +40,9 @@ std::string nrc_train(Nrc& n, const NrcQuery* q, const float* target, uint32_t c
 std::string nrc_get(const Nrc& n, int what, float* host);  // 0 MLP weights, 1 their gradients,
                                                             // 2 grid values, 3 grid gradients
 size_t nrc_count(const Nrc& n, int what);
+uint32_t nrc_max_queries(const Nrc& n);
+// error flag of the tensor-core waits of the launches on st (synchronises st)
+std::string nrc_poll_error(Nrc& n, cudaStream_t st);
 std::string nrc_set_weights(Nrc& n, const float* mlp, const float* grid);
 
 }  // namespace nr

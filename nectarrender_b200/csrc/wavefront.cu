@@ -38,7 +38,41 @@ enum : uint32_t {
   CTR_SH = 5,      // shadow rays queued by this bounce's shade (perf mode)
   CTR_SHWORK = 6,  // shadow kernel work counter
   CTR_TAIL = 7,    // set once the tail kernel has finished the wave's paths
+  CTR_NQ = 8,      // radiance-cache queries of the wave
+  CTR_NT = 9,      // radiance-cache training records of the wave
 };
+
+// Features of a hit for the radiance cache (NrcQuery layout, nrc.cuh).
+__device__ __forceinline__ void nrc_features(const DevMaterial& m, const Hit& rec, const V3& wo,
+                                             float4* out) {
+  V3 albedo{0.f, 0.f, 0.f};
+  float rough = 1.0f;
+  switch (m.type) {
+    case 2:
+      albedo = tex_sample(m.tex[0], rec.uv);
+      rough = tex_sample(m.tex[1], rec.uv).x;
+      break;
+    case 3:
+      albedo = V3{m.tint[0], m.tint[1], m.tint[2]};
+      rough = 0.0f;
+      break;
+    default:
+      albedo = tex_sample(m.tex[0], rec.uv);
+  }
+  out[0] = make_float4(rec.p.x, rec.p.y, rec.p.z, rough);
+  out[1] = make_float4(wo.x, wo.y, wo.z, 0.f);
+  out[2] = make_float4(rec.n.x, rec.n.y, rec.n.z, 0.f);
+  out[3] = make_float4(albedo.x, albedo.y, albedo.z, 0.f);
+}
+
+// One path in nrc_train_one_in trains the cache (a hash of pixel and sample).
+__device__ __forceinline__ bool nrc_training_path(uint32_t pix, uint32_t sample, uint32_t one_in) {
+  uint32_t h = pix * 0x9E3779B9u ^ (sample + 0x632BE5ABu) * 0x85EBCA6Bu;
+  h ^= h >> 16;
+  h *= 0x7FEB352Du;
+  h ^= h >> 15;
+  return one_in <= 1u || h % one_in == 0u;
+}
 
 // Tail hand-off (reference mode): once a wave's queue has shrunk to at most
 // kTailMaxPaths paths after bounce kTailFrom or later, one launch finishes
@@ -322,6 +356,8 @@ __global__ void k_wf_generate(WfParams W) {
     W.ctr[CTR_SH] = 0u;
     W.ctr[CTR_SHWORK] = 0u;
     W.ctr[CTR_TAIL] = 0u;
+    W.ctr[CTR_NQ] = 0u;
+    W.ctr[CTR_NT] = 0u;
   }
 }
 
@@ -711,9 +747,28 @@ __global__ void __launch_bounds__(kShadeThreads, kMinBlocks) k_wf_shade(WfParams
         if (kPerf && nee_sky && pdf_prev > 0.0f)
           w = power_heuristic(pdf_prev, sel * sky_dir_pdf(sc.sky, s.ray.d));
         s.beauty += s.atten * sky_sample(sc.sky, s.ray) * w;
+      } else if (kPerf && W.nrc_bounce &&
+                 !nrc_training_path(pix, wbase + k, W.nrc_train_one_in) &&
+                 bounce == W.nrc_bounce) {
+        // the radiance cache answers for the rest of the path
+        const uint32_t qi = atomicAdd(&W.ctr[CTR_NQ], 1u);
+        if (qi < W.nrc_q_cap) {
+          nrc_features(sc.materials[sc.objects[rec.obj].material], rec, normalize(-s.ray.d),
+                       W.nrc_q + 4 * (size_t)qi);
+          W.nrc_q_beta[qi] = make_float4(s.atten.x, s.atten.y, s.atten.z, __uint_as_float(p));
+        }
       } else {
         const DevMaterial& m = sc.materials[sc.objects[rec.obj].material];
         Ray r_in = s.ray;
+        if (kPerf && W.nrc_bounce && bounce >= 1u &&
+            nrc_training_path(pix, wbase + k, W.nrc_train_one_in)) {
+          const uint32_t ti = atomicAdd(&W.ctr[CTR_NT], 1u);
+          if (ti < W.nrc_t_cap) {
+            nrc_features(m, rec, normalize(-s.ray.d), W.nrc_t + 4 * (size_t)ti);
+            W.nrc_t_beta[ti] = make_float4(s.atten.x, s.atten.y, s.atten.z, __uint_as_float(p));
+            W.nrc_t_before[ti] = make_float4(s.beauty.x, s.beauty.y, s.beauty.z, 0.f);
+          }
+        }
         {
           float w = 1.0f;
           if (kPerf && nee_light && pdf_prev > 0.0f && (int32_t)rec.obj == sc.light)
@@ -948,6 +1003,29 @@ __global__ void k_wf_accumulate(WfParams W) {
   }
 }
 
+__global__ void k_nrc_apply(WfParams W, const float* radiance, uint32_t n) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const float4 b = W.nrc_q_beta[i];
+    const uint32_t p = __float_as_uint(b.w);
+    float4 acc = W.acc_b[p];
+    acc.x += b.x * radiance[3 * i];
+    acc.y += b.y * radiance[3 * i + 1];
+    acc.z += b.z * radiance[3 * i + 2];
+    W.acc_b[p] = acc;
+  }
+}
+
+__global__ void k_nrc_targets(WfParams W, float* target, uint32_t n) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const float4 b = W.nrc_t_beta[i], before = W.nrc_t_before[i];
+    const float4 after = W.acc_b[__float_as_uint(b.w)];
+    const float beta[3] = {b.x, b.y, b.z};
+    const float d[3] = {after.x - before.x, after.y - before.y, after.z - before.z};
+    for (int c = 0; c < 3; ++c)
+      target[3 * i + c] = beta[c] > 1e-6f ? fminf(fmaxf(d[c] / beta[c], 0.0f), 1e4f) : 0.0f;
+  }
+}
+
 __global__ void k_wf_set_base(uint32_t* ctr, uint32_t base) {
   if (threadIdx.x == 0) ctr[CTR_BASE] = base;
 }
@@ -968,6 +1046,27 @@ static int sm_count() {
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   }
   return sms;
+}
+
+cudaError_t wf_nrc_counts(const WfParams& W, uint32_t* n_q, uint32_t* n_t, cudaStream_t st) {
+  uint32_t c[2];
+  cudaError_t e = cudaMemcpyAsync(c, W.ctr + CTR_NQ, sizeof(c), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  *n_q = std::min(c[0], W.nrc_q_cap);
+  *n_t = std::min(c[1], W.nrc_t_cap);
+  return e;
+}
+
+cudaError_t wf_nrc_apply(const WfParams& W, const float* radiance, uint32_t n, cudaStream_t st) {
+  if (!n) return cudaSuccess;
+  k_nrc_apply<<<(int)std::min<uint32_t>((n + 255) / 256, 148 * 16), 256, 0, st>>>(W, radiance, n);
+  return cudaGetLastError();
+}
+
+cudaError_t wf_nrc_targets(const WfParams& W, float* target, uint32_t n, cudaStream_t st) {
+  if (!n) return cudaSuccess;
+  k_nrc_targets<<<(int)std::min<uint32_t>((n + 255) / 256, 148 * 16), 256, 0, st>>>(W, target, n);
+  return cudaGetLastError();
 }
 
 cudaError_t wf_set_base(const WfParams& W, uint32_t first_sample, cudaStream_t st) {
@@ -1071,7 +1170,8 @@ static int extend_blocks(ExtendFn fn, size_t smem) {
 }
 
 // Launch sequence of one wave (capturable: every size is read on the device).
-cudaError_t wf_launch_wave(const WfParams& W, bool counters, cudaStream_t st, WaveTimer* tm) {
+cudaError_t wf_launch_wave(const WfParams& W, bool counters, cudaStream_t st, WaveTimer* tm,
+                           const WaveHook* hook) {
   const KernelParams& P = W.kp;
   uint32_t total = P.W * P.H * W.count;
   int gen_blocks = (int)std::min<uint32_t>((total + 255) / 256, (uint32_t)sm_count() * 16);
@@ -1116,6 +1216,10 @@ cudaError_t wf_launch_wave(const WfParams& W, bool counters, cudaStream_t st, Wa
       k_wf_tail_mark<<<1, 32, 0, st>>>(W, 1 - q, W.tail_max_paths);
       if (tm) tm->mark(NR_KERNEL_ROTATE, st);
     }
+  }
+  if (hook && hook->fn) {
+    cudaError_t e = hook->fn(hook->ctx, W, st);
+    if (e != cudaSuccess) return e;
   }
   int acc_blocks = (int)std::min<uint32_t>((P.W * P.H + 255) / 256, (uint32_t)sm_count() * 16);
   k_wf_accumulate<<<acc_blocks, 256, 0, st>>>(W);

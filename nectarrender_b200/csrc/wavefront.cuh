@@ -34,6 +34,18 @@ struct WfParams {
   float4* sh_d;
   float4* sh_c;
   uint32_t* sh_queue;
+  // radiance cache (perf mode with a cache attached; nrc_bounce = 0: off).
+  // Paths other than training paths stop at hit index nrc_bounce and leave
+  // a query (features, and throughput + path index); training paths (one in
+  // nrc_train_one_in) run to full depth and leave a record at every hit from
+  // index 1 on: features, throughput + path index, beauty before the hit.
+  uint32_t nrc_bounce, nrc_train_one_in;
+  uint32_t nrc_q_cap, nrc_t_cap;
+  float4* nrc_q;       // [cap][4] (NrcQuery layout)
+  float4* nrc_q_beta;  // xyz throughput, w path index
+  float4* nrc_t;       // [cap][4]
+  float4* nrc_t_beta;  // xyz throughput, w path index
+  float4* nrc_t_before;
 };
 
 size_t wf_state_bytes(uint32_t n_paths, bool perf = false);
@@ -63,8 +75,22 @@ struct WaveTimer {
 // Launches one wave: generate, depth x (extend, shade, rotate), accumulate,
 // advance. The wave's first sample index must have been set on the stream by
 // wf_set_base (for the first wave of a run; each wave advances it).
+// Called after the last bounce of a wave, before its samples are folded into
+// the layers (the radiance cache queries and trains there).
+struct WaveHook {
+  cudaError_t (*fn)(void* ctx, const WfParams& W, cudaStream_t st) = nullptr;
+  void* ctx = nullptr;
+};
+
 cudaError_t wf_launch_wave(const WfParams& W, bool counters, cudaStream_t st,
-                           WaveTimer* timer = nullptr);
+                           WaveTimer* timer = nullptr, const WaveHook* hook = nullptr);
+// Radiance-cache helpers for the hook: counts of queries and training
+// records of the wave just traced, adding the cache's answers to the paths'
+// beauty, and the training targets (beauty after the hit minus beauty
+// before it, over the throughput at the hit).
+cudaError_t wf_nrc_counts(const WfParams& W, uint32_t* n_q, uint32_t* n_t, cudaStream_t st);
+cudaError_t wf_nrc_apply(const WfParams& W, const float* radiance, uint32_t n_q, cudaStream_t st);
+cudaError_t wf_nrc_targets(const WfParams& W, float* target, uint32_t n_t, cudaStream_t st);
 cudaError_t wf_set_base(const WfParams& W, uint32_t first_sample, cudaStream_t st);
 
 }  // namespace nr

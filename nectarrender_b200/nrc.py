@@ -30,7 +30,7 @@ class RadianceCache:
     def __del__(self):
         if getattr(self, "h", None) and self.h.value:
             self.lib.nr_nrc_destroy(self.h)
-            self.h = C.c_void_p()
+            self.h = None  # module globals may already be gone at exit
 
     @staticmethod
     def _stream():
