@@ -468,8 +468,9 @@ int nr_denoiser_layers(const nr_denoiser* d, int32_t* count, int32_t* cin_cout);
 /* Neural radiance cache (no reference counterpart): a multiresolution
  * hash-grid encoding of position (16 levels x 2 features, 2^19 entries per
  * level, resolutions 16..2048 inside [lo, hi]) plus direction, normal,
- * roughness and albedo, into a 64-wide, 4-layer MLP whose GEMMs run on the
- * tcgen05 tensor cores; trained online with a relative squared error.
+ * roughness and albedo, into an MLP of four hidden layers of width 64 (its
+ * GEMMs run on the tcgen05 tensor cores), trained online with a relative
+ * squared error.
  * Queries are device float [count][16]: position, roughness, outgoing
  * direction (unit, away from the surface), -, normal, -, diffuse albedo, -.
  * Radiance in and out: device float [count][3]. */
@@ -479,11 +480,12 @@ int nr_nrc_create(uint32_t max_queries, const float lo[3], const float hi[3], ui
 int nr_nrc_destroy(nr_nrc* n);
 int nr_nrc_infer(nr_nrc* n, const float* queries, uint32_t count, float* radiance,
                  uint64_t stream);
-/* One Adam step (lr <= 0: gradients only); *loss (if not null) = mean
- * relative squared error before the step. */
+/* One Adam step (lr <= 0: gradients only; on the hash grid only the entries
+ * the queries touched move); *loss (if not null) = mean relative squared
+ * error before the step. */
 int nr_nrc_train(nr_nrc* n, const float* queries, const float* target, uint32_t count,
                  float lr, double* loss, uint64_t stream);
-/* Host copies: what = 0 MLP weights ([64][64] x 3 then [16][64], out x in),
+/* Host copies: what = 0 MLP weights ([64][64] x 4 then [16][64], out x in),
  * 1 their gradients, 2 grid values, 3 grid gradients, 4 the encoded inputs
  * of the last train call ([count][64]). */
 int nr_nrc_count(const nr_nrc* n, int32_t what, uint64_t* out);
@@ -493,12 +495,13 @@ int nr_nrc_set(nr_nrc* n, const float* mlp, const float* grid);
 /* Attaches a radiance cache to a render in NR_MODE_PERF (cache = NULL
  * detaches it). Paths stop at hit index terminate_bounce and add the
  * cache's radiance times their throughput; one path in train_one_in runs to
- * full depth and, when lr > 0, trains the cache after every wave on the
- * radiance measured behind each of its hits. The cache must have been
- * created for at least as many queries as a wave holds paths to train on all
- * records of a wave at once. */
+ * full depth and leaves a training record at every hit after the first (the
+ * radiance measured behind the hit). When lr > 0, after every wave the cache
+ * takes max(min_steps, records / batch) Adam steps (batch 0: 16384, capped
+ * at the cache's max_queries; min_steps 0: 4), each on an interleaved subset
+ * of the wave's records, every record used once. */
 int nr_render_set_nrc(nr_render* render, nr_nrc* cache, uint32_t terminate_bounce,
-                      uint32_t train_one_in, float lr);
+                      uint32_t train_one_in, float lr, uint32_t batch, uint32_t min_steps);
 /* Cache queries answered and training records used since attached. */
 int nr_render_nrc_stats(const nr_render* render, uint64_t* queries, uint64_t* records);
 

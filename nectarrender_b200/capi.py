@@ -372,11 +372,12 @@ class Render:
         return out
 
     def set_nrc(self, cache, terminate_bounce: int = 2, train_one_in: int = 32,
-                lr: float = 5e-3) -> None:
+                lr: float = 1e-2, batch: int = 16384, min_steps: int = 4) -> None:
         """Attach a nectarrender_b200.nrc.RadianceCache (None detaches)."""
         self._nrc = cache  # keep it alive while attached
         _check(self.lib.nr_render_set_nrc(self.h, cache.h if cache else None, terminate_bounce,
-                                          train_one_in, C.c_float(lr)), "nr_render_set_nrc")
+                                          train_one_in, C.c_float(lr), batch, min_steps),
+               "nr_render_set_nrc")
 
     def nrc_stats(self) -> tuple[int, int]:
         q, t = C.c_uint64(), C.c_uint64()

@@ -1051,10 +1051,10 @@ struct nr_render {
   std::vector<WaveGraph> graphs;
   // radiance cache attached with nr_render_set_nrc (perf mode)
   nr_nrc* nrc = nullptr;
-  uint32_t nrc_bounce = 2, nrc_one_in = 32;
+  uint32_t nrc_bounce = 2, nrc_one_in = 32, nrc_batch = 16384, nrc_min_steps = 4;
   float nrc_lr = 0.0f;
   float4 *nrc_q = nullptr, *nrc_q_beta = nullptr, *nrc_t = nullptr, *nrc_t_beta = nullptr,
-         *nrc_t_before = nullptr;
+         *nrc_t_before = nullptr, *nrc_t_perm = nullptr;
   float *nrc_radiance = nullptr, *nrc_target = nullptr;
   uint32_t nrc_cap = 0;
   uint64_t nrc_queries = 0, nrc_records = 0;  // totals since attached
@@ -1084,7 +1084,8 @@ struct nr_render {
     cudaFree(d_pick);
     cudaFree(d_mask);
     for (void* q : {(void*)nrc_q, (void*)nrc_q_beta, (void*)nrc_t, (void*)nrc_t_beta,
-                    (void*)nrc_t_before, (void*)nrc_radiance, (void*)nrc_target})
+                    (void*)nrc_t_before, (void*)nrc_t_perm, (void*)nrc_radiance,
+                    (void*)nrc_target})
       cudaFree(q);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
@@ -1325,6 +1326,8 @@ struct nr_nrc {
   Nrc n;
 };
 
+constexpr uint32_t kNrcMaxGroups = 4096;  // Adam steps per wave at most
+
 // After the bounces of a wave: the cache answers the queries of the paths
 // that stopped at the cache bounce, then trains on the training paths.
 static cudaError_t nrc_hook(void* ctx, const WfParams& W, cudaStream_t st) {
@@ -1345,11 +1348,20 @@ static cudaError_t nrc_hook(void* ctx, const WfParams& W, cudaStream_t st) {
   }
   r->nrc_queries += n_q;
   if (msg.empty() && n_t && r->nrc_lr > 0.0f) {
-    if ((e = wf_nrc_targets(W, r->nrc_target, n_t, st)) != cudaSuccess) return e;
-    const uint32_t c = std::min(n_t, chunk);
-    msg = nrc_train(cache, reinterpret_cast<const NrcQuery*>(W.nrc_t), r->nrc_target, c,
-                    r->nrc_lr, nullptr, st);
-    r->nrc_records += c;
+    // one Adam step per batch; batch g holds records g, g + groups, ...
+    const uint32_t batch = std::min(r->nrc_batch, chunk);
+    const uint32_t groups =
+        std::min(std::max((n_t + batch - 1) / batch, std::min(r->nrc_min_steps, n_t)),
+                 kNrcMaxGroups);
+    const uint32_t per = (n_t + groups - 1) / groups;
+    if ((e = wf_nrc_targets(W, r->nrc_target, r->nrc_t_perm, n_t, groups, st)) != cudaSuccess)
+      return e;
+    for (uint32_t g = 0; g < groups && msg.empty(); ++g) {
+      const uint32_t c = std::min(n_t / groups + (g < n_t % groups ? 1u : 0u), chunk);
+      msg = nrc_train(cache, reinterpret_cast<const NrcQuery*>(r->nrc_t_perm + 4 * (size_t)g * per),
+                      r->nrc_target + 3 * (size_t)g * per, c, r->nrc_lr, nullptr, st);
+      r->nrc_records += c;
+    }
   }
   if (!msg.empty()) {
     r->nrc_error = msg;
@@ -1385,15 +1397,19 @@ static int launch(nr_render* r, const KernelParams& P, WaveTimer* tm) {
     const uint32_t cap = r->wf.capacity;
     if (r->nrc_cap < cap) {
       for (void* q : {(void*)r->nrc_q, (void*)r->nrc_q_beta, (void*)r->nrc_t, (void*)r->nrc_t_beta,
-                      (void*)r->nrc_t_before, (void*)r->nrc_radiance, (void*)r->nrc_target})
+                      (void*)r->nrc_t_before, (void*)r->nrc_t_perm, (void*)r->nrc_radiance,
+                      (void*)r->nrc_target})
         cudaFree(q);
       CU(cudaMalloc(&r->nrc_q, sizeof(float4) * 4 * (size_t)cap), "alloc cache queries");
       CU(cudaMalloc(&r->nrc_q_beta, sizeof(float4) * (size_t)cap), "alloc cache queries");
       CU(cudaMalloc(&r->nrc_t, sizeof(float4) * 4 * (size_t)cap), "alloc cache records");
       CU(cudaMalloc(&r->nrc_t_beta, sizeof(float4) * (size_t)cap), "alloc cache records");
       CU(cudaMalloc(&r->nrc_t_before, sizeof(float4) * (size_t)cap), "alloc cache records");
+      // regrouped records: n + groups - 1 slots at most
+      const size_t slots = (size_t)cap + kNrcMaxGroups;
+      CU(cudaMalloc(&r->nrc_t_perm, sizeof(float4) * 4 * slots), "alloc cache records");
       CU(cudaMalloc(&r->nrc_radiance, sizeof(float) * 3 * (size_t)cap), "alloc cache output");
-      CU(cudaMalloc(&r->nrc_target, sizeof(float) * 3 * (size_t)cap), "alloc cache targets");
+      CU(cudaMalloc(&r->nrc_target, sizeof(float) * 3 * slots), "alloc cache targets");
       r->nrc_cap = cap;
     }
     W.nrc_bounce = r->nrc_bounce;
@@ -1647,7 +1663,7 @@ int nr_render_selection_mask(nr_render* r, uint32_t object_id, int32_t outline_r
 }
 
 int nr_render_set_nrc(nr_render* r, nr_nrc* cache, uint32_t terminate_bounce,
-                      uint32_t train_one_in, float lr) {
+                      uint32_t train_one_in, float lr, uint32_t batch, uint32_t min_steps) {
   if (!r) return fail(NR_ERR_INVALID, "null render");
   if (cache && r->cfg.mode != NR_MODE_PERF)
     return fail(NR_ERR_STATE, "the radiance cache needs NR_MODE_PERF");
@@ -1657,6 +1673,8 @@ int nr_render_set_nrc(nr_render* r, nr_nrc* cache, uint32_t terminate_bounce,
   r->nrc_bounce = terminate_bounce;
   r->nrc_one_in = std::max(1u, train_one_in);
   r->nrc_lr = lr;
+  r->nrc_batch = batch ? batch : 16384u;
+  r->nrc_min_steps = min_steps ? std::min(min_steps, kNrcMaxGroups) : 4u;
   return NR_OK;
 }
 

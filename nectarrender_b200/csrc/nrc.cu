@@ -3,8 +3,8 @@
 // Input vector (64 BF16 channels): [0, 32) hash-grid features (16 levels x 2),
 // [32, 48) real spherical harmonics of degree 0-3 of the outgoing direction,
 // [48, 51) normal * 0.5 + 0.5, [51] roughness, [52, 55) diffuse albedo, zero
-// padding. MLP: 64 -> 64 -> 64 -> 64 (ReLU) -> 16 (linear; the first three
-// outputs are the radiance), no biases. Loss: relative squared error
+// padding. MLP: four hidden layers 64 -> 64 (ReLU), then 64 -> 16 (linear;
+// the first three outputs are the radiance), no biases. Loss: relative squared error
 // (o - t)^2 / (o^2 + 0.01) with o held constant in the denominator.
 #include "nrc.cuh"
 
@@ -21,6 +21,7 @@ namespace {
 constexpr int kLevels = 16, kFeat = 2, kLog2T = 19;
 constexpr uint32_t kT = 1u << kLog2T;
 constexpr int kWidth = 64, kOutCh = 16;
+constexpr int kHidden = 4, kLayers = kHidden + 1;
 constexpr float kNmin = 16.0f, kNmax = 2048.0f;
 
 #define GRID_STRIDE(i, n) \
@@ -191,6 +192,28 @@ __global__ void k_adam(float* w, float* m, float* v, const float* g, size_t n, f
   }
 }
 
+// Adam on the hash grid, lazily: only entries with a nonzero gradient move
+// (the others keep their moments), and the gradient is cleared as it is
+// read, so the next step needs no memset of the 64 MB gradient table.
+__global__ void k_adam_grid(float* w, float* m, float* v, float4* g4, size_t n4, float lr,
+                            float b1, float b2, float eps, float c1, float c2) {
+  GRID_STRIDE(i, n4) {
+    const float4 g = g4[i];
+    if (g.x == 0.0f && g.y == 0.0f && g.z == 0.0f && g.w == 0.0f) continue;
+    g4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    const float gs[4] = {g.x, g.y, g.z, g.w};
+    for (int k = 0; k < 4; ++k) {
+      if (gs[k] == 0.0f) continue;
+      const size_t j = 4 * i + k;
+      const float mi = b1 * m[j] + (1.0f - b1) * gs[k];
+      const float vi = b2 * v[j] + (1.0f - b2) * gs[k] * gs[k];
+      m[j] = mi;
+      v[j] = vi;
+      w[j] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+    }
+  }
+}
+
 // BF16 forward [out][in] and transposed [in][out] copies of a layer
 __global__ void k_pack(const float* w, __nv_bfloat16* wf, __nv_bfloat16* wt, int nout, int nin) {
   const size_t n = (size_t)nout * nin;
@@ -207,16 +230,17 @@ __global__ void k_pack(const float* w, __nv_bfloat16* wf, __nv_bfloat16* wt, int
 struct NrcNet {
   uint32_t max_q = 0;
   GridGeo geo{};
-  int nout[4] = {kWidth, kWidth, kWidth, kOutCh};
-  float *w[4], *mw[4], *vw[4], *gw[4];
-  __nv_bfloat16 *wf[4], *wt[4];
+  int nout[kLayers] = {kWidth, kWidth, kWidth, kWidth, kOutCh};
+  float *w[kLayers], *mw[kLayers], *vw[kLayers], *gw[kLayers];
+  __nv_bfloat16 *wf[kLayers], *wt[kLayers];
   float *grid, *mg, *vg, *gg;
-  __nv_bfloat16 *x0, *h[3], *o, *d_o, *dh, *dz;
+  __nv_bfloat16 *x0, *h[kHidden], *o, *d_o, *dh, *dz;
   double* d_loss = nullptr;
   uint32_t* d_err = nullptr;
   std::vector<void*> allocs;
   int step = 0;
   uint32_t last_count = 0;
+  bool gg_clear = false;  // the grid gradient table is all zero
 };
 
 Nrc::~Nrc() {
@@ -265,11 +289,11 @@ cudaError_t forward(NrcNet& n, const NrcQuery* q, uint32_t count, cudaStream_t s
   k_encode<<<blocks_for(count), 256, 0, st>>>(n.geo, q, n.grid, n.x0, count);
   cudaError_t e;
   const __nv_bfloat16* in = n.x0;
-  for (int l = 0; l < 3; ++l) {
+  for (int l = 0; l < kHidden; ++l) {
     if ((e = gemm(n, in, kWidth, n.wf[l], n.h[l], kWidth, count, true, st))) return e;
     in = n.h[l];
   }
-  if ((e = gemm(n, in, kWidth, n.wf[3], n.o, kOutCh, count, false, st))) return e;
+  if ((e = gemm(n, in, kWidth, n.wf[kHidden], n.o, kOutCh, count, false, st))) return e;
   return cudaGetLastError();
 }
 
@@ -309,7 +333,7 @@ std::string nrc_create(Nrc& c, uint32_t max_queries, const float lo[3], const fl
   if ((e = alloc(n, p, cnt)) != cudaSuccess) return cuda_msg(e, "nrc buffers");
   std::mt19937 rng(seed);
   std::vector<float> host;
-  for (int l = 0; l < 4; ++l) {
+  for (int l = 0; l < kLayers; ++l) {
     const size_t k = (size_t)n.nout[l] * kWidth;
     AL(n.w[l], k);
     AL(n.mw[l], k);
@@ -338,7 +362,7 @@ std::string nrc_create(Nrc& c, uint32_t max_queries, const float lo[3], const fl
   cudaMemset(n.vg, 0, ng * 4);
   const size_t q = max_queries;
   AL(n.x0, q * kWidth);
-  for (int l = 0; l < 3; ++l) AL(n.h[l], q * kWidth);
+  for (int l = 0; l < kHidden; ++l) AL(n.h[l], q * kWidth);
   AL(n.o, q * kOutCh);
   AL(n.d_o, q * kOutCh);
   AL(n.dh, q * kWidth);
@@ -369,18 +393,21 @@ std::string nrc_train(Nrc& c, const NrcQuery* q, const float* target, uint32_t c
   NrcNet& n = *c.net;
   if (count > n.max_q) return "nrc: more queries than the cache was created for";
   if (count == 0) return {};
-  for (int l = 0; l < 4; ++l) cudaMemsetAsync(n.gw[l], 0, (size_t)n.nout[l] * kWidth * 4, st);
+  for (int l = 0; l < kLayers; ++l) cudaMemsetAsync(n.gw[l], 0, (size_t)n.nout[l] * kWidth * 4, st);
   const size_t ng = (size_t)kLevels * kT * kFeat;
-  cudaMemsetAsync(n.gg, 0, ng * 4, st);
+  if (!n.gg_clear) cudaMemsetAsync(n.gg, 0, ng * 4, st);
+  n.gg_clear = false;
   cudaMemsetAsync(n.d_loss, 0, sizeof(double), st);
   cudaError_t e = forward(n, q, count, st);
   if (e != cudaSuccess) return cuda_msg(e, "nrc forward");
   k_loss<<<blocks_for(count), 256, 0, st>>>(n.o, target, n.d_o, count, n.d_loss);
   // output layer
-  if ((e = gemm_wgrad(n, n.d_o, kOutCh, n.h[2], kWidth, n.gw[3], count, st))) return cuda_msg(e, "nrc");
-  if ((e = gemm(n, n.d_o, kOutCh, n.wt[3], n.dh, kWidth, count, false, st))) return cuda_msg(e, "nrc");
-  // hidden layers 2, 1, 0: dz = dh * (h > 0)
-  for (int l = 2; l >= 0; --l) {
+  if ((e = gemm_wgrad(n, n.d_o, kOutCh, n.h[kHidden - 1], kWidth, n.gw[kHidden], count, st)))
+    return cuda_msg(e, "nrc");
+  if ((e = gemm(n, n.d_o, kOutCh, n.wt[kHidden], n.dh, kWidth, count, false, st)))
+    return cuda_msg(e, "nrc");
+  // hidden layers, last to first: dz = dh * (h > 0)
+  for (int l = kHidden - 1; l >= 0; --l) {
     k_mask<<<blocks_for((size_t)count * kWidth), 256, 0, st>>>(n.dh, n.h[l], (size_t)count * kWidth);
     const __nv_bfloat16* in = l > 0 ? n.h[l - 1] : n.x0;
     if ((e = gemm_wgrad(n, n.dh, kWidth, in, kWidth, n.gw[l], count, st))) return cuda_msg(e, "nrc");
@@ -394,12 +421,16 @@ std::string nrc_train(Nrc& c, const NrcQuery* q, const float* target, uint32_t c
     n.step++;
     const float b1 = 0.9f, b2 = 0.99f, eps = 1e-10f;
     const float c1 = 1.0f - std::pow(b1, (float)n.step), c2 = 1.0f - std::pow(b2, (float)n.step);
-    for (int l = 0; l < 4; ++l) {
+    for (int l = 0; l < kLayers; ++l) {
       const size_t k = (size_t)n.nout[l] * kWidth;
       k_adam<<<blocks_for(k), 256, 0, st>>>(n.w[l], n.mw[l], n.vw[l], n.gw[l], k, lr, b1, b2, eps, c1, c2);
       k_pack<<<blocks_for(k), 256, 0, st>>>(n.w[l], n.wf[l], n.wt[l], n.nout[l], kWidth);
     }
-    k_adam<<<blocks_for(ng), 256, 0, st>>>(n.grid, n.mg, n.vg, n.gg, ng, lr, b1, b2, eps, c1, c2);
+    static_assert((kLevels * kT * kFeat) % 4 == 0, "grid table in float4 units");
+    k_adam_grid<<<blocks_for(ng / 4), 256, 0, st>>>(n.grid, n.mg, n.vg,
+                                                    reinterpret_cast<float4*>(n.gg), ng / 4, lr,
+                                                    b1, b2, eps, c1, c2);
+    n.gg_clear = true;
   }
   e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_msg(e, "nrc train");
@@ -432,7 +463,7 @@ size_t nrc_count(const Nrc& c, int what) {
   if (!c.net) return 0;
   if (what <= 1) {
     size_t s = 0;
-    for (int l = 0; l < 4; ++l) s += (size_t)c.net->nout[l] * kWidth;
+    for (int l = 0; l < kLayers; ++l) s += (size_t)c.net->nout[l] * kWidth;
     return s;
   }
   if (what <= 3) return (size_t)kLevels * kT * kFeat;
@@ -444,7 +475,7 @@ std::string nrc_get(const Nrc& c, int what, float* host) {
   const NrcNet& n = *c.net;
   cudaDeviceSynchronize();
   if (what <= 1) {
-    for (int l = 0; l < 4; ++l) {
+    for (int l = 0; l < kLayers; ++l) {
       const size_t k = (size_t)n.nout[l] * kWidth;
       cudaMemcpy(host, what ? n.gw[l] : n.w[l], k * 4, cudaMemcpyDeviceToHost);
       host += k;
@@ -465,7 +496,7 @@ std::string nrc_set_weights(Nrc& c, const float* mlp, const float* grid) {
   if (!c.net) return "nrc: not created";
   NrcNet& n = *c.net;
   if (mlp)
-    for (int l = 0; l < 4; ++l) {
+    for (int l = 0; l < kLayers; ++l) {
       const size_t k = (size_t)n.nout[l] * kWidth;
       cudaMemcpy(n.w[l], mlp, k * 4, cudaMemcpyHostToDevice);
       k_pack<<<blocks_for(k), 256>>>(n.w[l], n.wf[l], n.wt[l], n.nout[l], kWidth);

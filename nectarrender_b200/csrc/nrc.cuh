@@ -31,7 +31,8 @@ std::string nrc_create(Nrc& n, uint32_t max_queries, const float bounds_lo[3],
                        const float bounds_hi[3], uint32_t seed);
 // radiance out[q] (float3 per query, stride 3) for q < count
 std::string nrc_infer(Nrc& n, const NrcQuery* q, uint32_t count, float* out, cudaStream_t st);
-// one Adam step toward target radiance (float3 per query); *loss = mean
+// one Adam step toward target radiance (float3 per query; lazy on the hash
+// grid: entries that no query touched keep their values and moments); *loss = mean
 // relative squared error before the step (when loss is not null; reading
 // it synchronises the stream)
 std::string nrc_train(Nrc& n, const NrcQuery* q, const float* target, uint32_t count, float lr,

@@ -1015,14 +1015,19 @@ __global__ void k_nrc_apply(WfParams W, const float* radiance, uint32_t n) {
   }
 }
 
-__global__ void k_nrc_targets(WfParams W, float* target, uint32_t n) {
+// The radiance behind a training record: what the path gathered from this
+// hit on, divided by its throughput at the hit.
+__global__ void k_nrc_targets(WfParams W, float* target, float4* records, uint32_t n,
+                              uint32_t groups, uint32_t per) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const float4 b = W.nrc_t_beta[i], before = W.nrc_t_before[i];
     const float4 after = W.acc_b[__float_as_uint(b.w)];
     const float beta[3] = {b.x, b.y, b.z};
     const float d[3] = {after.x - before.x, after.y - before.y, after.z - before.z};
+    const size_t slot = (size_t)(i % groups) * per + i / groups;
     for (int c = 0; c < 3; ++c)
-      target[3 * i + c] = beta[c] > 1e-6f ? fminf(fmaxf(d[c] / beta[c], 0.0f), 1e4f) : 0.0f;
+      target[3 * slot + c] = beta[c] > 1e-6f ? fminf(fmaxf(d[c] / beta[c], 0.0f), 1e4f) : 0.0f;
+    for (int k = 0; k < 4; ++k) records[4 * slot + k] = W.nrc_t[4 * (size_t)i + k];
   }
 }
 
@@ -1063,9 +1068,13 @@ cudaError_t wf_nrc_apply(const WfParams& W, const float* radiance, uint32_t n, c
   return cudaGetLastError();
 }
 
-cudaError_t wf_nrc_targets(const WfParams& W, float* target, uint32_t n, cudaStream_t st) {
+cudaError_t wf_nrc_targets(const WfParams& W, float* target, float4* records, uint32_t n,
+                           uint32_t groups, cudaStream_t st) {
   if (!n) return cudaSuccess;
-  k_nrc_targets<<<(int)std::min<uint32_t>((n + 255) / 256, 148 * 16), 256, 0, st>>>(W, target, n);
+  groups = std::max(1u, std::min(groups, n));
+  const uint32_t per = (n + groups - 1) / groups;
+  k_nrc_targets<<<(int)std::min<uint32_t>((n + 255) / 256, 148 * 16), 256, 0, st>>>(
+      W, target, records, n, groups, per);
   return cudaGetLastError();
 }
 

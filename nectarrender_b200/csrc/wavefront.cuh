@@ -90,7 +90,11 @@ cudaError_t wf_launch_wave(const WfParams& W, bool counters, cudaStream_t st,
 // before it, over the throughput at the hit).
 cudaError_t wf_nrc_counts(const WfParams& W, uint32_t* n_q, uint32_t* n_t, cudaStream_t st);
 cudaError_t wf_nrc_apply(const WfParams& W, const float* radiance, uint32_t n_q, cudaStream_t st);
-cudaError_t wf_nrc_targets(const WfParams& W, float* target, uint32_t n_t, cudaStream_t st);
+// Training targets of the wave's n_t records, regrouped into `groups`
+// interleaved batches: record i goes to slot (i % groups) * per + i / groups
+// of target (float3) and of records (4 float4), per = ceil(n_t / groups).
+cudaError_t wf_nrc_targets(const WfParams& W, float* target, float4* records, uint32_t n_t,
+                           uint32_t groups, cudaStream_t st);
 cudaError_t wf_set_base(const WfParams& W, uint32_t first_sample, cudaStream_t st);
 
 }  // namespace nr

@@ -11,6 +11,7 @@ import numpy as np
 from . import capi, library
 
 LEVELS, FEAT, LOG2T = 16, 2, 19
+LAYERS = (64, 64, 64, 64, 16)  # output widths: four hidden layers, then the output
 
 
 def _f(t):
@@ -63,7 +64,7 @@ class RadianceCache:
 
     def mlp_layers(self, flat):
         out, o = [], 0
-        for nout in (64, 64, 64, 16):
+        for nout in LAYERS:
             out.append(flat[o:o + nout * 64].reshape(nout, 64))
             o += nout * 64
         return out

@@ -20,6 +20,8 @@ the reference's factories; ``to_pathtracer`` turns a spec into objects of the
   256 spheres with radii U(0.05, 0.3) and materials drawn uniformly from
   Lambertian/PBR/dielectric; a 2048x1024 equirectangular HDRI with a
   log-normal sky (mu=0, sigma=1) and a sun disk of radiance 1e4.
+* ``medium_stress`` — the radiance-cache configuration: ``mesh_stress`` plus
+  a 2x2x2 box of isotropic medium (sigma_t 0.5, albedo 0.9), depth 32.
 """
 from __future__ import annotations
 
@@ -306,6 +308,19 @@ def mesh_stress(levels: int = 8, res_h: int = 1080, res_w: int = 1920, spp: int 
     sky = {"type": SKY_HDRI, "path": str(hdr_path), "rotation": 0.0, "intensity": 1.0}
     return SceneSpec(objects=objs, camera=cam, ray_depth=depth, seed=seed, sky=sky,
                      meshes=[str(obj_path)], name=f"mesh_stress_l{levels}_{res_h}x{res_w}")
+
+
+def medium_stress(levels: int = 8, res_h: int = 1080, res_w: int = 1920, spp: int = 256,
+                  depth: int = 32, seed: int = 0, n_spheres: int = 256,
+                  hdri_size: tuple[int, int] = (2048, 1024), scene_seed: int = 0) -> SceneSpec:
+    """The mesh-stress scene inside a 2x2x2 box of isotropic homogeneous
+    medium (sigma_t = 0.5, albedo 0.9) centred on the mesh, depth 32: the
+    radiance-cache configuration."""
+    spec = mesh_stress(levels, res_h, res_w, spp, depth, seed, n_spheres, hdri_size, scene_seed)
+    spec.objects.append(obj(MEDIUM, isotropic((0.9, 0.9, 0.9)), (0, 0, 0), (0, 0, 0), (2, 2, 2),
+                            wrapped=CUBE, density=0.5))
+    spec.name = f"medium_stress_l{levels}_{res_h}x{res_w}"
+    return spec
 
 
 # ---------------------------------------------------------------------------

@@ -72,10 +72,11 @@ def test_encoding_and_gradients_match_fp64():
     assert (x0[:, 55:] == 0).all()
     # MLP forward and backward in FP64 on the BF16 weights
     W = [bf(w) for w in cache.mlp_layers(cache.get(0))]
+    hidden = len(nrc.LAYERS) - 1
     h = [x0]
-    for l in range(3):
+    for l in range(hidden):
         h.append(bf(np.maximum(h[-1] @ W[l].T, 0)))
-    o = bf(h[-1] @ W[3].T)
+    o = bf(h[-1] @ W[hidden].T)
     oc = o[:, :3]
     den = oc * oc + 0.01
     loss_ref = ((oc - target) ** 2 / den).mean()
@@ -83,15 +84,15 @@ def test_encoding_and_gradients_match_fp64():
     g = np.zeros_like(o)
     g[:, :3] = 2 * (oc - target) / den
     g = bf(g)
-    grads = [None] * 4
-    grads[3] = g.T @ h[3]
-    dh = g @ W[3]
-    for l in (2, 1, 0):
+    grads = [None] * (hidden + 1)
+    grads[hidden] = g.T @ h[hidden]
+    dh = g @ W[hidden]
+    for l in reversed(range(hidden)):
         dz = dh * (h[l + 1] > 0)
         grads[l] = dz.T @ h[l]
         dh = dz @ W[l]
     got = cache.mlp_layers(cache.get(1))
-    for l in range(4):
+    for l in range(hidden + 1):
         a, b = got[l].ravel().astype(np.float64), grads[l].ravel()
         cos = a @ b / (np.linalg.norm(a) * np.linalg.norm(b))
         rel = np.linalg.norm(a - b) / np.linalg.norm(b)
