@@ -59,10 +59,14 @@ def parse():
     p.add_argument("--mesh-leaf", type=int, default=1)
     p.add_argument("--shade-variant", type=int, default=0,
                    help="shading kernel register budget (0: library default)")
+    p.add_argument("--sort-materials", type=int, default=0,
+                   help="shade each bounce's queue grouped by material type: 1 on, -1 off, "
+                        "0 the library default (on)")
     p.add_argument("--no-rmse", action="store_true", help="skip the time-to-RMSE measurement")
     p.add_argument("--rmse-oracle-spp", type=int, default=8192)
     p.add_argument("--no-denoiser", action="store_true", help="skip training the learned denoiser")
     p.add_argument("--no-multi", action="store_true", help="skip the multi-scene measurement")
+    p.add_argument("--no-nrc", action="store_true", help="skip the radiance-cache measurement")
     p.add_argument("--denoiser-seconds", type=float, default=40.0)
     return p.parse_args()
 
@@ -83,6 +87,8 @@ def config_json(args, h, w, spec, l2):
             "spp_per_step": args.spp_per_step,
             "integrator": f"reference-compatible, {args.schedule} schedule",
             "extend_variant": args.extend_variant or "default", "mesh_leaf": args.mesh_leaf,
+            "shade_variant": args.shade_variant or "default",
+            "sort_materials": args.sort_materials,
             "parallelism": f"sample-sharded x{args.gpus}", "l2": l2}
 
 
@@ -220,7 +226,8 @@ def run_ours(args):
     build_wall = time.perf_counter() - t_build
     stats = scene.stats()
     render = capi.Render(scene, schedule=1 if args.schedule == "wavefront" else 0,
-                         extend_variant=args.extend_variant, shade_variant=args.shade_variant)
+                         extend_variant=args.extend_variant, shade_variant=args.shade_variant,
+                         sort_materials=args.sort_materials)
     stream_handle = ctypes.c_uint64()
     lib.nr_render_stream(render.h, ctypes.byref(stream_handle))
     stream = torch.cuda.ExternalStream(stream_handle.value)
@@ -342,6 +349,9 @@ def run_ours(args):
     learned = None
     if rank == 0 and world == 1 and not args.no_denoiser:
         learned = learned_kernels(peaks)
+    cache = None
+    if rank == 0 and world == 1 and not args.no_nrc:
+        cache = radiance_cache(args)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -375,6 +385,7 @@ def run_ours(args):
                 "reference_cuda": ref_cuda,
                 "time_to_rmse": rmse,
                 "learned_kernels": learned,
+                "radiance_cache": cache,
                 "multi_scene": multi,
                 "scene": {"build_ms_device": stats["build_ms"], "build_wall_s": build_wall,
                           "triangles": stats["n_triangles"], "wide_nodes": stats["wide_nodes"],
@@ -464,6 +475,90 @@ def multi_scene(args):
                                              "CUDA events, scene builds excluded"}
         except Exception as e:  # noqa: BLE001 - reported, not fatal
             out["reference_cuda"] = {"unavailable": repr(e)[:200]}
+    return out
+
+
+def radiance_cache(args, top=512):
+    """The online radiance cache against plain perf mode, on the
+    radiance-cache configuration (mesh-stress scene in a 2x2x2 box of
+    isotropic medium, depth 32) and on the closed Cornell box at depth 32,
+    both small enough for an FP64 high-sample oracle. Curves of (samples,
+    device ms, RMSE) in the time-to-RMSE domain; the cached render's time
+    includes its 32-sample warm-up (trained, then discarded) and every
+    training step. Plus the cost of one training step and one inference on
+    16384 records."""
+    import torch
+    from nectarrender_b200 import capi, nrc
+    out = {"settings": {"terminate_bounce": 2, "train_one_in": 16, "lr": 1e-2, "batch": 16384,
+                        "min_steps_per_wave": 8, "samples_per_wave": 8, "warmup_spp": 32},
+           "domain": "sqrt(clamp(x,0,1)), all pixels x 3 channels"}
+    n_or = args.rmse_oracle_spp
+    cases = (("medium_stress 320x192, depth 32",
+              scenes.medium_stress(levels=args.levels, res_h=192, res_w=320, spp=n_or + 1)),
+             ("cornell 128x128, depth 32", scenes.cornell(res=128, spp=n_or + 1, depth=32, seed=0)))
+    for name, spec in cases:
+        sc = capi.Scene(spec, mesh_leaf=args.mesh_leaf)
+        orc = capi.Render(sc, mode=capi.MODE_PERF, fp64_accumulate=1, seed=spec.seed + 1000)
+        orc.samples(1, n_or)
+        disp_o = np.sqrt(np.clip(orc.beauty_fp64(), 0.0, 1.0))
+        del orc
+        rmse_of = lambda img: float(np.sqrt(np.mean((np.sqrt(np.clip(img, 0.0, 1.0)) - disp_o) ** 2)))
+
+        def curve(r, t_ms):
+            done, n, pts = 0, 1, []
+            while done + n <= top:
+                r.samples(done + 1, n)
+                t_ms += r.last_ms()
+                done += n
+                pts.append([done, round(t_ms, 3), round(rmse_of(r.beauty_fp64()), 5)])
+                n = done
+            return pts
+
+        plain = capi.Render(sc, mode=capi.MODE_PERF, fp64_accumulate=1, seed=spec.seed)
+        plain.samples(1, 1)  # first call allocates the wave state: not part of the curve
+        plain.reset()
+        p_curve = curve(plain, 0.0)
+        del plain
+        lo, hi = sc.bounds()
+        c = nrc.RadianceCache(1 << 18, lo, hi, seed=1)
+        st = out["settings"]
+        r = capi.Render(sc, mode=capi.MODE_PERF, fp64_accumulate=1, seed=spec.seed,
+                        samples_per_wave=st["samples_per_wave"])
+        r.set_nrc(c, st["terminate_bounce"], st["train_one_in"], st["lr"], st["batch"],
+                  st["min_steps_per_wave"])
+        r.samples(n_or // 2, st["warmup_spp"])
+        warm_ms = r.last_ms()
+        r.reset()
+        c_curve = curve(r, warm_ms)
+        queries, records = r.nrc_stats()
+        del r, c
+        at = lambda cv, spp: next(e for n, _, e in cv if n == spp)
+        best = None
+        for spp_c, ms_c, e_c in c_curve:
+            hit = next((ms for _, ms, e in p_curve if e <= e_c), None)
+            if hit is not None and (best is None or hit / ms_c > best[0]):
+                best = (hit / ms_c, e_c, spp_c)
+        out[name] = {
+            "plain_perf": p_curve, "cached": c_curve, "warmup_ms": warm_ms,
+            "cache_queries": queries, "training_records": records,
+            "rmse_at_16spp": {"plain": at(p_curve, 16), "cached": at(c_curve, 16)},
+            "speedup_at_equal_rmse": ({"speedup": best[0], "rmse": best[1], "cached_spp": best[2]}
+                                      if best else "plain perf mode reaches no cached error "
+                                                   "point later than the cache does")}
+    c = nrc.RadianceCache(1 << 14, (-1, -1, -1), (1, 1, 1), seed=0)
+    q = torch.rand((1 << 14, 16), device="cuda")
+    t = torch.rand((1 << 14, 3), device="cuda")
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for what, fn in (("train_step_ms_16384", lambda: c.train(q, t, 1e-2, want_loss=False)),
+                     ("infer_ms_16384", lambda: c.infer(q))):
+        for _ in range(3):
+            fn()
+        e0.record()
+        for _ in range(20):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        out[what] = e0.elapsed_time(e1) / 20
     return out
 
 

@@ -180,6 +180,11 @@ typedef struct nr_render_config {
   int32_t shade_variant;    /* wavefront shading kernel register budget: 5 or
                                6 CTAs of 128 threads per SM, any other value
                                128 registers; 0 = default (6)               */
+  int32_t sort_materials;   /* wavefront: from bounce 1 on, shade the queue
+                               grouped by material type (misses first): the
+                               extend kernel counts the keys, one pass sorts
+                               the queue; 1 = on, negative = off, 0 = default
+                               (on)                                         */
 } nr_render_config;
 
 /* StreamConfig display fields (nectar_render/csrc/data/include/data/stream.h:13-30). */

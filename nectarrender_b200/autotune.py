@@ -14,6 +14,8 @@ speed but never the image:
     of the path queues (paths = W*H*samples_per_wave);
   * ``shade_variant`` - register budget of the shading kernel (5 or 6 CTAs
     per SM, or 128 registers);
+  * ``sort_materials`` - shade each bounce's queue grouped by material type
+    (1) or in queue order (-1);
   * ``schedule`` - wavefront or the per-pixel megakernel.
 
 Every candidate renders the same samples (the parity tests cover each knob),
@@ -40,13 +42,15 @@ class Tuning:
     extend_variant: int = 514
     samples_per_wave: int = 0
     shade_variant: int = 6
+    sort_materials: int = 1
     schedule: int = capi.SCHEDULE_WAVEFRONT
     ms_per_sample: float = 0.0
     table: list = field(default_factory=list)
 
     def render_overrides(self) -> dict:
         return {"extend_variant": self.extend_variant, "samples_per_wave": self.samples_per_wave,
-                "shade_variant": self.shade_variant, "schedule": self.schedule}
+                "shade_variant": self.shade_variant, "sort_materials": self.sort_materials,
+                "schedule": self.schedule}
 
     def scene_overrides(self) -> dict:
         return {"mesh_leaf": self.mesh_leaf, "tlas_leaf": self.tlas_leaf}
@@ -71,19 +75,20 @@ def _time(scene: capi.Scene, spec: SceneSpec, over: dict, samples: int, reps: in
 
 
 def tune(spec: SceneSpec, samples: int = 4, reps: int = 2, leaves=((1, 1), (2, 1), (3, 1), (1, 2)),
-         variants=VARIANTS, waves=(0, 2, 4, 8), shades=(5, 6), megakernel: bool = True) -> Tuning:
+         variants=VARIANTS, waves=(0, 2, 4, 8), shades=(5, 6), sorts=(1, -1),
+         megakernel: bool = True) -> Tuning:
     """Times every candidate on `spec` (device time of `samples` sample
     indices, best of `reps`) and returns the fastest as a :class:`Tuning`."""
     table = []
     best = None
     for mesh_leaf, tlas_leaf in leaves:
         scene = capi.Scene(spec, mesh_leaf=mesh_leaf, tlas_leaf=tlas_leaf)
-        cands = [dict(extend_variant=v, samples_per_wave=w, shade_variant=sv,
+        cands = [dict(extend_variant=v, samples_per_wave=w, shade_variant=sv, sort_materials=so,
                       schedule=capi.SCHEDULE_WAVEFRONT)
-                 for v, w, sv in itertools.product(variants, waves, shades)]
+                 for v, w, sv, so in itertools.product(variants, waves, shades, sorts)]
         if megakernel:
             cands.append(dict(extend_variant=0, samples_per_wave=0, shade_variant=0,
-                              schedule=capi.SCHEDULE_MEGAKERNEL))
+                              sort_materials=-1, schedule=capi.SCHEDULE_MEGAKERNEL))
         for over in cands:
             ms = _time(scene, spec, over, samples, reps)
             row = dict(mesh_leaf=mesh_leaf, tlas_leaf=tlas_leaf, ms_per_sample=ms, **over)
@@ -92,8 +97,8 @@ def tune(spec: SceneSpec, samples: int = 4, reps: int = 2, leaves=((1, 1), (2, 1
                 best = row
         del scene
     t = Tuning(**{k: best[k] for k in ("mesh_leaf", "tlas_leaf", "extend_variant",
-                                       "samples_per_wave", "shade_variant", "schedule",
-                                       "ms_per_sample")})
+                                       "samples_per_wave", "shade_variant", "sort_materials",
+                                       "schedule", "ms_per_sample")})
     t.table = table
     return t
 

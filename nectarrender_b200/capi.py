@@ -46,7 +46,7 @@ class RenderConfig(C.Structure):
                 ("schedule", C.c_int32), ("fp64_accumulate", C.c_int32), ("layer_mask", C.c_uint32),
                 ("extend_variant", C.c_int32), ("samples_per_wave", C.c_uint32),
                 ("use_graphs", C.c_int32), ("tail_max_paths", C.c_uint32),
-                ("shade_variant", C.c_int32)]
+                ("shade_variant", C.c_int32), ("sort_materials", C.c_int32)]
 
 
 class StreamConfig(C.Structure):

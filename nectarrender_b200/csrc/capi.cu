@@ -1381,7 +1381,8 @@ static int launch(nr_render* r, const KernelParams& P, WaveTimer* tm) {
   uint32_t N = r->W * r->H;
   if (!r->wf.capacity) {
     r->samples_per_wave = waves_of(r);
-    CU(wf_alloc(r->wf, r->samples_per_wave * N, r->cfg.mode == NR_MODE_PERF),
+    CU(wf_alloc(r->wf, r->samples_per_wave * N, r->cfg.mode == NR_MODE_PERF,
+                r->cfg.sort_materials >= 0),
        "allocate wavefront state");
   }
   uint32_t per = P.write_raw ? 1u : r->samples_per_wave;

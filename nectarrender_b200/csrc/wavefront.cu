@@ -42,6 +42,38 @@ enum : uint32_t {
   CTR_NT = 9,      // radiance-cache training records of the wave
 };
 
+constexpr int kSortKeys = 8;  // shade_key values
+
+// Shading key of a hit: 0 for a miss, else its material type (1..7), so
+// that a warp of the binned queue runs one branch of the BSDF dispatch.
+__device__ __forceinline__ uint32_t shade_key(const DevScene& sc, uint32_t obj) {
+  if (obj == 0xffffffffu) return 0u;
+  const int32_t t = sc.materials[sc.objects[obj].material].type;
+  return (uint32_t)min(max(t, 1), (int32_t)kSortKeys - 1);
+}
+
+// Material sort of a bounce's queue, pass 1 inside the extend kernels: the
+// kernel that writes a path's hit also stores its shading key (skey, one
+// byte per path: 8 MB for 8 M paths, resident in L2) and counts the keys
+// in a shared-memory histogram that is added to sort_ctr[0..7] at exit.
+// Pass 2 (k_wf_bin_scatter) moves the queue into key order.
+struct KeyHist {
+  uint32_t* h;  // shared memory, kSortKeys counters
+  __device__ void init() {
+    if (threadIdx.x < kSortKeys) h[threadIdx.x] = 0u;
+    __syncthreads();
+  }
+  __device__ void add(const WfParams& W, const DevScene& sc, uint32_t p, uint32_t obj) {
+    const uint32_t key = shade_key(sc, obj);
+    W.skey[p] = (uint8_t)key;
+    atomicAdd(h + key, 1u);
+  }
+  __device__ void flush(const WfParams& W) {  // every thread of the block
+    __syncthreads();
+    if (threadIdx.x < kSortKeys && h[threadIdx.x]) atomicAdd(&W.sort_ctr[threadIdx.x], h[threadIdx.x]);
+  }
+};
+
 // Features of a hit for the radiance cache (NrcQuery layout, nrc.cuh).
 __device__ __forceinline__ void nrc_features(const DevMaterial& m, const Hit& rec, const V3& wo,
                                              float4* out) {
@@ -376,6 +408,10 @@ __global__ void __launch_bounds__(kExtThreads, kMinBlocks) k_wf_extend(WfParams 
   uint2* blas_stk = wf_smem + kTlasStack * kExtThreads + threadIdx.x;
   TraceStats st{0u, 0u, 0u};
   uint32_t rays = 0;
+  const bool binned = W.queue_s && !identity;  // block-uniform
+  __shared__ uint32_t key_hist[kSortKeys];
+  KeyHist kh{key_hist};
+  if (binned) kh.init();
   while (true) {
     uint32_t base = 0;
     if (lane == 0) base = atomicAdd(&W.ctr[CTR_WORK], 32u);
@@ -383,7 +419,7 @@ __global__ void __launch_bounds__(kExtThreads, kMinBlocks) k_wf_extend(WfParams 
     if (base >= n) break;
     uint32_t i = base + lane;
     if (i < n) {
-      uint32_t p = identity ? i : __ldg(queue + i);
+      const uint32_t p = identity ? i : __ldg(queue + i);
       float4 o = ld4(W.ray_o + p), d = ld4(W.ray_d + p);
       Ray r = make_ray(V3{o.x, o.y, o.z}, V3{d.x, d.y, d.z}, o.w);
       uint32_t obj, slot;
@@ -391,9 +427,11 @@ __global__ void __launch_bounds__(kExtThreads, kMinBlocks) k_wf_extend(WfParams 
       trace_closest<kCount>(P.scene, r, tlas_stk, blas_stk, kExtThreads, obj, slot, t, u, v, st, P.err);
       W.hit[p] = make_uint4(obj, slot, __float_as_uint(u), __float_as_uint(v));
       W.hit_t[p] = t;
+      if (binned) kh.add(W, P.scene, p, obj);
       rays++;
     }
   }
+  if (binned) kh.flush(W);
   if (kCount) {
     unsigned long long vals[4] = {rays, st.nodes, st.tris, st.objs};
 #pragma unroll
@@ -473,6 +511,10 @@ __global__ void __launch_bounds__(kExtThreads, kMinBlocks) k_wf_extend_flat(WfPa
   int sp = 0, best_slot = -1;
   const Bvh8Node* cur_nodes = sc.tlas8;
   const TriRecord* cur_tris = nullptr;
+  const bool binned = W.queue_s && !identity;  // block-uniform
+  __shared__ uint32_t key_hist[kSortKeys];
+  KeyHist kh{key_hist};
+  if (binned) kh.init();
 
   while (true) {
     if (!exhausted) {
@@ -676,9 +718,11 @@ __global__ void __launch_bounds__(kExtThreads, kMinBlocks) k_wf_extend_flat(WfPa
       const uint32_t p = cu(FS_PATH);
       W.hit[p] = make_uint4(cu(FS_OUT_OBJ), cu(FS_OUT_SLOT), cu(FS_OUT_U), cu(FS_OUT_V));
       W.hit_t[p] = cf(FS_OUT_T);
+      if (binned) kh.add(W, sc, p, cu(FS_OUT_OBJ));
       active = false;
     }
   }
+  if (binned) kh.flush(W);
   if (kCount) {
     unsigned long long vals[4] = {rays, nodes, tris, objs};
 #pragma unroll
@@ -694,13 +738,13 @@ __global__ void __launch_bounds__(kExtThreads, kMinBlocks) k_wf_extend_flat(WfPa
 // reference's estimator draw for draw.
 template <bool kPerf, int kMinBlocks>
 __global__ void __launch_bounds__(kShadeThreads, kMinBlocks) k_wf_shade(WfParams W, int qsel,
-                                                                      int identity) {
+                                                                      int identity, int sorted) {
   if (W.ctr[CTR_TAIL]) return;
   __shared__ uint2 shade_stk[kBlasStack * kShadeThreads];
   const KernelParams& P = W.kp;
   const DevScene& sc = P.scene;
   const uint32_t n = W.ctr[qsel];
-  const uint32_t* queue = qsel == 0 ? W.queue0 : W.queue1;
+  const uint32_t* queue = sorted ? W.queue_s : (qsel == 0 ? W.queue0 : W.queue1);
   uint32_t* next_queue = qsel == 0 ? W.queue1 : W.queue0;
   uint32_t* next_n = &W.ctr[qsel == 0 ? CTR_N1 : CTR_N0];
   const uint32_t N = P.W * P.H;
@@ -962,6 +1006,40 @@ __global__ void k_wf_rotate(WfParams W, int consumed) {
     W.ctr[CTR_SH] = 0u;
     W.ctr[CTR_SHWORK] = 0u;
   }
+  if (W.sort_ctr && threadIdx.x < 2 * kSortKeys) W.sort_ctr[threadIdx.x] = 0u;
+}
+
+// Material sort, pass 2: every path of the queue to its key's segment of
+// queue_s (segments in key order; within a segment, warps append in the
+// order they reach their atomics).
+__global__ void k_wf_bin_scatter(WfParams W, int qsel) {
+  if (W.ctr[CTR_TAIL]) return;
+  __shared__ uint32_t seg[kSortKeys];
+  if (threadIdx.x == 0) {
+    uint32_t acc = 0;
+    for (int k = 0; k < kSortKeys; ++k) {
+      seg[k] = acc;
+      acc += W.sort_ctr[k];
+    }
+  }
+  __syncthreads();
+  const uint32_t n = W.ctr[qsel];
+  const uint32_t* queue = qsel == 0 ? W.queue0 : W.queue1;
+  const uint32_t lane = threadIdx.x & 31u;
+  for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+    const uint32_t i = base + threadIdx.x;
+    const unsigned act = __ballot_sync(0xffffffffu, i < n);
+    if (i < n) {
+      const uint32_t p = __ldg(queue + i);
+      const uint32_t key = W.skey[p];
+      const unsigned peers = __match_any_sync(act, key);
+      const uint32_t leader = (uint32_t)(__ffs(peers) - 1);
+      uint32_t at = 0;
+      if (lane == leader) at = atomicAdd(&W.sort_ctr[kSortKeys + key], (uint32_t)__popc(peers));
+      at = __shfl_sync(peers, at, leader);
+      W.queue_s[seg[key] + at + __popc(peers & ((1u << lane) - 1u))] = p;
+    }
+  }
 }
 
 __global__ void k_wf_accumulate(WfParams W) {
@@ -1083,13 +1161,14 @@ cudaError_t wf_set_base(const WfParams& W, uint32_t first_sample, cudaStream_t s
   return cudaGetLastError();
 }
 
-size_t wf_state_bytes(uint32_t n_paths, bool perf) {
+size_t wf_state_bytes(uint32_t n_paths, bool perf, bool sort) {
   size_t per = 6 * sizeof(float4) + sizeof(uint4) + sizeof(float) + 2 * sizeof(uint32_t);
   if (perf) per += sizeof(float) + 3 * sizeof(float4) + sizeof(uint32_t);
+  if (sort) per += sizeof(uint32_t) + sizeof(uint8_t);
   return (size_t)n_paths * per;
 }
 
-cudaError_t wf_alloc(WfParams& W, uint32_t n_paths, bool perf) {
+cudaError_t wf_alloc(WfParams& W, uint32_t n_paths, bool perf, bool sort) {
   cudaError_t e;
 #define A(ptr, T) \
   if ((e = cudaMalloc(&W.ptr, sizeof(T) * (size_t)n_paths)) != cudaSuccess) return e;
@@ -1109,6 +1188,12 @@ cudaError_t wf_alloc(WfParams& W, uint32_t n_paths, bool perf) {
     A(sh_d, float4);
     A(sh_c, float4);
     A(sh_queue, uint32_t);
+  }
+  if (sort) {
+    A(queue_s, uint32_t);
+    A(skey, uint8_t);
+    if ((e = cudaMalloc(&W.sort_ctr, 2 * kSortKeys * sizeof(uint32_t))) != cudaSuccess) return e;
+    if ((e = cudaMemset(W.sort_ctr, 0, 2 * kSortKeys * sizeof(uint32_t))) != cudaSuccess) return e;
   }
 #undef A
   if ((e = cudaMalloc(&W.ctr, 16 * sizeof(uint32_t))) != cudaSuccess) return e;
@@ -1132,6 +1217,9 @@ void wf_free(WfParams& W) {
   cudaFree(W.sh_d);
   cudaFree(W.sh_c);
   cudaFree(W.sh_queue);
+  cudaFree(W.queue_s);
+  cudaFree(W.skey);
+  cudaFree(W.sort_ctr);
   cudaFree(W.ctr);
   W = WfParams{};
 }
@@ -1201,18 +1289,26 @@ cudaError_t wf_launch_wave(const WfParams& W, bool counters, cudaStream_t st, Wa
     if (b == 0) ext0<<<eb0, kExtThreads, smem0, st>>>(W, q, 1);
     else ext<<<eb, kExtThreads, smem, st>>>(W, q, 0);
     if (tm) tm->mark(NR_KERNEL_EXTEND, st);
+    // camera rays keep pixel order; from bounce 1 on the extend kernel
+    // counts the material keys and one pass sorts the queue by them
+    const int sorted = (W.queue_s && b > 0) ? 1 : 0;
+    if (sorted) {
+      k_wf_bin_scatter<<<shade_blocks, kShadeThreads, 0, st>>>(W, q);
+      if (tm) tm->mark(NR_KERNEL_ROTATE, st);
+    }
+    const int identity = b == 0 ? 1 : 0;
     if (W.mis_pdf) {
-      k_wf_shade<true, 1><<<shade_blocks, kShadeThreads, 0, st>>>(W, q, b == 0 ? 1 : 0);
+      k_wf_shade<true, 1><<<shade_blocks, kShadeThreads, 0, st>>>(W, q, identity, sorted);
       if (tm) tm->mark(NR_KERNEL_SHADE, st);
       k_wf_shadow<<<sm_count() * 4, kExtThreads, kExtStackBytes, st>>>(W);
       if (tm) tm->mark(NR_KERNEL_EXTEND, st);
     } else {
       if (W.shade_variant == 5)
-        k_wf_shade<false, 5><<<shade_blocks, kShadeThreads, 0, st>>>(W, q, b == 0 ? 1 : 0);
+        k_wf_shade<false, 5><<<shade_blocks, kShadeThreads, 0, st>>>(W, q, identity, sorted);
       else if (W.shade_variant == 6)
-        k_wf_shade<false, 6><<<shade_blocks, kShadeThreads, 0, st>>>(W, q, b == 0 ? 1 : 0);
+        k_wf_shade<false, 6><<<shade_blocks, kShadeThreads, 0, st>>>(W, q, identity, sorted);
       else
-        k_wf_shade<false, 1><<<shade_blocks, kShadeThreads, 0, st>>>(W, q, b == 0 ? 1 : 0);
+        k_wf_shade<false, 1><<<shade_blocks, kShadeThreads, 0, st>>>(W, q, identity, sorted);
       if (tm) tm->mark(NR_KERNEL_SHADE, st);
     }
     k_wf_rotate<<<1, 32, 0, st>>>(W, q);

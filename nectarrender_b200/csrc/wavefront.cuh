@@ -46,10 +46,17 @@ struct WfParams {
   float4* nrc_t;       // [cap][4]
   float4* nrc_t_beta;  // xyz throughput, w path index
   float4* nrc_t_before;
+  // material-key sort of each bounce's queue before shading (null: off):
+  // skey[p] is path p's key (miss, then material type) written by the
+  // extend kernel, queue_s receives the queue grouped by key, sort_ctr holds
+  // 8 key counts followed by 8 fill cursors
+  uint32_t* queue_s;
+  uint8_t* skey;
+  uint32_t* sort_ctr;
 };
 
-size_t wf_state_bytes(uint32_t n_paths, bool perf = false);
-cudaError_t wf_alloc(WfParams& W, uint32_t n_paths, bool perf = false);
+size_t wf_state_bytes(uint32_t n_paths, bool perf = false, bool sort = false);
+cudaError_t wf_alloc(WfParams& W, uint32_t n_paths, bool perf = false, bool sort = false);
 void wf_free(WfParams& W);
 // static_wave.cu: address of the library-owned wave buffer on the current
 // device, and its division into the wave's arrays (capacity
