@@ -6,13 +6,29 @@
 // padding. MLP: four hidden layers 64 -> 64 (ReLU), then 64 -> 16 (linear;
 // the first three outputs are the radiance), no biases. Loss: relative squared error
 // (o - t)^2 / (o^2 + 0.01) with o held constant in the denominator.
+//
+// The whole MLP is one fused tcgen05 kernel per call (k_mlp): a CTA of 128
+// threads takes 128 queries at a time, one row per thread and one
+// tensor-memory lane per row. The five weight matrices and every activation
+// tile stay in shared memory (BF16, no-swizzle canonical layouts), each layer
+// is 1-4 MMAs of M = 128, N = 64 (16 for the output layer), K = 16 issued by
+// one thread into a tensor-memory accumulator, and the epilogues (ReLU, the
+// loss gradient, the ReLU mask of the backward pass) run on the rows the
+// threads load back with tcgen05.ld. In training the backward-data GEMM of
+// each layer and its weight-gradient GEMM (dW += dZ^T X over the tile's rows,
+// both operands read MN-major from the same tiles) are issued together; the
+// weight gradients accumulate in tensor memory over all the CTA's tiles and
+// are added to the FP32 gradient with atomics once at the end, and the
+// hash-grid gradient is scattered straight from the input-gradient rows. A
+// training step is: encode, k_mlp, one Adam launch for the MLP and one for the
+// grid.
 #include "nrc.cuh"
 
 #include <cmath>
 #include <random>
 #include <vector>
 
-#include "conv_tc.cuh"
+#include "tcgen05.cuh"
 
 namespace nr {
 
@@ -22,6 +38,8 @@ constexpr int kLevels = 16, kFeat = 2, kLog2T = 19;
 constexpr uint32_t kT = 1u << kLog2T;
 constexpr int kWidth = 64, kOutCh = 16;
 constexpr int kHidden = 4, kLayers = kHidden + 1;
+constexpr int kRows = 128;  // queries per tile = threads per CTA of k_mlp
+constexpr uint32_t kWaitLimit = 1u << 26;
 constexpr float kNmin = 16.0f, kNmax = 2048.0f;
 
 #define GRID_STRIDE(i, n) \
@@ -126,70 +144,260 @@ __global__ void k_encode(GridGeo g, const NrcQuery* qs, const float* grid, __nv_
   }
 }
 
-// gradient of the loss with respect to the grid values: the adjoint of the
-// trilinear interpolation, scattered with atomics
-__global__ void k_encode_bwd(GridGeo g, const NrcQuery* qs, const __nv_bfloat16* dx, float* ggrid,
-                             uint32_t n) {
-  GRID_STRIDE(i, n) {
-    const NrcQuery q = qs[i];
-    const __nv_bfloat16* row = dx + i * kWidth;
-    float u[3];
-    unit_pos(g, q, u);
-    for (int l = 0; l < kLevels; ++l) {
-      const float d0 = __bfloat162float(row[2 * l]), d1 = __bfloat162float(row[2 * l + 1]);
-      if (d0 == 0.0f && d1 == 0.0f) continue;
-      float* lv = ggrid + (size_t)l * kT * kFeat;
-      corners(g, l, u, [&](uint32_t idx, float w) {
-        atomicAdd(lv + idx * kFeat, w * d0);
-        atomicAdd(lv + idx * kFeat + 1, w * d1);
-      });
+__device__ __forceinline__ uint4 pack_bf16x8(const float (&v)[8]) {
+  uint4 r;
+  __nv_bfloat162 h[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) h[i] = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
+  r.x = *reinterpret_cast<uint32_t*>(&h[0]);
+  r.y = *reinterpret_cast<uint32_t*>(&h[1]);
+  r.z = *reinterpret_cast<uint32_t*>(&h[2]);
+  r.w = *reinterpret_cast<uint32_t*>(&h[3]);
+  return r;
+}
+__device__ __forceinline__ void unpack_bf16x8(const uint4& r, float (&v)[8]) {
+  const uint32_t w[4] = {r.x, r.y, r.z, r.w};
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const __nv_bfloat162 h = *reinterpret_cast<const __nv_bfloat162*>(&w[i]);
+    v[2 * i] = __low2float(h);
+    v[2 * i + 1] = __high2float(h);
+  }
+}
+__device__ __forceinline__ float round_bf16(float x) { return __bfloat162float(__float2bfloat16(x)); }
+
+// Shared memory of k_mlp (bytes from the dynamic base). An activation tile
+// holds 128 rows x C columns (C = 64, or 16 for the output gradient) in the
+// K-major no-swizzle layout with the 8-row core matrices stacked along the
+// rows: element (r, c) at r * 16 + (c / 8) * 2048 + (c % 8) * 2, i.e.
+// LBO = 2048 (next 8 columns) and SBO = 128 (next 8 rows) when the rows are
+// the M dimension. Read as an MN-major operand over (column, row) the same
+// bytes have LBO = 128 and SBO = 2048: the weight-gradient GEMMs use that
+// view. Their A operand is M = 128 wide over at most 64 real columns and so
+// reads up to 32 KB past the tile start (rows of the accumulator that are
+// never read back): those tiles (dZ, G) come first.
+// A weight matrix W[o][i] (nout x 64) is the K-major B operand of the forward
+// GEMM (N = o, K = i): element (o, i) at o * 16 + (i / 8) * nout * 16 +
+// (i % 8) * 2 (SBO = 128, LBO = nout * 16); the backward-data GEMM reads it
+// MN-major over (i, o) (LBO = 128, SBO = nout * 16).
+constexpr uint32_t kTileBytes = kRows * kWidth * 2;        // 16 KB
+constexpr uint32_t kActLbo = kRows * 16;                   // 2048
+constexpr uint32_t kOffDz = 0;                             // dZ of a hidden layer
+constexpr uint32_t kOffG = kOffDz + kTileBytes;            // dZ of the output layer (4 KB)
+constexpr uint32_t kOffX = kOffG + kRows * kOutCh * 2;     // encoded inputs
+constexpr uint32_t kOffH = kOffX + kTileBytes;             // H0..H3
+constexpr uint32_t kOffW = kOffH + kHidden * kTileBytes;   // W0..W3, then W4
+constexpr uint32_t kWBytes = kWidth * kWidth * 2;          // 8 KB
+constexpr uint32_t kSmemBytes = kOffW + kHidden * kWBytes + kOutCh * kWidth * 2;  // 134 KB
+static_assert(kOffG + 32768u <= kSmemBytes && kOffDz + 32768u <= kSmemBytes,
+              "the padded weight-gradient reads stay inside the CTA's shared memory");
+static_assert(kSmemBytes <= 227u * 1024u, "shared memory per CTA");
+
+__device__ __forceinline__ uint32_t act_off(uint32_t r, uint32_t c) {
+  return r * 16u + (c >> 3) * kActLbo + (c & 7u) * 2u;
+}
+
+struct MlpArgs {
+  const __nv_bfloat16* x0;            // [count][64] encoded inputs
+  const __nv_bfloat16* w[kLayers];    // [out][in]
+  uint32_t count;
+  float* out;                         // inference: [count][3] radiance
+  const float* target;                // training: [count][3]
+  const NrcQuery* q;                  // training: queries (positions for the grid gradient)
+  float* gw[kLayers];                 // training: FP32 weight gradients, accumulated
+  float* ggrid;                       // training: FP32 grid gradients, accumulated
+  double* loss;                       // training: sum of the relative squared errors
+  uint32_t* err;
+  GridGeo geo;
+};
+
+// D[tmem_col] (+)= A * B^T over K = 16 * nk (one thread).
+__device__ __forceinline__ void issue_gemm(uint32_t d, uint32_t a, uint32_t a_lbo, uint32_t a_sbo,
+                                           uint32_t a_step, uint32_t b, uint32_t b_lbo,
+                                           uint32_t b_sbo, uint32_t b_step, int nk, uint32_t idesc,
+                                           bool acc) {
+  for (int k = 0; k < nk; ++k)
+    tc::mma_bf16(d, tc::smem_desc(a + k * a_step, a_lbo, a_sbo),
+                 tc::smem_desc(b + k * b_step, b_lbo, b_sbo), idesc, (acc || k > 0) ? 1u : 0u);
+}
+
+template <bool kTrain>
+__global__ void __launch_bounds__(kRows, 1) k_mlp(MlpArgs a) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ uint32_t tmem_base;
+  constexpr uint32_t kCols = kTrain ? 512u : 64u;  // D at 0; weight gradients at 64 + 64 * l
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const uint32_t base = tc::smem_u32(smem);
+  if (tid == 0) tc::mbar_init(&bar, 1);
+  if (warp == 0) tc::tmem_alloc(&tmem_base, kCols);
+  for (int l = 0; l < kLayers; ++l) {
+    const int nout = l < kHidden ? kWidth : kOutCh;
+    unsigned char* wl = smem + kOffW + l * kWBytes;
+    for (int i = tid; i < nout * 8; i += kRows) {
+      const int o = i >> 3, g = i & 7;
+      *reinterpret_cast<uint4*>(wl + o * 16 + g * nout * 16) =
+          *reinterpret_cast<const uint4*>(a.w[l] + (size_t)o * kWidth + g * 8);
     }
   }
-}
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tmem = tmem_base;
+  const uint32_t my_lane = tmem + ((uint32_t)(warp * 32) << 16);
+  uint32_t phase = 0;
+  bool ok = true, wg_acc = false;
+  double loss = 0.0;
+  // operands written, accumulators read: hand the tensor core the next GEMM
+  auto to_mma = [&]() {
+    tc::fence_smem_to_async();
+    tc::fence_before_sync();
+    __syncthreads();
+  };
+  // CTA-uniform wait for the last commit
+  auto wait = [&]() {
+    const bool w = tc::mbar_wait(&bar, phase, kWaitLimit);
+    ok = __syncthreads_and(w) != 0;
+    if (ok) phase ^= 1u;
+    tc::fence_after_sync();
+    return ok;
+  };
 
-__global__ void k_output(const __nv_bfloat16* o, float* out, uint32_t n) {
-  GRID_STRIDE(i, n) {
-    for (int c = 0; c < 3; ++c) out[i * 3 + c] = fmaxf(__bfloat162float(o[i * kOutCh + c]), 0.0f);
-  }
-}
-
-__global__ void k_loss(const __nv_bfloat16* o, const float* target, __nv_bfloat16* d_o, uint32_t n,
-                       double* loss) {
-  double local = 0.0;
-  GRID_STRIDE(i, n) {
-    for (int c = 0; c < kOutCh; ++c) {
-      float g = 0.0f;
-      if (c < 3) {
-        const float oc = __bfloat162float(o[i * kOutCh + c]);
-        const float t = target[i * 3 + c];
-        const float den = oc * oc + 0.01f;
-        const float d = oc - t;
-        local += (double)(d * d / den);
-        g = 2.0f * d / den;
+  const uint32_t tiles = (a.count + kRows - 1) / kRows;
+  for (uint32_t tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
+    const uint32_t row = tile * kRows + tid;
+    const bool valid = row < a.count;
+    for (int g = 0; g < 8; ++g) {
+      uint4 v = make_uint4(0u, 0u, 0u, 0u);
+      if (valid) v = *reinterpret_cast<const uint4*>(a.x0 + (size_t)row * kWidth + g * 8);
+      *reinterpret_cast<uint4*>(smem + kOffX + act_off(tid, g * 8)) = v;
+    }
+    // forward
+    uint32_t in_off = kOffX;
+    for (int l = 0; l < kLayers && ok; ++l) {
+      const uint32_t nout = l < kHidden ? kWidth : kOutCh;
+      to_mma();
+      if (tid == 0) {
+        tc::fence_after_sync();
+        issue_gemm(tmem, base + in_off, kActLbo, 128u, 2u * kActLbo, base + kOffW + l * kWBytes,
+                   nout * 16u, 128u, 2u * nout * 16u, kWidth / 16,
+                   tc::idesc_bf16(128, nout, false, false), false);
+        tc::mma_commit(&bar);
       }
-      d_o[i * kOutCh + c] = __float2bfloat16(g);
+      if (!wait()) break;
+      if (l < kHidden) {
+        const uint32_t h_off = kOffH + l * kTileBytes;
+        for (int c = 0; c < kWidth / 8; ++c) {
+          float v[8];
+          tc::tmem_ld8(my_lane + (uint32_t)(c * 8), v);
+#pragma unroll
+          for (int k = 0; k < 8; ++k) v[k] = fmaxf(v[k], 0.0f);
+          *reinterpret_cast<uint4*>(smem + h_off + act_off(tid, c * 8)) = pack_bf16x8(v);
+        }
+        in_off = h_off;
+      } else {
+        float o[16];
+        tc::tmem_ld8(my_lane, *reinterpret_cast<float(*)[8]>(o));
+        tc::tmem_ld8(my_lane + 8u, *reinterpret_cast<float(*)[8]>(o + 8));
+        if (!kTrain) {
+          if (valid)
+            for (int c = 0; c < 3; ++c) a.out[(size_t)row * 3 + c] = fmaxf(round_bf16(o[c]), 0.0f);
+        } else {
+          float g[16];
+#pragma unroll
+          for (int c = 0; c < 16; ++c) g[c] = 0.0f;
+          if (valid)
+            for (int c = 0; c < 3; ++c) {
+              const float oc = round_bf16(o[c]), t = a.target[(size_t)row * 3 + c];
+              const float den = oc * oc + 0.01f, d = oc - t;
+              loss += (double)(d * d / den);
+              g[c] = 2.0f * d / den;
+            }
+          *reinterpret_cast<uint4*>(smem + kOffG + act_off(tid, 0)) =
+              pack_bf16x8(*reinterpret_cast<float(*)[8]>(g));
+          *reinterpret_cast<uint4*>(smem + kOffG + act_off(tid, 8)) =
+              pack_bf16x8(*reinterpret_cast<float(*)[8]>(g + 8));
+        }
+      }
+    }
+    if (!kTrain || !ok) continue;
+    // backward: layer j from the output layer down
+    for (int j = kHidden; j >= 0 && ok; --j) {
+      const uint32_t nout = j == kHidden ? kOutCh : kWidth;
+      const uint32_t dz = j == kHidden ? kOffG : kOffDz;
+      const uint32_t in_j = j == 0 ? kOffX : kOffH + (j - 1) * kTileBytes;
+      to_mma();
+      if (tid == 0) {
+        tc::fence_after_sync();
+        // dIn = dZ_j W_j: A = dZ_j (M = rows, K = nout), B = W_j seen as N = 64 inputs x K = nout
+        issue_gemm(tmem, base + dz, kActLbo, 128u, 2u * kActLbo, base + kOffW + j * kWBytes, 128u,
+                   nout * 16u, 256u, (int)nout / 16, tc::idesc_bf16(128, kWidth, false, true),
+                   false);
+        // dW_j += dZ_j^T In_j over the rows: A = dZ_j seen as M = 128 (nout real) x K = rows,
+        // B = In_j seen as N = 64 x K = rows, both MN-major
+        issue_gemm(tmem + 64u + 64u * (uint32_t)j, base + dz, 128u, kActLbo, 256u, base + in_j, 128u,
+                   kActLbo, 256u, kRows / 16, tc::idesc_bf16(128, kWidth, true, true), wg_acc);
+        tc::mma_commit(&bar);
+      }
+      if (!wait()) break;
+      if (j > 0) {
+        // dZ_(j-1) = BF16(dH) where H_(j-1) > 0
+        const uint32_t h_off = kOffH + (j - 1) * kTileBytes;
+        for (int c = 0; c < kWidth / 8; ++c) {
+          float v[8], h[8];
+          tc::tmem_ld8(my_lane + (uint32_t)(c * 8), v);
+          unpack_bf16x8(*reinterpret_cast<const uint4*>(smem + h_off + act_off(tid, c * 8)), h);
+#pragma unroll
+          for (int k = 0; k < 8; ++k) v[k] = h[k] > 0.0f ? v[k] : 0.0f;
+          *reinterpret_cast<uint4*>(smem + kOffDz + act_off(tid, c * 8)) = pack_bf16x8(v);
+        }
+      } else {
+        // hash-grid gradient: the adjoint of the trilinear interpolation of
+        // the BF16-rounded feature gradients
+        float dx[32];
+        for (int c = 0; c < 4; ++c) tc::tmem_ld8(my_lane + (uint32_t)(c * 8), *reinterpret_cast<float(*)[8]>(dx + 8 * c));
+        if (valid) {
+          const NrcQuery q = a.q[row];
+          float u[3];
+          unit_pos(a.geo, q, u);
+          for (int l = 0; l < kLevels; ++l) {
+            const float d0 = round_bf16(dx[2 * l]), d1 = round_bf16(dx[2 * l + 1]);
+            if (d0 == 0.0f && d1 == 0.0f) continue;
+            float* lv = a.ggrid + (size_t)l * kT * kFeat;
+            corners(a.geo, l, u, [&](uint32_t idx, float w) {
+              atomicAdd(lv + idx * kFeat, w * d0);
+              atomicAdd(lv + idx * kFeat + 1, w * d1);
+            });
+          }
+        }
+      }
+    }
+    wg_acc = true;
+  }
+  if (kTrain && ok && wg_acc) {
+    // weight gradients: accumulator row o (lane) holds dW[o][0..64)
+    for (int j = 0; j < kLayers; ++j) {
+      const int nout = j < kHidden ? kWidth : kOutCh;
+      if (warp * 32 >= nout) continue;  // warp-uniform: tcgen05.ld is warp-wide
+      for (int c = 0; c < kWidth / 8; ++c) {
+        float v[8];
+        tc::tmem_ld8(my_lane + 64u + 64u * (uint32_t)j + (uint32_t)(c * 8), v);
+        if (tid < nout)
+          for (int k = 0; k < 8; ++k) atomicAdd(a.gw[j] + tid * kWidth + c * 8 + k, v[k]);
+      }
     }
   }
-  for (int off = 16; off > 0; off >>= 1) local += __shfl_down_sync(0xffffffffu, local, off);
-  if ((threadIdx.x & 31) == 0 && loss) atomicAdd(loss, local);
-}
-
-__global__ void k_mask(__nv_bfloat16* d, const __nv_bfloat16* h, size_t n) {
-  GRID_STRIDE(i, n) {
-    if (!(__bfloat162float(h[i]) > 0.0f)) d[i] = __float2bfloat16(0.0f);
+  if (kTrain && a.loss) {
+    for (int off = 16; off > 0; off >>= 1) loss += __shfl_down_sync(0xffffffffu, loss, off);
+    if ((tid & 31) == 0) atomicAdd(a.loss, loss);
   }
-}
-
-__global__ void k_adam(float* w, float* m, float* v, const float* g, size_t n, float lr, float b1,
-                       float b2, float eps, float c1, float c2) {
-  GRID_STRIDE(i, n) {
-    const float gi = g[i];
-    const float mi = b1 * m[i] + (1.0f - b1) * gi;
-    const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
-    m[i] = mi;
-    v[i] = vi;
-    w[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+  if (!ok) {
+    if (tid == 0) atomicOr(a.err, 4u);
+    tc::mbar_wait(&bar, phase, kWaitLimit);  // MMAs that may still be in flight
   }
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) tc::tmem_dealloc(tmem, kCols);
 }
 
 // Adam on the hash grid, lazily: only entries with a nonzero gradient move
@@ -214,15 +422,31 @@ __global__ void k_adam_grid(float* w, float* m, float* v, float4* g4, size_t n4,
   }
 }
 
-// BF16 forward [out][in] and transposed [in][out] copies of a layer
-__global__ void k_pack(const float* w, __nv_bfloat16* wf, __nv_bfloat16* wt, int nout, int nin) {
-  const size_t n = (size_t)nout * nin;
-  GRID_STRIDE(i, n) {
-    const int in = (int)(i % nin), out = (int)(i / nin);
-    const __nv_bfloat16 b = __float2bfloat16(w[i]);
-    wf[i] = b;
-    wt[(size_t)in * nout + out] = b;
+// Adam on the MLP weights (their gradients are cleared as they are read)
+// and the BF16 copies the MLP kernel reads.
+struct MlpOpt {
+  float *w[kLayers], *m[kLayers], *v[kLayers], *g[kLayers];
+  __nv_bfloat16* wf[kLayers];
+};
+__global__ void k_adam_mlp(MlpOpt o, float lr, float b1, float b2, float eps, float c1, float c2) {
+  for (int l = 0; l < kLayers; ++l) {
+    const size_t n = (size_t)(l < kHidden ? kWidth : kOutCh) * kWidth;
+    GRID_STRIDE(i, n) {
+      const float gi = o.g[l][i];
+      o.g[l][i] = 0.0f;
+      const float mi = b1 * o.m[l][i] + (1.0f - b1) * gi;
+      const float vi = b2 * o.v[l][i] + (1.0f - b2) * gi * gi;
+      o.m[l][i] = mi;
+      o.v[l][i] = vi;
+      const float w = o.w[l][i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+      o.w[l][i] = w;
+      o.wf[l][i] = __float2bfloat16(w);
+    }
   }
+}
+
+__global__ void k_pack(const float* w, __nv_bfloat16* wf, size_t n) {
+  GRID_STRIDE(i, n) { wf[i] = __float2bfloat16(w[i]); }
 }
 
 }  // namespace
@@ -232,15 +456,16 @@ struct NrcNet {
   GridGeo geo{};
   int nout[kLayers] = {kWidth, kWidth, kWidth, kWidth, kOutCh};
   float *w[kLayers], *mw[kLayers], *vw[kLayers], *gw[kLayers];
-  __nv_bfloat16 *wf[kLayers], *wt[kLayers];
+  __nv_bfloat16* wf[kLayers];
   float *grid, *mg, *vg, *gg;
-  __nv_bfloat16 *x0, *h[kHidden], *o, *d_o, *dh, *dz;
+  __nv_bfloat16* x0;
   double* d_loss = nullptr;
   uint32_t* d_err = nullptr;
   std::vector<void*> allocs;
   int step = 0;
   uint32_t last_count = 0;
   bool gg_clear = false;  // the grid gradient table is all zero
+  bool gw_clear = false;  // the MLP gradients are all zero
 };
 
 Nrc::~Nrc() {
@@ -267,34 +492,43 @@ cudaError_t alloc(NrcNet& n, T*& p, size_t count) {
   return e;
 }
 
-// y[q, :nout] = act(W x[q, :nin]) as a one-tap tcgen05 convolution over a
-// 1 x count "image"
-cudaError_t gemm(NrcNet& n, const __nv_bfloat16* x, int nin, const __nv_bfloat16* w, __nv_bfloat16* y,
-                 int nout, uint32_t count, bool relu, cudaStream_t st) {
-  ConvFwdArgs a{x, nin, 0, w, nullptr, y, nout, 0, nin, nout, 1, 1, (int32_t)count,
-                relu ? 1 : 0, n.d_err, 1};
-  return launch_conv_fwd(a, st);
-}
-
-// dw[nout][nin] += dy^T x over the queries
-cudaError_t gemm_wgrad(NrcNet& n, const __nv_bfloat16* dy, int nout, const __nv_bfloat16* x, int nin,
-                       float* dw, uint32_t count, cudaStream_t st) {
-  const int chunks = (int)((count + 127) / 128);
-  const int per = std::max(1, (chunks + 295) / 296);
-  ConvWgradArgs a{dy, nout, 0, x, nin, 0, dw, nin, nout, 1, 1, (int32_t)count, per, n.d_err, 1};
-  return launch_conv_wgrad(a, st);
-}
-
-cudaError_t forward(NrcNet& n, const NrcQuery* q, uint32_t count, cudaStream_t st) {
-  k_encode<<<blocks_for(count), 256, 0, st>>>(n.geo, q, n.grid, n.x0, count);
-  cudaError_t e;
-  const __nv_bfloat16* in = n.x0;
-  for (int l = 0; l < kHidden; ++l) {
-    if ((e = gemm(n, in, kWidth, n.wf[l], n.h[l], kWidth, count, true, st))) return e;
-    in = n.h[l];
+int sm_count() {
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   }
-  if ((e = gemm(n, in, kWidth, n.wf[kHidden], n.o, kOutCh, count, false, st))) return e;
+  return sms;
+}
+
+template <bool kTrain>
+cudaError_t launch_mlp(const MlpArgs& a, cudaStream_t st) {
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(k_mlp<kTrain>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kSmemBytes);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  const uint32_t tiles = (a.count + kRows - 1) / kRows;
+  const int grid = (int)std::min<uint32_t>(tiles, (uint32_t)sm_count());
+  k_mlp<kTrain><<<grid, kRows, kSmemBytes, st>>>(a);
   return cudaGetLastError();
+}
+
+MlpArgs mlp_args(NrcNet& n, uint32_t count) {
+  MlpArgs a{};
+  a.x0 = n.x0;
+  for (int l = 0; l < kLayers; ++l) {
+    a.w[l] = n.wf[l];
+    a.gw[l] = n.gw[l];
+  }
+  a.count = count;
+  a.ggrid = n.gg;
+  a.err = n.d_err;
+  a.geo = n.geo;
+  return a;
 }
 
 std::string finish(NrcNet& n, cudaStream_t st, const char* what) {
@@ -340,14 +574,13 @@ std::string nrc_create(Nrc& c, uint32_t max_queries, const float lo[3], const fl
     AL(n.vw[l], k);
     AL(n.gw[l], k);
     AL(n.wf[l], k);
-    AL(n.wt[l], k);
     std::normal_distribution<float> nd(0.0f, std::sqrt(2.0f / kWidth));
     host.resize(k);
     for (auto& v : host) v = nd(rng);
     cudaMemcpy(n.w[l], host.data(), k * 4, cudaMemcpyHostToDevice);
     cudaMemset(n.mw[l], 0, k * 4);
     cudaMemset(n.vw[l], 0, k * 4);
-    k_pack<<<blocks_for(k), 256>>>(n.w[l], n.wf[l], n.wt[l], n.nout[l], kWidth);
+    k_pack<<<blocks_for(k), 256>>>(n.w[l], n.wf[l], k);
   }
   const size_t ng = (size_t)kLevels * kT * kFeat;
   AL(n.grid, ng);
@@ -360,13 +593,7 @@ std::string nrc_create(Nrc& c, uint32_t max_queries, const float lo[3], const fl
   cudaMemcpy(n.grid, host.data(), ng * 4, cudaMemcpyHostToDevice);
   cudaMemset(n.mg, 0, ng * 4);
   cudaMemset(n.vg, 0, ng * 4);
-  const size_t q = max_queries;
-  AL(n.x0, q * kWidth);
-  for (int l = 0; l < kHidden; ++l) AL(n.h[l], q * kWidth);
-  AL(n.o, q * kOutCh);
-  AL(n.d_o, q * kOutCh);
-  AL(n.dh, q * kWidth);
-  AL(n.dz, q * kWidth);
+  AL(n.x0, (size_t)max_queries * kWidth);
   AL(n.d_loss, 1);
   AL(n.d_err, 1);
 #undef AL
@@ -380,11 +607,11 @@ std::string nrc_infer(Nrc& c, const NrcQuery* q, uint32_t count, float* out, cud
   NrcNet& n = *c.net;
   if (count > n.max_q) return "nrc: more queries than the cache was created for";
   if (count == 0) return {};
-  cudaError_t e = forward(n, q, count, st);
-  if (e != cudaSuccess) return cuda_msg(e, "nrc forward");
-  k_output<<<blocks_for(count), 256, 0, st>>>(n.o, out, count);
-  e = cudaGetLastError();
-  return e == cudaSuccess ? std::string() : cuda_msg(e, "nrc output");
+  k_encode<<<blocks_for(count), 256, 0, st>>>(n.geo, q, n.grid, n.x0, count);
+  MlpArgs a = mlp_args(n, count);
+  a.out = out;
+  cudaError_t e = launch_mlp<false>(a, st);
+  return e == cudaSuccess ? std::string() : cuda_msg(e, "nrc inference");
 }
 
 std::string nrc_train(Nrc& c, const NrcQuery* q, const float* target, uint32_t count, float lr,
@@ -393,44 +620,38 @@ std::string nrc_train(Nrc& c, const NrcQuery* q, const float* target, uint32_t c
   NrcNet& n = *c.net;
   if (count > n.max_q) return "nrc: more queries than the cache was created for";
   if (count == 0) return {};
-  for (int l = 0; l < kLayers; ++l) cudaMemsetAsync(n.gw[l], 0, (size_t)n.nout[l] * kWidth * 4, st);
+  if (!n.gw_clear)
+    for (int l = 0; l < kLayers; ++l) cudaMemsetAsync(n.gw[l], 0, (size_t)n.nout[l] * kWidth * 4, st);
   const size_t ng = (size_t)kLevels * kT * kFeat;
   if (!n.gg_clear) cudaMemsetAsync(n.gg, 0, ng * 4, st);
-  n.gg_clear = false;
+  n.gw_clear = n.gg_clear = false;
   cudaMemsetAsync(n.d_loss, 0, sizeof(double), st);
-  cudaError_t e = forward(n, q, count, st);
-  if (e != cudaSuccess) return cuda_msg(e, "nrc forward");
-  k_loss<<<blocks_for(count), 256, 0, st>>>(n.o, target, n.d_o, count, n.d_loss);
-  // output layer
-  if ((e = gemm_wgrad(n, n.d_o, kOutCh, n.h[kHidden - 1], kWidth, n.gw[kHidden], count, st)))
-    return cuda_msg(e, "nrc");
-  if ((e = gemm(n, n.d_o, kOutCh, n.wt[kHidden], n.dh, kWidth, count, false, st)))
-    return cuda_msg(e, "nrc");
-  // hidden layers, last to first: dz = dh * (h > 0)
-  for (int l = kHidden - 1; l >= 0; --l) {
-    k_mask<<<blocks_for((size_t)count * kWidth), 256, 0, st>>>(n.dh, n.h[l], (size_t)count * kWidth);
-    const __nv_bfloat16* in = l > 0 ? n.h[l - 1] : n.x0;
-    if ((e = gemm_wgrad(n, n.dh, kWidth, in, kWidth, n.gw[l], count, st))) return cuda_msg(e, "nrc");
-    if ((e = gemm(n, n.dh, kWidth, n.wt[l], n.dz, kWidth, count, false, st))) return cuda_msg(e, "nrc");
-    std::swap(n.dh, n.dz);
-  }
-  // n.dh now holds the gradient with respect to the encoded input
-  k_encode_bwd<<<blocks_for(count), 256, 0, st>>>(n.geo, q, n.dh, n.gg, count);
+  k_encode<<<blocks_for(count), 256, 0, st>>>(n.geo, q, n.grid, n.x0, count);
+  MlpArgs a = mlp_args(n, count);
+  a.target = target;
+  a.q = q;
+  a.loss = n.d_loss;
+  cudaError_t e = launch_mlp<true>(a, st);
+  if (e != cudaSuccess) return cuda_msg(e, "nrc training");
   n.last_count = count;
   if (lr > 0.0f) {
     n.step++;
     const float b1 = 0.9f, b2 = 0.99f, eps = 1e-10f;
     const float c1 = 1.0f - std::pow(b1, (float)n.step), c2 = 1.0f - std::pow(b2, (float)n.step);
+    MlpOpt o;
     for (int l = 0; l < kLayers; ++l) {
-      const size_t k = (size_t)n.nout[l] * kWidth;
-      k_adam<<<blocks_for(k), 256, 0, st>>>(n.w[l], n.mw[l], n.vw[l], n.gw[l], k, lr, b1, b2, eps, c1, c2);
-      k_pack<<<blocks_for(k), 256, 0, st>>>(n.w[l], n.wf[l], n.wt[l], n.nout[l], kWidth);
+      o.w[l] = n.w[l];
+      o.m[l] = n.mw[l];
+      o.v[l] = n.vw[l];
+      o.g[l] = n.gw[l];
+      o.wf[l] = n.wf[l];
     }
+    k_adam_mlp<<<blocks_for((size_t)kWidth * kWidth), 256, 0, st>>>(o, lr, b1, b2, eps, c1, c2);
     static_assert((kLevels * kT * kFeat) % 4 == 0, "grid table in float4 units");
     k_adam_grid<<<blocks_for(ng / 4), 256, 0, st>>>(n.grid, n.mg, n.vg,
                                                     reinterpret_cast<float4*>(n.gg), ng / 4, lr,
                                                     b1, b2, eps, c1, c2);
-    n.gg_clear = true;
+    n.gw_clear = n.gg_clear = true;
   }
   e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_msg(e, "nrc train");
@@ -499,7 +720,7 @@ std::string nrc_set_weights(Nrc& c, const float* mlp, const float* grid) {
     for (int l = 0; l < kLayers; ++l) {
       const size_t k = (size_t)n.nout[l] * kWidth;
       cudaMemcpy(n.w[l], mlp, k * 4, cudaMemcpyHostToDevice);
-      k_pack<<<blocks_for(k), 256>>>(n.w[l], n.wf[l], n.wt[l], n.nout[l], kWidth);
+      k_pack<<<blocks_for(k), 256>>>(n.w[l], n.wf[l], k);
       mlp += k;
     }
   if (grid) cudaMemcpy(n.grid, grid, (size_t)kLevels * kT * kFeat * 4, cudaMemcpyHostToDevice);
