@@ -18,10 +18,11 @@
 // each layer and its weight-gradient GEMM (dW += dZ^T X over the tile's rows,
 // both operands read MN-major from the same tiles) are issued together; the
 // weight gradients accumulate in tensor memory over all the CTA's tiles and
-// are added to the FP32 gradient with atomics once at the end, and the
-// hash-grid gradient is scattered straight from the input-gradient rows. A
-// training step is: encode, k_mlp, one Adam launch for the MLP and one for the
-// grid.
+// are added to the FP32 gradient with vector atomics once at the end; the
+// input-gradient rows go to global memory for the hash-grid scatter. A
+// training step is: encode, k_mlp, grid scatter, one Adam launch for the MLP
+// and one for the grid. The encoding and the scatter run one thread per
+// (query, level).
 #include "nrc.cuh"
 
 #include <cmath>
@@ -113,34 +114,51 @@ __device__ __forceinline__ void sh16(float x, float y, float z, float (&s)[16]) 
   s[15] = 0.59004358992664352f * x * (-xx + 3.0f * yy);
 }
 
+// One thread per (query, level): the 8 corner gathers of one level, one
+// spherical-harmonics coefficient and one of the remaining inputs.
 __global__ void k_encode(GridGeo g, const NrcQuery* qs, const float* grid, __nv_bfloat16* x,
                          uint32_t n) {
-  GRID_STRIDE(i, n) {
+  GRID_STRIDE(t, (size_t)n * kLevels) {
+    const size_t i = t / kLevels;
+    const int l = (int)(t % kLevels);
     const NrcQuery q = qs[i];
     __nv_bfloat16* row = x + i * kWidth;
     float u[3];
     unit_pos(g, q, u);
-    for (int l = 0; l < kLevels; ++l) {
-      float f0 = 0.0f, f1 = 0.0f;
-      const float* lv = grid + (size_t)l * kT * kFeat;
-      corners(g, l, u, [&](uint32_t idx, float w) {
-        f0 += w * lv[idx * kFeat];
-        f1 += w * lv[idx * kFeat + 1];
-      });
-      row[2 * l] = __float2bfloat16(f0);
-      row[2 * l + 1] = __float2bfloat16(f1);
-    }
-    float s[16];
-    sh16(q.b.x, q.b.y, q.b.z, s);
-    for (int k = 0; k < 16; ++k) row[32 + k] = __float2bfloat16(s[k]);
-    row[48] = __float2bfloat16(q.c.x * 0.5f + 0.5f);
-    row[49] = __float2bfloat16(q.c.y * 0.5f + 0.5f);
-    row[50] = __float2bfloat16(q.c.z * 0.5f + 0.5f);
-    row[51] = __float2bfloat16(q.a.w);
-    row[52] = __float2bfloat16(q.d.x);
-    row[53] = __float2bfloat16(q.d.y);
-    row[54] = __float2bfloat16(q.d.z);
-    for (int k = 55; k < kWidth; ++k) row[k] = __float2bfloat16(0.0f);
+    float2 f = make_float2(0.0f, 0.0f);
+    const float2* lv = reinterpret_cast<const float2*>(grid + (size_t)l * kT * kFeat);
+    corners(g, l, u, [&](uint32_t idx, float w) {
+      const float2 e = __ldg(lv + idx);
+      f.x += w * e.x;
+      f.y += w * e.y;
+    });
+    *reinterpret_cast<__nv_bfloat162*>(row + 2 * l) = __floats2bfloat162_rn(f.x, f.y);
+    float sh[16];
+    sh16(q.b.x, q.b.y, q.b.z, sh);
+    row[32 + l] = __float2bfloat16(sh[l]);
+    const float extra[16] = {q.c.x * 0.5f + 0.5f, q.c.y * 0.5f + 0.5f, q.c.z * 0.5f + 0.5f, q.a.w,
+                             q.d.x, q.d.y, q.d.z, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    row[48 + l] = __float2bfloat16(extra[l]);
+  }
+}
+
+// Hash-grid gradient, one thread per (query, level): the adjoint of the
+// trilinear interpolation of that level's two feature gradients (dx: the
+// BF16 gradient of the encoded input's grid features, [count][32]).
+__global__ void k_encode_bwd(GridGeo g, const NrcQuery* qs, const __nv_bfloat162* dx, float* ggrid,
+                             uint32_t n) {
+  GRID_STRIDE(t, (size_t)n * kLevels) {
+    const size_t i = t / kLevels;
+    const int l = (int)(t % kLevels);
+    const float2 d = __bfloat1622float2(dx[i * kLevels + l]);
+    if (d.x == 0.0f && d.y == 0.0f) continue;
+    float u[3];
+    unit_pos(g, qs[i], u);
+    static_assert(kFeat == 2, "one float2 per grid entry");
+    float2* lv = reinterpret_cast<float2*>(ggrid + (size_t)l * kT * kFeat);
+    corners(g, l, u, [&](uint32_t idx, float w) {
+      atomicAdd(lv + idx, make_float2(w * d.x, w * d.y));  // one 8-byte vector atomic
+    });
   }
 }
 
@@ -192,6 +210,9 @@ constexpr uint32_t kSmemBytes = kOffW + kHidden * kWBytes + kOutCh * kWidth * 2;
 static_assert(kOffG + 32768u <= kSmemBytes && kOffDz + 32768u <= kSmemBytes,
               "the padded weight-gradient reads stay inside the CTA's shared memory");
 static_assert(kSmemBytes <= 227u * 1024u, "shared memory per CTA");
+// Inference needs no gradient tiles and only two hidden tiles (ping-pong):
+// X, H(even), H(odd), weights = 82 KB, two CTAs per SM.
+constexpr uint32_t kInferSmemBytes = 3 * kTileBytes + kHidden * kWBytes + kOutCh * kWidth * 2;
 
 __device__ __forceinline__ uint32_t act_off(uint32_t r, uint32_t c) {
   return r * 16u + (c >> 3) * kActLbo + (c & 7u) * 2u;
@@ -205,7 +226,7 @@ struct MlpArgs {
   const float* target;                // training: [count][3]
   const NrcQuery* q;                  // training: queries (positions for the grid gradient)
   float* gw[kLayers];                 // training: FP32 weight gradients, accumulated
-  float* ggrid;                       // training: FP32 grid gradients, accumulated
+  __nv_bfloat16* dx;                  // training: [count][32] grid-feature gradients
   double* loss;                       // training: sum of the relative squared errors
   uint32_t* err;
   GridGeo geo;
@@ -222,18 +243,24 @@ __device__ __forceinline__ void issue_gemm(uint32_t d, uint32_t a, uint32_t a_lb
 }
 
 template <bool kTrain>
-__global__ void __launch_bounds__(kRows, 1) k_mlp(MlpArgs a) {
+__global__ void __launch_bounds__(kRows, kTrain ? 1 : 2) k_mlp(MlpArgs a) {
   extern __shared__ __align__(1024) unsigned char smem[];
   __shared__ __align__(8) uint64_t bar;
   __shared__ uint32_t tmem_base;
   constexpr uint32_t kCols = kTrain ? 512u : 64u;  // D at 0; weight gradients at 64 + 64 * l
+  constexpr uint32_t oX = kTrain ? kOffX : 0u;
+  constexpr uint32_t oW = kTrain ? kOffW : 3u * kTileBytes;
+  // hidden tile l: one per layer in training, ping-pong in inference
+  auto h_tile = [](int l) -> uint32_t {
+    return kTrain ? kOffH + (uint32_t)l * kTileBytes : kTileBytes * (1u + (uint32_t)(l & 1));
+  };
   const int tid = threadIdx.x, warp = tid >> 5;
   const uint32_t base = tc::smem_u32(smem);
   if (tid == 0) tc::mbar_init(&bar, 1);
   if (warp == 0) tc::tmem_alloc(&tmem_base, kCols);
   for (int l = 0; l < kLayers; ++l) {
     const int nout = l < kHidden ? kWidth : kOutCh;
-    unsigned char* wl = smem + kOffW + l * kWBytes;
+    unsigned char* wl = smem + oW + l * kWBytes;
     for (int i = tid; i < nout * 8; i += kRows) {
       const int o = i >> 3, g = i & 7;
       *reinterpret_cast<uint4*>(wl + o * 16 + g * nout * 16) =
@@ -270,23 +297,23 @@ __global__ void __launch_bounds__(kRows, 1) k_mlp(MlpArgs a) {
     for (int g = 0; g < 8; ++g) {
       uint4 v = make_uint4(0u, 0u, 0u, 0u);
       if (valid) v = *reinterpret_cast<const uint4*>(a.x0 + (size_t)row * kWidth + g * 8);
-      *reinterpret_cast<uint4*>(smem + kOffX + act_off(tid, g * 8)) = v;
+      *reinterpret_cast<uint4*>(smem + oX + act_off(tid, g * 8)) = v;
     }
     // forward
-    uint32_t in_off = kOffX;
+    uint32_t in_off = oX;
     for (int l = 0; l < kLayers && ok; ++l) {
       const uint32_t nout = l < kHidden ? kWidth : kOutCh;
       to_mma();
       if (tid == 0) {
         tc::fence_after_sync();
-        issue_gemm(tmem, base + in_off, kActLbo, 128u, 2u * kActLbo, base + kOffW + l * kWBytes,
+        issue_gemm(tmem, base + in_off, kActLbo, 128u, 2u * kActLbo, base + oW + l * kWBytes,
                    nout * 16u, 128u, 2u * nout * 16u, kWidth / 16,
                    tc::idesc_bf16(128, nout, false, false), false);
         tc::mma_commit(&bar);
       }
       if (!wait()) break;
       if (l < kHidden) {
-        const uint32_t h_off = kOffH + l * kTileBytes;
+        const uint32_t h_off = h_tile(l);
         for (int c = 0; c < kWidth / 8; ++c) {
           float v[8];
           tc::tmem_ld8(my_lane + (uint32_t)(c * 8), v);
@@ -352,23 +379,11 @@ __global__ void __launch_bounds__(kRows, 1) k_mlp(MlpArgs a) {
           *reinterpret_cast<uint4*>(smem + kOffDz + act_off(tid, c * 8)) = pack_bf16x8(v);
         }
       } else {
-        // hash-grid gradient: the adjoint of the trilinear interpolation of
-        // the BF16-rounded feature gradients
-        float dx[32];
-        for (int c = 0; c < 4; ++c) tc::tmem_ld8(my_lane + (uint32_t)(c * 8), *reinterpret_cast<float(*)[8]>(dx + 8 * c));
-        if (valid) {
-          const NrcQuery q = a.q[row];
-          float u[3];
-          unit_pos(a.geo, q, u);
-          for (int l = 0; l < kLevels; ++l) {
-            const float d0 = round_bf16(dx[2 * l]), d1 = round_bf16(dx[2 * l + 1]);
-            if (d0 == 0.0f && d1 == 0.0f) continue;
-            float* lv = a.ggrid + (size_t)l * kT * kFeat;
-            corners(a.geo, l, u, [&](uint32_t idx, float w) {
-              atomicAdd(lv + idx * kFeat, w * d0);
-              atomicAdd(lv + idx * kFeat + 1, w * d1);
-            });
-          }
+        // gradient of the grid features, rounded to BF16, for k_encode_bwd
+        for (int c = 0; c < 4; ++c) {
+          float v[8];
+          tc::tmem_ld8(my_lane + (uint32_t)(c * 8), v);
+          if (valid) *reinterpret_cast<uint4*>(a.dx + (size_t)row * 32 + c * 8) = pack_bf16x8(v);
         }
       }
     }
@@ -382,8 +397,11 @@ __global__ void __launch_bounds__(kRows, 1) k_mlp(MlpArgs a) {
       for (int c = 0; c < kWidth / 8; ++c) {
         float v[8];
         tc::tmem_ld8(my_lane + 64u + 64u * (uint32_t)j + (uint32_t)(c * 8), v);
-        if (tid < nout)
-          for (int k = 0; k < 8; ++k) atomicAdd(a.gw[j] + tid * kWidth + c * 8 + k, v[k]);
+        if (tid < nout) {  // two 16-byte vector atomics
+          float4* dst = reinterpret_cast<float4*>(a.gw[j] + tid * kWidth + c * 8);
+          atomicAdd(dst, make_float4(v[0], v[1], v[2], v[3]));
+          atomicAdd(dst + 1, make_float4(v[4], v[5], v[6], v[7]));
+        }
       }
     }
   }
@@ -429,19 +447,19 @@ struct MlpOpt {
   __nv_bfloat16* wf[kLayers];
 };
 __global__ void k_adam_mlp(MlpOpt o, float lr, float b1, float b2, float eps, float c1, float c2) {
-  for (int l = 0; l < kLayers; ++l) {
-    const size_t n = (size_t)(l < kHidden ? kWidth : kOutCh) * kWidth;
-    GRID_STRIDE(i, n) {
-      const float gi = o.g[l][i];
-      o.g[l][i] = 0.0f;
-      const float mi = b1 * o.m[l][i] + (1.0f - b1) * gi;
-      const float vi = b2 * o.v[l][i] + (1.0f - b2) * gi * gi;
-      o.m[l][i] = mi;
-      o.v[l][i] = vi;
-      const float w = o.w[l][i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
-      o.w[l][i] = w;
-      o.wf[l][i] = __float2bfloat16(w);
-    }
+  constexpr size_t kHid = (size_t)kWidth * kWidth;
+  GRID_STRIDE(t, kHidden * kHid + (size_t)kOutCh * kWidth) {
+    const int l = (int)min(t / kHid, (size_t)kHidden);
+    const size_t i = t - (size_t)l * kHid;
+    const float gi = o.g[l][i];
+    o.g[l][i] = 0.0f;
+    const float mi = b1 * o.m[l][i] + (1.0f - b1) * gi;
+    const float vi = b2 * o.v[l][i] + (1.0f - b2) * gi * gi;
+    o.m[l][i] = mi;
+    o.v[l][i] = vi;
+    const float w = o.w[l][i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+    o.w[l][i] = w;
+    o.wf[l][i] = __float2bfloat16(w);
   }
 }
 
@@ -458,7 +476,7 @@ struct NrcNet {
   float *w[kLayers], *mw[kLayers], *vw[kLayers], *gw[kLayers];
   __nv_bfloat16* wf[kLayers];
   float *grid, *mg, *vg, *gg;
-  __nv_bfloat16* x0;
+  __nv_bfloat16 *x0, *dx;
   double* d_loss = nullptr;
   uint32_t* d_err = nullptr;
   std::vector<void*> allocs;
@@ -507,13 +525,14 @@ cudaError_t launch_mlp(const MlpArgs& a, cudaStream_t st) {
   static bool attr = false;
   if (!attr) {
     cudaError_t e = cudaFuncSetAttribute(k_mlp<kTrain>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)kSmemBytes);
+                                         (int)(kTrain ? kSmemBytes : kInferSmemBytes));
     if (e != cudaSuccess) return e;
     attr = true;
   }
   const uint32_t tiles = (a.count + kRows - 1) / kRows;
-  const int grid = (int)std::min<uint32_t>(tiles, (uint32_t)sm_count());
-  k_mlp<kTrain><<<grid, kRows, kSmemBytes, st>>>(a);
+  const uint32_t bytes = kTrain ? kSmemBytes : kInferSmemBytes;
+  const int grid = (int)std::min<uint32_t>(tiles, (uint32_t)sm_count() * (kTrain ? 1u : 2u));
+  k_mlp<kTrain><<<grid, kRows, bytes, st>>>(a);
   return cudaGetLastError();
 }
 
@@ -525,7 +544,7 @@ MlpArgs mlp_args(NrcNet& n, uint32_t count) {
     a.gw[l] = n.gw[l];
   }
   a.count = count;
-  a.ggrid = n.gg;
+  a.dx = n.dx;
   a.err = n.d_err;
   a.geo = n.geo;
   return a;
@@ -594,6 +613,7 @@ std::string nrc_create(Nrc& c, uint32_t max_queries, const float lo[3], const fl
   cudaMemset(n.mg, 0, ng * 4);
   cudaMemset(n.vg, 0, ng * 4);
   AL(n.x0, (size_t)max_queries * kWidth);
+  AL(n.dx, (size_t)max_queries * 32);
   AL(n.d_loss, 1);
   AL(n.d_err, 1);
 #undef AL
@@ -607,7 +627,7 @@ std::string nrc_infer(Nrc& c, const NrcQuery* q, uint32_t count, float* out, cud
   NrcNet& n = *c.net;
   if (count > n.max_q) return "nrc: more queries than the cache was created for";
   if (count == 0) return {};
-  k_encode<<<blocks_for(count), 256, 0, st>>>(n.geo, q, n.grid, n.x0, count);
+  k_encode<<<blocks_for((size_t)count * kLevels), 256, 0, st>>>(n.geo, q, n.grid, n.x0, count);
   MlpArgs a = mlp_args(n, count);
   a.out = out;
   cudaError_t e = launch_mlp<false>(a, st);
@@ -626,13 +646,15 @@ std::string nrc_train(Nrc& c, const NrcQuery* q, const float* target, uint32_t c
   if (!n.gg_clear) cudaMemsetAsync(n.gg, 0, ng * 4, st);
   n.gw_clear = n.gg_clear = false;
   cudaMemsetAsync(n.d_loss, 0, sizeof(double), st);
-  k_encode<<<blocks_for(count), 256, 0, st>>>(n.geo, q, n.grid, n.x0, count);
+  k_encode<<<blocks_for((size_t)count * kLevels), 256, 0, st>>>(n.geo, q, n.grid, n.x0, count);
   MlpArgs a = mlp_args(n, count);
   a.target = target;
   a.q = q;
   a.loss = n.d_loss;
   cudaError_t e = launch_mlp<true>(a, st);
   if (e != cudaSuccess) return cuda_msg(e, "nrc training");
+  k_encode_bwd<<<blocks_for((size_t)count * kLevels), 256, 0, st>>>(
+      n.geo, q, reinterpret_cast<const __nv_bfloat162*>(n.dx), n.gg, count);
   n.last_count = count;
   if (lr > 0.0f) {
     n.step++;
@@ -646,9 +668,10 @@ std::string nrc_train(Nrc& c, const NrcQuery* q, const float* target, uint32_t c
       o.g[l] = n.gw[l];
       o.wf[l] = n.wf[l];
     }
-    k_adam_mlp<<<blocks_for((size_t)kWidth * kWidth), 256, 0, st>>>(o, lr, b1, b2, eps, c1, c2);
+    k_adam_mlp<<<blocks_for((size_t)kHidden * kWidth * kWidth + kOutCh * kWidth), 256, 0, st>>>(
+        o, lr, b1, b2, eps, c1, c2);
     static_assert((kLevels * kT * kFeat) % 4 == 0, "grid table in float4 units");
-    k_adam_grid<<<blocks_for(ng / 4), 256, 0, st>>>(n.grid, n.mg, n.vg,
+    k_adam_grid<<<(int)((ng / 4 + 255) / 256), 256, 0, st>>>(n.grid, n.mg, n.vg,
                                                     reinterpret_cast<float4*>(n.gg), ng / 4, lr,
                                                     b1, b2, eps, c1, c2);
     n.gw_clear = n.gg_clear = true;
