@@ -478,19 +478,24 @@ def multi_scene(args):
     return out
 
 
-def radiance_cache(args, top=512):
+def radiance_cache(args, top=1024):
     """The online radiance cache against plain perf mode, on the
     radiance-cache configuration (mesh-stress scene in a 2x2x2 box of
     isotropic medium, depth 32) and on the closed Cornell box at depth 32,
     both small enough for an FP64 high-sample oracle. Curves of (samples,
-    device ms, RMSE) in the time-to-RMSE domain; the cached render's time
+    device ms, RMSE) in the time-to-RMSE domain for two settings: the
+    configuration's (paths stop at hit 2, 1 in 32 paths trains) and one
+    that stops at hit 3 with 1 in 16 training paths. A cached render's time
     includes its 32-sample warm-up (trained, then discarded) and every
     training step. Plus the cost of one training step and one inference on
     16384 records."""
     import torch
     from nectarrender_b200 import capi, nrc
-    out = {"settings": {"terminate_bounce": 2, "train_one_in": 16, "lr": 1e-2, "batch": 16384,
-                        "min_steps_per_wave": 8, "samples_per_wave": 8, "warmup_spp": 32},
+    settings = {"config": {"terminate_bounce": 2, "train_one_in": 32},
+                "stop_at_3": {"terminate_bounce": 3, "train_one_in": 16}}
+    common = {"lr": 1e-2, "batch": 16384, "min_steps_per_wave": 4, "samples_per_wave": 8,
+              "warmup_spp": 32}
+    out = {"settings": settings, "common": common,
            "domain": "sqrt(clamp(x,0,1)), all pixels x 3 channels"}
     n_or = args.rmse_oracle_spp
     cases = (("medium_stress 320x192, depth 32",
@@ -519,32 +524,36 @@ def radiance_cache(args, top=512):
         plain.reset()
         p_curve = curve(plain, 0.0)
         del plain
+        res = {"plain_perf": p_curve}
         lo, hi = sc.bounds()
-        c = nrc.RadianceCache(1 << 18, lo, hi, seed=1)
-        st = out["settings"]
-        r = capi.Render(sc, mode=capi.MODE_PERF, fp64_accumulate=1, seed=spec.seed,
-                        samples_per_wave=st["samples_per_wave"])
-        r.set_nrc(c, st["terminate_bounce"], st["train_one_in"], st["lr"], st["batch"],
-                  st["min_steps_per_wave"])
-        r.samples(n_or // 2, st["warmup_spp"])
-        warm_ms = r.last_ms()
-        r.reset()
-        c_curve = curve(r, warm_ms)
-        queries, records = r.nrc_stats()
-        del r, c
-        at = lambda cv, spp: next(e for n, _, e in cv if n == spp)
-        best = None
-        for spp_c, ms_c, e_c in c_curve:
-            hit = next((ms for _, ms, e in p_curve if e <= e_c), None)
-            if hit is not None and (best is None or hit / ms_c > best[0]):
-                best = (hit / ms_c, e_c, spp_c)
-        out[name] = {
-            "plain_perf": p_curve, "cached": c_curve, "warmup_ms": warm_ms,
-            "cache_queries": queries, "training_records": records,
-            "rmse_at_16spp": {"plain": at(p_curve, 16), "cached": at(c_curve, 16)},
-            "speedup_at_equal_rmse": ({"speedup": best[0], "rmse": best[1], "cached_spp": best[2]}
-                                      if best else "plain perf mode reaches no cached error "
-                                                   "point later than the cache does")}
+        for sname, st in settings.items():
+            c = nrc.RadianceCache(1 << 18, lo, hi, seed=1)
+            r = capi.Render(sc, mode=capi.MODE_PERF, fp64_accumulate=1, seed=spec.seed,
+                            samples_per_wave=common["samples_per_wave"])
+            r.set_nrc(c, st["terminate_bounce"], st["train_one_in"], common["lr"], common["batch"],
+                      common["min_steps_per_wave"])
+            r.samples(n_or // 2, common["warmup_spp"])
+            warm_ms = r.last_ms()
+            r.reset()
+            c_curve = curve(r, warm_ms)
+            queries, records = r.nrc_stats()
+            del r, c
+            # time plain perf mode needs to reach each cached error (linear
+            # interpolation of log time over log error between curve points)
+            ratios = []
+            for spp_c, ms_c, e_c in c_curve:
+                for (s0, m0, e0), (s1, m1, e1) in zip(p_curve, p_curve[1:]):
+                    if e0 > e_c >= e1 and e1 < e0:
+                        f = (np.log(e_c) - np.log(e0)) / (np.log(e1) - np.log(e0))
+                        ratios.append([spp_c, e_c, round(float(np.exp(np.log(m0) + f * (np.log(m1) - np.log(m0)))) / ms_c, 3)])
+                        break
+            best = max(ratios, key=lambda x: x[2]) if ratios else None
+            res[sname] = {"cached": c_curve, "warmup_ms": warm_ms, "cache_queries": queries,
+                          "training_records": records,
+                          "time_ratio_plain_over_cached_at_equal_rmse": ratios,
+                          "best": ({"speedup": best[2], "rmse": best[1], "cached_spp": best[0]}
+                                   if best else None)}
+        out[name] = res
     c = nrc.RadianceCache(1 << 14, (-1, -1, -1), (1, 1, 1), seed=0)
     q = torch.rand((1 << 14, 16), device="cuda")
     t = torch.rand((1 << 14, 3), device="cuda")
