@@ -532,6 +532,9 @@ def radiance_cache(args, top=1024):
                             samples_per_wave=common["samples_per_wave"])
             r.set_nrc(c, st["terminate_bounce"], st["train_one_in"], common["lr"], common["batch"],
                       common["min_steps_per_wave"])
+            # first call allocates the wave state and the cache's record
+            # buffers: not part of the curve (as for plain perf mode)
+            r.samples(n_or // 2 - 1, 1)
             r.samples(n_or // 2, common["warmup_spp"])
             warm_ms = r.last_ms()
             r.reset()
