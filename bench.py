@@ -388,6 +388,7 @@ def run_ours(args):
                 "radiance_cache": cache,
                 "multi_scene": multi,
                 "scene": {"build_ms_device": stats["build_ms"], "build_wall_s": build_wall,
+                          "obj_load_s": obj_load_times(spec) if rank == 0 else None,
                           "triangles": stats["n_triangles"], "wide_nodes": stats["wide_nodes"],
                           "sah_cost_binary": stats["sah_cost_binary"]},
                 "step_ms": step_ms}
@@ -475,6 +476,28 @@ def multi_scene(args):
                                              "CUDA events, scene builds excluded"}
         except Exception as e:  # noqa: BLE001 - reported, not fatal
             out["reference_cuda"] = {"unavailable": repr(e)[:200]}
+    return out
+
+
+def obj_load_times(spec, reps=2):
+    """Wall time of loading the workload's OBJ mesh (parse + vertex
+    assembly) with the host assembly and with the GPU assembly, best of
+    `reps`; the GPU time includes the uploads and downloads."""
+    import ctypes as C
+    lib = capi.library()
+    out = {}
+    for name, fn in (("host_assembly", lib.nr_scene_load_obj),
+                     ("gpu_assembly", lib.nr_scene_load_obj_device)):
+        best = float("inf")
+        for _ in range(reps):
+            h = C.c_void_p()
+            capi._check(lib.nr_scene_create(C.byref(h)), "nr_scene_create")
+            t0 = time.perf_counter()
+            rc = fn(h, spec.meshes[0].encode(), None)
+            best = min(best, time.perf_counter() - t0)
+            lib.nr_scene_destroy(h)
+            capi._check(rc, name)
+        out[name] = best
     return out
 
 

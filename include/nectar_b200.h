@@ -281,6 +281,14 @@ int nr_scene_get_mesh(const nr_scene* scene, uint32_t mesh_id, float* positions,
  * vertices deduplicated on the (v, vt, vn) index triple, smooth normals when
  * the file has none, per-vertex tangents from uv gradients. */
 int nr_scene_load_obj(nr_scene* scene, const char* path, uint32_t* out_id);
+/* Same mesh as nr_scene_load_obj, bit for bit, with the vertex assembly
+ * (deduplication of the v/vt/vn triples in order of first use, missing
+ * normals, tangents) done on the current GPU: the file is parsed on the host,
+ * the assembly runs as hash-table, scan, sort and per-vertex kernels. The
+ * reference assembles on the host (tinyobjloader + mesh.h:57-116). Fails with
+ * NR_ERR_LIMIT when the v, vt and vn index ranges need more than 63 bits
+ * together, NR_ERR_NO_DEVICE without a GPU. */
+int nr_scene_load_obj_device(nr_scene* scene, const char* path, uint32_t* out_id);
 /* Appends a hittable; OBJECT_LIGHT objects are also lights. Scene(hittables,
  * lights, sky) appends lights after the hittables (scene.h:31-39). */
 int nr_scene_add_object(nr_scene* scene, const nr_object_desc* desc, uint32_t* out_id);

@@ -93,7 +93,7 @@ EXPORTS = [
     "nr_abi_version", "nr_last_error", "nr_device_count", "nr_device_draw_order",
     "nr_set_draw_order", "nr_scene_create", "nr_scene_destroy",
     "nr_scene_add_material", "nr_scene_add_image", "nr_scene_add_mesh", "nr_scene_get_mesh",
-    "nr_scene_load_obj",
+    "nr_scene_load_obj", "nr_scene_load_obj_device",
     "nr_scene_add_object", "nr_scene_set_sky_null", "nr_scene_set_sky_simple",
     "nr_scene_set_sky_hdri", "nr_scene_load_hdr", "nr_scene_set_hdri_params",
     "nr_scene_set_tuning", "nr_scene_build",
@@ -197,15 +197,19 @@ class Scene:
     """An nr_scene built from a SceneSpec (registry semantics of the
     reference: one material per hittable, lights after hittables)."""
 
-    def __init__(self, spec: SceneSpec, build: bool = True, mesh_leaf: int = 1, tlas_leaf: int = 1):
+    def __init__(self, spec: SceneSpec, build: bool = True, mesh_leaf: int = 1, tlas_leaf: int = 1,
+                 obj_on_device: bool = False):
+        """obj_on_device: assemble the OBJ meshes' vertices on the GPU
+        (nr_scene_load_obj_device; the same meshes as the host reader)."""
         self.lib = library()
         self.spec = spec
         self.h = C.c_void_p()
         _check(self.lib.nr_scene_create(C.byref(self.h)), "nr_scene_create")
         _check(self.lib.nr_scene_set_tuning(self.h, mesh_leaf, tlas_leaf), "nr_scene_set_tuning")
+        load = self.lib.nr_scene_load_obj_device if obj_on_device else self.lib.nr_scene_load_obj
         for path in spec.meshes:
             mid = C.c_uint32()
-            _check(self.lib.nr_scene_load_obj(self.h, path.encode(), C.byref(mid)), "nr_scene_load_obj")
+            _check(load(self.h, path.encode(), C.byref(mid)), "nr_scene_load_obj")
         for o in spec.objects:
             mid = C.c_uint32()
             _check(self.lib.nr_scene_add_material(self.h, C.byref(material_desc(o["material"])),

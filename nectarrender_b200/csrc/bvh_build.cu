@@ -1278,4 +1278,22 @@ int build_bvh(const float4* d_lo, const float4* d_hi, uint32_t n, bool want_bvh8
   return 0;
 }
 
+uint32_t radix_sort_hist_words(uint32_t n) { return 256u * ((n + kRsTile - 1) / kRsTile); }
+
+cudaError_t radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t* keys2, uint32_t* vals2,
+                             uint32_t n, int key_bits, uint32_t* hist, cudaStream_t st,
+                             uint32_t** out_keys, uint32_t** out_vals) {
+  const uint32_t blocks = (n + kRsTile - 1) / kRsTile;
+  for (int shift = 0; shift < key_bits && n; shift += 8) {
+    k_rs_hist<<<blocks, kRsThreads, 0, st>>>(keys, n, shift, hist, blocks);
+    k_scan_single<<<1, 1024, 0, st>>>(hist, 256 * blocks, nullptr);
+    k_rs_scatter<<<blocks, kRsThreads, 0, st>>>(keys, vals, keys2, vals2, n, shift, hist, blocks);
+    std::swap(keys, keys2);
+    std::swap(vals, vals2);
+  }
+  *out_keys = keys;
+  *out_vals = vals;
+  return cudaGetLastError();
+}
+
 }  // namespace nr

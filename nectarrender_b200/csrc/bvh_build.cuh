@@ -37,4 +37,13 @@ int build_bvh(const float4* d_lo, const float4* d_hi, uint32_t n, bool want_bvh8
 
 void free_build(BuildResult& r);
 
+// Stable LSD radix sort of (key, value) pairs over the low key_bits bits
+// (8 bits per pass); keys2 / vals2 are scratch of n entries, hist holds
+// radix_sort_hist_words(n) words. The sorted pairs end in whichever buffers
+// *out_keys / *out_vals name.
+uint32_t radix_sort_hist_words(uint32_t n);
+cudaError_t radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t* keys2, uint32_t* vals2,
+                             uint32_t n, int key_bits, uint32_t* hist, cudaStream_t st,
+                             uint32_t** out_keys, uint32_t** out_vals);
+
 }  // namespace nr

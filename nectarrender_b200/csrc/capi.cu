@@ -24,6 +24,7 @@
 #include "../../include/nectar_b200.h"
 #include "bvh_build.cuh"
 #include "host_io.h"
+#include "mesh_ingest.cuh"
 #include "image_ops.cuh"
 #include "integrator.cuh"
 #include "wavefront.cuh"
@@ -586,6 +587,27 @@ int nr_scene_load_obj(nr_scene* s, const char* path, uint32_t* out_id) {
   if (m.triangles.empty()) return fail(NR_ERR_INVALID, std::string("OBJ has no faces: ") + path);
   if (m.triangles.size() / 3 >= (1u << 22))
     return fail(NR_ERR_LIMIT, "nr_scene_load_obj: at most 4194303 triangles per mesh");
+  s->meshes.push_back(std::move(m));
+  if (out_id) *out_id = (uint32_t)(s->meshes.size() - 1);
+  s->built = false;
+  return NR_OK;
+}
+
+int nr_scene_load_obj_device(nr_scene* s, const char* path, uint32_t* out_id) {
+  if (!s || !path) return fail(NR_ERR_INVALID, "nr_scene_load_obj_device: null argument");
+  ObjRaw raw;
+  std::string err;
+  if (!parse_obj(path, raw, err)) return fail(NR_ERR_IO, err);
+  if (raw.corners.empty()) return fail(NR_ERR_INVALID, std::string("OBJ has no faces: ") + path);
+  if (raw.corners.size() / 9 >= (1u << 22))
+    return fail(NR_ERR_LIMIT, "nr_scene_load_obj_device: at most 4194303 triangles per mesh");
+  int dev_count = 0;
+  if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0)
+    return fail(NR_ERR_NO_DEVICE, "nr_scene_load_obj_device: no CUDA device");
+  HostMesh m;
+  err = assemble_obj_device(raw, m, nullptr);
+  if (!err.empty())
+    return fail(err.find("key bits") != std::string::npos ? NR_ERR_LIMIT : NR_ERR_CUDA, err);
   s->meshes.push_back(std::move(m));
   if (out_id) *out_id = (uint32_t)(s->meshes.size() - 1);
   s->built = false;

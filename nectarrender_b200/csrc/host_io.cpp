@@ -73,16 +73,25 @@ int resolve(long idx, size_t count) {
 
 }  // namespace
 
-bool load_obj(const std::string& path, HostMesh& out, std::string& err) {
+namespace {
+struct Corner {
+  int v, vt, vn;
+};
+static_assert(sizeof(Corner) == 3 * sizeof(int32_t), "corners are stored as int triples");
+}  // namespace
+
+bool parse_obj(const std::string& path, ObjRaw& raw, std::string& err) {
   std::ifstream f(path);
   if (!f) {
     err = "Failed to load OBJ '" + path + "': cannot open file";
     return false;
   }
-  std::vector<float> vpos, vnor, vtex;
-  struct Corner {
-    int v, vt, vn;
-  };
+  std::vector<float>& vpos = raw.vpos;
+  std::vector<float>& vnor = raw.vnor;
+  std::vector<float>& vtex = raw.vtex;
+  vpos.clear();
+  vnor.clear();
+  vtex.clear();
   std::vector<Corner> tris;  // 3 per triangle
   std::string line;
   std::vector<Corner> poly;
@@ -145,6 +154,12 @@ bool load_obj(const std::string& path, HostMesh& out, std::string& err) {
                 std::to_string(lineno);
           return false;
         }
+        if ((ti && (c.vt < 0 || (size_t)c.vt >= vtex.size() / 2)) ||
+            (ni && (c.vn < 0 || (size_t)c.vn >= vnor.size() / 3))) {
+          err = "Failed to load OBJ '" + path + "': texture or normal index out of range at line " +
+                std::to_string(lineno);
+          return false;
+        }
         poly.push_back(c);
         while (*p && *p != ' ' && *p != '\t') ++p;
       }
@@ -171,15 +186,26 @@ bool load_obj(const std::string& path, HostMesh& out, std::string& err) {
       }
     }
   }
+  raw.corners.resize(3 * tris.size());
+  std::memcpy(raw.corners.data(), tris.data(), tris.size() * sizeof(Corner));
+  return true;
+}
+
+void assemble_obj(const ObjRaw& raw, HostMesh& out) {
+  const std::vector<float>& vpos = raw.vpos;
+  const std::vector<float>& vnor = raw.vnor;
+  const std::vector<float>& vtex = raw.vtex;
+  const Corner* tris_p = reinterpret_cast<const Corner*>(raw.corners.data());
+  const size_t n_corners = raw.corners.size() / 3;
   bool has_normals = !vnor.empty();
   out = HostMesh{};
   std::unordered_map<Key, uint32_t, KeyHash> uniq;
-  uniq.reserve(tris.size());
+  uniq.reserve(n_corners);
   std::vector<H3> P, N, T;
   std::vector<float> UV;
-  out.triangles.reserve(tris.size());
-  for (size_t i = 0; i < tris.size(); ++i) {
-    const Corner& c = tris[i];
+  out.triangles.reserve(n_corners);
+  for (size_t i = 0; i < n_corners; ++i) {
+    const Corner& c = tris_p[i];
     Key k{c.v, c.vt, c.vn};
     auto it = uniq.find(k);
     if (it != uniq.end()) {
@@ -240,6 +266,12 @@ bool load_obj(const std::string& path, HostMesh& out, std::string& err) {
     out.tangents[3 * i + 1] = T[i].y;
     out.tangents[3 * i + 2] = T[i].z;
   }
+}
+
+bool load_obj(const std::string& path, HostMesh& out, std::string& err) {
+  ObjRaw raw;
+  if (!parse_obj(path, raw, err)) return false;
+  assemble_obj(raw, out);
   return true;
 }
 
