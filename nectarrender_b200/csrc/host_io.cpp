@@ -23,6 +23,9 @@
 #include <cstring>
 #include <fstream>
 #include <sstream>
+#include <algorithm>
+#include <atomic>
+#include <thread>
 #include <unordered_map>
 
 namespace nr {
@@ -80,49 +83,166 @@ struct Corner {
 static_assert(sizeof(Corner) == 3 * sizeof(int32_t), "corners are stored as int triples");
 }  // namespace
 
-bool parse_obj(const std::string& path, ObjRaw& raw, std::string& err) {
-  std::ifstream f(path);
-  if (!f) {
-    err = "Failed to load OBJ '" + path + "': cannot open file";
-    return false;
+namespace {
+
+enum LineKind { kOther, kV, kVN, kVT, kF };
+
+// The kind of an OBJ line (leading blanks skipped) and where its data starts.
+LineKind classify(const char*& s) {
+  while (*s == ' ' || *s == '\t') ++s;
+  if (s[0] == 'v' && (s[1] == ' ' || s[1] == '\t')) return kV;
+  if (s[0] == 'v' && s[1] == 'n' && (s[2] == ' ' || s[2] == '\t')) return kVN;
+  if (s[0] == 'v' && s[1] == 't' && (s[2] == ' ' || s[2] == '\t')) return kVT;
+  if (s[0] == 'f' && (s[1] == ' ' || s[1] == '\t')) return kF;
+  return kOther;
+}
+
+// Calls fn(line, number) for every line of [begin, end) (split at '\n', as
+// std::getline does), each copied into a NUL-terminated buffer so that the
+// number parsers stop at its end.
+template <typename F>
+void for_lines(const char* begin, const char* end, size_t first_lineno, F&& fn) {
+  std::string line;
+  size_t lineno = first_lineno;
+  for (const char* p = begin; p < end;) {
+    const char* q = static_cast<const char*>(memchr(p, '\n', (size_t)(end - p)));
+    if (!q) q = end;
+    line.assign(p, (size_t)(q - p));
+    fn(line.c_str(), ++lineno);
+    p = q + 1;
   }
+}
+
+struct ChunkCounts {
+  size_t lines = 0, v = 0, vn = 0, vt = 0;
+};
+
+}  // namespace
+
+// The file is read whole and cut at line ends into chunks that the host
+// threads take in turn. Pass 1 counts each chunk's lines and v / vn /
+// vt records; pass 2 parses the v / vn / vt records into their final places;
+// pass 3 parses the faces, resolving indices against the counts of records
+// before the face's line (a prefix over the chunks). The result and the
+// first error reported are those of reading the lines in order.
+bool parse_obj(const std::string& path, ObjRaw& raw, std::string& err) {
+  std::string data;
+  {
+    FILE* f = fopen(path.c_str(), "rb");
+    if (!f) {
+      err = "Failed to load OBJ '" + path + "': cannot open file";
+      return false;
+    }
+    fseek(f, 0, SEEK_END);
+    const long len = ftell(f);
+    fseek(f, 0, SEEK_SET);
+    data.resize(len > 0 ? (size_t)len : 0);
+    const size_t got = data.empty() ? 0 : fread(&data[0], 1, data.size(), f);
+    fclose(f);
+    data.resize(got);
+  }
+  const char* base = data.data();
+  const size_t size = data.size();
+  // chunks of >= 256 KB, several per thread, taken by the threads in turn
+  // (the records of an OBJ file come in long runs of one kind)
+  const size_t hw = std::max(1u, std::thread::hardware_concurrency());
+  const size_t nch = std::max<size_t>(1, std::min<size_t>({8 * hw, 1024, size >> 18}));
+  const size_t nthreads = std::min(hw, nch);
+  std::vector<size_t> cut(nch + 1, size);
+  cut[0] = 0;
+  for (size_t k = 1; k < nch; ++k) {
+    size_t at = std::max(cut[k - 1], size * k / nch);
+    const void* nl = at < size ? memchr(base + at, '\n', size - at) : nullptr;
+    cut[k] = nl ? (size_t)(static_cast<const char*>(nl) - base) + 1 : size;
+  }
+  auto run = [&](auto&& job) {
+    std::atomic<size_t> next{0};
+    auto worker = [&]() {
+      for (size_t k; (k = next.fetch_add(1)) < nch;) job(k);
+    };
+    std::vector<std::thread> pool;
+    for (size_t t = 1; t < nthreads; ++t) pool.emplace_back(worker);
+    worker();
+    for (auto& t : pool) t.join();
+  };
+  // pass 1: counts
+  std::vector<ChunkCounts> cnt(nch);
+  run([&](size_t k) {
+    ChunkCounts& c = cnt[k];
+    for_lines(base + cut[k], base + cut[k + 1], 0, [&](const char* s, size_t) {
+      ++c.lines;
+      switch (classify(s)) {
+        case kV: ++c.v; break;
+        case kVN: ++c.vn; break;
+        case kVT: ++c.vt; break;
+        default: break;
+      }
+    });
+  });
+  std::vector<ChunkCounts> pre(nch);
+  for (size_t k = 1; k < nch; ++k) {
+    pre[k].lines = pre[k - 1].lines + cnt[k - 1].lines;
+    pre[k].v = pre[k - 1].v + cnt[k - 1].v;
+    pre[k].vn = pre[k - 1].vn + cnt[k - 1].vn;
+    pre[k].vt = pre[k - 1].vt + cnt[k - 1].vt;
+  }
+  const ChunkCounts& last = pre[nch - 1];
   std::vector<float>& vpos = raw.vpos;
   std::vector<float>& vnor = raw.vnor;
   std::vector<float>& vtex = raw.vtex;
-  vpos.clear();
-  vnor.clear();
-  vtex.clear();
-  std::vector<Corner> tris;  // 3 per triangle
-  std::string line;
-  std::vector<Corner> poly;
-  size_t lineno = 0;
-  while (std::getline(f, line)) {
-    ++lineno;
-    const char* s = line.c_str();
-    while (*s == ' ' || *s == '\t') ++s;
-    if (s[0] == 'v' && (s[1] == ' ' || s[1] == '\t')) {
+  vpos.assign(3 * (last.v + cnt[nch - 1].v), 0.0f);
+  vnor.assign(3 * (last.vn + cnt[nch - 1].vn), 0.0f);
+  vtex.assign(2 * (last.vt + cnt[nch - 1].vt), 0.0f);
+  // pass 2: vertex records
+  run([&](size_t k) {
+    size_t iv = pre[k].v, in = pre[k].vn, it = pre[k].vt;
+    for_lines(base + cut[k], base + cut[k + 1], 0, [&](const char* s, size_t) {
       char* e;
-      float a = strtof(s + 2, &e);
-      float b = strtof(e, &e);
-      float c = strtof(e, &e);
-      vpos.push_back(a);
-      vpos.push_back(b);
-      vpos.push_back(c);
-    } else if (s[0] == 'v' && s[1] == 'n' && (s[2] == ' ' || s[2] == '\t')) {
-      char* e;
-      float a = strtof(s + 3, &e);
-      float b = strtof(e, &e);
-      float c = strtof(e, &e);
-      vnor.push_back(a);
-      vnor.push_back(b);
-      vnor.push_back(c);
-    } else if (s[0] == 'v' && s[1] == 't' && (s[2] == ' ' || s[2] == '\t')) {
-      char* e;
-      float a = strtof(s + 3, &e);
-      float b = strtof(e, &e);
-      vtex.push_back(a);
-      vtex.push_back(b);
-    } else if (s[0] == 'f' && (s[1] == ' ' || s[1] == '\t')) {
+      switch (classify(s)) {
+        case kV: {
+          const float a = strtof(s + 2, &e), b = strtof(e, &e), c = strtof(e, &e);
+          vpos[3 * iv] = a;
+          vpos[3 * iv + 1] = b;
+          vpos[3 * iv + 2] = c;
+          ++iv;
+          break;
+        }
+        case kVN: {
+          const float a = strtof(s + 3, &e), b = strtof(e, &e), c = strtof(e, &e);
+          vnor[3 * in] = a;
+          vnor[3 * in + 1] = b;
+          vnor[3 * in + 2] = c;
+          ++in;
+          break;
+        }
+        case kVT: {
+          const float a = strtof(s + 3, &e), b = strtof(e, &e);
+          vtex[2 * it] = a;
+          vtex[2 * it + 1] = b;
+          ++it;
+          break;
+        }
+        default: break;
+      }
+    });
+  });
+  // pass 3: faces
+  std::vector<std::vector<Corner>> tris_k(nch);
+  std::vector<std::string> err_k(nch);
+  run([&](size_t k) {
+    size_t nv = pre[k].v, nn = pre[k].vn, nt = pre[k].vt;  // records before the line
+    std::vector<Corner>& tris = tris_k[k];
+    std::vector<Corner> poly;
+    bool bad = false;
+    for_lines(base + cut[k], base + cut[k + 1], pre[k].lines, [&](const char* s, size_t lineno) {
+      if (bad) return;
+      switch (classify(s)) {
+        case kV: ++nv; return;
+        case kVN: ++nn; return;
+        case kVT: ++nt; return;
+        case kF: break;
+        default: return;
+      }
       poly.clear();
       const char* p = s + 2;
       while (*p) {
@@ -131,8 +251,9 @@ bool parse_obj(const std::string& path, ObjRaw& raw, std::string& err) {
         char* e;
         long vi = strtol(p, &e, 10), ti = 0, ni = 0;
         if (e == p) {
-          err = "Failed to load OBJ '" + path + "': bad face at line " + std::to_string(lineno);
-          return false;
+          err_k[k] = "Failed to load OBJ '" + path + "': bad face at line " + std::to_string(lineno);
+          bad = true;
+          return;
         }
         p = e;
         if (*p == '/') {
@@ -147,25 +268,25 @@ bool parse_obj(const std::string& path, ObjRaw& raw, std::string& err) {
             p = e;
           }
         }
-        Corner c{resolve(vi, vpos.size() / 3), ti ? resolve(ti, vtex.size() / 2) : -1,
-                 ni ? resolve(ni, vnor.size() / 3) : -1};
-        if (c.v < 0 || (size_t)c.v >= vpos.size() / 3) {
-          err = "Failed to load OBJ '" + path + "': vertex index out of range at line " +
-                std::to_string(lineno);
-          return false;
+        Corner c{resolve(vi, nv), ti ? resolve(ti, nt) : -1, ni ? resolve(ni, nn) : -1};
+        if (c.v < 0 || (size_t)c.v >= nv) {
+          err_k[k] = "Failed to load OBJ '" + path + "': vertex index out of range at line " +
+                     std::to_string(lineno);
+          bad = true;
+          return;
         }
-        if ((ti && (c.vt < 0 || (size_t)c.vt >= vtex.size() / 2)) ||
-            (ni && (c.vn < 0 || (size_t)c.vn >= vnor.size() / 3))) {
-          err = "Failed to load OBJ '" + path + "': texture or normal index out of range at line " +
-                std::to_string(lineno);
-          return false;
+        if ((ti && (c.vt < 0 || (size_t)c.vt >= nt)) || (ni && (c.vn < 0 || (size_t)c.vn >= nn))) {
+          err_k[k] = "Failed to load OBJ '" + path + "': texture or normal index out of range at line " +
+                     std::to_string(lineno);
+          bad = true;
+          return;
         }
         poly.push_back(c);
         while (*p && *p != ' ' && *p != '\t') ++p;
       }
       if (poly.size() == 4) {
         // quads split along the shorter diagonal, as tinyobjloader does
-        auto coord = [&](int v, int k) { return vpos[3 * (size_t)v + k]; };
+        auto coord = [&](int v, int kk) { return vpos[3 * (size_t)v + kk]; };
         float e02x = coord(poly[2].v, 0) - coord(poly[0].v, 0);
         float e02y = coord(poly[2].v, 1) - coord(poly[0].v, 1);
         float e02z = coord(poly[2].v, 2) - coord(poly[0].v, 2);
@@ -175,19 +296,30 @@ bool parse_obj(const std::string& path, ObjRaw& raw, std::string& err) {
         float s02 = e02x * e02x + e02y * e02y + e02z * e02z;
         float s13 = e13x * e13x + e13y * e13y + e13z * e13z;
         const int a[6] = {0, 1, 2, 0, 2, 3}, b[6] = {0, 1, 3, 1, 2, 3};
-        for (int k = 0; k < 6; ++k) tris.push_back(poly[s02 < s13 ? a[k] : b[k]]);
+        for (int j = 0; j < 6; ++j) tris.push_back(poly[s02 < s13 ? a[j] : b[j]]);
       } else {
         // larger polygons are fanned (tinyobjloader ear-clips them)
-        for (size_t k = 2; k < poly.size(); ++k) {
+        for (size_t j = 2; j < poly.size(); ++j) {
           tris.push_back(poly[0]);
-          tris.push_back(poly[k - 1]);
-          tris.push_back(poly[k]);
+          tris.push_back(poly[j - 1]);
+          tris.push_back(poly[j]);
         }
       }
+    });
+  });
+  for (size_t k = 0; k < nch; ++k)
+    if (!err_k[k].empty()) {
+      err = err_k[k];
+      return false;
     }
+  size_t total = 0;
+  for (auto& t : tris_k) total += t.size();
+  raw.corners.resize(3 * total);
+  size_t at = 0;
+  for (auto& t : tris_k) {
+    std::memcpy(raw.corners.data() + 3 * at, t.data(), t.size() * sizeof(Corner));
+    at += t.size();
   }
-  raw.corners.resize(3 * tris.size());
-  std::memcpy(raw.corners.data(), tris.data(), tris.size() * sizeof(Corner));
   return true;
 }
 

@@ -85,6 +85,28 @@ def test_product_obj_reader_matches_reference_fixture():
         assert np.array_equal(a, g[k]), k
 
 
+def test_product_obj_reader_in_chunks_matches_the_oracle(tmp_path):
+    """A multi-megabyte OBJ is parsed by several host threads in line-aligned
+    chunks; the mesh equals the oracle's single-pass reader (and the
+    reference's own, when its build is present), including relative indices
+    and quads that refer to vertices of earlier chunks."""
+    import oracle
+    v, f, n = scenes.displaced_icosphere(6, seed=4)
+    p = tmp_path / "big.obj"
+    scenes.write_obj(p, v, f, n)
+    with open(p, "a") as fh:  # faces whose indices reach back across the chunks
+        fh.write("f -1//-1 -2//-2 -3//-3 -4//-4\nf 1//1 2//2 3//3 4//4\n")
+    assert p.stat().st_size > 4 << 20
+    spec = scenes.SceneSpec(objects=[], camera={}, meshes=[str(p)])
+    got = capi.Scene(spec, build=False).mesh(0)
+    refs = [oracle.Oracle().load_obj(str(p))]
+    if oracle.REF_CPU_SO.exists():
+        refs.append(oracle.RefCPU().load_obj(str(p)))
+    for ref in refs:
+        for name, a, b in zip(("P", "N", "T", "UV", "tris"), got, ref):
+            np.testing.assert_array_equal(a, np.asarray(b).reshape(a.shape), err_msg=name)
+
+
 @pytest.mark.parametrize("verts,expected", [
     ("v 0 0 0\nv 2 0 0\nv 1 1 0\nv -1 1 0\n", [0, 1, 2, 0, 2, 3]),   # 0-2 shorter
     ("v 0 0 0\nv 2 0 0\nv 2 1 0\nv 1 1 0\n", [0, 1, 2, 1, 3, 2]),    # 1-3 shorter
