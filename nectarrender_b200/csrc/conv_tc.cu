@@ -17,6 +17,8 @@
 // (cout rows padded to the M = 128 tile with zeros), then adds its FP32
 // partial sums to dW with atomics.
 #include "conv_tc.cuh"
+
+#include <algorithm>
 #include "tcgen05.cuh"
 
 namespace nr {
@@ -372,6 +374,123 @@ __global__ void __launch_bounds__(kThreads) k_conv_wgrad(ConvWgradArgs a) {
   if (warp == 0) tc::tmem_dealloc(tmem, ncols);
 }
 
+// Halo-tile weight gradient: a CTA reduces a run of 8 x 16 pixel tiles for
+// one group of taps. Per tile the dY rows (MN-major over output channels,
+// padded to the M = 128 tile; rows >= cout are never read back) and the
+// tile's 10 x 18 input halo are copied into shared memory once; the B
+// operand of tap (dy, dx) is the halo seen MN-major over input channels from
+// start (dy * 10 + dx) * 16 with LBO = 160 (next tile row of 8 pixels) and
+// SBO = 180 * 16 (next 8 channels), so no per-tap gather is needed. Each tap
+// of the group accumulates in its own cin tensor-memory columns over all the
+// CTA's tiles (two shared-memory stages: tile j loads while tile j - 1's
+// MMAs run); the partial sums go to dW with vector atomics at the end.
+__global__ void __launch_bounds__(kThreads) k_conv_wgrad_halo(ConvWgradArgs a, int tpg,
+                                                               int tiles_per_cta) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  __shared__ __align__(8) uint64_t bar[2];
+  __shared__ uint32_t tmem_base;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int cin = a.cin, cout = a.cout, kg_n = cin >> 3;
+  const int tw = a.W / kTileW, th = a.H / kTileH, n_tiles = tw * th * a.B;
+  const int t0 = blockIdx.x * tiles_per_cta, t1 = min(n_tiles, t0 + tiles_per_cta);
+  const int tap0 = blockIdx.y * tpg, ntap = min(tpg, 9 - tap0);
+  const uint32_t a_bytes = 16u * 2048u, b_bytes = (uint32_t)kg_n * kHalo * 16u;
+  const uint32_t stage_bytes = a_bytes + b_bytes;
+  const uint32_t base = tc::smem_u32(smem);
+  const uint32_t ncols = (uint32_t)ntap * cin <= 256u ? 256u : 512u;
+
+  for (uint32_t i = tid * 16u; i < 2u * stage_bytes; i += kThreads * 16u)
+    *reinterpret_cast<uint4*>(smem + i) = make_uint4(0u, 0u, 0u, 0u);
+  if (tid == 0) {
+    tc::mbar_init(&bar[0], 1);
+    tc::mbar_init(&bar[1], 1);
+  }
+  if (warp == 0) tc::tmem_alloc(&tmem_base, ncols);
+  tc::fence_smem_to_async();
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tmem = tmem_base;
+  const uint32_t idesc = tc::idesc_bf16(128, (uint32_t)cin, true, true);
+
+  bool ok = true;
+  int uses[2] = {0, 0};
+  for (int t = t0; t < t1 && ok; ++t) {
+    const int j = t - t0, s = j & 1;
+    if (j >= 2) {
+      const bool w = tc::mbar_wait(&bar[s], (uint32_t)(uses[s] - 1) & 1u, kWaitLimit);
+      if (!__syncthreads_and(w)) {
+        ok = false;
+        break;
+      }
+    }
+    const int b = t / (tw * th), rest = t % (tw * th);
+    const int y0 = (rest / tw) * kTileH, x0 = (rest % tw) * kTileW;
+    const uint32_t sa = base + s * stage_bytes, sb = sa + a_bytes;
+    for (int i = tid; i < (cout >> 3) * 128; i += kThreads) {
+      const int pl = i & 127, cg = i >> 7;
+      const size_t p = (size_t)(b * a.H + y0 + pl / kTileW) * a.W + x0 + pl % kTileW;
+      cp_async16(sa + (uint32_t)cg * 2048u + (uint32_t)pl * 16u,
+                 a.dy + p * a.dy_stride + a.dy_off + cg * 8, true);
+    }
+    for (int i = tid; i < kHalo * kg_n; i += kThreads) {
+      const int h = i % kHalo, kg = i / kHalo;
+      const int yy = y0 - 1 + h / kHaloW, xx = x0 - 1 + h % kHaloW;
+      const bool valid = yy >= 0 && yy < a.H && xx >= 0 && xx < a.W;
+      const __nv_bfloat16* src =
+          valid ? a.x + ((size_t)(b * a.H + yy) * a.W + xx) * a.x_stride + a.x_off + kg * 8 : a.x;
+      cp_async16(sb + (uint32_t)kg * kHalo * 16u + (uint32_t)h * 16u, src, valid);
+    }
+    cp_async_wait_all();
+    tc::fence_smem_to_async();
+    __syncthreads();
+    if (tid == 0) {
+      tc::fence_after_sync();
+      for (int q = 0; q < ntap; ++q) {
+        const int tap = tap0 + q;
+        const uint32_t tap_off = (uint32_t)((tap / 3) * kHaloW + (tap % 3)) * 16u;
+        for (int kk = 0; kk < 8; ++kk) {  // K = 128 pixels = 16 tile rows, two per MMA
+          const uint64_t da = tc::smem_desc(sa + 256u * kk, 128u, 2048u);
+          const uint64_t db = tc::smem_desc(sb + tap_off + 2u * kk * kHaloW * 16u, kHaloW * 16u,
+                                            kHalo * 16u);
+          tc::mma_bf16(tmem + (uint32_t)(q * cin), da, db, idesc, (j > 0 || kk > 0) ? 1u : 0u);
+        }
+      }
+      tc::mma_commit(&bar[s]);
+    }
+    uses[s]++;
+  }
+  const int n_local = t1 - t0;
+  if (ok && n_local > 0) {
+    const int s_last = (n_local - 1) & 1;
+    ok = __syncthreads_and(tc::mbar_wait(&bar[s_last], (uint32_t)(uses[s_last] - 1) & 1u, kWaitLimit));
+  }
+  if (!ok && tid == 0) atomicOr(a.err, 2u);
+  tc::fence_after_sync();
+  __syncthreads();
+  if (ok && n_local > 0) {
+    const int co = warp * 32 + lane;
+    for (int q = 0; q < ntap; ++q) {
+      if (warp * 32 >= cout) break;  // warp-uniform: tcgen05.ld is warp-wide
+      for (int cg = 0; cg < kg_n; ++cg) {
+        float v[8];
+        tc::tmem_ld8(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(q * cin + cg * 8), v);
+        if (co < cout) {
+          float4* dst = reinterpret_cast<float4*>(a.dw + ((size_t)(tap0 + q) * cout + co) * cin + cg * 8);
+          atomicAdd(dst, make_float4(v[0], v[1], v[2], v[3]));
+          atomicAdd(dst + 1, make_float4(v[4], v[5], v[6], v[7]));
+        }
+      }
+    }
+  } else if (!ok) {
+    tc::mbar_wait(&bar[0], (uint32_t)(uses[0] - 1) & 1u, kWaitLimit);  // MMAs still in flight
+    tc::mbar_wait(&bar[1], (uint32_t)(uses[1] - 1) & 1u, kWaitLimit);
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) tc::tmem_dealloc(tmem, ncols);
+}
+
 }  // namespace
 
 size_t conv_fwd_smem_bytes(int cin, int cout) {
@@ -406,6 +525,23 @@ cudaError_t launch_conv_wgrad(const ConvWgradArgs& a, cudaStream_t st) {
   if (a.cin % 16 || a.cout % 16 || a.cin < 16 || a.cout < 16 || a.cin > 256 || a.cout > 128 ||
       a.x_stride % 8 || a.x_off % 8 || a.dy_stride % 8 || a.dy_off % 8 || a.chunks_per_cta < 1)
     return cudaErrorInvalidValue;
+  const size_t halo_smem = 2u * (16u * 2048u + (size_t)(a.cin >> 3) * kHalo * 16u);
+  if (a.taps != 1 && a.W % kTileW == 0 && a.H % kTileH == 0 && halo_smem <= 200u * 1024u) {
+    cudaError_t e = cudaFuncSetAttribute(k_conv_wgrad_halo,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)halo_smem);
+    if (e != cudaSuccess) return e;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int tpg = std::min(9, 512 / a.cin);  // taps whose accumulators fit in 512 columns
+    const int groups = (9 + tpg - 1) / tpg;
+    const int n_tiles = (a.W / kTileW) * (a.H / kTileH) * a.B;
+    const int ctas = std::max(1, std::min(n_tiles, sms / groups));  // one CTA per SM
+    const int per = (n_tiles + ctas - 1) / ctas;
+    dim3 grid((n_tiles + per - 1) / per, groups);
+    k_conv_wgrad_halo<<<grid, kThreads, halo_smem, st>>>(a, tpg, per);
+    return cudaGetLastError();
+  }
   const size_t smem = conv_wgrad_smem_bytes(a.cin);
   if (smem > 200u * 1024u) return cudaErrorInvalidValue;
   cudaError_t e = cudaFuncSetAttribute(k_conv_wgrad, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -101,7 +101,11 @@ def test_backward_data_via_rotated_weights():
     assert abs(lhs - rhs) <= 1e-9 * max(1.0, abs(lhs))
 
 
-@pytest.mark.parametrize("B,H,W,ci,co", [(2, 16, 24, 32, 48), (1, 64, 64, 128, 128), (1, 16, 16, 160, 16)])
+@pytest.mark.parametrize("B,H,W,ci,co", [
+    (2, 16, 24, 32, 48), (1, 64, 64, 128, 128), (1, 16, 16, 160, 16),  # halo tiles (H % 16, W % 8)
+    (2, 32, 16, 96, 96),                                                # two tap groups of 5 and 4
+    (1, 12, 20, 32, 16),                                                # per-tap gathers
+])
 def test_weight_gradient(B, H, W, ci, co):
     lib = capi.library()
     rng = np.random.default_rng(ci + co)
