@@ -67,6 +67,9 @@ def parse():
     p.add_argument("--no-denoiser", action="store_true", help="skip training the learned denoiser")
     p.add_argument("--no-multi", action="store_true", help="skip the multi-scene measurement")
     p.add_argument("--no-nrc", action="store_true", help="skip the radiance-cache measurement")
+    p.add_argument("--batch-rmse", action="store_true",
+                   help="also render the 64-scene batched configuration and report every "
+                        "scene's RMSE against an FP64 perf-mode render (about 2 minutes)")
     p.add_argument("--denoiser-seconds", type=float, default=40.0)
     return p.parse_args()
 
@@ -352,6 +355,9 @@ def run_ours(args):
     cache = None
     if rank == 0 and world == 1 and not args.no_nrc:
         cache = radiance_cache(args)
+    batch = None
+    if rank == 0 and world == 1 and args.batch_rmse:
+        batch = batch_rmse(args)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -387,6 +393,7 @@ def run_ours(args):
                 "learned_kernels": learned,
                 "radiance_cache": cache,
                 "multi_scene": multi,
+                "batch_rmse": batch,
                 "scene": {"build_ms_device": stats["build_ms"], "build_wall_s": build_wall,
                           "obj_load_s": obj_load_times(spec) if rank == 0 else None,
                           "triangles": stats["n_triangles"], "wide_nodes": stats["wide_nodes"],
@@ -476,6 +483,57 @@ def multi_scene(args):
                                              "CUDA events, scene builds excluded"}
         except Exception as e:  # noqa: BLE001 - reported, not fatal
             out["reference_cuda"] = {"unavailable": repr(e)[:200]}
+    return out
+
+
+def batch_rmse(args, oracle_spp=1024):
+    """The batched configuration (scenes.batch_set: 64 scenes, 10k-2M
+    triangles, 256-1024 pixels a side, 16-256 samples, depth 4-16): every
+    scene's samples in one nr_render_samples_batch call and one scene after
+    another (host wall time, best of 2), then each scene's RMSE in the
+    time-to-RMSE domain against a perf-mode FP64 render of `oracle_spp`
+    samples with another seed."""
+    import copy
+    from nectarrender_b200 import capi
+    specs = scenes.batch_set(64, seed=0)
+    scs = [capi.Scene(s, mesh_leaf=args.mesh_leaf) for s in specs]
+    counts = [s.camera["samples_per_pixel"] - 1 for s in specs]
+    px = [int(s.camera["resolution"][0]) * int(s.camera["resolution"][1]) for s in specs]
+    total = float(sum(p * c for p, c in zip(px, counts)))
+    out = {"scenes": len(specs), "pixel_samples": total, "oracle_spp": oracle_spp,
+           "domain": "sqrt(clamp(x,0,1)), all pixels x 3 channels"}
+    rs = None
+    for mode in ("sequential", "batched"):
+        best = None
+        for _ in range(2):
+            rs = [capi.Render(sc, fp64_accumulate=1, samples_per_wave=2) for sc in scs]
+            for r in rs:  # first call allocates: keep it out of the timing
+                r.samples(1, 1)
+                r.reset()
+            t0 = time.perf_counter()
+            if mode == "sequential":
+                for r, c in zip(rs, counts):
+                    r.samples(1, c)
+            else:
+                capi.render_batch(rs, [1] * len(rs), counts)
+            dt = time.perf_counter() - t0
+            best = dt if best is None else min(best, dt)
+        out[mode] = {"wall_s": best, "samples_per_s": total / best}
+    out["speedup"] = out["sequential"]["wall_s"] / out["batched"]["wall_s"]
+    per = []
+    for spec, sc, r, c in zip(specs, scs, rs, counts):
+        ospec = copy.deepcopy(spec)
+        ospec.camera["samples_per_pixel"] = oracle_spp + 1
+        orc = capi.Render(sc, ospec, mode=capi.MODE_PERF, fp64_accumulate=1,
+                          seed=spec.seed + 1000, samples_per_wave=2)
+        orc.samples(1, oracle_spp)
+        d = lambda x: np.sqrt(np.clip(x, 0.0, 1.0))
+        rmse = float(np.sqrt(np.mean((d(r.beauty_fp64()) - d(orc.beauty_fp64())) ** 2)))
+        del orc
+        per.append({"scene": spec.name, "triangles": sc.stats()["n_triangles"],
+                    "res": [int(spec.camera["resolution"][0]), int(spec.camera["resolution"][1])],
+                    "spp": c, "depth": spec.ray_depth, "rmse": round(rmse, 5)})
+    out["per_scene"] = per
     return out
 
 

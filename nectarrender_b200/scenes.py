@@ -323,6 +323,32 @@ def medium_stress(levels: int = 8, res_h: int = 1080, res_w: int = 1920, spp: in
     return spec
 
 
+def batch_set(n: int = 64, seed: int = 0) -> list[SceneSpec]:
+    """The batched configuration: n independent scenes from the Cornell and
+    mesh-stress generators, triangle counts log-uniform in 10k-2M (rounded
+    to the nearest icosphere subdivision, levels 5-8), resolutions 256-1024
+    a side in steps of 16, 16-256 samples, depth 4-16. Meshes of one level
+    share their OBJ file (and the level-8 one is the mesh-stress workload's);
+    the spheres, camera, samples and depth differ per scene."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        res_h, res_w = (int(rng.integers(16, 65)) * 16 for _ in range(2))
+        spp = int(rng.integers(1, 17)) * 16
+        depth = int(rng.integers(4, 17))
+        if i % 4 == 0:
+            s = cornell(res=res_h, spp=spp, depth=depth, seed=int(rng.integers(1 << 16)))
+        else:
+            tris = math.exp(rng.uniform(math.log(1e4), math.log(2e6)))
+            level = int(min(8, max(5, round(math.log(tris / 20.0, 4)))))
+            s = mesh_stress(levels=level, res_h=res_h, res_w=res_w, spp=spp, depth=depth,
+                            n_spheres=int(rng.integers(8, 129)), hdri_size=(512, 256),
+                            scene_seed=0, seed=int(rng.integers(1 << 16)))
+        s.name = f"batch{seed}_{i}"
+        out.append(s)
+    return out
+
+
 # ---------------------------------------------------------------------------
 # spec -> _pathtracer objects (the reference's Python API)
 
