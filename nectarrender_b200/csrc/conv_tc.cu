@@ -35,6 +35,9 @@ __device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, bool v
 __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
 }
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+// waits until at most one committed group is still in flight
+__device__ __forceinline__ void cp_async_wait_1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 
 __host__ __device__ inline uint32_t tmem_cols(int n) {
   return n <= 32 ? 32u : (n <= 64 ? 64u : (n <= 128 ? 128u : 256u));
@@ -257,6 +260,152 @@ __global__ void __launch_bounds__(kThreads) k_conv_fwd_halo(ConvFwdArgs a) {
       }
       *reinterpret_cast<uint4*>(a.y + p * a.y_stride + a.y_off + c * 8) = pack_bf16x8(v);
     }
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) tc::tmem_dealloc(tmem, ncols);
+}
+
+// Persistent halo-tile forward with resident weights: the CTA keeps the
+// weights of all nine taps for its slice of nco output channels in shared
+// memory for its whole run of 8 x 16 pixel tiles, and streams only the input
+// halos through three stages (two tiles ahead). Two tensor-memory
+// accumulators alternate, so tile j's MMAs run while tile j - 1's epilogue
+// stores and tile j + 2's halo loads. Weights of tap t: K-major over (output channel, input channel),
+// element (n, k) at t * nco * cin * 2 + n * 16 + (k / 8) * nco * 16.
+constexpr int kFwdStages = 3;
+
+__global__ void __launch_bounds__(kThreads) k_conv_fwd_res(ConvFwdArgs a, int nco) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  __shared__ __align__(8) uint64_t bar[2];
+  __shared__ uint32_t tmem_base;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int cin = a.cin, kg_n = cin >> 3;
+  const int co0 = blockIdx.y * nco;
+  const int tw = a.W / kTileW, th = a.H / kTileH, n_tiles = tw * th * a.B;
+  const uint32_t lbo_a = (uint32_t)kHalo * 16u, sbo_a = (uint32_t)kHaloW * 16u;
+  const uint32_t h_bytes = (uint32_t)kg_n * lbo_a;
+  const uint32_t w_tap = (uint32_t)nco * cin * 2u, lbo_b = (uint32_t)nco * 16u;
+  const uint32_t base = tc::smem_u32(smem);
+  const uint32_t sw = base, sh0 = base + 9u * w_tap;  // then kFwdStages halo stages
+  const uint32_t ncols = 2u * nco <= 64u ? 64u : (2u * nco <= 128u ? 128u : 256u);
+
+  if (tid == 0) {
+    tc::mbar_init(&bar[0], 1);
+    tc::mbar_init(&bar[1], 1);
+  }
+  if (warp == 0) tc::tmem_alloc(&tmem_base, ncols);
+  auto load_halo = [&](int t, uint32_t dst) {
+    const int b = t / (tw * th), rest = t % (tw * th);
+    const int y0 = (rest / tw) * kTileH, x0 = (rest % tw) * kTileW;
+    for (int i = tid; i < kHalo * kg_n; i += kThreads) {
+      const int h = i % kHalo, kg = i / kHalo;
+      const int yy = y0 - 1 + h / kHaloW, xx = x0 - 1 + h % kHaloW;
+      const bool valid = yy >= 0 && yy < a.H && xx >= 0 && xx < a.W;
+      const __nv_bfloat16* src =
+          valid ? a.x + ((size_t)(b * a.H + yy) * a.W + xx) * a.x_stride + a.x_off + kg * 8 : a.x;
+      cp_async16(dst + (uint32_t)kg * lbo_a + (uint32_t)h * 16u, src, valid);
+    }
+  };
+  // resident weights of the slice, and the first halo
+  for (int i = tid; i < 9 * nco * kg_n; i += kThreads) {
+    const int n = i % nco, rest = i / nco, kg = rest % kg_n, t = rest / kg_n;
+    cp_async16(sw + (uint32_t)t * w_tap + (uint32_t)n * 16u + (uint32_t)kg * lbo_b,
+               a.w + ((size_t)t * a.cout + co0 + n) * cin + kg * 8, true);
+  }
+  const int first = blockIdx.x, step = (int)gridDim.x;
+  load_halo(first, sh0);  // first < n_tiles: the grid has at most n_tiles columns
+  cp_async_commit();
+  if (first + step < n_tiles) load_halo(first + step, sh0 + h_bytes);
+  cp_async_commit();
+  cp_async_wait_1();
+  tc::fence_smem_to_async();
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tmem = tmem_base;
+  const uint32_t idesc = tc::idesc_bf16(128, (uint32_t)nco, false, false);
+
+  auto epilogue = [&](int t, int s) {
+    const int b = t / (tw * th), rest = t % (tw * th);
+    const int y0 = (rest / tw) * kTileH, x0 = (rest % tw) * kTileW;
+    const int r = warp * 32 + lane;
+    const size_t p = (size_t)(b * a.H + y0 + r / kTileW) * a.W + x0 + r % kTileW;
+    // up to 64 columns in flight per wait
+    for (int c0 = 0; c0 < (nco >> 3); c0 += 8) {
+      uint32_t r[8][8];
+      const int nc = min(8, (nco >> 3) - c0);
+#pragma unroll
+      for (int c = 0; c < 8; ++c)
+        if (c < nc)
+          tc::tmem_ld8_nowait(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(s * nco + (c0 + c) * 8),
+                              r[c]);
+      tc::tmem_wait_ld();
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        if (c >= nc) break;
+        float v[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          v[q] = __uint_as_float(r[c][q]);
+          if (a.bias) v[q] += a.bias[co0 + (c0 + c) * 8 + q];
+          if (a.relu) v[q] = fmaxf(v[q], 0.0f);
+        }
+        *reinterpret_cast<uint4*>(a.y + p * a.y_stride + a.y_off + co0 + (c0 + c) * 8) = pack_bf16x8(v);
+      }
+    }
+  };
+
+  bool ok = true;
+  int j = 0;
+  for (int t = first; t < n_tiles; t += step, ++j) {
+    const int s = j & 1, hs = j % kFwdStages;
+    if (tid == 0) {
+      tc::fence_after_sync();
+      // descriptors advance by adding (byte offset >> 4) to the start-address
+      // field: every operand lies below 256 KB, so the field never carries
+      const uint64_t da0 = tc::smem_desc(sh0 + (uint32_t)hs * h_bytes, lbo_a, sbo_a);
+      const uint64_t db0 = tc::smem_desc(sw, lbo_b, 128u);
+      const uint32_t d = tmem + (uint32_t)(s * nco);
+      const int nk = cin >> 4;
+      for (int tap = 0; tap < 9; ++tap) {
+        const uint64_t da_t = da0 + (uint64_t)(((tap / 3) * kHaloW + (tap % 3)));  // 16-byte units
+        const uint64_t db_t = db0 + (uint64_t)(((uint32_t)tap * w_tap) >> 4);
+        for (int kk = 0; kk < nk; ++kk)
+          tc::mma_bf16(d, da_t + (uint64_t)((2u * kk * lbo_a) >> 4),
+                       db_t + (uint64_t)((2u * kk * lbo_b) >> 4), idesc, (tap > 0 || kk > 0) ? 1u : 0u);
+      }
+      tc::mma_commit(&bar[s]);
+    }
+    if (j >= 1) {
+      // tile j - 1's MMAs: their accumulator and halo stage become free
+      const bool w = tc::mbar_wait(&bar[s ^ 1], (uint32_t)((j - 1) >> 1) & 1u, kWaitLimit);
+      if (!__syncthreads_and(w)) {
+        ok = false;
+        break;
+      }
+      tc::fence_after_sync();
+    }
+    // tile j + 2's halo streams into the stage tile j - 1 used while tile
+    // j - 1's accumulator is stored; tile j + 1's halo must be complete
+    if (t + 2 * step < n_tiles) load_halo(t + 2 * step, sh0 + (uint32_t)((j + 2) % kFwdStages) * h_bytes);
+    cp_async_commit();
+    if (j >= 1) epilogue(t - step, s ^ 1);
+    cp_async_wait_1();
+    tc::fence_smem_to_async();
+    tc::fence_before_sync();
+    __syncthreads();
+  }
+  if (ok && j >= 1) {
+    const int s = (j - 1) & 1;
+    ok = __syncthreads_and(tc::mbar_wait(&bar[s], (uint32_t)((j - 1) >> 1) & 1u, kWaitLimit));
+    tc::fence_after_sync();
+    if (ok) epilogue(first + (j - 1) * step, s);
+  }
+  if (!ok) {
+    if (tid == 0) atomicOr(a.err, 2u);
+    tc::mbar_wait(&bar[0], 0u, kWaitLimit);  // bounded: MMAs that may still be in flight
+    tc::mbar_wait(&bar[1], 0u, kWaitLimit);
   }
   tc::fence_before_sync();
   __syncthreads();
@@ -502,8 +651,33 @@ cudaError_t launch_conv_fwd(const ConvFwdArgs& a, cudaStream_t st) {
   if (a.cin % 16 || a.cout % 16 || a.cin < 16 || a.cout < 16 || a.cin > 256 || a.cout > 256 ||
       a.x_stride % 8 || a.x_off % 8 || a.y_stride % 8 || a.y_off % 8)
     return cudaErrorInvalidValue;
+  const bool tiles_fit = a.taps != 1 && a.W % kTileW == 0 && a.H % kTileH == 0;
+  if (tiles_fit) {
+    // resident weights: the widest output-channel slice whose nine taps and
+    // kFwdStages halos fit
+    const size_t halo = (size_t)(a.cin >> 3) * kHalo * 16u;
+    int nco = a.cout;
+    while (nco >= 16 && (9u * (size_t)nco * a.cin * 2u + kFwdStages * halo > 200u * 1024u ||
+                         a.cout % nco != 0 || nco % 16 != 0))
+      nco -= 16;
+    if ((nco >= 32 || nco == a.cout) && nco >= 16 && nco <= 128) {
+      const size_t smem = 9u * (size_t)nco * a.cin * 2u + kFwdStages * halo;
+      cudaError_t e = cudaFuncSetAttribute(k_conv_fwd_res, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)smem);
+      if (e != cudaSuccess) return e;
+      int dev = 0, sms = 148, per_sm = 1;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_conv_fwd_res, kThreads, smem);
+      const int slices = a.cout / nco;
+      const int n_tiles = (a.W / kTileW) * (a.H / kTileH) * a.B;
+      const int workers = std::max(1, std::min(n_tiles, sms * std::max(1, per_sm) / slices));
+      k_conv_fwd_res<<<dim3(workers, slices), kThreads, smem, st>>>(a, nco);
+      return cudaGetLastError();
+    }
+  }
   const size_t halo_smem = (size_t)(a.cin >> 3) * kHalo * 16u + 2u * (size_t)a.cout * a.cin * 2u;
-  if (a.taps != 1 && a.W % kTileW == 0 && a.H % kTileH == 0 && halo_smem <= 200u * 1024u) {
+  if (tiles_fit && halo_smem <= 200u * 1024u) {
     cudaError_t e = cudaFuncSetAttribute(k_conv_fwd_halo,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)halo_smem);
     if (e != cudaSuccess) return e;

@@ -120,6 +120,19 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, float (&v)[8]) {
   for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// The same load without the wait: the registers are valid only after
+// tmem_wait_ld(), so several loads can be in flight at once.
+__device__ __forceinline__ void tmem_ld8_nowait(uint32_t taddr, uint32_t (&r)[8]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7])
+      : "r"(taddr) : "memory");
+}
+__device__ __forceinline__ void tmem_wait_ld() {
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
 // Byte offsets of the canonical layouts (see the file comment).
 __host__ __device__ constexpr uint32_t kmajor_off(uint32_t r, uint32_t k, uint32_t lbo, uint32_t sbo) {
   return (r >> 3) * sbo + (k >> 3) * lbo + (r & 7u) * 16u + (k & 7u) * 2u;

@@ -47,11 +47,14 @@ def ptr(t):
     return C.c_void_p(t.data_ptr())
 
 
-# H % 16 == 0 and W % 8 == 0 take the halo-tile kernel, the others the
-# per-tap gather kernel
+# H % 16 == 0 and W % 8 == 0 take the halo-tile kernels (resident weights
+# when a slice of at least 32 output channels fits with two halos, else
+# streamed weights), the others the per-tap gather kernel
 @pytest.mark.parametrize("B,H,W,ci,co,relu", [(2, 16, 24, 32, 48, 1), (1, 32, 32, 16, 32, 0),
                                               (1, 8, 48, 160, 96, 1), (1, 16, 16, 64, 256, 0),
-                                              (2, 48, 40, 176, 80, 1), (1, 24, 20, 48, 64, 1)])
+                                              (2, 48, 40, 176, 80, 1), (1, 24, 20, 48, 64, 1),
+                                              (4, 128, 128, 32, 32, 1),  # several tiles per CTA
+                                              (4, 64, 64, 96, 96, 0)])   # two 48-channel slices
 def test_forward(B, H, W, ci, co, relu):
     lib = capi.library()
     rng = np.random.default_rng(ci * 1000 + co)
