@@ -181,10 +181,12 @@ def run_reference(args):
     spec, h, w = workload(args)
     handle, kind = cpu_reference(spec)
     cores = os.cpu_count() or 1
-    per_step_rows = max(4, h // 128)
+    # four rows per host thread per step (the reference's host loop splits
+    # rows among the threads), bands walking down the frame and wrapping
+    per_step_rows = min(h, max(4, 4 * cores))
     times = []
     for i in range(args.warmup + args.steps):
-        r0 = (i * per_step_rows) % max(1, h - per_step_rows)
+        r0 = (i * per_step_rows) % max(1, h - per_step_rows + 1)
         t0 = time.perf_counter()
         handle.render(1, 1, mode=0, rows=(r0, r0 + per_step_rows), threads=cores)
         if i >= args.warmup:
