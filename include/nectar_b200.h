@@ -344,6 +344,15 @@ int nr_render_samples(nr_render* render, uint32_t first, uint32_t count);
 int nr_render_samples_batch(nr_render* const* renders, uint32_t n, const uint32_t* first,
                             const uint32_t* count);
 
+/* Fuses the display transform into accumulation: with c set, every later
+ * render call's accumulate pass also writes the beauty layer's display bytes
+ * (uint8 CHW, the same values nr_render_readback computes for config c), and
+ * nr_render_readback of the beauty layer with an identical config only
+ * copies them to the host. c = NULL turns it off. No counterpart in the
+ * reference, whose accumulate (data.cu:28-50) and process_stream
+ * (stream.cu:146-159) are separate kernels. */
+int nr_render_set_fused_display(nr_render* render, const nr_stream_config* c);
+
 /* nr_render_samples_static: no counterpart in the reference.
  * Renders exactly like nr_render_samples (same sample indices, same layers,
  * same results; always the wavefront schedule) but allocates no device memory

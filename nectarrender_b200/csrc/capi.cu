@@ -1081,6 +1081,10 @@ struct nr_render {
   uint32_t nrc_cap = 0;
   uint64_t nrc_queries = 0, nrc_records = 0;  // totals since attached
   std::string nrc_error;                       // set by the wave hook
+  // fused display of the beauty layer (nr_render_set_fused_display)
+  bool fused_on = false, fused_valid = false;
+  nr_stream_config fused_cfg{};
+  DisplayParams fused_p{};
   PickOut* d_pick = nullptr;        // viewport queries (allocated on first use)
   uint8_t* d_mask = nullptr;        // 2 x W*H selection masks
   uint32_t graphs_captured = 0;
@@ -1234,6 +1238,7 @@ int nr_render_destroy(nr_render* r) {
 
 int nr_render_reset(nr_render* r) {
   if (!r) return fail(NR_ERR_INVALID, "null render");
+  r->fused_valid = false;
   size_t hw = (size_t)r->W * r->H;
   for (int l = 0; l < 9; ++l)
     if (r->layer[l]) CU(cudaMemsetAsync(r->layer[l], 0, sizeof(float) * r->layer_c[l] * hw, r->stream), "clear");
@@ -1414,6 +1419,11 @@ static int launch(nr_render* r, const KernelParams& P, WaveTimer* tm) {
   W.shade_variant = r->cfg.shade_variant > 0 ? r->cfg.shade_variant : kDefaultShadeVariant;
   W.tail_max_paths = r->cfg.tail_max_paths == 0 ? kDefaultTailPaths
                      : (r->cfg.tail_max_paths == UINT32_MAX ? 0u : r->cfg.tail_max_paths);
+  const bool fused = r->fused_on && r->disp8 && !P.write_raw && P.beauty;
+  if (fused) {
+    W.disp8 = r->disp8;
+    W.disp_p = r->fused_p;
+  }
   WaveHook hook;
   const bool nrc = r->nrc && r->cfg.mode == NR_MODE_PERF && !P.write_raw;
   if (nrc) {
@@ -1467,11 +1477,13 @@ static int launch(nr_render* r, const KernelParams& P, WaveTimer* tm) {
     const std::string m = nrc_poll_error(r->nrc->n, r->stream);  // the last wave's cache launches
     if (!m.empty()) return fail(NR_ERR_DEVICE, m);
   }
+  r->fused_valid = fused;
   return NR_OK;
 }
 
 // Enqueues a render call on the render's stream (events around it).
 static int enqueue_kernel(nr_render* r, const KernelParams& P, WaveTimer& tm) {
+  r->fused_valid = false;  // set again when the wavefront's accumulate writes the display
   if (r->counters_on) CU(cudaMemsetAsync(r->counters, 0, 8 * 5, r->stream), "clear counters");
   CU(cudaEventRecord(r->ev0, r->stream), "event");
   if (r->profile_on) {
@@ -1578,6 +1590,7 @@ static std::atomic<uintptr_t> g_static_wave_addr[64];
 
 int nr_render_samples_static(nr_render* r, uint32_t first, uint32_t count) {
   if (!r) return fail(NR_ERR_INVALID, "null render");
+  r->fused_valid = false;  // this path leaves the fused display untouched
   if (count == 0) return NR_OK;
   if (first == 0) return fail(NR_ERR_INVALID, "sample indices start at 1");
   if ((uint64_t)first + count > r->cam.samples_per_pixel)
@@ -1751,13 +1764,7 @@ int nr_render_read_beauty_fp64(nr_render* r, double* host) {
   return NR_OK;
 }
 
-static int display(nr_render* r, int32_t layer, const nr_stream_config* c, uint8_t* h8, float* hf) {
-  if (!r || !c || layer < 0 || layer > 8) return fail(NR_ERR_INVALID, "bad argument");
-  if (!r->layer[layer] || r->layer_c[layer] != 3)
-    return fail(NR_ERR_STATE, "display needs an enabled 3-channel layer");
-  size_t hw = (size_t)r->W * r->H;
-  if (h8 && !r->disp8) CU(cudaMalloc(&r->disp8, 3 * hw), "alloc");
-  if (hf && !r->dispf) CU(cudaMalloc(&r->dispf, sizeof(float) * 3 * hw), "alloc");
+static DisplayParams display_params(const nr_stream_config* c) {
   DisplayParams p{};
   p.linear_to_gamma = c->linear_to_gamma;
   p.apply_white_balance = c->apply_white_balance;
@@ -1766,6 +1773,24 @@ static int display(nr_render* r, int32_t layer, const nr_stream_config* c, uint8
   p.tm_method = c->tm_method;
   p.tm_white_point = c->tm_white_point;
   p.tm_alpha = c->tm_alpha;
+  return p;
+}
+
+static int display(nr_render* r, int32_t layer, const nr_stream_config* c, uint8_t* h8, float* hf) {
+  if (!r || !c || layer < 0 || layer > 8) return fail(NR_ERR_INVALID, "bad argument");
+  if (!r->layer[layer] || r->layer_c[layer] != 3)
+    return fail(NR_ERR_STATE, "display needs an enabled 3-channel layer");
+  size_t hw = (size_t)r->W * r->H;
+  if (h8 && !hf && layer == NR_LAYER_BEAUTY && r->fused_on && r->fused_valid &&
+      memcmp(c, &r->fused_cfg, sizeof(*c)) == 0) {
+    // the last render call's accumulate pass already wrote these bytes
+    CU(cudaMemcpyAsync(h8, r->disp8, 3 * hw, cudaMemcpyDeviceToHost, r->stream), "read");
+    CU(cudaStreamSynchronize(r->stream), "display");
+    return NR_OK;
+  }
+  if (h8 && !r->disp8) CU(cudaMalloc(&r->disp8, 3 * hw), "alloc");
+  if (hf && !r->dispf) CU(cudaMalloc(&r->dispf, sizeof(float) * 3 * hw), "alloc");
+  DisplayParams p = display_params(c);
   CU(display_params_resolve(p, c->wb_temperature, r->wb_scratch, r->stream), "white balance");
   CU(launch_display(r->layer[layer], h8 ? r->disp8 : nullptr, hf ? r->dispf : nullptr, hw, p,
                     r->stream),
@@ -1773,6 +1798,24 @@ static int display(nr_render* r, int32_t layer, const nr_stream_config* c, uint8
   if (h8) CU(cudaMemcpyAsync(h8, r->disp8, 3 * hw, cudaMemcpyDeviceToHost, r->stream), "read");
   if (hf) CU(cudaMemcpyAsync(hf, r->dispf, sizeof(float) * 3 * hw, cudaMemcpyDeviceToHost, r->stream), "read");
   CU(cudaStreamSynchronize(r->stream), "display");
+  return NR_OK;
+}
+
+int nr_render_set_fused_display(nr_render* r, const nr_stream_config* c) {
+  if (!r) return fail(NR_ERR_INVALID, "null render");
+  r->fused_valid = false;
+  if (!c) {
+    r->fused_on = false;
+    return NR_OK;
+  }
+  if (!r->layer[NR_LAYER_BEAUTY]) return fail(NR_ERR_STATE, "the beauty layer is not enabled");
+  const size_t hw = (size_t)r->W * r->H;
+  if (!r->disp8) CU(cudaMalloc(&r->disp8, 3 * hw), "alloc");
+  DisplayParams p = display_params(c);
+  CU(display_params_resolve(p, c->wb_temperature, r->wb_scratch, r->stream), "white balance");
+  r->fused_p = p;
+  r->fused_cfg = *c;
+  r->fused_on = true;
   return NR_OK;
 }
 

@@ -28,47 +28,6 @@ __device__ __forceinline__ V3 kelvin_to_rgb(float kelvin) {
             fminf(1.0f, fmaxf(0.0f, b / 255.0f))};
 }
 
-// white_balance (stream.cu:88-109), tonemaps (stream.cu:7-59), gamma (:115-121)
-__device__ __forceinline__ V3 display_pixel(V3 c, const DisplayParams& p) {
-  if (p.apply_white_balance) {
-    c = c * p.wb_ratio;
-    float tint = p.wb_tint * 0.0025f;
-    c = V3{c.x * (1.0f + tint * 0.5f), c.y * (1.0f - tint), c.z * (1.0f + tint * 0.5f)};
-  }
-  if (p.apply_tonemapping) {
-    V3 col = c;
-    if (p.tm_method == 1) {  // REINHARD_EXTENDED
-      float inv_white2 = 1.0f / (p.tm_white_point * p.tm_white_point);
-      V3 num = col * (v3(1.0f) + col * inv_white2);
-      col = num / (v3(1.0f) + col);
-    } else if (p.tm_method == 2) {  // ACES fit
-      const float a = 2.51f, b = 0.03f, cc = 2.43f, d = 0.59f, e = 0.14f;
-      V3 x = col;
-      V3 num = x * (x * a + b);
-      V3 den = x * (x * cc + d) + e;
-      col = V3{fminf(1.0f, fmaxf(0.0f, num.x / den.x)), fminf(1.0f, fmaxf(0.0f, num.y / den.y)),
-               fminf(1.0f, fmaxf(0.0f, num.z / den.z))};
-    }
-    // REINHARD leaves col unchanged: the reference discards its result.
-    float alpha = p.tm_alpha;
-    c = ((1.0f - alpha) * c + alpha * col);
-    c = V3{fminf(1.0f, fmaxf(0.0f, c.x)), fminf(1.0f, fmaxf(0.0f, c.y)),
-           fminf(1.0f, fmaxf(0.0f, c.z))};
-  }
-  if (p.linear_to_gamma) {
-    c = V3{c.x > 0.0f ? sqrtf(c.x) : 0.0f, c.y > 0.0f ? sqrtf(c.y) : 0.0f,
-           c.z > 0.0f ? sqrtf(c.z) : 0.0f};
-  }
-  return c;
-}
-
-// to_image (stream.cu:123-140): NaN -> 0, clamp, *255, truncate.
-__device__ __forceinline__ float quant_pre(float v) {
-  if (isnan(v)) v = 0.0f;
-  v = fmaxf(0.0f, fminf(1.0f, v));
-  return v * 255.0f;
-}
-
 __global__ void k_display(const float* __restrict__ src, uint8_t* __restrict__ dst8,
                           float* __restrict__ dstf, size_t hw, DisplayParams p) {
   size_t n4 = hw / 4;

@@ -21,6 +21,7 @@
 
 #include <array>
 #include <atomic>
+#include <cstring>
 #include <cmath>
 #include <fstream>
 #include <memory>
@@ -371,6 +372,9 @@ struct TransferStream {
   StreamConfig cfg;
   int layer = (int)LayerType::BEAUTY;
   std::vector<uint8_t> buffer;
+  // the config the render's accumulate pass already applies (fused display)
+  nr_render* fused_render = nullptr;
+  nr_stream_config fused_cfg{};
   uintptr_t readback();
   uintptr_t buffer_ptr() { return reinterpret_cast<uintptr_t>(buffer.data()); }
   std::array<size_t, 3> shape() const;
@@ -587,6 +591,13 @@ uintptr_t TransferStream::readback() {
   if (state == StreamState::FROZEN) return buffer_ptr();
   buffer.resize((size_t)3 * eng->H() * eng->W());
   nr_stream_config c = cfg.desc();
+  if (layer == (int)LayerType::BEAUTY &&
+      (fused_render != eng->render || memcmp(&c, &fused_cfg, sizeof(c)) != 0)) {
+    // later renders write this stream's bytes in their accumulate pass
+    check(nr_render_set_fused_display(eng->render, &c), "TransferStream.readback");
+    fused_render = eng->render;
+    fused_cfg = c;
+  }
   check(nr_render_readback(eng->render, layer, &c, buffer.data()), "TransferStream.readback");
   return buffer_ptr();
 }

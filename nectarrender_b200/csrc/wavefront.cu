@@ -1073,6 +1073,12 @@ __global__ void k_wf_accumulate(WfParams W) {
     if (P.beauty) store3(P.beauty, hw, pix, ab);
     if (P.diffuse) store3(P.diffuse, hw, pix, ad);
     if (P.normal) store3(P.normal, hw, pix, an);
+    if (W.disp8) {  // the display transform of the new running mean, in the same pass
+      const V3 c = display_pixel(ab, W.disp_p);
+      W.disp8[pix] = (uint8_t)quant_pre(c.x);
+      W.disp8[hw + pix] = (uint8_t)quant_pre(c.y);
+      W.disp8[2 * hw + pix] = (uint8_t)quant_pre(c.z);
+    }
     if (P.beauty64) {
       P.beauty64[pix] += s64[0];
       P.beauty64[hw + pix] += s64[1];

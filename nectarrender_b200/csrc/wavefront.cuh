@@ -1,5 +1,6 @@
 // wavefront.cuh — launch interface of the wavefront integrator.
 #pragma once
+#include "image_ops.cuh"
 #include "integrator.cuh"
 #include "../../include/nectar_b200.h"
 
@@ -53,6 +54,10 @@ struct WfParams {
   uint32_t* queue_s;
   uint8_t* skey;
   uint32_t* sort_ctr;
+  // fused display (null: off): the accumulate kernel also writes the beauty
+  // layer's display transform as uint8 CHW
+  uint8_t* disp8;
+  DisplayParams disp_p;
 };
 
 size_t wf_state_bytes(uint32_t n_paths, bool perf = false, bool sort = false);
