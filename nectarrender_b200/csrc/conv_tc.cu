@@ -274,8 +274,9 @@ __global__ void __launch_bounds__(kThreads) k_conv_fwd_halo(ConvFwdArgs a) {
 // stores and tile j + 2's halo loads. Weights of tap t: K-major over (output channel, input channel),
 // element (n, k) at t * nco * cin * 2 + n * 16 + (k / 8) * nco * 16.
 constexpr int kFwdStages = 3;
+constexpr int kResThreads = 256;  // 8 warps: an MMA issuer, loaders, four storers
 
-__global__ void __launch_bounds__(kThreads) k_conv_fwd_res(ConvFwdArgs a, int nco) {
+__global__ void __launch_bounds__(kResThreads) k_conv_fwd_res(ConvFwdArgs a, int nco) {
   extern __shared__ __align__(1024) unsigned char smem[];
   __shared__ __align__(8) uint64_t bar[2];
   __shared__ uint32_t tmem_base;
@@ -295,10 +296,14 @@ __global__ void __launch_bounds__(kThreads) k_conv_fwd_res(ConvFwdArgs a, int nc
     tc::mbar_init(&bar[1], 1);
   }
   if (warp == 0) tc::tmem_alloc(&tmem_base, ncols);
+  // warp roles: warp 0 issues the MMAs, warps 1-7 load halos, warps 4-7
+  // store the accumulators (one per tensor-memory subpartition), so that
+  // the MMAs of one tile overlap the loads and stores of the others
   auto load_halo = [&](int t, uint32_t dst) {
     const int b = t / (tw * th), rest = t % (tw * th);
     const int y0 = (rest / tw) * kTileH, x0 = (rest % tw) * kTileW;
-    for (int i = tid; i < kHalo * kg_n; i += kThreads) {
+    if (tid < 32) return;
+    for (int i = tid - 32; i < kHalo * kg_n; i += kResThreads - 32) {
       const int h = i % kHalo, kg = i / kHalo;
       const int yy = y0 - 1 + h / kHaloW, xx = x0 - 1 + h % kHaloW;
       const bool valid = yy >= 0 && yy < a.H && xx >= 0 && xx < a.W;
@@ -308,7 +313,7 @@ __global__ void __launch_bounds__(kThreads) k_conv_fwd_res(ConvFwdArgs a, int nc
     }
   };
   // resident weights of the slice, and the first halo
-  for (int i = tid; i < 9 * nco * kg_n; i += kThreads) {
+  for (int i = tid; i < 9 * nco * kg_n; i += kResThreads) {
     const int n = i % nco, rest = i / nco, kg = rest % kg_n, t = rest / kg_n;
     cp_async16(sw + (uint32_t)t * w_tap + (uint32_t)n * 16u + (uint32_t)kg * lbo_b,
                a.w + ((size_t)t * a.cout + co0 + n) * cin + kg * 8, true);
@@ -329,16 +334,20 @@ __global__ void __launch_bounds__(kThreads) k_conv_fwd_res(ConvFwdArgs a, int nc
   auto epilogue = [&](int t, int s) {
     const int b = t / (tw * th), rest = t % (tw * th);
     const int y0 = (rest / tw) * kTileH, x0 = (rest % tw) * kTileW;
-    const int r = warp * 32 + lane;
+    // warp w (4..7) reads tensor-memory lanes 32 (w % 4) .. +31, its subpartition
+    if (warp < 4) return;
+    const int sub = warp & 3;
+    const int r = sub * 32 + lane;
     const size_t p = (size_t)(b * a.H + y0 + r / kTileW) * a.W + x0 + r % kTileW;
+    const int g0 = 0, gend = nco >> 3;
     // up to 64 columns in flight per wait
-    for (int c0 = 0; c0 < (nco >> 3); c0 += 8) {
+    for (int c0 = g0; c0 < gend; c0 += 8) {
       uint32_t r[8][8];
-      const int nc = min(8, (nco >> 3) - c0);
+      const int nc = min(8, gend - c0);
 #pragma unroll
       for (int c = 0; c < 8; ++c)
         if (c < nc)
-          tc::tmem_ld8_nowait(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(s * nco + (c0 + c) * 8),
+          tc::tmem_ld8_nowait(tmem + ((uint32_t)(sub * 32) << 16) + (uint32_t)(s * nco + (c0 + c) * 8),
                               r[c]);
       tc::tmem_wait_ld();
 #pragma unroll
@@ -356,51 +365,64 @@ __global__ void __launch_bounds__(kThreads) k_conv_fwd_res(ConvFwdArgs a, int nc
     }
   };
 
+  // One CTA barrier per tile, at its end. Warp 0 issues tile j's MMAs while
+  // the other warps wait (each on the mbarrier) for tile j - 1's, load tile
+  // j + 2's halo into the stage tile j - 1 used and store tile j - 1's
+  // accumulator.
   bool ok = true;
   int j = 0;
   for (int t = first; t < n_tiles; t += step, ++j) {
     const int s = j & 1, hs = j % kFwdStages;
-    if (tid == 0) {
-      tc::fence_after_sync();
-      // descriptors advance by adding (byte offset >> 4) to the start-address
-      // field: every operand lies below 256 KB, so the field never carries
-      const uint64_t da0 = tc::smem_desc(sh0 + (uint32_t)hs * h_bytes, lbo_a, sbo_a);
-      const uint64_t db0 = tc::smem_desc(sw, lbo_b, 128u);
-      const uint32_t d = tmem + (uint32_t)(s * nco);
-      const int nk = cin >> 4;
-      for (int tap = 0; tap < 9; ++tap) {
-        const uint64_t da_t = da0 + (uint64_t)(((tap / 3) * kHaloW + (tap % 3)));  // 16-byte units
-        const uint64_t db_t = db0 + (uint64_t)(((uint32_t)tap * w_tap) >> 4);
-        for (int kk = 0; kk < nk; ++kk)
-          tc::mma_bf16(d, da_t + (uint64_t)((2u * kk * lbo_a) >> 4),
-                       db_t + (uint64_t)((2u * kk * lbo_b) >> 4), idesc, (tap > 0 || kk > 0) ? 1u : 0u);
+    bool fail = false;
+    if (warp == 0) {
+      if (lane == 0) {
+        tc::fence_after_sync();
+        // descriptors advance by adding (byte offset >> 4) to the start-address
+        // field: every operand lies below 256 KB, so the field never carries
+        const uint64_t da0 = tc::smem_desc(sh0 + (uint32_t)hs * h_bytes, lbo_a, sbo_a);
+        const uint64_t db0 = tc::smem_desc(sw, lbo_b, 128u);
+        const uint32_t d = tmem + (uint32_t)(s * nco);
+        const int nk = cin >> 4;
+        for (int tap = 0; tap < 9; ++tap) {
+          const uint64_t da_t = da0 + (uint64_t)(((tap / 3) * kHaloW + (tap % 3)));  // 16-byte units
+          const uint64_t db_t = db0 + (uint64_t)(((uint32_t)tap * w_tap) >> 4);
+          for (int kk = 0; kk < nk; ++kk)
+            tc::mma_bf16(d, da_t + (uint64_t)((2u * kk * lbo_a) >> 4),
+                         db_t + (uint64_t)((2u * kk * lbo_b) >> 4), idesc, (tap > 0 || kk > 0) ? 1u : 0u);
+        }
+        tc::mma_commit(&bar[s]);
       }
-      tc::mma_commit(&bar[s]);
-    }
-    if (j >= 1) {
-      // tile j - 1's MMAs: their accumulator and halo stage become free
-      const bool w = tc::mbar_wait(&bar[s ^ 1], (uint32_t)((j - 1) >> 1) & 1u, kWaitLimit);
-      if (!__syncthreads_and(w)) {
-        ok = false;
-        break;
+      __syncwarp();
+    } else {
+      if (j >= 1) {
+        // tile j - 1's MMAs: their accumulator and halo stage become free
+        fail = !tc::mbar_wait(&bar[s ^ 1], (uint32_t)((j - 1) >> 1) & 1u, kWaitLimit);
+        tc::fence_after_sync();
       }
-      tc::fence_after_sync();
+      if (!fail) {
+        if (t + 2 * step < n_tiles)
+          load_halo(t + 2 * step, sh0 + (uint32_t)((j + 2) % kFwdStages) * h_bytes);
+        cp_async_commit();
+        if (j >= 1) epilogue(t - step, s ^ 1);
+        cp_async_wait_1();  // tile j + 1's halo is complete
+        tc::fence_smem_to_async();
+      }
     }
-    // tile j + 2's halo streams into the stage tile j - 1 used while tile
-    // j - 1's accumulator is stored; tile j + 1's halo must be complete
-    if (t + 2 * step < n_tiles) load_halo(t + 2 * step, sh0 + (uint32_t)((j + 2) % kFwdStages) * h_bytes);
-    cp_async_commit();
-    if (j >= 1) epilogue(t - step, s ^ 1);
-    cp_async_wait_1();
-    tc::fence_smem_to_async();
     tc::fence_before_sync();
-    __syncthreads();
+    if (__syncthreads_or(fail)) {
+      ok = false;
+      break;
+    }
   }
   if (ok && j >= 1) {
     const int s = (j - 1) & 1;
-    ok = __syncthreads_and(tc::mbar_wait(&bar[s], (uint32_t)((j - 1) >> 1) & 1u, kWaitLimit));
-    tc::fence_after_sync();
-    if (ok) epilogue(first + (j - 1) * step, s);
+    bool w = true;
+    if (warp >= 4) {
+      w = tc::mbar_wait(&bar[s], (uint32_t)((j - 1) >> 1) & 1u, kWaitLimit);
+      tc::fence_after_sync();
+      if (w) epilogue(first + (j - 1) * step, s);
+    }
+    ok = __syncthreads_and(w);
   }
   if (!ok) {
     if (tid == 0) atomicOr(a.err, 2u);
@@ -668,11 +690,11 @@ cudaError_t launch_conv_fwd(const ConvFwdArgs& a, cudaStream_t st) {
       int dev = 0, sms = 148, per_sm = 1;
       cudaGetDevice(&dev);
       cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_conv_fwd_res, kThreads, smem);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_conv_fwd_res, kResThreads, smem);
       const int slices = a.cout / nco;
       const int n_tiles = (a.W / kTileW) * (a.H / kTileH) * a.B;
       const int workers = std::max(1, std::min(n_tiles, sms * std::max(1, per_sm) / slices));
-      k_conv_fwd_res<<<dim3(workers, slices), kThreads, smem, st>>>(a, nco);
+      k_conv_fwd_res<<<dim3(workers, slices), kResThreads, smem, st>>>(a, nco);
       return cudaGetLastError();
     }
   }
