@@ -275,6 +275,7 @@ __global__ void __launch_bounds__(kThreads) k_conv_fwd_halo(ConvFwdArgs a) {
 // element (n, k) at t * nco * cin * 2 + n * 16 + (k / 8) * nco * 16.
 constexpr int kFwdStages = 3;
 constexpr int kResThreads = 256;  // 8 warps: an MMA issuer, loaders, four storers
+constexpr int kWgThreads = 256;   // 8 warps: an MMA issuer and seven loaders
 
 __global__ void __launch_bounds__(kResThreads) k_conv_fwd_res(ConvFwdArgs a, int nco) {
   extern __shared__ __align__(1024) unsigned char smem[];
@@ -555,7 +556,7 @@ __global__ void __launch_bounds__(kThreads) k_conv_wgrad(ConvWgradArgs a) {
 // of the group accumulates in its own cin tensor-memory columns over all the
 // CTA's tiles (two shared-memory stages: tile j loads while tile j - 1's
 // MMAs run); the partial sums go to dW with vector atomics at the end.
-__global__ void __launch_bounds__(kThreads) k_conv_wgrad_halo(ConvWgradArgs a, int tpg,
+__global__ void __launch_bounds__(kWgThreads) k_conv_wgrad_halo(ConvWgradArgs a, int tpg,
                                                                int tiles_per_cta) {
   extern __shared__ __align__(1024) unsigned char smem[];
   __shared__ __align__(8) uint64_t bar[2];
@@ -570,7 +571,7 @@ __global__ void __launch_bounds__(kThreads) k_conv_wgrad_halo(ConvWgradArgs a, i
   const uint32_t base = tc::smem_u32(smem);
   const uint32_t ncols = (uint32_t)ntap * cin <= 256u ? 256u : 512u;
 
-  for (uint32_t i = tid * 16u; i < 2u * stage_bytes; i += kThreads * 16u)
+  for (uint32_t i = tid * 16u; i < 2u * stage_bytes; i += kWgThreads * 16u)
     *reinterpret_cast<uint4*>(smem + i) = make_uint4(0u, 0u, 0u, 0u);
   if (tid == 0) {
     tc::mbar_init(&bar[0], 1);
@@ -584,50 +585,57 @@ __global__ void __launch_bounds__(kThreads) k_conv_wgrad_halo(ConvWgradArgs a, i
   const uint32_t tmem = tmem_base;
   const uint32_t idesc = tc::idesc_bf16(128, (uint32_t)cin, true, true);
 
+  // warp 0 issues the MMAs; warps 1-7 wait (each on the mbarrier) for the
+  // stage to come free and load the next tile; one CTA barrier per tile
   bool ok = true;
   int uses[2] = {0, 0};
-  for (int t = t0; t < t1 && ok; ++t) {
+  for (int t = t0; t < t1; ++t) {
     const int j = t - t0, s = j & 1;
-    if (j >= 2) {
-      const bool w = tc::mbar_wait(&bar[s], (uint32_t)(uses[s] - 1) & 1u, kWaitLimit);
-      if (!__syncthreads_and(w)) {
-        ok = false;
-        break;
-      }
-    }
-    const int b = t / (tw * th), rest = t % (tw * th);
-    const int y0 = (rest / tw) * kTileH, x0 = (rest % tw) * kTileW;
     const uint32_t sa = base + s * stage_bytes, sb = sa + a_bytes;
-    for (int i = tid; i < (cout >> 3) * 128; i += kThreads) {
-      const int pl = i & 127, cg = i >> 7;
-      const size_t p = (size_t)(b * a.H + y0 + pl / kTileW) * a.W + x0 + pl % kTileW;
-      cp_async16(sa + (uint32_t)cg * 2048u + (uint32_t)pl * 16u,
-                 a.dy + p * a.dy_stride + a.dy_off + cg * 8, true);
-    }
-    for (int i = tid; i < kHalo * kg_n; i += kThreads) {
-      const int h = i % kHalo, kg = i / kHalo;
-      const int yy = y0 - 1 + h / kHaloW, xx = x0 - 1 + h % kHaloW;
-      const bool valid = yy >= 0 && yy < a.H && xx >= 0 && xx < a.W;
-      const __nv_bfloat16* src =
-          valid ? a.x + ((size_t)(b * a.H + yy) * a.W + xx) * a.x_stride + a.x_off + kg * 8 : a.x;
-      cp_async16(sb + (uint32_t)kg * kHalo * 16u + (uint32_t)h * 16u, src, valid);
-    }
-    cp_async_wait_all();
-    tc::fence_smem_to_async();
-    __syncthreads();
-    if (tid == 0) {
-      tc::fence_after_sync();
-      for (int q = 0; q < ntap; ++q) {
-        const int tap = tap0 + q;
-        const uint32_t tap_off = (uint32_t)((tap / 3) * kHaloW + (tap % 3)) * 16u;
-        for (int kk = 0; kk < 8; ++kk) {  // K = 128 pixels = 16 tile rows, two per MMA
-          const uint64_t da = tc::smem_desc(sa + 256u * kk, 128u, 2048u);
-          const uint64_t db = tc::smem_desc(sb + tap_off + 2u * kk * kHaloW * 16u, kHaloW * 16u,
-                                            kHalo * 16u);
-          tc::mma_bf16(tmem + (uint32_t)(q * cin), da, db, idesc, (j > 0 || kk > 0) ? 1u : 0u);
+    bool fail = false;
+    if (warp != 0) {
+      if (j >= 2) fail = !tc::mbar_wait(&bar[s], (uint32_t)(uses[s] - 1) & 1u, kWaitLimit);
+      if (!fail) {
+        const int b = t / (tw * th), rest = t % (tw * th);
+        const int y0 = (rest / tw) * kTileH, x0 = (rest % tw) * kTileW;
+        for (int i = tid - 32; i < (cout >> 3) * 128; i += kWgThreads - 32) {
+          const int pl = i & 127, cg = i >> 7;
+          const size_t p = (size_t)(b * a.H + y0 + pl / kTileW) * a.W + x0 + pl % kTileW;
+          cp_async16(sa + (uint32_t)cg * 2048u + (uint32_t)pl * 16u,
+                     a.dy + p * a.dy_stride + a.dy_off + cg * 8, true);
         }
+        for (int i = tid - 32; i < kHalo * kg_n; i += kWgThreads - 32) {
+          const int h = i % kHalo, kg = i / kHalo;
+          const int yy = y0 - 1 + h / kHaloW, xx = x0 - 1 + h % kHaloW;
+          const bool valid = yy >= 0 && yy < a.H && xx >= 0 && xx < a.W;
+          const __nv_bfloat16* src =
+              valid ? a.x + ((size_t)(b * a.H + yy) * a.W + xx) * a.x_stride + a.x_off + kg * 8 : a.x;
+          cp_async16(sb + (uint32_t)kg * kHalo * 16u + (uint32_t)h * 16u, src, valid);
+        }
+        cp_async_wait_all();
+        tc::fence_smem_to_async();
       }
-      tc::mma_commit(&bar[s]);
+    }
+    if (__syncthreads_or(fail)) {
+      ok = false;
+      break;
+    }
+    if (warp == 0) {
+      if (lane == 0) {
+        tc::fence_after_sync();
+        for (int q = 0; q < ntap; ++q) {
+          const int tap = tap0 + q;
+          const uint32_t tap_off = (uint32_t)((tap / 3) * kHaloW + (tap % 3)) * 16u;
+          for (int kk = 0; kk < 8; ++kk) {  // K = 128 pixels = 16 tile rows, two per MMA
+            const uint64_t da = tc::smem_desc(sa + 256u * kk, 128u, 2048u);
+            const uint64_t db = tc::smem_desc(sb + tap_off + 2u * kk * kHaloW * 16u, kHaloW * 16u,
+                                              kHalo * 16u);
+            tc::mma_bf16(tmem + (uint32_t)(q * cin), da, db, idesc, (j > 0 || kk > 0) ? 1u : 0u);
+          }
+        }
+        tc::mma_commit(&bar[s]);
+      }
+      __syncwarp();
     }
     uses[s]++;
   }
@@ -639,7 +647,7 @@ __global__ void __launch_bounds__(kThreads) k_conv_wgrad_halo(ConvWgradArgs a, i
   if (!ok && tid == 0) atomicOr(a.err, 2u);
   tc::fence_after_sync();
   __syncthreads();
-  if (ok && n_local > 0) {
+  if (ok && n_local > 0 && warp < 4) {  // warps 0-3: one tensor-memory subpartition each
     const int co = warp * 32 + lane;
     for (int q = 0; q < ntap; ++q) {
       if (warp * 32 >= cout) break;  // warp-uniform: tcgen05.ld is warp-wide
@@ -735,7 +743,7 @@ cudaError_t launch_conv_wgrad(const ConvWgradArgs& a, cudaStream_t st) {
     const int ctas = std::max(1, std::min(n_tiles, sms / groups));  // one CTA per SM
     const int per = (n_tiles + ctas - 1) / ctas;
     dim3 grid((n_tiles + per - 1) / per, groups);
-    k_conv_wgrad_halo<<<grid, kThreads, halo_smem, st>>>(a, tpg, per);
+    k_conv_wgrad_halo<<<grid, kWgThreads, halo_smem, st>>>(a, tpg, per);
     return cudaGetLastError();
   }
   const size_t smem = conv_wgrad_smem_bytes(a.cin);
