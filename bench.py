@@ -336,10 +336,19 @@ def run_ours(args):
             traffic = None
 
     # end to end through the public API: render + display readback to host
+    # end to end through the public API on every rank (weak scaling: each
+    # rank's engine renders its own S samples per step); the job's value is
+    # the ranks' samples over the slowest rank's time
     e2e = None
-    if rank == 0 and not args.no_e2e:
+    if not args.no_e2e:
         pt = pathtracer()
         e2e = e2e_public_api(pt, spec, S, args)
+        seconds = e2e.pop("seconds")
+        if dist:
+            tt = torch.tensor([seconds], device="cuda", dtype=torch.float64)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            seconds = float(tt.item())
+        e2e["value"] = world * e2e.pop("samples") / seconds
 
     ref_cuda = None
     if rank == 0 and not args.no_reference_cuda:
@@ -433,13 +442,14 @@ def e2e_public_api(pt, spec, S, args):
         if i >= args.warmup:
             times.append(dt)
     w, h = int(spec.camera["resolution"][1]), int(spec.camera["resolution"][0])
-    v = w * h * S * len(times) / sum(times)
+    samples = float(w * h * S * len(times))
     # per step the host sends the camera, the render settings and the stream
     # (display) settings; the scene stays resident like the reference's
     import ctypes
     h2d = (ctypes.sizeof(capi.CameraDesc) + ctypes.sizeof(capi.RenderConfig)
            + ctypes.sizeof(capi.StreamConfig))
-    return {"value": v, "unit": "samples/s", "h2d_bytes_per_step": h2d,
+    return {"samples": samples, "seconds": sum(times), "unit": "samples/s",
+            "h2d_bytes_per_step": h2d,
             "d2h_bytes_per_step": 3 * w * h,
             "path": "_pathtracer RenderEngine.render + TransferStream.readback (uint8 CHW)"}
 
