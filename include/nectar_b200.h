@@ -313,6 +313,15 @@ int nr_scene_get_stats(const nr_scene* scene, nr_scene_stats* out);
  * top-level leaf boxes); the radiance cache's grid spans it. No counterpart
  * in the reference. */
 int nr_scene_get_bounds(const nr_scene* scene, float lo[3], float hi[3]);
+/* The HDRI importance-sampling tables of a built scene (NR_MODE_PERF; no
+ * counterpart in the reference), built on the GPU: texel probabilities
+ * [H][W], a row alias table (acceptance probabilities and alias rows, [H])
+ * and one column alias table per row ([H][W]); a texel is drawn as row, then
+ * column. W and H are 0 without an HDRI; null outputs are skipped; the
+ * tables are left unread when the HDRI carries no energy. */
+int nr_scene_get_sky_tables(const nr_scene* scene, float* texel_pdf, float* row_prob,
+                            uint32_t* row_alias, float* col_prob, uint32_t* col_alias,
+                            int32_t* W, int32_t* H);
 /* Binary SAH tree of mesh `mesh_id` as built on the GPU, for checks:
  * nodes as float[8] {lo.xyz, hi.xyz, left|prim, right|count} bit patterns
  * (int32 stored in the float slots). Pass NULL to query the count. */

@@ -34,7 +34,7 @@ NVCC_FLAGS = ARCH + [
 ]
 CU_SOURCES = ["capi.cu", "integrator.cu", "wavefront.cu", "bvh_build.cu", "image_ops.cu",
               "static_wave.cu", "viewport.cu", "conv_tc.cu",
-              "denoiser.cu", "nrc.cu", "mesh_ingest.cu"]
+              "denoiser.cu", "nrc.cu", "mesh_ingest.cu", "sky_alias.cu"]
 CPP_SOURCES = ["host_io.cpp"]
 LIB = HERE / "libnectar_b200.so"
 

@@ -97,7 +97,7 @@ EXPORTS = [
     "nr_scene_add_object", "nr_scene_set_sky_null", "nr_scene_set_sky_simple",
     "nr_scene_set_sky_hdri", "nr_scene_load_hdr", "nr_scene_set_hdri_params",
     "nr_scene_set_tuning", "nr_scene_build",
-    "nr_scene_get_stats", "nr_scene_get_bounds", "nr_scene_get_binary_bvh", "nr_render_config_default",
+    "nr_scene_get_stats", "nr_scene_get_bounds", "nr_scene_get_sky_tables", "nr_scene_get_binary_bvh", "nr_render_config_default",
     "nr_render_create", "nr_render_destroy", "nr_render_reset", "nr_render_samples",
     "nr_render_samples_static", "nr_render_samples_batch", "nr_render_set_profiling",
     "nr_render_get_profile",

@@ -25,6 +25,7 @@
 #include "bvh_build.cuh"
 #include "host_io.h"
 #include "mesh_ingest.cuh"
+#include "sky_alias.cuh"
 #include "image_ops.cuh"
 #include "integrator.cuh"
 #include "wavefront.cuh"
@@ -379,9 +380,7 @@ struct nr_scene {
   DevObject* d_objects = nullptr;
   DevMesh* d_mesh_table = nullptr;
   float* d_hdri = nullptr;
-  float* d_alias_prob = nullptr;    // HDRI importance sampling (perf mode)
-  uint32_t* d_alias_idx = nullptr;
-  float* d_texel_pdf = nullptr;
+  SkyTables sky_tables;             // HDRI importance sampling (perf mode)
   CubeFace* d_cube_faces = nullptr;
   BuildResult tlas;
   DevScene dev{};
@@ -400,18 +399,13 @@ struct nr_scene {
     cudaFree(d_objects);
     cudaFree(d_mesh_table);
     cudaFree(d_hdri);
-    cudaFree(d_alias_prob);
-    cudaFree(d_alias_idx);
-    cudaFree(d_texel_pdf);
+    sky_tables.release();
     cudaFree(d_cube_faces);
     d_cube_faces = nullptr;
     d_materials = nullptr;
     d_objects = nullptr;
     d_mesh_table = nullptr;
     d_hdri = nullptr;
-    d_alias_prob = nullptr;
-    d_alias_idx = nullptr;
-    d_texel_pdf = nullptr;
     free_build(tlas);
     built = false;
   }
@@ -706,65 +700,6 @@ int nr_scene_set_hdri_params(nr_scene* s, float rotation, float intensity) {
   return NR_OK;
 }
 
-// Sampling table of an equirectangular HDRI for NR_MODE_PERF: texel weight =
-// the largest luminance in the texel's 3x3 neighbourhood (the bilinear lookup
-// spreads a bright texel into its neighbours, so their density must not be
-// small) x sin(theta) (the solid angle of the texel row); a Walker alias
-// table built with Vose's method (IEEE TSE 17(9), 1991) and the normalised
-// texel probabilities. Returns false when the image carries no energy.
-static bool build_sky_alias(const HostImageF& im, std::vector<float>& prob,
-                            std::vector<uint32_t>& alias, std::vector<float>& texel_pdf) {
-  const size_t W = im.W, H = im.H, n = W * H, hw = n;
-  std::vector<double> lum(n), w(n);
-  for (size_t i = 0; i < n; ++i)
-    lum[i] = std::max(0.0, 0.2126 * im.chw[i] + 0.7152 * im.chw[hw + i] + 0.0722 * im.chw[2 * hw + i]);
-  double sum = 0.0;
-  for (size_t y = 0; y < H; ++y) {
-    const double st = std::sin(M_PI * ((double)y + 0.5) / (double)H);
-    for (size_t x = 0; x < W; ++x) {
-      double m = 0.0;
-      for (int dy = -1; dy <= 1; ++dy) {
-        const size_t yy = (size_t)std::min<long>((long)H - 1, std::max<long>(0, (long)y + dy));
-        for (int dx = -1; dx <= 1; ++dx) {
-          const size_t xx = (x + W + dx) % W;
-          m = std::max(m, lum[yy * W + xx]);
-        }
-      }
-      const size_t i = y * W + x;
-      w[i] = m * st;
-      sum += w[i];
-    }
-  }
-  if (!(sum > 0.0)) return false;
-  prob.assign(n, 1.0f);
-  alias.resize(n);
-  texel_pdf.resize(n);
-  std::vector<double> q(n);
-  std::vector<uint32_t> small, large;
-  small.reserve(n);
-  large.reserve(n);
-  for (size_t i = 0; i < n; ++i) {
-    texel_pdf[i] = (float)(w[i] / sum);
-    q[i] = w[i] * (double)n / sum;
-    alias[i] = (uint32_t)i;
-    (q[i] < 1.0 ? small : large).push_back((uint32_t)i);
-  }
-  while (!small.empty() && !large.empty()) {
-    const uint32_t l = small.back(), g = large.back();
-    small.pop_back();
-    prob[l] = (float)q[l];
-    alias[l] = g;
-    q[g] = (q[g] + q[l]) - 1.0;
-    if (q[g] < 1.0) {
-      large.pop_back();
-      small.push_back(g);
-    }
-  }
-  for (uint32_t i : large) prob[i] = 1.0f;
-  for (uint32_t i : small) prob[i] = 1.0f;  // round-off leftovers
-  return true;
-}
-
 int nr_scene_set_tuning(nr_scene* s, uint32_t mesh_leaf_max, uint32_t tlas_leaf_max) {
   if (!s || mesh_leaf_max < 1 || mesh_leaf_max > 3 || tlas_leaf_max < 1 || tlas_leaf_max > 3)
     return fail(NR_ERR_INVALID, "nr_scene_set_tuning: leaf sizes must be 1..3");
@@ -930,16 +865,16 @@ int nr_scene_build(nr_scene* s) {
     sky.H = (int)s->hdri.H;
     sky.W = (int)s->hdri.W;
     dev_bytes += s->hdri.chw.size() * 4;
-    std::vector<float> prob, tpdf;
-    std::vector<uint32_t> alias;
-    if (build_sky_alias(s->hdri, prob, alias, tpdf)) {
-      CU(upload(s->d_alias_prob, prob.data(), prob.size(), st), "upload sky table");
-      CU(upload(s->d_alias_idx, alias.data(), alias.size(), st), "upload sky table");
-      CU(upload(s->d_texel_pdf, tpdf.data(), tpdf.size(), st), "upload sky table");
-      sky.alias_prob = s->d_alias_prob;
-      sky.alias_idx = s->d_alias_idx;
-      sky.texel_pdf = s->d_texel_pdf;
-      dev_bytes += prob.size() * 12;
+    bool has_energy = false;
+    CU(build_sky_tables(s->d_hdri, sky.W, sky.H, s->sky_tables, has_energy, st),
+       "build sky sampling tables");
+    if (has_energy) {
+      sky.row_prob = s->sky_tables.row_prob;
+      sky.row_alias = s->sky_tables.row_alias;
+      sky.col_prob = s->sky_tables.col_prob;
+      sky.col_alias = s->sky_tables.col_alias;
+      sky.texel_pdf = s->sky_tables.texel_pdf;
+      dev_bytes += (size_t)sky.W * sky.H * 12 + (size_t)sky.H * 8;
     }
   }
 
@@ -980,6 +915,27 @@ int nr_scene_build(nr_scene* s) {
   S.build_ms = ms;
   S.device_bytes = dev_bytes;
   s->built = true;
+  return NR_OK;
+}
+
+int nr_scene_get_sky_tables(const nr_scene* s, float* texel_pdf, float* row_prob,
+                            uint32_t* row_alias, float* col_prob, uint32_t* col_alias,
+                            int32_t* W, int32_t* H) {
+  if (!s) return fail(NR_ERR_INVALID, "nr_scene_get_sky_tables: null scene");
+  if (!s->built) return fail(NR_ERR_STATE, "nr_scene_get_sky_tables: scene not built");
+  const SkyTables& t = s->sky_tables;
+  if (W) *W = t.W;
+  if (H) *H = t.H;
+  if (!t.texel_pdf) return NR_OK;
+  const size_t hw = (size_t)t.W * t.H;
+  auto rd = [&](void* dst, const void* src, size_t bytes) {
+    return dst ? cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost) : cudaSuccess;
+  };
+  CU(rd(texel_pdf, t.texel_pdf, hw * 4), "read sky tables");
+  CU(rd(row_prob, t.row_prob, (size_t)t.H * 4), "read sky tables");
+  CU(rd(row_alias, t.row_alias, (size_t)t.H * 4), "read sky tables");
+  CU(rd(col_prob, t.col_prob, hw * 4), "read sky tables");
+  CU(rd(col_alias, t.col_alias, hw * 4), "read sky tables");
   return NR_OK;
 }
 

@@ -132,15 +132,19 @@ __device__ __forceinline__ float sky_dir_pdf(const DevSky& s, const V3& d) {
   return __ldg(s.texel_pdf + (size_t)y * s.W + x) * n / (2.0f * PI * PI * sin_t);
 }
 
-// Alias-table sample of a texel (Walker 1977; table built with Vose's
-// method), then a uniform point inside it, as a world direction.
+// Alias-table sample of a texel (Walker 1977): a row from the row table,
+// then a column from that row's table; then a uniform point inside the
+// texel, as a world direction.
 __device__ __forceinline__ V3 sky_sample_dir(const DevSky& s, Rng& g, float& pdf) {
   const uint32_t n = (uint32_t)s.W * (uint32_t)s.H;
-  const float fi = g.random_float() * (float)n;
-  uint32_t i = min(n - 1u, (uint32_t)fi);
-  const float frac = fi - (float)i;
-  const uint32_t t = frac < __ldg(s.alias_prob + i) ? i : __ldg(s.alias_idx + i);
-  const uint32_t x = t % (uint32_t)s.W, y = t / (uint32_t)s.W;
+  const float fr = g.random_float() * (float)s.H;
+  const uint32_t rb = min((uint32_t)s.H - 1u, (uint32_t)fr);
+  const uint32_t y = fr - (float)rb < __ldg(s.row_prob + rb) ? rb : __ldg(s.row_alias + rb);
+  const float fc = g.random_float() * (float)s.W;
+  const uint32_t cb = min((uint32_t)s.W - 1u, (uint32_t)fc);
+  const size_t o = (size_t)y * (uint32_t)s.W;
+  const uint32_t x = fc - (float)cb < __ldg(s.col_prob + o + cb) ? cb : __ldg(s.col_alias + o + cb);
+  const uint32_t t = y * (uint32_t)s.W + x;
   const float u = ((float)x + g.random_float()) / (float)s.W;
   const float v = ((float)y + g.random_float()) / (float)s.H;
   const float theta = v * PI, phi = (u - 0.5f) * PI2;

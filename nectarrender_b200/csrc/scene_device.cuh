@@ -116,10 +116,13 @@ struct DevSky {
   M3 rot;             // rotation_y(deg2rad(rotation)) built as the reference does
   const float* data;  // planar CHW float
   int32_t C, H, W;
-  // importance sampling (alias table over texels, perf mode)
-  const float* alias_prob;   // H*W acceptance probabilities
-  const uint32_t* alias_idx; // H*W alias texel indices
-  const float* texel_pdf;    // H*W probability of each texel
+  // importance sampling (perf mode): alias tables over rows and, per row,
+  // over its columns; the probability of each texel
+  const float* row_prob;       // H acceptance probabilities
+  const uint32_t* row_alias;   // H alias rows
+  const float* col_prob;       // H*W acceptance probabilities
+  const uint32_t* col_alias;   // H*W alias columns
+  const float* texel_pdf;      // H*W probability of each texel
   float total_weight;
 };
 
