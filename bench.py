@@ -67,6 +67,9 @@ def parse():
     p.add_argument("--no-denoiser", action="store_true", help="skip training the learned denoiser")
     p.add_argument("--no-multi", action="store_true", help="skip the multi-scene measurement")
     p.add_argument("--no-nrc", action="store_true", help="skip the radiance-cache measurement")
+    p.add_argument("--rmse-cornell", action="store_true",
+                   help="also time perf mode, the reference estimator and the radiance cache to "
+                        "RMSE 0.01 on the Cornell box against a 65,536-sample FP64 render")
     p.add_argument("--batch-rmse", action="store_true",
                    help="also render the 64-scene batched configuration and report every "
                         "scene's RMSE against an FP64 perf-mode render (about 2 minutes)")
@@ -369,6 +372,9 @@ def run_ours(args):
     batch = None
     if rank == 0 and world == 1 and args.batch_rmse:
         batch = batch_rmse(args)
+    cornell01 = None
+    if rank == 0 and world == 1 and args.rmse_cornell:
+        cornell01 = cornell_time_to_rmse(args)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -405,6 +411,7 @@ def run_ours(args):
                 "radiance_cache": cache,
                 "multi_scene": multi,
                 "batch_rmse": batch,
+                "time_to_rmse_cornell": cornell01,
                 "scene": {"build_ms_device": stats["build_ms"], "build_wall_s": build_wall,
                           "obj_load_s": obj_load_times(spec) if rank == 0 else None,
                           "triangles": stats["n_triangles"], "wide_nodes": stats["wide_nodes"],
@@ -495,6 +502,77 @@ def multi_scene(args):
                                              "CUDA events, scene builds excluded"}
         except Exception as e:  # noqa: BLE001 - reported, not fatal
             out["reference_cuda"] = {"unavailable": repr(e)[:200]}
+    return out
+
+
+def cornell_time_to_rmse(args, target=0.01, res=128, depth=8, oracle_spp=65536, top=65536):
+    """Device time to RMSE `target` (time-to-RMSE domain) on the small
+    configuration's Cornell box (res x res, depth 8, no HDRI, so an FP64
+    perf-mode render of `oracle_spp` samples with another seed sits far below
+    the target): perf mode, the reference estimator and perf mode with the
+    radiance cache (stop at hit 3, 1 in 16 paths trains, 32-sample warm-up
+    counted), sample counts doubling until the target is passed; the time
+    at the target is interpolated in log-log between the last two points."""
+    from nectarrender_b200 import capi, nrc
+    spec = scenes.cornell(res=res, spp=max(oracle_spp, top) + 1, depth=depth, seed=0)
+    sc = capi.Scene(spec, mesh_leaf=args.mesh_leaf)
+    orc = capi.Render(sc, mode=capi.MODE_PERF, fp64_accumulate=1, seed=spec.seed + 1000)
+    t0 = time.perf_counter()
+    orc.samples(1, oracle_spp)
+    oracle_s = time.perf_counter() - t0
+    disp_o = np.sqrt(np.clip(orc.beauty_fp64(), 0.0, 1.0))
+    del orc
+    # NaN samples (the reference estimator produces some on this scene, as the
+    # reference does) count as 0, as the display transform maps them
+    rmse_of = lambda img: float(np.sqrt(np.mean(
+        (np.sqrt(np.clip(np.nan_to_num(img, nan=0.0), 0.0, 1.0)) - disp_o) ** 2)))
+
+    def curve(r, t_ms):
+        done, n, pts = 0, 1, []
+        while done + n <= top:
+            r.samples(done + 1, n)
+            t_ms += r.last_ms()
+            done += n
+            pts.append([done, round(t_ms, 3), round(rmse_of(r.beauty_fp64()), 5)])
+            if pts[-1][2] <= target:
+                break
+            n = done
+        return pts
+
+    def at_target(pts):
+        for (s0, m0, e0), (s1, m1, e1) in zip(pts, pts[1:]):
+            if e0 > target >= e1:
+                f = (np.log(target) - np.log(e0)) / (np.log(e1) - np.log(e0))
+                return float(np.exp(np.log(m0) + f * (np.log(m1) - np.log(m0))))
+        return None
+
+    out = {"workload": f"cornell {res}x{res}, depth {depth}", "target_rmse": target,
+           "oracle_spp": oracle_spp, "oracle_wall_s": oracle_s,
+           "domain": "sqrt(clamp(x,0,1)), all pixels x 3 channels"}
+    for name, mode in (("perf_mode", capi.MODE_PERF), ("reference_estimator", capi.MODE_REFERENCE)):
+        r = capi.Render(sc, mode=mode, fp64_accumulate=1, seed=spec.seed)
+        r.samples(1, 1)
+        r.reset()
+        pts = curve(r, 0.0)
+        out[name] = {"curve_spp_ms_rmse": pts, "ms_to_target": at_target(pts)}
+        del r
+    lo, hi = sc.bounds()
+    c = nrc.RadianceCache(1 << 18, lo, hi, seed=1)
+    r = capi.Render(sc, mode=capi.MODE_PERF, fp64_accumulate=1, seed=spec.seed, samples_per_wave=8)
+    r.set_nrc(c, 3, 16, 1e-2, 16384, 4)
+    r.samples(top - 40, 1)  # allocation, outside the curve
+    r.samples(top - 32, 32)
+    warm = r.last_ms()
+    r.reset()
+    pts = curve(r, warm)
+    out["perf_mode_radiance_cache"] = {"curve_spp_ms_rmse": pts, "ms_to_target": at_target(pts),
+                                       "warmup_ms": warm}
+    del r, c
+    p_ms = out["perf_mode"]["ms_to_target"]
+    for k in ("reference_estimator", "perf_mode_radiance_cache"):
+        m = out[k]["ms_to_target"]
+        if m and p_ms:
+            out[k]["time_ratio_vs_perf_mode"] = m / p_ms
     return out
 
 
