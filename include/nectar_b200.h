@@ -362,6 +362,12 @@ int nr_render_samples_batch(nr_render* const* renders, uint32_t n, const uint32_
  * (stream.cu:146-159) are separate kernels. */
 int nr_render_set_fused_display(nr_render* render, const nr_stream_config* c);
 
+/* Page-locked host memory for readback buffers (the reference's
+ * TransferStream reads back into pinned memory, stream.h:154-182): device to
+ * host copies into it run at full link speed. Free with nr_host_free. */
+int nr_host_alloc(uint64_t bytes, void** out);
+int nr_host_free(void* p);
+
 /* nr_render_samples_static: no counterpart in the reference.
  * Renders exactly like nr_render_samples (same sample indices, same layers,
  * same results; always the wavefront schedule) but allocates no device memory

@@ -101,7 +101,7 @@ EXPORTS = [
     "nr_render_create", "nr_render_destroy", "nr_render_reset", "nr_render_samples",
     "nr_render_samples_static", "nr_render_samples_batch", "nr_render_set_profiling",
     "nr_render_get_profile",
-    "nr_render_graph_stats", "nr_render_set_fused_display", "nr_render_viewport", "nr_render_pick", "nr_render_selection_mask",
+    "nr_render_graph_stats", "nr_render_set_fused_display", "nr_host_alloc", "nr_host_free", "nr_render_viewport", "nr_render_pick", "nr_render_selection_mask",
     "nr_conv3x3_forward_device", "nr_conv3x3_wgrad_device",
     "nr_denoiser_create", "nr_denoiser_destroy", "nr_denoiser_train_step", "nr_denoiser_infer",
     "nr_denoiser_param_count", "nr_denoiser_get_params", "nr_denoiser_set_params",

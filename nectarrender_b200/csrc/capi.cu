@@ -1775,6 +1775,19 @@ int nr_render_set_fused_display(nr_render* r, const nr_stream_config* c) {
   return NR_OK;
 }
 
+int nr_host_alloc(uint64_t bytes, void** out) {
+  if (!out) return fail(NR_ERR_INVALID, "nr_host_alloc: null output");
+  *out = nullptr;
+  if (bytes == 0) return NR_OK;
+  CU(cudaMallocHost(out, bytes), "nr_host_alloc");
+  return NR_OK;
+}
+
+int nr_host_free(void* p) {
+  if (p) CU(cudaFreeHost(p), "nr_host_free");
+  return NR_OK;
+}
+
 int nr_render_readback(nr_render* r, int32_t layer, const nr_stream_config* c, uint8_t* h8) {
   if (!h8) return fail(NR_ERR_INVALID, "null output");
   return display(r, layer, c, h8, nullptr);

@@ -366,12 +366,35 @@ struct RenderLayers {
   }
 };
 
+// Page-locked host bytes (nr_host_alloc), grown on demand.
+struct PinnedBytes {
+  uint8_t* p = nullptr;
+  size_t n = 0;
+  PinnedBytes() = default;
+  PinnedBytes(const PinnedBytes&) = delete;
+  PinnedBytes& operator=(const PinnedBytes&) = delete;
+  ~PinnedBytes() { nr_host_free(p); }
+  void resize(size_t bytes) {
+    if (bytes == n) return;
+    nr_host_free(p);
+    p = nullptr;
+    n = 0;
+    void* q = nullptr;
+    check(nr_host_alloc(bytes, &q), "TransferStream buffer");
+    p = static_cast<uint8_t*>(q);
+    n = bytes;
+  }
+  uint8_t* data() { return p; }
+  const uint8_t* data() const { return p; }
+  size_t size() const { return n; }
+};
+
 struct TransferStream {
   EngineCore* eng = nullptr;
   std::atomic<StreamState> state{StreamState::INACTIVE};
   StreamConfig cfg;
   int layer = (int)LayerType::BEAUTY;
-  std::vector<uint8_t> buffer;
+  PinnedBytes buffer;  // page-locked, like the reference's readback buffer
   // the config the render's accumulate pass already applies (fused display)
   nr_render* fused_render = nullptr;
   nr_stream_config fused_cfg{};
