@@ -207,7 +207,7 @@ def run_reference(args):
                              "sample": sample_desc},
             "e2e": {"value": value, "unit": "samples/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
-    print(json.dumps(line), flush=True)
+    emit(line)
 
 
 # ---------------------------------------------------------------------------
@@ -419,7 +419,7 @@ def run_ours(args):
                 "step_ms": step_ms}
         if combine_ms is not None:
             line["combine_allreduce_ms"] = combine_ms
-        print(json.dumps(line), flush=True)
+        emit(line)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -936,8 +936,25 @@ def reference_cuda_rate(spec, w, h):
         return {"unavailable": repr(e)[:200]}
 
 
+_JSON_OUT = None
+
+
+def emit(line):
+    """Prints the one JSON line on the process's original standard output."""
+    out = _JSON_OUT or sys.stdout
+    out.write(json.dumps(line) + "\n")
+    out.flush()
+
+
 def main():
+    global _JSON_OUT
     args = parse()
+    # Native code loaded by the run (the reference's CUDA build among it)
+    # writes diagnostics to file descriptor 1; send those to standard error
+    # so that standard output carries the JSON line alone.
+    sys.stdout.flush()
+    _JSON_OUT = os.fdopen(os.dup(1), "w")
+    os.dup2(2, 1)
     if args.impl == "reference":
         run_reference(args)
     else:

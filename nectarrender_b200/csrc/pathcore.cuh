@@ -259,6 +259,15 @@ __device__ __forceinline__ int mesh_closest_bvh2(const DevMesh& m, const Ray& r,
 __device__ __forceinline__ uint32_t extract_byte(uint32_t x, uint32_t i) {
   return (x >> (i * 8u)) & 0xffu;
 }
+// Byte i of x as a float, exactly (float)byte: the byte is placed in the
+// mantissa of 2^23 (0x4B0000bb = 2^23 + b) and 2^23 is subtracted, which is
+// exact for b < 2^23. One byte permute (integer pipe) and one add (FMA pipe)
+// instead of a conversion (the narrow XU pipe). The box test converts the
+// near-plane bytes one way and the far-plane bytes the other, so neither the
+// XU nor the integer pipe saturates.
+__device__ __forceinline__ float byte_to_float(uint32_t x, uint32_t i) {
+  return __uint_as_float(__byte_perm(x, 0x4Bu, 0x4550u | i)) - 8388608.0f;
+}
 __device__ __forceinline__ uint32_t s8x4_mask(uint32_t x) {
   // x has only bit 7 of each byte possibly set; spread it to the whole byte
   uint32_t m = x & 0x80808080u;
@@ -302,9 +311,9 @@ __device__ __forceinline__ uint32_t bvh8_intersect(const Bvh8Node* nd, const V3&
       float tx0 = fmaf((float)extract_byte(sxlo, j), adx, aox);
       float ty0 = fmaf((float)extract_byte(sylo, j), ady, aoy);
       float tz0 = fmaf((float)extract_byte(szlo, j), adz, aoz);
-      float tx1 = fmaf((float)extract_byte(sxhi, j), adx, aox);
-      float ty1 = fmaf((float)extract_byte(syhi, j), ady, aoy);
-      float tz1 = fmaf((float)extract_byte(szhi, j), adz, aoz);
+      float tx1 = fmaf(byte_to_float(sxhi, j), adx, aox);
+      float ty1 = fmaf(byte_to_float(syhi, j), ady, aoy);
+      float tz1 = fmaf(byte_to_float(szhi, j), adz, aoz);
       float tn = fmaxf(fmaxf(tx0, ty0), fmaxf(tz0, tmin));
       float tf = fminf(fminf(tx1, ty1), fminf(tz1, tmax));
       if (tn <= tf) {
