@@ -408,7 +408,7 @@ __global__ void __launch_bounds__(kExtThreads, kMinBlocks) k_wf_extend(WfParams 
   uint2* blas_stk = wf_smem + kTlasStack * kExtThreads + threadIdx.x;
   TraceStats st{0u, 0u, 0u};
   uint32_t rays = 0;
-  const bool binned = W.queue_s && !identity;  // block-uniform
+  const bool binned = W.queue_s != nullptr;  // block-uniform
   __shared__ uint32_t key_hist[kSortKeys];
   KeyHist kh{key_hist};
   if (binned) kh.init();
@@ -511,7 +511,7 @@ __global__ void __launch_bounds__(kExtThreads, kMinBlocks) k_wf_extend_flat(WfPa
   int sp = 0, best_slot = -1;
   const Bvh8Node* cur_nodes = sc.tlas8;
   const TriRecord* cur_tris = nullptr;
-  const bool binned = W.queue_s && !identity;  // block-uniform
+  const bool binned = W.queue_s != nullptr;  // block-uniform
   __shared__ uint32_t key_hist[kSortKeys];
   KeyHist kh{key_hist};
   if (binned) kh.init();
@@ -764,7 +764,7 @@ __global__ void __launch_bounds__(kShadeThreads, kMinBlocks) k_wf_shade(WfParams
     bool alive = false, shadow = false;
     uint32_t p = 0;
     if (i < n) {
-      p = identity ? i : __ldg(queue + i);
+      p = (identity && !sorted) ? i : __ldg(queue + i);
       float4 o = W.ray_o[p], d = W.ray_d[p], at = W.atten[p], ab = W.acc_b[p];
       uint32_t bounce = __float_as_uint(d.w);
       PathState s;
@@ -1010,11 +1010,19 @@ __global__ void k_wf_rotate(WfParams W, int consumed) {
 }
 
 // Material sort, pass 2: every path of the queue to its key's segment of
-// queue_s (segments in key order; within a segment, warps append in the
-// order they reach their atomics).
-__global__ void k_wf_bin_scatter(WfParams W, int qsel) {
+// queue_s (segments in key order). A block takes 256 queue entries at a time:
+// each warp ranks its lanes per key with one ballot per key, the warps'
+// counts are scanned in shared memory, and one atomic per key and block
+// reserves the block's run in the segment. Within a segment, blocks append
+// in the order they reach their atomics and keep queue order inside a run.
+constexpr int kScatterThreads = 256;
+__global__ void __launch_bounds__(kScatterThreads) k_wf_bin_scatter(WfParams W, int qsel,
+                                                                    int identity) {
   if (W.ctr[CTR_TAIL]) return;
+  constexpr int kWarps = kScatterThreads / 32;
   __shared__ uint32_t seg[kSortKeys];
+  __shared__ uint32_t run[kSortKeys];
+  __shared__ uint32_t woff[kWarps][kSortKeys];
   if (threadIdx.x == 0) {
     uint32_t acc = 0;
     for (int k = 0; k < kSortKeys; ++k) {
@@ -1022,23 +1030,39 @@ __global__ void k_wf_bin_scatter(WfParams W, int qsel) {
       acc += W.sort_ctr[k];
     }
   }
-  __syncthreads();
   const uint32_t n = W.ctr[qsel];
   const uint32_t* queue = qsel == 0 ? W.queue0 : W.queue1;
-  const uint32_t lane = threadIdx.x & 31u;
-  for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+  const uint32_t below = (1u << lane) - 1u;
+  // the loop bound depends on the block only, so every thread reaches the
+  // barriers inside it
+  for (uint32_t base = blockIdx.x * kScatterThreads; base < n; base += gridDim.x * kScatterThreads) {
     const uint32_t i = base + threadIdx.x;
-    const unsigned act = __ballot_sync(0xffffffffu, i < n);
+    uint32_t p = 0, key = kSortKeys, rank = 0;
     if (i < n) {
-      const uint32_t p = __ldg(queue + i);
-      const uint32_t key = W.skey[p];
-      const unsigned peers = __match_any_sync(act, key);
-      const uint32_t leader = (uint32_t)(__ffs(peers) - 1);
-      uint32_t at = 0;
-      if (lane == leader) at = atomicAdd(&W.sort_ctr[kSortKeys + key], (uint32_t)__popc(peers));
-      at = __shfl_sync(peers, at, leader);
-      W.queue_s[seg[key] + at + __popc(peers & ((1u << lane) - 1u))] = p;
+      p = identity ? i : __ldg(queue + i);
+      key = W.skey[p];
     }
+#pragma unroll
+    for (uint32_t k = 0; k < (uint32_t)kSortKeys; ++k) {
+      const uint32_t m = __ballot_sync(0xffffffffu, key == k);
+      if (lane == 0) woff[warp][k] = (uint32_t)__popc(m);
+      if (key == k) rank = (uint32_t)__popc(m & below);
+    }
+    __syncthreads();
+    if (threadIdx.x < (unsigned)kSortKeys) {
+      const uint32_t k = threadIdx.x;
+      uint32_t acc = 0;
+      for (int w = 0; w < kWarps; ++w) {
+        const uint32_t c = woff[w][k];
+        woff[w][k] = acc;
+        acc += c;
+      }
+      run[k] = acc ? atomicAdd(&W.sort_ctr[kSortKeys + k], acc) : 0u;
+    }
+    __syncthreads();
+    if (key < (uint32_t)kSortKeys) W.queue_s[seg[key] + run[key] + woff[warp][key] + rank] = p;
+    __syncthreads();
   }
 }
 
@@ -1290,19 +1314,21 @@ cudaError_t wf_launch_wave(const WfParams& W, bool counters, cudaStream_t st, Wa
   int eb = extend_blocks(ext, smem), eb0 = extend_blocks(ext0, smem0);
   int shade_blocks = (int)std::min<uint32_t>((total + kShadeThreads - 1) / kShadeThreads,
                                              (uint32_t)sm_count() * 16);
+  int scatter_blocks = (int)std::min<uint32_t>((total + kScatterThreads - 1) / kScatterThreads,
+                                               (uint32_t)sm_count() * 8);
   for (uint32_t b = 0; b < P.depth; ++b) {
     int q = (int)(b & 1u);
     if (b == 0) ext0<<<eb0, kExtThreads, smem0, st>>>(W, q, 1);
     else ext<<<eb, kExtThreads, smem, st>>>(W, q, 0);
     if (tm) tm->mark(NR_KERNEL_EXTEND, st);
-    // camera rays keep pixel order; from bounce 1 on the extend kernel
-    // counts the material keys and one pass sorts the queue by them
-    const int sorted = (W.queue_s && b > 0) ? 1 : 0;
+    // the extend kernel counts the material keys and one pass sorts the
+    // queue by them (the camera rays' queue is the identity)
+    const int identity = b == 0 ? 1 : 0;
+    const int sorted = W.queue_s ? 1 : 0;
     if (sorted) {
-      k_wf_bin_scatter<<<shade_blocks, kShadeThreads, 0, st>>>(W, q);
+      k_wf_bin_scatter<<<scatter_blocks, kScatterThreads, 0, st>>>(W, q, identity);
       if (tm) tm->mark(NR_KERNEL_ROTATE, st);
     }
-    const int identity = b == 0 ? 1 : 0;
     if (W.mis_pdf) {
       k_wf_shade<true, 1><<<shade_blocks, kShadeThreads, 0, st>>>(W, q, identity, sorted);
       if (tm) tm->mark(NR_KERNEL_SHADE, st);
