@@ -229,6 +229,10 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     spec, h, w = workload(args)
     lib = library()
+    # the first build also pays for loading the build kernels' code; the
+    # build reported is a second one
+    warm_scene = capi.Scene(spec, mesh_leaf=args.mesh_leaf)
+    del warm_scene
     t_build = time.perf_counter()
     scene = capi.Scene(spec, mesh_leaf=args.mesh_leaf)
     build_wall = time.perf_counter() - t_build

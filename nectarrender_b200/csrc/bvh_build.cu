@@ -172,6 +172,51 @@ __global__ void k_scan_single(uint32_t* a, uint32_t n, uint32_t* total) {
   if (threadIdx.x == 0 && total) *total = carry;
 }
 
+// Multi-block exclusive scan (scan_exclusive): pass 1, the sum of each
+// kScanTile-element tile.
+constexpr uint32_t kScanTile = 1024;
+__global__ void __launch_bounds__(kScanTile) k_scan_tile_sums(const uint32_t* a, uint32_t n,
+                                                              uint32_t* sums) {
+  __shared__ uint32_t w[32];
+  const uint32_t i = blockIdx.x * kScanTile + threadIdx.x;
+  uint32_t v = i < n ? a[i] : 0u;
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31u) == 0) w[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    uint32_t t = w[threadIdx.x];
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+    if (threadIdx.x == 0) sums[blockIdx.x] = t;
+  }
+}
+
+// Pass 3: the scan inside each tile plus the tile's offset (out may be in).
+__global__ void __launch_bounds__(kScanTile) k_scan_tile_apply(const uint32_t* in, uint32_t n,
+                                                               const uint32_t* sums,
+                                                               uint32_t* out) {
+  __shared__ uint32_t w[32];
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const uint32_t i = blockIdx.x * kScanTile + threadIdx.x;
+  const uint32_t v = i < n ? in[i] : 0u;
+  uint32_t x = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= (uint32_t)o) x += y;
+  }
+  if (lane == 31) w[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t t = w[lane];
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, t, o);
+      if (lane >= (uint32_t)o) t += y;
+    }
+    w[lane] = t;
+  }
+  __syncthreads();
+  if (i < n) out[i] = sums[blockIdx.x] + (warp ? w[warp - 1] : 0u) + x - v;
+}
+
 __global__ void k_rs_scatter(const uint32_t* kin, const uint32_t* vin, uint32_t* kout,
                              uint32_t* vout, uint32_t n, int shift, const uint32_t* hist,
                              uint32_t nblocks) {
@@ -1067,7 +1112,7 @@ int build_bvh(const float4* d_lo, const float4* d_hi, uint32_t n, bool want_bvh8
   NR_TRY(dalloc(vals2, n));
   NR_TRY(dalloc(counters, 16));
   uint32_t rs_blocks = (n + kRsTile - 1) / kRsTile;
-  NR_TRY(dalloc(hist, 256 * (size_t)rs_blocks));
+  NR_TRY(dalloc(hist, (size_t)radix_sort_hist_words(n)));
 
   // bounds and Morton codes
   {
@@ -1079,7 +1124,7 @@ int build_bvh(const float4* d_lo, const float4* d_hi, uint32_t n, bool want_bvh8
     k_morton<<<(n + 255) / 256, 256, 0, st>>>(d_lo, d_hi, n, gk, keys, vals);
     for (int shift = 0; shift < 32; shift += 8) {
       k_rs_hist<<<rs_blocks, kRsThreads, 0, st>>>(keys, n, shift, hist, rs_blocks);
-      k_scan_single<<<1, 1024, 0, st>>>(hist, 256 * rs_blocks, nullptr);
+      NR_TRY(scan_exclusive(hist, hist, 256 * rs_blocks, hist + 256 * rs_blocks, nullptr, st));
       k_rs_scatter<<<rs_blocks, kRsThreads, 0, st>>>(keys, vals, keys2, vals2, n, shift, hist, rs_blocks);
       std::swap(keys, keys2);
       std::swap(vals, vals2);
@@ -1202,9 +1247,9 @@ int build_bvh(const float4* d_lo, const float4* d_hi, uint32_t n, bool want_bvh8
 
   // 2-wide layout
   uint32_t* idx2 = nullptr;
-  NR_TRY(dalloc(idx2, n_nodes));
+  NR_TRY(dalloc(idx2, (size_t)n_nodes + scan_scratch_words(n_nodes)));
   k_inner_flags<<<(n_nodes + 255) / 256, 256, 0, st>>>(nodes, n_nodes, idx2);
-  k_scan_single<<<1, 1024, 0, st>>>(idx2, n_nodes, counters + 7);
+  NR_TRY(scan_exclusive(idx2, idx2, n_nodes, idx2 + n_nodes, counters + 7, st));
   uint32_t n_inner = 0;
   NR_TRY(cudaMemcpyAsync(&n_inner, counters + 7, 4, cudaMemcpyDeviceToHost, st));
   NR_TRY(cudaStreamSynchronize(st));
@@ -1278,7 +1323,23 @@ int build_bvh(const float4* d_lo, const float4* d_hi, uint32_t n, bool want_bvh8
   return 0;
 }
 
-uint32_t radix_sort_hist_words(uint32_t n) { return 256u * ((n + kRsTile - 1) / kRsTile); }
+uint32_t scan_scratch_words(uint32_t n) { return (n + kScanTile - 1) / kScanTile + 1u; }
+
+cudaError_t scan_exclusive(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* sums,
+                           uint32_t* total, cudaStream_t st) {
+  if (n == 0) return total ? cudaMemsetAsync(total, 0, sizeof(uint32_t), st) : cudaSuccess;
+  const uint32_t tiles = (n + kScanTile - 1) / kScanTile;
+  k_scan_tile_sums<<<tiles, kScanTile, 0, st>>>(in, n, sums);
+  // one CTA scans the tile sums; the last scratch word takes the total
+  k_scan_single<<<1, 1024, 0, st>>>(sums, tiles, total ? total : sums + tiles);
+  k_scan_tile_apply<<<tiles, kScanTile, 0, st>>>(in, n, sums, out);
+  return cudaGetLastError();
+}
+
+uint32_t radix_sort_hist_words(uint32_t n) {
+  const uint32_t h = 256u * ((n + kRsTile - 1) / kRsTile);
+  return h + scan_scratch_words(h);
+}
 
 cudaError_t radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t* keys2, uint32_t* vals2,
                              uint32_t n, int key_bits, uint32_t* hist, cudaStream_t st,
@@ -1286,7 +1347,8 @@ cudaError_t radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t* keys2, ui
   const uint32_t blocks = (n + kRsTile - 1) / kRsTile;
   for (int shift = 0; shift < key_bits && n; shift += 8) {
     k_rs_hist<<<blocks, kRsThreads, 0, st>>>(keys, n, shift, hist, blocks);
-    k_scan_single<<<1, 1024, 0, st>>>(hist, 256 * blocks, nullptr);
+    cudaError_t e = scan_exclusive(hist, hist, 256 * blocks, hist + 256 * blocks, nullptr, st);
+    if (e != cudaSuccess) return e;
     k_rs_scatter<<<blocks, kRsThreads, 0, st>>>(keys, vals, keys2, vals2, n, shift, hist, blocks);
     std::swap(keys, keys2);
     std::swap(vals, vals2);

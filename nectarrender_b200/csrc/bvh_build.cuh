@@ -37,6 +37,14 @@ int build_bvh(const float4* d_lo, const float4* d_hi, uint32_t n, bool want_bvh8
 
 void free_build(BuildResult& r);
 
+// Exclusive prefix sum of in[0..n) into out (out == in allowed): tile sums,
+// one CTA over the tile sums, tile scans plus offsets. `sums` is scratch of
+// scan_scratch_words(n) words; the sum of all n values goes to *total
+// (device memory) when total is not null.
+uint32_t scan_scratch_words(uint32_t n);
+cudaError_t scan_exclusive(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* sums,
+                           uint32_t* total, cudaStream_t st);
+
 // Stable LSD radix sort of (key, value) pairs over the low key_bits bits
 // (8 bits per pass); keys2 / vals2 are scratch of n entries, hist holds
 // radix_sort_hist_words(n) words. The sorted pairs end in whichever buffers

@@ -28,7 +28,6 @@ namespace nr {
 namespace {
 
 constexpr uint64_t kEmpty = ~0ull;
-constexpr int kScanBlock = 1024;
 
 #define GRID_STRIDE(i, n) \
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < (n); i += (size_t)gridDim.x * blockDim.x)
@@ -113,81 +112,6 @@ __device__ __forceinline__ uint32_t first_of(const uint32_t* slot, const uint32_
 
 __global__ void k_first_flags(const uint32_t* slot, const uint32_t* tfirst, uint32_t n, uint32_t* flags) {
   GRID_STRIDE(c, n) { flags[c] = first_of(slot, tfirst, c, n) == c ? 1u : 0u; }
-}
-
-// Exclusive scan, pass 1: the sum of each kScanBlock-element block.
-__global__ void k_block_sums(const uint32_t* a, uint32_t n, uint32_t* sums) {
-  __shared__ uint32_t w[32];
-  const uint32_t i = blockIdx.x * kScanBlock + threadIdx.x;
-  uint32_t v = i < n ? a[i] : 0u;
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-  if ((threadIdx.x & 31) == 0) w[threadIdx.x >> 5] = v;
-  __syncthreads();
-  if (threadIdx.x < 32) {
-    uint32_t s = w[threadIdx.x];
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-    if (threadIdx.x == 0) sums[blockIdx.x] = s;
-  }
-}
-
-// Pass 2 (one CTA): exclusive scan of the block sums in place; total in *total.
-__global__ void k_scan_sums(uint32_t* sums, uint32_t nb, uint32_t* total) {
-  __shared__ uint32_t w[32];
-  __shared__ uint32_t carry;
-  if (threadIdx.x == 0) carry = 0;
-  __syncthreads();
-  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-  for (uint32_t base = 0; base < nb; base += blockDim.x) {
-    const uint32_t i = base + threadIdx.x;
-    const uint32_t v = i < nb ? sums[i] : 0u;
-    uint32_t x = v;
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-      if (lane >= (uint32_t)o) x += y;
-    }
-    if (lane == 31) w[warp] = x;
-    __syncthreads();
-    if (warp == 0) {
-      uint32_t s = w[lane];
-      for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t y = __shfl_up_sync(0xffffffffu, s, o);
-        if (lane >= (uint32_t)o) s += y;
-      }
-      w[lane] = s;
-    }
-    __syncthreads();
-    const uint32_t ex = carry + (warp ? w[warp - 1] : 0u) + x - v;
-    if (i < nb) sums[i] = ex;
-    __syncthreads();
-    if (threadIdx.x == blockDim.x - 1) carry = ex + v;
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) *total = carry;
-}
-
-// Pass 3: exclusive scan within each block plus the block's offset.
-__global__ void k_scan_apply(const uint32_t* a, uint32_t n, const uint32_t* sums, uint32_t* out) {
-  __shared__ uint32_t w[32];
-  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-  const uint32_t i = blockIdx.x * kScanBlock + threadIdx.x;
-  const uint32_t v = i < n ? a[i] : 0u;
-  uint32_t x = v;
-  for (int o = 1; o < 32; o <<= 1) {
-    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-    if (lane >= (uint32_t)o) x += y;
-  }
-  if (lane == 31) w[warp] = x;
-  __syncthreads();
-  if (warp == 0) {
-    uint32_t s = w[lane];
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t y = __shfl_up_sync(0xffffffffu, s, o);
-      if (lane >= (uint32_t)o) s += y;
-    }
-    w[lane] = s;
-  }
-  __syncthreads();
-  if (i < n) out[i] = sums[blockIdx.x] + (warp ? w[warp - 1] : 0u) + x - v;
 }
 
 // Vertex numbers of all corners; the first corner of each key writes its
@@ -295,7 +219,6 @@ std::string assemble_obj_device(const ObjRaw& raw, HostMesh& out, cudaStream_t s
     return "device OBJ assembly: the v/vt/vn index ranges need more than 63 key bits";
   uint32_t cap = 1;
   while (cap < 2u * n) cap <<= 1;
-  const uint32_t nb = (n + kScanBlock - 1) / kScanBlock;
   DevBufs b;
   int32_t* corners;
   float *vpos, *vnor, *vtex;
@@ -312,7 +235,7 @@ std::string assemble_obj_device(const ObjRaw& raw, HostMesh& out, cudaStream_t s
   DB(tfirst, cap);
   DB(slot, n);
   DB(flags, n);
-  DB(sums, nb);
+  DB(sums, scan_scratch_words(n));
   DB(num, n);
   DB(counts, 2);
   DB(tri, n);
@@ -329,9 +252,8 @@ std::string assemble_obj_device(const ObjRaw& raw, HostMesh& out, cudaStream_t s
   if (e != cudaSuccess) return std::string("device OBJ assembly: ") + cudaGetErrorString(e);
   k_insert<<<blocks_for(n), 256, 0, st>>>(corners, n, bv, bt, tkeys, tfirst, cap - 1, slot, counts + 1);
   k_first_flags<<<blocks_for(n), 256, 0, st>>>(slot, tfirst, n, flags);
-  k_block_sums<<<nb, kScanBlock, 0, st>>>(flags, n, sums);
-  k_scan_sums<<<1, 1024, 0, st>>>(sums, nb, counts);
-  k_scan_apply<<<nb, kScanBlock, 0, st>>>(flags, n, sums, num);
+  e = scan_exclusive(flags, num, n, sums, counts, st);
+  if (e != cudaSuccess) return std::string("device OBJ assembly: ") + cudaGetErrorString(e);
   uint32_t hc[2] = {0, 0};
   e = cudaMemcpyAsync(hc, counts, 8, cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);

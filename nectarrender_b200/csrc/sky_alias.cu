@@ -6,9 +6,9 @@
 // density must not be small) times sin(theta) of the texel row (its solid
 // angle). The distribution over texels factors into a marginal over rows
 // and a conditional over the columns of each row; each is an alias table
-// (Walker, 1977) built with Vose's method (IEEE TSE 17(9), 1991): one
-// thread per row builds that row's table, one thread builds the row table,
-// and texel_pdf = weight / total. A texel is drawn as row then column.
+// (Walker, 1977) built with Vose's method (IEEE TSE 17(9), 1991): one warp
+// per row builds that row's table, one warp builds the row table, and
+// texel_pdf = weight / total. A texel is drawn as row then column.
 #include "sky_alias.cuh"
 
 #include <vector>
@@ -42,64 +42,91 @@ __global__ void k_weights(const float* lum, int W, int H, float* w) {
   }
 }
 
-// Vose's method over n weights w[0..n) (sum > 0): q = w * n / sum, then
-// small entries take their deficit from large ones. q, small and large are
-// scratch of n entries.
-__device__ void vose(const float* w, uint32_t n, double sum, float* prob, uint32_t* alias, float* q,
-                     uint32_t* small, uint32_t* large) {
-  uint32_t ns = 0, nl = 0;
-  for (uint32_t i = 0; i < n; ++i) {
-    q[i] = (float)((double)w[i] * (double)n / sum);
-    prob[i] = 1.0f;
-    alias[i] = i;
-    if (q[i] < 1.0f)
-      small[ns++] = i;
-    else
-      large[nl++] = i;
-  }
-  while (ns > 0 && nl > 0) {
-    const uint32_t l = small[--ns], g = large[nl - 1];
-    prob[l] = q[l];
-    alias[l] = g;
-    q[g] = (q[g] + q[l]) - 1.0f;
-    if (q[g] < 1.0f) {
-      --nl;
-      small[ns++] = g;
+// Vose's method over n weights w[0..n) (sum > 0) by one warp: q = w * n /
+// sum and the small / large stacks (in index order) are built by all lanes,
+// then lane 0 pairs them: each small entry takes its deficit from the large
+// entry on top of the large stack. q, small and large are scratch of n
+// entries.
+__device__ void vose_warp(const float* w, uint32_t n, double sum, float* prob, uint32_t* alias,
+                          float* q, uint32_t* small, uint32_t* large) {
+  const uint32_t lane = threadIdx.x & 31u, below = (1u << lane) - 1u;
+  uint32_t ns = 0, nl = 0;  // the same in every lane
+  for (uint32_t b = 0; b < n; b += 32) {
+    const uint32_t i = b + lane;
+    const bool valid = i < n;
+    float qi = 0.0f;
+    if (valid) {
+      qi = (float)((double)w[i] * (double)n / sum);
+      q[i] = qi;
+      prob[i] = 1.0f;
+      alias[i] = i;
     }
+    const bool is_small = valid && qi < 1.0f, is_large = valid && !(qi < 1.0f);
+    const uint32_t ms = __ballot_sync(0xffffffffu, is_small), ml = __ballot_sync(0xffffffffu, is_large);
+    if (is_small) small[ns + __popc(ms & below)] = i;
+    if (is_large) large[nl + __popc(ml & below)] = i;
+    ns += (uint32_t)__popc(ms);
+    nl += (uint32_t)__popc(ml);
   }
-  // entries left in either stack keep prob 1 (round-off leftovers)
+  __syncwarp();
+  if (lane == 0) {
+    while (ns > 0 && nl > 0) {
+      const uint32_t l = small[--ns], g = large[nl - 1];
+      prob[l] = q[l];
+      alias[l] = g;
+      q[g] = (q[g] + q[l]) - 1.0f;
+      if (q[g] < 1.0f) {
+        --nl;
+        small[ns++] = g;
+      }
+    }
+    // entries left in either stack keep prob 1 (round-off leftovers)
+  }
+  __syncwarp();
 }
 
-// One thread per row: the row's weight sum and its column table.
+// Sum of w[0..n) in double by one warp (the same value in every lane).
+__device__ double warp_sum(const float* w, uint32_t n) {
+  const uint32_t lane = threadIdx.x & 31u;
+  double s = 0.0;
+  for (uint32_t x = lane; x < n; x += 32) s += (double)w[x];
+  for (int k = 16; k > 0; k >>= 1) s += __shfl_xor_sync(0xffffffffu, s, k);
+  return s;
+}
+
+// One warp per row: the row's weight sum and its column table.
 __global__ void k_row_tables(const float* w, int W, int H, double* row_sum, float* col_prob,
                              uint32_t* col_alias, float* q, uint32_t* small, uint32_t* large) {
-  const int y = blockIdx.x * blockDim.x + threadIdx.x;
-  if (y >= H) return;
+  const int y = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  if (y >= H) return;  // the whole warp
+  const uint32_t lane = threadIdx.x & 31u;
   const size_t o = (size_t)y * W;
-  double s = 0.0;
-  for (int x = 0; x < W; ++x) s += (double)w[o + x];
-  row_sum[y] = s;
+  const double s = warp_sum(w + o, (uint32_t)W);
+  if (lane == 0) row_sum[y] = s;
   if (s > 0.0) {
-    vose(w + o, (uint32_t)W, s, col_prob + o, col_alias + o, q + o, small + o, large + o);
+    vose_warp(w + o, (uint32_t)W, s, col_prob + o, col_alias + o, q + o, small + o, large + o);
   } else {
-    for (int x = 0; x < W; ++x) {
+    for (int x = (int)lane; x < W; x += 32) {
       col_prob[o + x] = 1.0f;
       col_alias[o + x] = (uint32_t)x;
     }
   }
 }
 
-// One thread: the total, and the row table over the row sums.
+// One warp: the total, and the row table over the row sums.
 __global__ void k_marginal(const double* row_sum, int H, float* row_w, double* total, float* row_prob,
                            uint32_t* row_alias, float* q, uint32_t* small, uint32_t* large) {
-  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  if (blockIdx.x != 0 || threadIdx.x >= 32) return;
+  const uint32_t lane = threadIdx.x;
   double s = 0.0;
-  for (int y = 0; y < H; ++y) {
+  for (int y = (int)lane; y < H; y += 32) {
     s += row_sum[y];
     row_w[y] = (float)row_sum[y];
   }
-  *total = s;
-  if (s > 0.0) vose(row_w, (uint32_t)H, s, row_prob, row_alias, q, small, large);
+  for (int k = 16; k > 0; k >>= 1) s += __shfl_xor_sync(0xffffffffu, s, k);
+  if (lane == 0) *total = s;
+  __syncwarp();
+  if (s > 0.0) vose_warp(row_w, (uint32_t)H, s, row_prob, row_alias, q, small, large);
 }
 
 __global__ void k_texel_pdf(const float* w, size_t n, const double* total, float* pdf) {
@@ -146,8 +173,8 @@ cudaError_t build_sky_tables(const float* chw, int W, int H, SkyTables& t, bool&
   if (e == cudaSuccess) {
     k_luminance<<<blocks_for(hw), 256, 0, st>>>(chw, W, H, lum);
     k_weights<<<blocks_for(hw), 256, 0, st>>>(lum, W, H, w);
-    k_row_tables<<<(H + 127) / 128, 128, 0, st>>>(w, W, H, row_sum, t.col_prob, t.col_alias, q,
-                                                 small, large);
+    k_row_tables<<<(H + 3) / 4, 128, 0, st>>>(w, W, H, row_sum, t.col_prob, t.col_alias, q, small,
+                                             large);
     // the row table reuses the head of the scratch arrays
     k_marginal<<<1, 32, 0, st>>>(row_sum, H, row_w, total, t.row_prob, t.row_alias, q, small, large);
     k_texel_pdf<<<blocks_for(hw), 256, 0, st>>>(w, hw, total, t.texel_pdf);
