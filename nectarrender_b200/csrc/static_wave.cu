@@ -38,10 +38,7 @@ void static_wave_carve(void* base, WfParams& W) {
     p += round_up(bytes);
     return q;
   };
-  W.ray_o = reinterpret_cast<float4*>(take(kPaths * sizeof(float4)));
-  W.ray_d = reinterpret_cast<float4*>(take(kPaths * sizeof(float4)));
-  W.atten = reinterpret_cast<float4*>(take(kPaths * sizeof(float4)));
-  W.acc_b = reinterpret_cast<float4*>(take(kPaths * sizeof(float4)));
+  W.path = reinterpret_cast<float4*>(take(kRecWords * kPaths * sizeof(float4)));
   W.acc_d = reinterpret_cast<float4*>(take(kPaths * sizeof(float4)));
   W.acc_n = reinterpret_cast<float4*>(take(kPaths * sizeof(float4)));
   W.hit = reinterpret_cast<uint4*>(take(kPaths * sizeof(uint4)));

@@ -121,6 +121,21 @@ __device__ __forceinline__ uint32_t wave_base(const WfParams& W) { return W.ctr[
 
 __device__ __forceinline__ float4 ld4(const float4* p) { return __ldg(p); }
 
+// One aligned 32-byte sector of a path record (two float4) in one 256-bit
+// global load or store (sm_100), so that a lane moves a whole sector.
+__device__ __forceinline__ void ld8(const float4* p, float4& a, float4& b) {
+  asm volatile("ld.global.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+               : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w), "=f"(b.x), "=f"(b.y), "=f"(b.z),
+                 "=f"(b.w)
+               : "l"(p)
+               : "memory");
+}
+__device__ __forceinline__ void st8(float4* p, const float4& a, const float4& b) {
+  asm volatile("st.global.v8.f32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(p), "f"(a.x),
+               "f"(a.y), "f"(a.z), "f"(a.w), "f"(b.x), "f"(b.y), "f"(b.z), "f"(b.w)
+               : "memory");
+}
+
 // ---------------------------------------------------------------------------
 // compressed 8-wide traversal with a shared-memory stack; `leaf(slot, tmax)`
 // is called for every primitive slot whose leaf box the ray enters.
@@ -373,10 +388,11 @@ __global__ void k_wf_generate(WfParams W) {
     Rng g;
     g.init(P.seed, pix + sample * (P.W * P.H));
     Ray r = camera_ray(P.cam, x, y, pix, sample, P.seed, g, P.rtl != 0);
-    W.ray_o[p] = make_float4(r.o.x, r.o.y, r.o.z, r.tm);
-    W.ray_d[p] = make_float4(r.d.x, r.d.y, r.d.z, __uint_as_float(0u));
-    W.atten[p] = make_float4(1.0f, 1.0f, 1.0f, __uint_as_float(g.draw));
-    W.acc_b[p] = make_float4(0.f, 0.f, 0.f, __uint_as_float(0xffffffffu));
+    float4* rp = W.path + path_at(p, 0);
+    st8(rp + kRecO, make_float4(r.o.x, r.o.y, r.o.z, r.tm),
+        make_float4(r.d.x, r.d.y, r.d.z, __uint_as_float(0u)));
+    st8(rp + kRecAtten, make_float4(1.0f, 1.0f, 1.0f, __uint_as_float(g.draw)),
+        make_float4(0.f, 0.f, 0.f, __uint_as_float(0xffffffffu)));
     W.acc_d[p] = make_float4(0.f, 0.f, 0.f, 0.f);
     W.acc_n[p] = make_float4(0.f, 0.f, 0.f, 0.f);
     if (W.mis_pdf) W.mis_pdf[p] = 0.0f;  // camera rays: emission is not MIS-weighted
@@ -420,7 +436,7 @@ __global__ void __launch_bounds__(kExtThreads, kMinBlocks) k_wf_extend(WfParams 
     uint32_t i = base + lane;
     if (i < n) {
       const uint32_t p = identity ? i : __ldg(queue + i);
-      float4 o = ld4(W.ray_o + p), d = ld4(W.ray_d + p);
+      float4 o = ld4(W.path + path_at(p, kRecO)), d = ld4(W.path + path_at(p, kRecD));
       Ray r = make_ray(V3{o.x, o.y, o.z}, V3{d.x, d.y, d.z}, o.w);
       uint32_t obj, slot;
       float t, u, v;
@@ -530,7 +546,8 @@ __global__ void __launch_bounds__(kExtThreads, kMinBlocks) k_wf_extend_flat(WfPa
           const uint32_t i = base + __popc(idle & lt_mask);
           if (i < n) {
             const uint32_t p = identity ? i : __ldg(queue + i);
-            const float4 ro = ld4(W.ray_o + p), rd = ld4(W.ray_d + p);
+            const float4 ro = ld4(W.path + path_at(p, kRecO));
+            const float4 rd = ld4(W.path + path_at(p, kRecD));
             o = V3{ro.x, ro.y, ro.z};
             d = V3{rd.x, rd.y, rd.z};
             inv = V3{1.0f / d.x, 1.0f / d.y, 1.0f / d.z};
@@ -765,7 +782,10 @@ __global__ void __launch_bounds__(kShadeThreads, kMinBlocks) k_wf_shade(WfParams
     uint32_t p = 0;
     if (i < n) {
       p = (identity && !sorted) ? i : __ldg(queue + i);
-      float4 o = W.ray_o[p], d = W.ray_d[p], at = W.atten[p], ab = W.acc_b[p];
+      float4* rp = W.path + path_at(p, 0);
+      float4 o, d, at, ab;
+      ld8(rp + kRecO, o, d);
+      ld8(rp + kRecAtten, at, ab);
       uint32_t bounce = __float_as_uint(d.w);
       PathState s;
       s.ray = make_ray(V3{o.x, o.y, o.z}, V3{d.x, d.y, d.z}, o.w);
@@ -886,13 +906,17 @@ __global__ void __launch_bounds__(kShadeThreads, kMinBlocks) k_wf_shade(WfParams
         }
         if (cont && bounce + 1u < P.depth) {
           alive = true;
-          W.ray_o[p] = make_float4(s.ray.o.x, s.ray.o.y, s.ray.o.z, s.ray.tm);
-          W.ray_d[p] = make_float4(s.ray.d.x, s.ray.d.y, s.ray.d.z, __uint_as_float(bounce + 1u));
-          W.atten[p] = make_float4(s.atten.x, s.atten.y, s.atten.z, __uint_as_float(g.draw));
           if (kPerf) W.mis_pdf[p] = pdf_next;
         }
       }
-      W.acc_b[p] = make_float4(s.beauty.x, s.beauty.y, s.beauty.z, __uint_as_float(s.primary));
+      const float4 b4 = make_float4(s.beauty.x, s.beauty.y, s.beauty.z, __uint_as_float(s.primary));
+      if (alive) {
+        st8(rp + kRecO, make_float4(s.ray.o.x, s.ray.o.y, s.ray.o.z, s.ray.tm),
+            make_float4(s.ray.d.x, s.ray.d.y, s.ray.d.z, __uint_as_float(bounce + 1u)));
+        st8(rp + kRecAtten, make_float4(s.atten.x, s.atten.y, s.atten.z, __uint_as_float(g.draw)), b4);
+      } else {
+        rp[kRecBeauty] = b4;
+      }
     }
     // warp-aggregated append of the surviving paths (and, in perf mode, of
     // the shadow rays)
@@ -933,8 +957,10 @@ __global__ void __launch_bounds__(128) k_wf_tail(WfParams W, int qsel, uint32_t 
   TraceStats st{0u, 0u, 0u};
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const uint32_t p = __ldg(queue + i);
-    const float4 o = W.ray_o[p], d = W.ray_d[p], at = W.atten[p], ab = W.acc_b[p], ad = W.acc_d[p],
-                 an = W.acc_n[p];
+    float4 o, d, at, ab;
+    ld8(W.path + path_at(p, kRecO), o, d);
+    ld8(W.path + path_at(p, kRecAtten), at, ab);
+    const float4 ad = W.acc_d[p], an = W.acc_n[p];
     PathState s;
     s.ray = make_ray(V3{o.x, o.y, o.z}, V3{d.x, d.y, d.z}, o.w);
     s.atten = V3{at.x, at.y, at.z};
@@ -948,7 +974,7 @@ __global__ void __launch_bounds__(128) k_wf_tail(WfParams W, int qsel, uint32_t 
     g.init(P.seed, pix + (wbase + k) * N, __float_as_uint(at.w));
     while (bounce_ref(P, s, g, st)) {
     }
-    W.acc_b[p] = make_float4(s.beauty.x, s.beauty.y, s.beauty.z, __uint_as_float(s.primary));
+    W.path[path_at(p, kRecBeauty)] = make_float4(s.beauty.x, s.beauty.y, s.beauty.z, __uint_as_float(s.primary));
     W.acc_d[p] = make_float4(s.diffuse.x, s.diffuse.y, s.diffuse.z, 0.f);
     W.acc_n[p] = make_float4(s.normal.x, s.normal.y, s.normal.z, 0.f);
   }
@@ -986,11 +1012,11 @@ __global__ void __launch_bounds__(kExtThreads) k_wf_shadow(WfParams W) {
                            P.err, o.w);
       if (obj == 0xffffffffu) {
         const float4 c = W.sh_c[p];
-        float4 b = W.acc_b[p];
+        float4 b = W.path[path_at(p, kRecBeauty)];
         b.x += c.x;
         b.y += c.y;
         b.z += c.z;
-        W.acc_b[p] = b;
+        W.path[path_at(p, kRecBeauty)] = b;
       }
     }
   }
@@ -1073,7 +1099,7 @@ __global__ void k_wf_accumulate(WfParams W) {
   const uint32_t base = wave_base(W);
   for (uint32_t pix = blockIdx.x * blockDim.x + threadIdx.x; pix < N; pix += gridDim.x * blockDim.x) {
     if (P.write_raw) {
-      float4 b = W.acc_b[pix], d = W.acc_d[pix], n = W.acc_n[pix];
+      float4 b = W.path[path_at(pix, kRecBeauty)], d = W.acc_d[pix], n = W.acc_n[pix];
       if (P.beauty) store3(P.beauty, hw, pix, V3{b.x, b.y, b.z});
       if (P.diffuse) store3(P.diffuse, hw, pix, V3{d.x, d.y, d.z});
       if (P.normal) store3(P.normal, hw, pix, V3{n.x, n.y, n.z});
@@ -1086,7 +1112,7 @@ __global__ void k_wf_accumulate(WfParams W) {
     double s64[3] = {0, 0, 0};
     for (uint32_t k = 0; k < W.count; ++k) {
       uint32_t p = k * N + pix, smp = base + k;
-      float4 b = W.acc_b[p], d = W.acc_d[p], n = W.acc_n[p];
+      float4 b = W.path[path_at(p, kRecBeauty)], d = W.acc_d[p], n = W.acc_n[p];
       ab = running_mean(ab, V3{b.x, b.y, b.z}, smp);
       ad = running_mean(ad, V3{d.x, d.y, d.z}, smp);
       an = running_mean(an, V3{n.x, n.y, n.z}, smp);
@@ -1115,11 +1141,11 @@ __global__ void k_nrc_apply(WfParams W, const float* radiance, uint32_t n) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const float4 b = W.nrc_q_beta[i];
     const uint32_t p = __float_as_uint(b.w);
-    float4 acc = W.acc_b[p];
+    float4 acc = W.path[path_at(p, kRecBeauty)];
     acc.x += b.x * radiance[3 * i];
     acc.y += b.y * radiance[3 * i + 1];
     acc.z += b.z * radiance[3 * i + 2];
-    W.acc_b[p] = acc;
+    W.path[path_at(p, kRecBeauty)] = acc;
   }
 }
 
@@ -1129,7 +1155,7 @@ __global__ void k_nrc_targets(WfParams W, float* target, float4* records, uint32
                               uint32_t groups, uint32_t per) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const float4 b = W.nrc_t_beta[i], before = W.nrc_t_before[i];
-    const float4 after = W.acc_b[__float_as_uint(b.w)];
+    const float4 after = W.path[path_at(__float_as_uint(b.w), kRecBeauty)];
     const float beta[3] = {b.x, b.y, b.z};
     const float d[3] = {after.x - before.x, after.y - before.y, after.z - before.z};
     const size_t slot = (size_t)(i % groups) * per + i / groups;
@@ -1202,10 +1228,7 @@ cudaError_t wf_alloc(WfParams& W, uint32_t n_paths, bool perf, bool sort) {
   cudaError_t e;
 #define A(ptr, T) \
   if ((e = cudaMalloc(&W.ptr, sizeof(T) * (size_t)n_paths)) != cudaSuccess) return e;
-  A(ray_o, float4);
-  A(ray_d, float4);
-  A(atten, float4);
-  A(acc_b, float4);
+  if ((e = cudaMalloc(&W.path, sizeof(float4) * kRecWords * (size_t)n_paths)) != cudaSuccess) return e;
   A(acc_d, float4);
   A(acc_n, float4);
   A(hit, uint4);
@@ -1232,10 +1255,7 @@ cudaError_t wf_alloc(WfParams& W, uint32_t n_paths, bool perf, bool sort) {
 }
 
 void wf_free(WfParams& W) {
-  cudaFree(W.ray_o);
-  cudaFree(W.ray_d);
-  cudaFree(W.atten);
-  cudaFree(W.acc_b);
+  cudaFree(W.path);
   cudaFree(W.acc_d);
   cudaFree(W.acc_n);
   cudaFree(W.hit);

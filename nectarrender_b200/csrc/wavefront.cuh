@@ -6,6 +6,17 @@
 
 namespace nr {
 
+// Fields of the per-path record WfParams::path.
+constexpr int kRecWords = 4;
+constexpr int kRecO = 0, kRecD = 1, kRecAtten = 2, kRecBeauty = 3;
+// the kernels move (origin, direction) and (throughput, beauty) as 32-byte
+// sectors of a 64-byte aligned record
+static_assert(kRecWords == 4 && kRecD == kRecO + 1 && kRecAtten == 2 && kRecBeauty == 3,
+              "path record layout");
+__host__ __device__ __forceinline__ size_t path_at(uint32_t p, int field) {
+  return (size_t)kRecWords * p + (size_t)field;
+}
+
 struct WfParams {
   KernelParams kp;
   uint32_t base;   // first sample index of the wave (host side; the kernels
@@ -16,10 +27,11 @@ struct WfParams {
   int32_t extend_variant;  // traversal kernel (see extend_fn)
   uint32_t tail_max_paths; // tail hand-off bound (0: none)
   int32_t shade_variant;   // 5 or 6: register budget for that many CTAs per SM; else none
-  float4* ray_o;
-  float4* ray_d;
-  float4* atten;
-  float4* acc_b;
+  // one 64-byte record per path, kRecWords float4 (path_at(p, field)): ray
+  // origin + time, ray direction + bounce, throughput + draw counter, beauty
+  // + primary id. A path's state is two whole 32-byte sectors, so the
+  // sorted (scattered) shading reads and writes no half-used sectors.
+  float4* path;
   float4* acc_d;
   float4* acc_n;
   uint4* hit;
