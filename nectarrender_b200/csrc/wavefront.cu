@@ -393,8 +393,8 @@ __global__ void k_wf_generate(WfParams W) {
         make_float4(r.d.x, r.d.y, r.d.z, __uint_as_float(0u)));
     st8(rp + kRecAtten, make_float4(1.0f, 1.0f, 1.0f, __uint_as_float(g.draw)),
         make_float4(0.f, 0.f, 0.f, __uint_as_float(0xffffffffu)));
-    W.acc_d[p] = make_float4(0.f, 0.f, 0.f, 0.f);
-    W.acc_n[p] = make_float4(0.f, 0.f, 0.f, 0.f);
+    // acc_d / acc_n are written by the shading of bounce 0, which every
+    // path of the wave reaches
     if (W.mis_pdf) W.mis_pdf[p] = 0.0f;  // camera rays: emission is not MIS-weighted
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -793,6 +793,7 @@ __global__ void __launch_bounds__(kShadeThreads, kMinBlocks) k_wf_shade(WfParams
       s.beauty = V3{ab.x, ab.y, ab.z};
       s.primary = __float_as_uint(ab.w);
       s.bounce = bounce;
+      float4 aov_d = make_float4(0.f, 0.f, 0.f, 0.f), aov_n = aov_d;  // bounce 0 only
       const float pdf_prev = kPerf ? W.mis_pdf[p] : 0.0f;
       uint32_t k = p / N, pix = p - k * N;
       Rng g;
@@ -893,9 +894,10 @@ __global__ void __launch_bounds__(kShadeThreads, kMinBlocks) k_wf_shade(WfParams
         }
         if (cont) {
           if (bounce == 0u) {
-            float4 ad = W.acc_d[p], an = W.acc_n[p];
-            W.acc_d[p] = make_float4(ad.x + s.atten.x, ad.y + s.atten.y, ad.z + s.atten.z, 0.f);
-            W.acc_n[p] = make_float4(an.x + rec.n.x, an.y + rec.n.y, an.z + rec.n.z, 0.f);
+            // the first-hit AOV sums start from zero (0 + x, as a running
+            // sum from a cleared buffer computes it)
+            aov_d = make_float4(0.f + s.atten.x, 0.f + s.atten.y, 0.f + s.atten.z, 0.f);
+            aov_n = make_float4(0.f + rec.n.x, 0.f + rec.n.y, 0.f + rec.n.z, 0.f);
           }
           if (P.rr_enabled && bounce >= P.rr_start) {
             float survival = fmaxf(s.atten.x, fmaxf(s.atten.y, s.atten.z));
@@ -908,6 +910,10 @@ __global__ void __launch_bounds__(kShadeThreads, kMinBlocks) k_wf_shade(WfParams
           alive = true;
           if (kPerf) W.mis_pdf[p] = pdf_next;
         }
+      }
+      if (bounce == 0u) {
+        W.acc_d[p] = aov_d;
+        W.acc_n[p] = aov_n;
       }
       const float4 b4 = make_float4(s.beauty.x, s.beauty.y, s.beauty.z, __uint_as_float(s.primary));
       if (alive) {
