@@ -500,10 +500,15 @@ def multi_scene(args):
         try:
             import oracle
             rc = oracle.RefCUDA()
-            ms = sum(rc.render(s, 1, count=c, mode=1)[3] for s, c in zip(specs, counts))
-            out["reference_cuda"] = {"device_s": ms * 1e-3, "samples_per_s": total / (ms * 1e-3),
+            ms, ref_total = 0.0, 0
+            for s, c in zip(specs, counts):
+                rspec, pixels = padded_for_reference_cuda(s)
+                ms += rc.render(rspec, 1, count=c, mode=1)[3]
+                ref_total += pixels * c
+            out["reference_cuda"] = {"device_s": ms * 1e-3, "samples_per_s": ref_total / (ms * 1e-3),
                                      "note": "reference render loop per scene (sm_100a build), "
-                                             "CUDA events, scene builds excluded"}
+                                             "CUDA events, scene builds excluded, image sizes "
+                                             "rounded up to multiples of 16"}
         except Exception as e:  # noqa: BLE001 - reported, not fatal
             out["reference_cuda"] = {"unavailable": repr(e)[:200]}
     return out
@@ -926,16 +931,32 @@ def time_to_rmse(args, target=0.01):
     return out
 
 
+def padded_for_reference_cuda(spec):
+    """A copy of `spec` whose image sizes are rounded up to multiples of 16,
+    and its pixel count: the reference's 16x16-block accumulation kernels
+    have no bounds guard, so it only runs on such sizes."""
+    import copy
+    s = copy.deepcopy(spec)
+    h, w = (int(x) for x in s.camera["resolution"])
+    h, w = (h + 15) // 16 * 16, (w + 15) // 16 * 16
+    s.camera["resolution"] = (float(h), float(w))
+    return s, h * w
+
+
 def reference_cuda_rate(spec, w, h):
     """The reference's CUDA path (sm_100a build) on the same scene: 2 samples,
-    its render loop timed with CUDA events."""
+    its render loop timed with CUDA events (at the image size rounded up to
+    multiples of 16, counting the pixels it renders)."""
     try:
         import oracle
         rc = oracle.RefCUDA()
-        res = rc.render(spec, 1, count=2, mode=1)
+        rspec, pixels = padded_for_reference_cuda(spec)
+        res = rc.render(rspec, 1, count=2, mode=1)
         ms = res[3]
-        return {"value": w * h * 2 / (ms * 1e-3), "unit": "samples/s", "samples": 2,
-                "note": "reference trace_full + accumulate loop compiled for sm_100a, same scene"}
+        rh, rw = (int(x) for x in rspec.camera["resolution"])
+        return {"value": pixels * 2 / (ms * 1e-3), "unit": "samples/s", "samples": 2,
+                "note": f"reference trace_full + accumulate loop compiled for sm_100a, same scene "
+                        f"rendered at {rw}x{rh}"}
     except Exception as e:  # noqa: BLE001 - reported, not fatal
         return {"unavailable": repr(e)[:200]}
 

@@ -344,6 +344,9 @@ class RefCUDA(_Lib):
         cam = camera_desc(spec.camera)
         cfg = cfg or render_config(spec)
         H, W = int(spec.camera["resolution"][0]), int(spec.camera["resolution"][1])
+        if H % 16 or W % 16:
+            # the reference's 16x16-block kernels have no bounds guard
+            raise ValueError(f"reference CUDA build needs both sizes a multiple of 16, got {H}x{W}")
         b = np.zeros((3, H, W), np.float32)
         d, n = np.zeros_like(b), np.zeros_like(b)
         req = OrRequest(first, count, mode, 0, 0, H, 0, _f(b), _f(d), _f(n), None, None)
