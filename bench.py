@@ -816,7 +816,7 @@ def _layer_ptr(render, layer):
 def train_denoiser(args, log=None):
     """Trains the U-Net denoiser on mesh-stress scenes other than the
     evaluated one (scene seeds 21-28, icosphere level 6, 256x256): inputs are
-    perf-mode renders at 1 to 16 samples, targets 1024-sample renders.
+    perf-mode renders at 1 to 256 samples, targets 1024-sample renders.
     Returns (denoiser, info)."""
     import torch
     from nectarrender_b200 import capi, denoise
@@ -830,7 +830,7 @@ def train_denoiser(args, log=None):
         tgt = capi.Render(sc, mode=capi.MODE_PERF, seed=1000 + ss)
         tgt.samples(1, 1024)
         target = denoise.render_layers(tgt)[0]
-        for n in (1, 2, 4, 8, 16):
+        for n in (1, 2, 4, 8, 16, 64, 256):
             r = capi.Render(sc, mode=capi.MODE_PERF, seed=ss)
             r.samples(1, n)
             pairs.append((denoise.render_layers(r), target))
@@ -899,7 +899,7 @@ def time_to_rmse(args, target=0.01):
         done, n, t_ms = 0, 1, 0.0
         curve = []
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        while done + n <= 256:
+        while done + n <= 4096:
             r.samples(done + 1, n)
             t_ms += r.last_ms()
             done += n
@@ -915,10 +915,15 @@ def time_to_rmse(args, target=0.01):
         # speed-up at equal error against the plain perf-mode curve
         plain = out["perf_mode"]["curve_spp_ms_rmse"]
         best = None
+        ratios = []
         for spp_d, ms_d, r_d in curve:
             hit = next((ms for _, ms, rr in plain if rr <= r_d), None)
+            ratios.append([spp_d, r_d, None if hit is None else round(hit / ms_d, 3)])
             if hit is not None and (best is None or hit / ms_d > best[0]):
                 best = (hit / ms_d, r_d, spp_d)
+        # plain perf-mode time to the denoised error (first plain point at or
+        # below it) over the denoised time, per denoised point
+        info["time_ratio_plain_over_denoised"] = ratios
         if best:
             info["speedup_vs_perf_at_equal_rmse"] = {"speedup": best[0], "rmse": best[1],
                                                      "denoised_spp": best[2]}

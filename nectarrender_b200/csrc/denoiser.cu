@@ -52,21 +52,30 @@ __global__ void k_prep(const float* beauty, const float* diffuse, const float* n
   }
 }
 
-// Squared error in log space, 0.5 * (pred - log(1 + target))^2 on the first
-// three output channels; d(loss)/d(pred) = pred - log(1 + target) (Adam is
-// invariant to the gradient scale, so the 1/N of the mean is left out), zero
-// on the others. A squared error estimates the conditional mean of the noisy
-// targets (an absolute error would estimate their median, which sits below
-// the mean under the heavy-tailed noise of path tracing).
-__global__ void k_loss(View out, const float* target, View dout, int B, int H, int W,
-                       double* loss) {
+// The prediction is residual in log space: pred = log(1 + noisy beauty) +
+// the network's first three output channels, so an untrained network (small
+// output layer) starts near the identity and a clean input needs only a small
+// correction. Loss: squared error in log space, 0.5 * (pred - log(1 +
+// target))^2; d(loss)/d(output) = pred - log(1 + target) on the first three
+// channels (Adam is invariant to the gradient scale, so the 1/N of the mean
+// is left out), zero on the others. A squared error estimates the
+// conditional mean of the noisy targets (an absolute error would estimate
+// their median, which sits below the mean under the heavy-tailed noise of
+// path tracing).
+__device__ __forceinline__ float log_beauty(const float* beauty, size_t b, size_t hw, int c,
+                                            size_t i) {
+  return log1pf(fmaxf(beauty[b * 3 * hw + c * hw + i], 0.0f));
+}
+
+__global__ void k_loss(View out, const float* beauty, const float* target, View dout, int B, int H,
+                       int W, double* loss) {
   const size_t hw = (size_t)H * W, P = (size_t)B * hw;
   double local = 0.0;
   GRID_STRIDE(p, P) {
     const size_t b = p / hw, i = p - b * hw;
     for (int c = 0; c < 3; ++c) {
-      const float t = log1pf(fmaxf(target[b * 3 * hw + c * hw + i], 0.0f));
-      const float d = ld(out, p, c) - t;
+      const float t = log_beauty(target, b, hw, c, i);
+      const float d = (log_beauty(beauty, b, hw, c, i) + ld(out, p, c)) - t;
       local += 0.5 * (double)d * (double)d;
       st(dout, p, c, d);
     }
@@ -76,12 +85,15 @@ __global__ void k_loss(View out, const float* target, View dout, int B, int H, i
   if ((threadIdx.x & 31) == 0) atomicAdd(loss, local);
 }
 
-// Output: beauty = exp(pred) - 1, planar CHW.
-__global__ void k_output(View out, float* beauty, int B, int H, int W) {
+// Output: exp(pred) - 1, planar CHW (res may be beauty: each element is read
+// before it is written, by the same thread).
+__global__ void k_output(View out, const float* beauty, float* res, int B, int H, int W) {
   const size_t hw = (size_t)H * W, P = (size_t)B * hw;
   GRID_STRIDE(p, P) {
     const size_t b = p / hw, i = p - b * hw;
-    for (int c = 0; c < 3; ++c) beauty[b * 3 * hw + c * hw + i] = fmaxf(expm1f(ld(out, p, c)), 0.0f);
+    for (int c = 0; c < 3; ++c)
+      res[b * 3 * hw + c * hw + i] =
+          fmaxf(expm1f(log_beauty(beauty, b, hw, c, i) + ld(out, p, c)), 0.0f);
   }
 }
 
@@ -500,7 +512,8 @@ std::string denoiser_forward_backward(Denoiser& d, const float* beauty, const fl
   cudaError_t e = forward(n, beauty, diffuse, normal, B, H, W, st);
   if (e != cudaSuccess) return cuda_msg(e, "denoiser forward");
   const size_t P0 = (size_t)B * H * W;
-  k_loss<<<blocks_for(P0), 256, 0, st>>>(n.out.v(), target, n.g_out.v(), B, H, W, n.d_loss);
+  k_loss<<<blocks_for(P0), 256, 0, st>>>(n.out.v(), beauty, target, n.g_out.v(), B, H, W,
+                                         n.d_loss);
   e = backward(n, B, H, W, st);
   if (e != cudaSuccess) return cuda_msg(e, "denoiser backward");
   s = finish(n, st, "denoiser training step");
@@ -538,7 +551,7 @@ std::string denoiser_infer(Denoiser& d, const float* beauty, const float* diffus
   if (!s.empty()) return s;
   cudaError_t e = forward(n, beauty, diffuse, normal, B, H, W, st);
   if (e != cudaSuccess) return cuda_msg(e, "denoiser forward");
-  k_output<<<blocks_for((size_t)B * H * W), 256, 0, st>>>(n.out.v(), out, B, H, W);
+  k_output<<<blocks_for((size_t)B * H * W), 256, 0, st>>>(n.out.v(), beauty, out, B, H, W);
   return finish(n, st, "denoiser inference");
 }
 

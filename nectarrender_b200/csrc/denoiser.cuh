@@ -9,7 +9,8 @@
 //   input 16 = log(1 + beauty) 3, diffuse 3, normal 3, zeros 7
 //   encoder  32, 48, 64, 80, 96 (two convolutions per level)
 //   decoder  80, 64, 48, 32 (two convolutions per level, after concat)
-//   output   16 (first 3 = log(1 + beauty), no activation)
+//   output   16 (first 3 = correction to log(1 + beauty), no activation:
+//            the prediction is log(1 + noisy beauty) + output)
 // Loss: squared error in log space; Adam.
 #pragma once
 #include <cuda_bf16.h>

@@ -54,9 +54,10 @@ def up_bwd(g):
     return g[0::2, 0::2] + g[1::2, 0::2] + g[0::2, 1::2] + g[1::2, 1::2]
 
 
-def unet_grads(params, x0, target):
-    """FP64 forward + backward of the network in denoiser.cuh; returns the
-    loss and [(dw, db)] in parameter order."""
+def unet_grads(params, x0, target, base):
+    """FP64 forward + backward of the network in denoiser.cuh (prediction =
+    base + the first three output channels); returns the loss and [(dw, db)]
+    in parameter order."""
     P = [(w.astype(np.float64), b.astype(np.float64)) for w, b in params]
     acts = {}
     relu = lambda a: np.maximum(a, 0)
@@ -75,7 +76,7 @@ def unet_grads(params, x0, target):
         b = relu(conv(a, *P[i])); acts[i] = (a, b); i += 1
         below = b
     out = conv(below, *P[i]); acts[i] = (below, out)
-    d = out[..., :3] - target
+    d = (base + out[..., :3]) - target
     loss = (0.5 * d * d).mean()
     g_out = np.zeros_like(out)
     g_out[..., :3] = d
@@ -119,7 +120,8 @@ def test_gradients_match_fp64_network():
     x0[..., 0:3] = np.log1p(beauty[0].transpose(1, 2, 0))
     x0[..., 3:6] = diffuse[0].transpose(1, 2, 0)
     x0[..., 6:9] = normal[0].transpose(1, 2, 0)
-    loss_ref, ref = unet_grads(params64, bf(x0), np.log1p(target[0].transpose(1, 2, 0).astype(np.float64)))
+    loss_ref, ref = unet_grads(params64, bf(x0), np.log1p(target[0].transpose(1, 2, 0).astype(np.float64)),
+                               np.log1p(beauty[0].transpose(1, 2, 0).astype(np.float64)))
     assert abs(loss_gpu - loss_ref) <= 0.02 * loss_ref
     for k, ((gw, gb), (rw, rb)) in enumerate(zip(grads, ref)):
         rw = rw.astype(np.float64)
