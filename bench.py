@@ -85,7 +85,7 @@ def workload(args):
     return spec, h, w
 
 
-def config_json(args, h, w, spec, l2):
+def config_json(args, h, w, spec):
     return {"workload": f"mesh_stress: icosphere L{args.levels} "
                         f"({20 * 4 ** args.levels} tris) + 256 spheres + 2048x1024 HDRI, "
                         f"{w}x{h}, depth {spec.ray_depth}",
@@ -95,7 +95,9 @@ def config_json(args, h, w, spec, l2):
             "extend_variant": args.extend_variant or "default", "mesh_leaf": args.mesh_leaf,
             "shade_variant": args.shade_variant or "default",
             "sort_materials": args.sort_materials,
-            "parallelism": f"sample-sharded x{args.gpus}", "l2": l2}
+            "parallelism": f"sample-sharded x{args.gpus}",
+            "l2": "inputs larger than L2 (126 MB); L2 flushed between timed GPU steps "
+                  "(256 MiB write)"}
 
 
 # ---------------------------------------------------------------------------
@@ -202,7 +204,7 @@ def run_reference(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded scene generator)", "impl": "reference",
-            "config": config_json(args, h, w, spec, "n/a (CPU)"),
+            "config": config_json(args, h, w, spec),
             "cpu_baseline": {"value": value, "unit": "samples/s", "cores": cores, "kind": kind,
                              "sample": sample_desc},
             "e2e": {"value": value, "unit": "samples/s", "h2d_bytes_per_step": 0,
@@ -392,7 +394,7 @@ def run_ours(args):
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_ms / args.steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic (seeded scene generator)",
-                "config": config_json(args, h, w, spec, "flushed between timed steps (256 MiB write)"),
+                "config": config_json(args, h, w, spec),
                 "clocks": clk.summary(),
                 "e2e": e2e,
                 "gpu_launches": sum(kernel_launches.values()),

@@ -246,6 +246,12 @@ int nr_abi_version(void);
 const char* nr_last_error(void);
 /* Number of CUDA devices visible (0 without a GPU; never fails). */
 int nr_device_count(void);
+/* Device memory of the current device in bytes: used = total - free
+ * (replaces get_cuda_meminfo / CUDAMemInfo,
+ * nectar_render/csrc/host/include/host/utils.h:34-38, bound as
+ * _pathtracer.host.memory). NR_ERR_NO_DEVICE without a GPU, where the
+ * reference ignores cudaMemGetInfo's status. */
+int nr_device_memory_info(uint64_t* used, uint64_t* free_bytes, uint64_t* total);
 /* Order in which NR_MODE_REFERENCE consumes random draws for the reference's
  * constructor calls that take several draws as arguments (Vector3::random,
  * Quad::random, random_in_unit_disk; C++ leaves it unspecified): 0 = left to
@@ -384,9 +390,19 @@ int nr_host_free(void* p);
  *    fail with NR_ERR_LIMIT before any work. A wave holds
  *    NR_STATIC_WAVE_PATHS / (W*H) sample indices (at most the render's
  *    samples_per_wave setting).
- *  - Setup: the first call on each device looks up the buffer's address
- *    (cudaGetSymbolAddress, with the render's device current). Make that
- *    first call before any stream capture on that device.
+ *  - Mode: NR_MODE_REFERENCE renders only; a render created with another
+ *    mode fails with NR_ERR_STATE.
+ *  - Setup: the first call on each device, with that device current, looks
+ *    up the buffer's address (cudaGetSymbolAddress). With CUDA's lazy module
+ *    loading this is also when the driver loads the module that holds the
+ *    buffer and reserves its NR_STATIC_WAVE_BYTES of device memory, so a
+ *    caller that hands its free memory to another allocator, or captures
+ *    streams, should make this first call before doing so. A call with
+ *    count = 0 does only this set-up (and the argument checks), e.g.
+ *    nr_render_samples_static(render, 1, 0). The address is kept per device
+ *    ordinal for the rest of the process: it assumes the device's primary
+ *    context lives as long as the process (after cudaDeviceReset the library
+ *    must not be used on that device again).
  *  - Nothing in the buffer has to start at zero: the first kernel of every
  *    wave resets the queue counters the later kernels read.
  *  - There is one buffer per device per process. Calls that overlap in time

@@ -2,7 +2,7 @@
 
 `Scene` and `Render` wrap the opaque handles; every call checks the status
 code and raises RuntimeError with nr_last_error() on failure. This is the
-plain-pointer boundary a non-Python host would bind (see INTEGRATION.md);
+plain-pointer boundary a non-Python host would bind;
 the pybind11 module `_pathtracer` sits on the same functions.
 """
 from __future__ import annotations
@@ -90,7 +90,8 @@ MODE_REFERENCE = 0
 MODE_PERF = 1
 
 EXPORTS = [
-    "nr_abi_version", "nr_last_error", "nr_device_count", "nr_device_draw_order",
+    "nr_abi_version", "nr_last_error", "nr_device_count", "nr_device_memory_info",
+    "nr_device_draw_order",
     "nr_set_draw_order", "nr_scene_create", "nr_scene_destroy",
     "nr_scene_add_material", "nr_scene_add_image", "nr_scene_add_mesh", "nr_scene_get_mesh",
     "nr_scene_load_obj", "nr_scene_load_obj_device",

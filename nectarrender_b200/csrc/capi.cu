@@ -507,6 +507,17 @@ int nr_device_count(void) {
   return n;
 }
 
+int nr_device_memory_info(uint64_t* used, uint64_t* free_bytes, uint64_t* total) {
+  if (!used || !free_bytes || !total) return fail(NR_ERR_INVALID, "nr_device_memory_info: null output");
+  if (!device_available()) return fail(NR_ERR_NO_DEVICE, "no CUDA device is available");
+  size_t f = 0, t = 0;
+  CU(cudaMemGetInfo(&f, &t), "cudaMemGetInfo");
+  *used = t - f;
+  *free_bytes = f;
+  *total = t;
+  return NR_OK;
+}
+
 int nr_scene_create(nr_scene** out) {
   if (!out) return fail(NR_ERR_INVALID, "nr_scene_create: null output");
   nr_scene* s = new nr_scene();
@@ -1546,8 +1557,18 @@ static std::atomic<uintptr_t> g_static_wave_addr[64];
 
 int nr_render_samples_static(nr_render* r, uint32_t first, uint32_t count) {
   if (!r) return fail(NR_ERR_INVALID, "null render");
-  r->fused_valid = false;  // this path leaves the fused display untouched
-  if (count == 0) return NR_OK;
+  // set-up on this device (also for count == 0): the buffer's address, whose
+  // first lookup makes the driver load the module that holds the buffer
+  int dev = 0;
+  CU(cudaGetDevice(&dev), "cudaGetDevice");
+  if (dev < 0 || dev >= 64) return fail(NR_ERR_LIMIT, "device ordinal beyond 63");
+  uintptr_t addr = g_static_wave_addr[dev].load(std::memory_order_acquire);
+  if (!addr) {
+    void* p = nullptr;
+    CU(static_wave_address(&p), "cudaGetSymbolAddress(static wave buffer)");
+    addr = (uintptr_t)p;
+    g_static_wave_addr[dev].store(addr, std::memory_order_release);
+  }
   if (first == 0) return fail(NR_ERR_INVALID, "sample indices start at 1");
   if ((uint64_t)first + count > r->cam.samples_per_pixel)
     return fail(NR_ERR_INVALID, "sample index beyond samples_per_pixel");
@@ -1559,16 +1580,8 @@ int nr_render_samples_static(nr_render* r, uint32_t first, uint32_t count) {
                                   std::to_string(r->H) + " = " + std::to_string(N) +
                                   " pixels exceeds the static wave buffer's " +
                                   std::to_string(NR_STATIC_WAVE_PATHS) + " paths");
-  int dev = 0;
-  CU(cudaGetDevice(&dev), "cudaGetDevice");
-  if (dev < 0 || dev >= 64) return fail(NR_ERR_LIMIT, "device ordinal beyond 63");
-  uintptr_t addr = g_static_wave_addr[dev].load(std::memory_order_acquire);
-  if (!addr) {
-    void* p = nullptr;
-    CU(static_wave_address(&p), "cudaGetSymbolAddress(static wave buffer)");
-    addr = (uintptr_t)p;
-    g_static_wave_addr[dev].store(addr, std::memory_order_release);
-  }
+  if (count == 0) return NR_OK;
+  r->fused_valid = false;  // this path leaves the fused display untouched
   WfParams W{};
   static_wave_carve((void*)addr, W);
   KernelParams P = make_params(r, first, count, false);

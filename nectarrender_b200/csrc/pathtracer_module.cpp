@@ -24,8 +24,11 @@
 #include <cstring>
 #include <cmath>
 #include <fstream>
+#include <chrono>
 #include <memory>
+#include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/nectar_b200.h"
@@ -83,6 +86,16 @@ Matrix3 rot_euler(const Vector3& r) {
 struct Transform {
   Vector3 position{0.f}, rotation{0.f}, scale{1.f};
 };
+
+// host/include/host/utils.h:34-38
+struct CUDAMemInfo {
+  size_t used = 0, free = 0, total = 0;
+};
+CUDAMemInfo cuda_meminfo() {
+  uint64_t u = 0, f = 0, t = 0;
+  check(nr_device_memory_info(&u, &f, &t), "get_cuda_meminfo");
+  return CUDAMemInfo{(size_t)u, (size_t)f, (size_t)t};
+}
 
 // ---------------------------------------------------------------------------
 // textures and materials (material.h:453-532, texture.h:93-192)
@@ -219,6 +232,33 @@ struct Scene {
   Skylight sky;
 };
 
+// SceneNode / SceneOutline (scene/include/outliner.h:7-40): one node per
+// registry entry in registration order; name and type_name are both the
+// hittable type's name (registry.h:84), parent_id is never set (0).
+struct SceneNode {
+  size_t object_id = 0, parent_id = 0, material_id = 0;
+  bool is_light = false;
+  std::string name, type_name;
+};
+struct SceneOutline {
+  std::vector<SceneNode> nodes;
+};
+constexpr size_t kMaxOutlinerItems = 512;  // outliner.h:5 MAX_OUTLINER_ITEMS
+
+// hittabletype_to_string (hittable/include/hittable/hittable.h:17-28)
+const char* hittable_type_name(int t) {
+  switch (t) {
+    case NR_HITTABLE_NULL: return "Null";
+    case NR_HITTABLE_QUAD: return "Quad";
+    case NR_HITTABLE_SPHERE: return "Sphere";
+    case NR_HITTABLE_CUBE: return "Cube";
+    case NR_HITTABLE_MESH: return "Mesh";
+    case NR_HITTABLE_CONSTANT_MEDIUM: return "ConstantMedium";
+    case NR_HITTABLE_OBJECT_LIGHT: return "ObjectLight";
+  }
+  return "UNKNOWN";
+}
+
 nr_texture_desc tex_desc(nr_scene* s, const std::shared_ptr<Texture>& t) {
   nr_texture_desc d{};
   d.scale = 1.0f;
@@ -235,11 +275,21 @@ nr_texture_desc tex_desc(nr_scene* s, const std::shared_ptr<Texture>& t) {
   return d;
 }
 
-nr_scene* build_scene_desc(const Scene& sc) {
+// Registers the objects (hittables, then lights) and the sky in a new
+// nr_scene. `nodes` receives the outline entries and `materials` the
+// registry's materials by id (id 0: the default material).
+nr_scene* build_scene_desc(const std::vector<Hittable*>& objects, const Skylight& sky,
+                           std::vector<SceneNode>* nodes = nullptr,
+                           std::vector<Material>* materials = nullptr) {
   nr_scene* s = nullptr;
   check(nr_scene_create(&s), "Scene");
+  if (nodes) nodes->clear();
+  if (materials) {
+    materials->clear();
+    materials->push_back(make_lambertian(Texture::from_color(Color::purple())));
+  }
   try {
-    for (Hittable* h : sc.objects) {
+    for (Hittable* h : objects) {
       nr_object_desc o{};
       o.type = h->type;
       o.wrapped_type = h->wrapped_type;
@@ -270,21 +320,30 @@ nr_scene* build_scene_desc(const Scene& sc) {
         uint32_t id = 0;
         check(nr_scene_add_material(s, &m, &id), "material registry");
         o.material = (int32_t)id;
+        if (materials) materials->push_back(h->mat);
       }
       uint32_t oid = 0;
       check(nr_scene_add_object(s, &o, &oid), "hittables registry");
       h->object_id = (int)oid;
+      if (nodes) {
+        SceneNode n;
+        n.object_id = oid;
+        n.material_id = (size_t)o.material;
+        n.is_light = h->is_light();
+        n.name = n.type_name = hittable_type_name(h->type);
+        nodes->push_back(std::move(n));
+      }
     }
-    switch (sc.sky.type) {
+    switch (sky.type) {
       case SkylightType::Null: check(nr_scene_set_sky_null(s), "Skylight"); break;
       case SkylightType::Simple:
-        check(nr_scene_set_sky_simple(s, sc.sky.simple.start.e, sc.sky.simple.end.e), "Skylight");
+        check(nr_scene_set_sky_simple(s, sky.simple.start.e, sky.simple.end.e), "Skylight");
         break;
       case SkylightType::HDRI:
-        if (sc.sky.hdri_path.empty())
-          check(nr_scene_set_sky_hdri(s, nullptr, 0, 0, 0, sc.sky.hdri.rotation, sc.sky.hdri.intensity), "Skylight");
+        if (sky.hdri_path.empty())
+          check(nr_scene_set_sky_hdri(s, nullptr, 0, 0, 0, sky.hdri.rotation, sky.hdri.intensity), "Skylight");
         else
-          check(nr_scene_load_hdr(s, sc.sky.hdri_path.c_str(), sc.sky.hdri.rotation, sc.sky.hdri.intensity),
+          check(nr_scene_load_hdr(s, sky.hdri_path.c_str(), sky.hdri.rotation, sky.hdri.intensity),
                 "Skylight.hdri");
         break;
     }
@@ -431,14 +490,28 @@ struct HitRecord {
   bool hit = false;
 };
 
-// SceneInterface's picking and selection (scene/include/interface.h:60-71,
-// 193-199): query_scene(u, v) casts the screen-space ray and keeps the hit.
+// SceneInterface (scene/include/interface.h:36-200): picking and selection
+// (query_scene casts the screen-space ray and keeps the hit), the scene
+// outline, and edits of the selected object, the sky and the object list.
+// Edits change the engine's copy of the scene and request a restart; the
+// render loop rebuilds the device scene before its next sample, where the
+// reference marks the registry entry dirty and rebuilds in its update step.
 struct SceneInterface {
   EngineCore* eng = nullptr;
   HitRecord rec;
   std::atomic<bool> enabled{false};
   int outline_radius = 2;
   void query_scene(float u, float v);
+  void select_scene_node(const SceneNode& n);
+  SceneOutline get_scene_outline() const;
+  Transform get_transform() const;
+  void set_transform(const Transform& x);
+  Material& get_material();
+  void set_material(const Material& m);
+  void add_object(const Hittable& h);
+  Skylight& get_skylight();
+  void request_skylight_update();
+  void swap_skylight(const Skylight& sky);
   py::array selection_mask() const;
 };
 
@@ -457,6 +530,14 @@ struct EngineCore {
   SceneInterface scene_interface;
   int mode = NR_MODE_REFERENCE;
   bool hooks_set = false;
+  // the scene as last set or edited: objects (hittables, then lights), sky,
+  // the outline and the material registry built from them
+  std::mutex scene_mu;
+  std::vector<Hittable> objects;
+  Skylight sky;
+  std::vector<SceneNode> nodes;
+  std::vector<Material> materials;
+  std::atomic<bool> scene_dirty{false};
   std::function<void()> on_render_started = [] {}, on_render_finished = [] {}, on_stopped = [] {},
                         on_restarted = [] {}, on_reset = [] {}, on_shutdown = [] {};
   std::function<void(uint32_t)> on_frame_finished = [](uint32_t) {};
@@ -504,6 +585,38 @@ struct EngineCore {
     check(nr_render_create(scene, &d, &cfg, &render), "RenderEngine");
     sample_idx = 1;
   }
+  // Builds the device scene from `objects` and `sky` and replaces the
+  // current one (and its render). Called with the GIL released.
+  void rebuild_scene() {
+    std::vector<Hittable*> ptrs;
+    std::vector<SceneNode> new_nodes;
+    std::vector<Material> new_mats;
+    nr_scene* s = nullptr;
+    {
+      std::lock_guard<std::mutex> lk(scene_mu);
+      for (Hittable& h : objects) ptrs.push_back(&h);
+      s = build_scene_desc(ptrs, sky, &new_nodes, &new_mats);
+    }
+    int rc = nr_scene_build(s);
+    if (rc != NR_OK) {
+      std::string msg = nr_last_error();
+      nr_scene_destroy(s);
+      throw std::runtime_error("RenderEngine.set_scene: " + msg);
+    }
+    if (render) { nr_render_destroy(render); render = nullptr; }
+    if (scene) nr_scene_destroy(scene);
+    scene = s;
+    {
+      std::lock_guard<std::mutex> lk(scene_mu);
+      nodes = std::move(new_nodes);
+      materials = std::move(new_mats);
+    }
+    make_render();
+  }
+  // Scene edits made through the SceneInterface since the last sample.
+  void apply_scene_edits() {
+    if (scene_dirty.exchange(false)) rebuild_scene();
+  }
   // RenderEngine::reset (engine.cpp:216-220): the next sample is 1, whose
   // running mean overwrites the layers; they are not cleared (a viewport
   // frame or a stopped render stays visible until then).
@@ -516,6 +629,7 @@ struct EngineCore {
   // layers; returns 3 (waiting for the next refresh), 1 stopped, 2 restarted.
   int run_viewport() {
     if (!render) throw std::runtime_error("RenderEngine.render() called before set_scene()");
+    apply_scene_edits();
     EnginePollResponse resp;
     {
       py::gil_scoped_acquire gil;
@@ -533,6 +647,7 @@ struct EngineCore {
   // RenderEngine::render (engine.cpp:42-74): samples sample_idx .. n-1
   int run() {
     if (!render) throw std::runtime_error("RenderEngine.render() called before set_scene()");
+    apply_scene_edits();
     uint32_t n = cam.p.samples_per_pixel;
     if (!hooks_set && sample_idx < n) {
       int rc = nr_render_samples(render, sample_idx, n - sample_idx);
@@ -552,6 +667,7 @@ struct EngineCore {
         make_render();
         requests.restart();
       }
+      apply_scene_edits();
       check(nr_render_samples(render, sample_idx, 1), "RenderEngine.render");
       sample_idx++;
       {
@@ -582,12 +698,93 @@ void SceneInterface::query_scene(float u, float v) {
   }
 }
 
+void SceneInterface::select_scene_node(const SceneNode& n) {
+  rec.object_id = n.object_id;
+  rec.material_id = n.material_id;
+  enabled = true;
+}
+
+// SceneOutliner::build_outline (outliner.h:48-66) with SceneOutline's limit
+SceneOutline SceneInterface::get_scene_outline() const {
+  if (!eng) throw std::runtime_error("get_scene_outline() before set_scene()");
+  std::lock_guard<std::mutex> lk(eng->scene_mu);
+  if (eng->nodes.size() > kMaxOutlinerItems)
+    throw std::runtime_error("SceneOutline exceeded maximum node count [" +
+                             std::to_string(kMaxOutlinerItems) + "].");
+  return SceneOutline{eng->nodes};
+}
+
+static Hittable& selected_object(EngineCore* eng, size_t id) {
+  if (!eng || id >= eng->objects.size()) throw std::runtime_error("Object index not valid.");
+  return eng->objects[id];
+}
+
+Transform SceneInterface::get_transform() const {
+  std::lock_guard<std::mutex> lk(eng->scene_mu);
+  const Hittable& h = selected_object(eng, rec.object_id);
+  Transform t;
+  t.position = h.position;
+  t.rotation = h.rotation;
+  t.scale = h.scale;
+  return t;
+}
+
+void SceneInterface::set_transform(const Transform& x) {
+  {
+    std::lock_guard<std::mutex> lk(eng->scene_mu);
+    Hittable& h = selected_object(eng, rec.object_id);
+    h.position = x.position;
+    h.rotation = x.rotation;
+    h.scale = x.scale;
+  }
+  eng->scene_dirty = true;
+  eng->requests.restart();
+}
+
+Material& SceneInterface::get_material() {
+  std::lock_guard<std::mutex> lk(eng->scene_mu);
+  if (rec.material_id >= eng->materials.size()) throw std::runtime_error("Material index not valid.");
+  return eng->materials[rec.material_id];
+}
+
+// The reference's set_material only requests a restart; its registry update
+// is commented out (interface.h:154-159).
+void SceneInterface::set_material(const Material&) { eng->requests.restart(); }
+
+void SceneInterface::add_object(const Hittable& h) {
+  {
+    std::lock_guard<std::mutex> lk(eng->scene_mu);
+    if (eng->objects.size() >= NR_MAX_OBJECTS)
+      throw std::runtime_error("Hittables registry exceeded maximum registry entries [" +
+                               std::to_string(NR_MAX_OBJECTS) + "]. Exiting...");
+    eng->objects.push_back(h);
+  }
+  eng->scene_dirty = true;
+  eng->requests.restart();
+}
+
+Skylight& SceneInterface::get_skylight() { return eng->sky; }
+
+void SceneInterface::request_skylight_update() {
+  eng->scene_dirty = true;
+  eng->requests.restart();
+}
+
+void SceneInterface::swap_skylight(const Skylight& sky) {
+  {
+    std::lock_guard<std::mutex> lk(eng->scene_mu);
+    eng->sky = sky;
+  }
+  eng->scene_dirty = true;
+  eng->requests.restart();
+}
+
 py::array SceneInterface::selection_mask() const {
   if (!eng || !eng->render) throw std::runtime_error("selection mask before set_scene()");
   py::array_t<uint8_t> out({(size_t)eng->H(), (size_t)eng->W()});
   check(nr_render_selection_mask(eng->render, (uint32_t)rec.object_id, outline_radius,
                                  out.mutable_data()),
-        "SceneInterface.get_scene_outline");
+        "SceneInterface.selection_mask");
   return std::move(out);
 }
 
@@ -626,6 +823,46 @@ uintptr_t TransferStream::readback() {
 }
 std::array<size_t, 3> TransferStream::shape() const {
   return {3, (size_t)eng->H(), (size_t)eng->W()};
+}
+
+// Not in the reference: a hittable's and a sky's settings as stored, for
+// tools that convert a scene built through this API into another form.
+py::tuple v3_tuple(const Vector3& v) { return py::make_tuple(v.e[0], v.e[1], v.e[2]); }
+
+py::dict describe_hittable(const Hittable& h) {
+  py::dict d, m;
+  d["type"] = h.type;
+  d["wrapped_type"] = h.wrapped_type;
+  d["position"] = v3_tuple(h.position);
+  d["rotation"] = v3_tuple(h.rotation);
+  d["scale"] = v3_tuple(h.scale);
+  d["radius"] = h.radius;
+  d["density"] = h.density;
+  d["mesh_path"] = h.mesh_path;
+  m["type"] = (int)h.mat.type;
+  m["ior"] = h.mat.ior;
+  m["brightness"] = h.mat.brightness;
+  m["tint"] = v3_tuple(h.mat.tint);
+  py::list tex;
+  for (auto& t : h.mat.tex) {
+    if (!t) tex.append(py::make_tuple(0.f, 0.f, 0.f));
+    else if (t->type == TextureType::IMAGE) tex.append(py::str(t->filepath));
+    else tex.append(v3_tuple(t->constant_color));
+  }
+  m["tex"] = tex;
+  d["material"] = m;
+  return d;
+}
+
+py::dict describe_sky(const Skylight& s) {
+  py::dict d;
+  d["type"] = (int)s.type;
+  d["start"] = v3_tuple(s.simple.start);
+  d["end"] = v3_tuple(s.simple.end);
+  d["path"] = s.hdri_path;
+  d["rotation"] = s.hdri.rotation;
+  d["intensity"] = s.hdri.intensity;
+  return d;
 }
 
 }  // namespace
@@ -704,8 +941,21 @@ PYBIND11_MODULE(_pathtracer, m) {
   m_cuda.def("destroy_cublas_handle", []() {});
   m_cuda.def("cudaDeviceSynchronize", []() {});
   auto m_host = m.def_submodule("host", "Host module.");
-  m_host.def_submodule("memory", "Memory utils submodule.");
+  auto m_memory = m_host.def_submodule("memory", "Memory utils submodule.");
   m_host.def_submodule("devtools", "Devtools submodule.");
+  // CUDAMemInfo and its getters (host/include/host/utils.h:34-42)
+  py::class_<CUDAMemInfo>(m_memory, "CUDAMemInfo")
+      .def_readonly("used", &CUDAMemInfo::used)
+      .def_readonly("free", &CUDAMemInfo::free)
+      .def_readonly("total", &CUDAMemInfo::total)
+      .def("__repr__", [](const CUDAMemInfo& i) {
+        return "CUDAMemInfo(used=" + std::to_string(i.used) + ", free=" + std::to_string(i.free) +
+               ", total=" + std::to_string(i.total) + ")";
+      });
+  m_memory.def("get_cuda_meminfo", &cuda_meminfo);
+  m_memory.def("get_cuda_memory_used", []() { return cuda_meminfo().used; });
+  m_memory.def("get_cuda_memory_free", []() { return cuda_meminfo().free; });
+  m_memory.def("get_cuda_memory_total", []() { return cuda_meminfo().total; });
 
   // ---- material
   auto m_material = m.def_submodule("material", "Material module.");
@@ -884,7 +1134,10 @@ PYBIND11_MODULE(_pathtracer, m) {
                   },
                   py::arg("bound_obj"), py::arg("brightness") = 1.0f, py::arg("albedo") = Color(1.f, 1.f, 1.f))
       .def("is_light", &Hittable::is_light)
-      .def("get_object_id", [](const Hittable& h) { return h.object_id; });
+      .def("get_object_id", [](const Hittable& h) { return h.object_id; })
+      // not in the reference: the factory arguments as stored, for tools
+      // that convert a scene built through this API into another form
+      .def("describe", &describe_hittable);
 
   // ---- light
   auto m_light = m.def_submodule("light", "Lights module.");
@@ -927,7 +1180,9 @@ PYBIND11_MODULE(_pathtracer, m) {
              s.hdri_path = path;
            })
       .def("config_simple", [](Skylight& s) -> SimpleSkylightConfig& { return s.simple; }, py::return_value_policy::reference_internal)
-      .def("config_hdri", [](Skylight& s) -> HDRISkylightConfig& { return s.hdri; }, py::return_value_policy::reference_internal);
+      .def("config_hdri", [](Skylight& s) -> HDRISkylightConfig& { return s.hdri; }, py::return_value_policy::reference_internal)
+      // not in the reference: the sky's settings as stored
+      .def("describe", &describe_sky);
 
   // ---- scene
   auto m_scene = m.def_submodule("scene", "Scene module.");
@@ -940,17 +1195,48 @@ PYBIND11_MODULE(_pathtracer, m) {
              return s;
            }),
            py::arg("hittables"), py::arg("lights"), py::arg("skylight"), py::keep_alive<1, 2>(),
-           py::keep_alive<1, 3>());
+           py::keep_alive<1, 3>())
+      // not in the reference: the registered objects (hittables, then
+      // lights) and the sky, as describe() dicts
+      .def("describe", [](const Scene& sc) {
+        py::dict d;
+        py::list objs;
+        for (Hittable* h : sc.objects) objs.append(describe_hittable(*h));
+        d["objects"] = objs;
+        d["sky"] = describe_sky(sc.sky);
+        return d;
+      });
+
+  py::class_<SceneNode>(m_scene, "SceneNode")
+      .def_readonly("object_id", &SceneNode::object_id)
+      .def_readonly("parent_id", &SceneNode::parent_id)
+      .def_readonly("material_id", &SceneNode::material_id)
+      .def_readonly("name", &SceneNode::name)
+      .def_readonly("type_name", &SceneNode::type_name);
+  py::class_<SceneOutline>(m_scene, "SceneOutline")
+      .def_readonly("nodes", &SceneOutline::nodes);
 
   py::class_<SceneInterface>(m_scene, "SceneInterface")
+      .def("set_material", &SceneInterface::set_material, py::arg("mat"))
+      .def("add_object", &SceneInterface::add_object, py::arg("obj"))
       .def("query_scene", &SceneInterface::query_scene, py::arg("u"), py::arg("v"))
-      .def("get_hit_record", [](SceneInterface& si) -> HitRecord& { return si.rec; },
-           py::return_value_policy::reference_internal)
+      .def("select_scene_node", &SceneInterface::select_scene_node, py::arg("node"))
       .def("enable", [](SceneInterface& si) { si.enabled = true; })
       .def("disable", [](SceneInterface& si) { si.enabled = false; })
       .def("is_enabled", [](SceneInterface& si) { return si.enabled.load(); })
       .def("is_disabled", [](SceneInterface& si) { return !si.enabled.load(); })
-      .def("get_scene_outline", &SceneInterface::selection_mask);
+      .def("get_scene_outline", &SceneInterface::get_scene_outline)
+      .def("get_transform", &SceneInterface::get_transform)
+      .def("set_transform", &SceneInterface::set_transform)
+      .def("get_material", &SceneInterface::get_material, py::return_value_policy::reference_internal)
+      .def("get_hit_record", [](SceneInterface& si) -> HitRecord& { return si.rec; },
+           py::return_value_policy::reference_internal)
+      .def("request_skylight_update", &SceneInterface::request_skylight_update)
+      .def("get_skylight", &SceneInterface::get_skylight, py::return_value_policy::reference_internal)
+      .def("swap_skylight", &SceneInterface::swap_skylight, py::arg("new_skylight"))
+      // not in the reference (its mask goes straight into the stream's
+      // overlay): the selection outline as an H x W uint8 mask
+      .def("selection_mask", &SceneInterface::selection_mask);
 
   // ---- data
   auto m_data = m.def_submodule("data", "Data module.");
@@ -1098,21 +1384,19 @@ PYBIND11_MODULE(_pathtracer, m) {
            py::arg("camera"), py::arg("ray_depth") = 8u, py::arg("seed") = 54321u)
       .def("set_scene",
            [](EngineCore& e, const Scene& sc) {
-             nr_scene* s = build_scene_desc(sc);
-             int rc;
+             {
+               std::lock_guard<std::mutex> lk(e.scene_mu);
+               e.objects.clear();
+               for (Hittable* h : sc.objects) e.objects.push_back(*h);
+               e.sky = sc.sky;
+             }
+             e.scene_dirty = false;
              {
                py::gil_scoped_release nogil;
-               rc = nr_scene_build(s);
+               e.rebuild_scene();
              }
-             if (rc != NR_OK) {
-               std::string msg = nr_last_error();
-               nr_scene_destroy(s);
-               throw std::runtime_error("RenderEngine.set_scene: " + msg);
-             }
-             if (e.render) { nr_render_destroy(e.render); e.render = nullptr; }
-             if (e.scene) nr_scene_destroy(e.scene);
-             e.scene = s;
-             e.make_render();
+             // registry ids back onto the caller's objects (Hittable.get_object_id)
+             for (size_t i = 0; i < sc.objects.size(); ++i) sc.objects[i]->object_id = (int)i;
              e.stream.state = StreamState::ACTIVE;
            })
       .def("render",

@@ -420,6 +420,78 @@ def to_pathtracer(spec: SceneSpec, pt=None):
     return scene, cam, (hittables, lights, sky)
 
 
+def from_pathtracer(scene, camera, ray_depth: int, seed: int, name: str = "") -> SceneSpec:
+    """The SceneSpec of a scene built with the `_pathtracer` factories
+    (``Scene(hittables, lights, skylight)``, ``Camera(params)``), read back
+    through ``Scene.describe()``; the inverse of ``to_pathtracer``. Values
+    are the stored float32 ones."""
+    meshes: list[str] = []
+    objects = []
+    desc = scene.describe()
+    for d in desc["objects"]:
+        m = d["material"]
+        tex = [tuple(t) if not isinstance(t, str) else t for t in m["tex"]]
+        mat = {"type": m["type"], "ior": m["ior"], "brightness": m["brightness"],
+               "tint": tuple(m["tint"]), "tex": tex}
+        base = d["wrapped_type"] or d["type"]
+        mesh = -1
+        if base == MESH:
+            if d["mesh_path"] not in meshes:
+                meshes.append(d["mesh_path"])
+            mesh = meshes.index(d["mesh_path"])
+        objects.append(obj(d["type"], mat, d["position"], d["rotation"], d["scale"], d["radius"],
+                           mesh=mesh, wrapped=d["wrapped_type"], density=d["density"]))
+    s = desc["sky"]
+    if s["type"] == SKY_SIMPLE:
+        sky = {"type": SKY_SIMPLE, "start": tuple(s["start"]), "end": tuple(s["end"])}
+    elif s["type"] == SKY_HDRI:
+        sky = {"type": SKY_HDRI, "path": s["path"], "rotation": s["rotation"],
+               "intensity": s["intensity"]}
+    else:
+        sky = {"type": SKY_NULL}
+    p = camera.parameters()
+    cam = {"resolution": (p.resolution.x(), p.resolution.y()),
+           "position": (p.position.x(), p.position.y(), p.position.z()),
+           "rotation": (p.rotation.x(), p.rotation.y(), p.rotation.z()),
+           "samples_per_pixel": int(p.samples_per_pixel), "focal_length": p.focal_length,
+           "focus_distance": p.focus_distance, "aperture": p.aperture,
+           "sensor_width": p.sensor_width, "shutter_speed": p.shutter_speed}
+    return SceneSpec(objects=objects, camera=cam, ray_depth=int(ray_depth), seed=int(seed),
+                     sky=sky, meshes=meshes, name=name)
+
+
+def spec_to_json(spec: SceneSpec) -> dict:
+    """A JSON-ready dict of a spec (tuples become lists)."""
+    import dataclasses
+    return json_ready(dataclasses.asdict(spec))
+
+
+def json_ready(x):
+    if isinstance(x, dict):
+        return {k: json_ready(v) for k, v in x.items()}
+    if isinstance(x, (list, tuple)):
+        return [json_ready(v) for v in x]
+    return x
+
+
+def spec_from_json(d: dict) -> SceneSpec:
+    """Inverse of spec_to_json (lists become tuples where the spec has tuples)."""
+    def tup(v):
+        return tuple(tup(x) for x in v) if isinstance(v, list) else v
+    objects = []
+    for o in d["objects"]:
+        o = {k: tup(v) if k != "material" else v for k, v in o.items()}
+        m = dict(o["material"])
+        m["tint"] = tuple(m["tint"])
+        m["tex"] = [tuple(t) if isinstance(t, list) else t for t in m["tex"]]
+        o["material"] = m
+        objects.append(o)
+    cam = {k: tup(v) for k, v in d["camera"].items()}
+    sky = {k: tup(v) for k, v in d["sky"].items()}
+    return SceneSpec(objects=objects, camera=cam, ray_depth=d["ray_depth"], seed=d["seed"],
+                     sky=sky, meshes=list(d["meshes"]), name=d.get("name", ""))
+
+
 def scene_set(n: int = 16, seed: int = 0, max_level: int = 6) -> list[SceneSpec]:
     """A seeded set of small scenes of mixed size for the multi-scene
     workload: Cornell boxes and mesh-stress scenes (icosphere levels 3 to

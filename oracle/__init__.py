@@ -13,36 +13,76 @@ it.
   sm_100a.
 
 Parity is pinned: the restatement is compared bit for bit with RefCPU on the
-same seeded scenes (tests/test_oracle_pin.py), and RefCPU/RefCUDA are the
-reference code.
+same seeded scenes and with fixtures generated from it
+(tests/test_oracle_golden.py), and RefCPU/RefCUDA are the reference code.
+
+Nothing here loads the product library (libnectar_b200.so): the descriptor
+structs below are plain ctypes layouts, and render settings are filled from
+this module's own copy of the defaults, so timing a checker never maps the
+product. The reference sources are located by the NECTAR_REFERENCE
+environment variable (the reference project root); without it only the
+prebuilt checkers are used.
 """
 from __future__ import annotations
 
 import ctypes as C
+import os
 import subprocess
 from pathlib import Path
 
 import numpy as np
 
+# plain ctypes layouts of include/nectar_b200.h (importing them loads no library)
 from nectarrender_b200.capi import CameraDesc, MaterialDesc, ObjectDesc, RenderConfig
-from nectarrender_b200.capi import camera_desc, material_desc, object_desc, render_config
+from nectarrender_b200.capi import camera_desc, material_desc, object_desc
 from nectarrender_b200.scenes import SKY_HDRI, SKY_SIMPLE, SceneSpec
 
 HERE = Path(__file__).resolve().parent
 ORACLE_SO = HERE / "liboracle.so"
 REF_CPU_SO = HERE / "_ref" / "libref_cpu.so"
 REF_CUDA_SO = HERE / "_ref" / "libref_cuda.so"
-REF_SRC = Path("/root/reference/nectar_render/csrc")
+
+# nr_render_config_default (include/nectar_b200.h); tests check that the two agree
+RENDER_CONFIG_DEFAULTS = {"ray_depth": 8, "seed": 54321, "rr_enabled": 1, "rr_start_bounce": 3,
+                          "rr_survival": 0.95, "mode": 0, "schedule": 1, "fp64_accumulate": 0,
+                          "layer_mask": (1 << 0) | (1 << 1) | (1 << 4), "extend_variant": 0,
+                          "samples_per_wave": 0, "use_graphs": 1, "tail_max_paths": 0,
+                          "shade_variant": 0, "sort_materials": 0}
 
 
-def build(reference: bool | None = None) -> None:
-    """make -C oracle (reference targets only where the reference sources exist)."""
+def render_config(spec: SceneSpec, **over) -> RenderConfig:
+    """The render settings of `spec` over the library defaults."""
+    cfg = RenderConfig()
+    for k, v in RENDER_CONFIG_DEFAULTS.items():
+        setattr(cfg, k, v)
+    cfg.ray_depth = spec.ray_depth
+    cfg.seed = spec.seed
+    for k, v in over.items():
+        setattr(cfg, k, v)
+    return cfg
+
+
+def reference_sources(root: str | os.PathLike | None = None) -> Path | None:
+    """The reference's csrc tree under `root` (default: $NECTAR_REFERENCE), or
+    None where it is absent."""
+    root = root if root is not None else os.environ.get("NECTAR_REFERENCE")
+    if not root:
+        return None
+    src = Path(root) / "nectar_render" / "csrc"
+    return src if src.exists() else None
+
+
+def build(reference_root: str | os.PathLike | None = None) -> None:
+    """make -C oracle: the restatement, and the reference's CPU and CUDA
+    builds where the reference sources exist under `reference_root` (default:
+    $NECTAR_REFERENCE)."""
     targets = [str(ORACLE_SO)]
-    if reference is None:
-        reference = REF_SRC.exists()
-    if reference:
+    src = reference_sources(reference_root)
+    extra = []
+    if src is not None:
         targets += [str(REF_CPU_SO), str(REF_CUDA_SO)]
-    r = subprocess.run(["make", "-C", str(HERE), *targets], capture_output=True, text=True)
+        extra = [f"REF={src}"]
+    r = subprocess.run(["make", "-C", str(HERE), *extra, *targets], capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError("oracle build failed:\n" + r.stdout[-4000:] + r.stderr[-4000:])
 

@@ -21,5 +21,5 @@ def built():
         from nectarrender_b200 import build
         build.build_all()
     if not oracle.ORACLE_SO.exists():
-        oracle.build(reference=False)
+        oracle.build(reference_root="")
     yield

@@ -14,7 +14,7 @@ GOLDEN = Path(__file__).parent / "golden"
 
 @pytest.fixture(scope="module")
 def orc():
-    oracle.build(reference=False)
+    oracle.build(reference_root="")
     return oracle.Oracle()
 
 

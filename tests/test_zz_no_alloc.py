@@ -10,6 +10,7 @@ from nectarrender_b200 import capi, last_error, scenes
 pytestmark = pytest.mark.gpu
 
 NR_ERR_LIMIT = -3
+NR_ERR_STATE = -6
 NR_STATIC_WAVE_PATHS = 270528
 LAYERS = (0, 1, 4)  # beauty, diffuse, world normal
 
@@ -62,3 +63,29 @@ def test_static_rejects_images_beyond_the_buffer():
     msg = last_error()
     assert str(NR_STATIC_WAVE_PATHS) in msg and "544x544" in msg
     assert r.lib.nr_render_samples_static(r.h, 0, 1) != 0  # sample indices start at 1
+
+
+def test_static_call_allocates_no_device_memory():
+    import torch
+    spec = scenes.cornell(res=256, spp=8, depth=8, seed=2)
+    sc = capi.Scene(spec)
+    warm = capi.Render(sc, tail_max_paths=TAIL_OFF)
+    # set-up call (count 0): loads the buffer's module on this device
+    assert warm.lib.nr_render_samples_static(warm.h, 1, 0) == 0, last_error()
+    assert warm.lib.nr_render_samples_static(warm.h, 1, 2) == 0, last_error()
+    fresh = capi.Render(sc, tail_max_paths=TAIL_OFF)
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    assert fresh.lib.nr_render_samples_static(fresh.h, 1, 4) == 0, last_error()
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+    assert fresh.layer(0).mean() > 0
+
+
+def test_static_renders_reference_mode_only():
+    spec = scenes.cornell(res=32, spp=3, depth=4, seed=0)
+    sc = capi.Scene(spec)
+    r = capi.Render(sc, mode=capi.MODE_PERF)
+    assert r.lib.nr_render_samples_static(r.h, 1, 1) == NR_ERR_STATE
+    assert "NR_MODE_REFERENCE" in last_error()
