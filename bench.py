@@ -239,9 +239,11 @@ def run_ours(args):
     scene = capi.Scene(spec, mesh_leaf=args.mesh_leaf)
     build_wall = time.perf_counter() - t_build
     stats = scene.stats()
+    # FP64 sums of beauty ride along (3 doubles per pixel per wave): N > 1
+    # ranks combine them into the image of every rank's sample indices
     render = capi.Render(scene, schedule=1 if args.schedule == "wavefront" else 0,
                          extend_variant=args.extend_variant, shade_variant=args.shade_variant,
-                         sort_materials=args.sort_materials)
+                         sort_materials=args.sort_materials, fp64_accumulate=1)
     stream_handle = ctypes.c_uint64()
     lib.nr_render_stream(render.h, ctypes.byref(stream_handle))
     stream = torch.cuda.ExternalStream(stream_handle.value)
@@ -274,6 +276,9 @@ def run_ours(args):
             ev[k][1].record(stream)
         torch.cuda.synchronize()
     graphs = render.graph_stats()
+    # this rank's FP64 sum over the sample indices it rendered so far (each
+    # index once): combined across ranks after the profiling pass below
+    rank_sum, rank_n = render.beauty_fp64_sum()
     # Per-kernel device time: the same steps again with an event recorded
     # after every launch on the render stream (direct launches instead of
     # the wave graphs, so that each kernel is bracketed by events).
@@ -302,15 +307,20 @@ def run_ours(args):
     samples = float(w * h * S * args.steps * world)
     value = samples / (t_ms * 1e-3)
 
-    # combine the ranks' accumulators once (after timing)
+    # combine the ranks' FP64 sums once (after timing): one NCCL sum of the
+    # sums and of the sample counts, then the mean over every rank's samples
     combine_ms = None
     if dist:
-        img = torch.from_numpy(render.layer(0)).cuda()
+        from nectarrender_b200.sharding import combine_sums
+        img = torch.from_numpy(rank_sum).cuda()
+        cnt = torch.tensor([rank_n], dtype=torch.float64, device="cuda")
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        dist.all_reduce(img)
+        dist.all_reduce(cnt)
+        combined = combine_sums(img, int(cnt.item()), dist.all_reduce)
         torch.cuda.synchronize()
         combine_ms = 1e3 * (time.perf_counter() - t0)
+        del combined
 
     # Roofline of the dominant kernel from counted record fetches. Per ray
     # query: wide nodes 80 B, triangle records 48 B, object records 128 B,
@@ -361,7 +371,10 @@ def run_ours(args):
 
     ref_cuda = None
     if rank == 0 and not args.no_reference_cuda:
-        ref_cuda = reference_cuda_rate(spec, w, h)
+        ref_cuda = reference_cuda_rate(spec, args, local)
+        if "value" in ref_cuda:
+            # per GPU: this arm's value over N GPUs against the reference on one
+            ref_cuda["ratio"] = value / world / ref_cuda["value"]
 
     rmse = None
     if rank == 0 and world == 1 and not args.no_rmse:
@@ -950,20 +963,32 @@ def padded_for_reference_cuda(spec):
     return s, h * w
 
 
-def reference_cuda_rate(spec, w, h):
-    """The reference's CUDA path (sm_100a build) on the same scene: 2 samples,
-    its render loop timed with CUDA events (at the image size rounded up to
-    multiples of 16, counting the pixels it renders)."""
+def reference_cuda_rate(spec, args, gpu: int):
+    """The reference's CUDA path (sm_100a build of its trace_full +
+    accumulate loop) on the same scene and the same step shape as this
+    arm: `args.warmup` untimed steps, then `args.steps` steps of
+    `args.spp_per_step` sample indices, each timed with CUDA events, L2
+    overwritten between steps, SM clocks sampled meanwhile. The image is
+    rendered at the size rounded up to multiples of 16 (its kernels need
+    whole 16x16 blocks), counting the pixels it renders."""
     try:
+        import copy
         import oracle
         rc = oracle.RefCUDA()
         rspec, pixels = padded_for_reference_cuda(spec)
-        res = rc.render(rspec, 1, count=2, mode=1)
-        ms = res[3]
+        S = args.spp_per_step
+        rspec = copy.deepcopy(rspec)
+        rspec.camera["samples_per_pixel"] = max(rspec.camera["samples_per_pixel"],
+                                                1 + (args.warmup + args.steps) * S)
+        with Clocks(gpu) as clk:
+            step_ms = rc.time_steps(rspec, 1, args.warmup, args.steps, S)
+        t = sum(step_ms) * 1e-3
         rh, rw = (int(x) for x in rspec.camera["resolution"])
-        return {"value": pixels * 2 / (ms * 1e-3), "unit": "samples/s", "samples": 2,
+        return {"value": pixels * S * args.steps / t, "unit": "samples/s",
+                "samples": pixels * S * args.steps, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": 1e3 * t / args.steps, "clocks": clk.summary(),
                 "note": f"reference trace_full + accumulate loop compiled for sm_100a, same scene "
-                        f"rendered at {rw}x{rh}"}
+                        f"rendered at {rw}x{rh}, L2 overwritten between steps"}
     except Exception as e:  # noqa: BLE001 - reported, not fatal
         return {"unavailable": repr(e)[:200]}
 

@@ -185,6 +185,14 @@ typedef struct nr_render_config {
                                extend kernel counts the keys, one pass sorts
                                the queue; 1 = on, negative = off, 0 = default
                                (on)                                         */
+  uint32_t max_traversal_steps;   /* bound on the steps of one BVH traversal;
+                                     reaching it ends that query and sets
+                                     error bit 8 (the call returns
+                                     NR_ERR_DEVICE): 0 = default (2^20)     */
+  uint32_t traversal_stack_limit; /* bound on the entries of a traversal
+                                     stack (below each kernel's own depth);
+                                     a push past it is dropped and sets
+                                     error bit 1: 0 = no extra bound        */
 } nr_render_config;
 
 /* StreamConfig display fields (nectar_render/csrc/data/include/data/stream.h:13-30). */
@@ -422,8 +430,14 @@ int nr_render_sample_layers(nr_render* render, uint32_t sample_idx, float* beaut
 int nr_render_layer_device_ptr(nr_render* render, int32_t layer, uint64_t* out_ptr);
 /* Copies an accumulated layer to a host float CHW buffer of C*H*W floats. */
 int nr_render_read_layer(nr_render* render, int32_t layer, float* host_chw);
-/* FP64 running sum of beauty (when fp64_accumulate), divided by the count. */
+/* FP64 sum of beauty (when fp64_accumulate) over every sample rendered since
+ * the render was created or reset, divided by the number of those samples:
+ * their mean, whatever sample indices they had (a rank's shard of sample
+ * indices gives the mean of its shard). */
 int nr_render_read_beauty_fp64(nr_render* render, double* host_chw);
+/* The same FP64 sum undivided, and the number of samples in it: what a rank
+ * rendering a shard of sample indices contributes to a sum over ranks. */
+int nr_render_read_beauty_fp64_sum(nr_render* render, double* host_chw, uint64_t* n_samples);
 /* Display transform of a layer (process_stream_kernel, stream.cu:146-159):
  * white balance -> tonemap -> sqrt gamma -> clamp -> uint8 CHW, into host memory. */
 int nr_render_readback(nr_render* render, int32_t layer, const nr_stream_config* cfg,

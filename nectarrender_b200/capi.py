@@ -46,7 +46,8 @@ class RenderConfig(C.Structure):
                 ("schedule", C.c_int32), ("fp64_accumulate", C.c_int32), ("layer_mask", C.c_uint32),
                 ("extend_variant", C.c_int32), ("samples_per_wave", C.c_uint32),
                 ("use_graphs", C.c_int32), ("tail_max_paths", C.c_uint32),
-                ("shade_variant", C.c_int32), ("sort_materials", C.c_int32)]
+                ("shade_variant", C.c_int32), ("sort_materials", C.c_int32),
+                ("max_traversal_steps", C.c_uint32), ("traversal_stack_limit", C.c_uint32)]
 
 
 class StreamConfig(C.Structure):
@@ -109,7 +110,7 @@ EXPORTS = [
     "nr_denoiser_layers", "nr_nrc_create", "nr_nrc_destroy", "nr_nrc_infer", "nr_nrc_train",
     "nr_nrc_count", "nr_nrc_get", "nr_nrc_set", "nr_render_set_nrc", "nr_render_nrc_stats",
     "nr_render_sample_layers", "nr_render_layer_device_ptr", "nr_render_read_layer",
-    "nr_render_read_beauty_fp64", "nr_render_readback", "nr_render_display_float",
+    "nr_render_read_beauty_fp64", "nr_render_read_beauty_fp64_sum", "nr_render_readback", "nr_render_display_float",
     "nr_render_dims", "nr_render_set_counters", "nr_render_get_counters", "nr_render_last_ms",
     "nr_render_stream", "nr_accumulate_device", "nr_display_device",
 ]
@@ -327,6 +328,15 @@ class Render:
         _check(self.lib.nr_render_read_beauty_fp64(self.h, out.ctypes.data_as(C.POINTER(C.c_double))),
                "nr_render_read_beauty_fp64")
         return out
+
+    def beauty_fp64_sum(self) -> tuple[np.ndarray, int]:
+        """(FP64 sum of beauty over the samples since the last reset, their count)."""
+        out = np.zeros((3, self.H, self.W), np.float64)
+        n = C.c_uint64()
+        _check(self.lib.nr_render_read_beauty_fp64_sum(
+            self.h, out.ctypes.data_as(C.POINTER(C.c_double)), C.byref(n)),
+            "nr_render_read_beauty_fp64_sum")
+        return out, int(n.value)
 
     def readback(self, layer: int = 0, cfg: StreamConfig | None = None) -> np.ndarray:
         out = np.zeros((3, self.H, self.W), np.uint8)

@@ -45,6 +45,11 @@ static int fail(int code, const std::string& msg) {
   g_last_error = msg;
   return code;
 }
+static std::string hex_word(uint32_t w) {
+  char b[16];
+  snprintf(b, sizeof(b), "%x", w);
+  return b;
+}
 static int cuda_fail(cudaError_t e, const char* what) {
   return fail(NR_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
@@ -559,6 +564,16 @@ int nr_scene_add_image(nr_scene* s, const uint8_t* chw, uint32_t C, uint32_t H, 
   return NR_OK;
 }
 
+// Vertex positions and transforms must be finite: the reference renders
+// NaN geometry as undefined results, and the GPU builder's Morton codes and
+// SAH bins are only defined for finite boxes, so such input is refused on
+// the host before anything reaches the device.
+static bool all_finite(const float* v, size_t n) {
+  for (size_t i = 0; i < n; ++i)
+    if (!std::isfinite(v[i])) return false;
+  return true;
+}
+
 int nr_scene_add_mesh(nr_scene* s, const float* positions, const float* normals,
                       const float* tangents, const float* uvs, uint32_t n_vertices,
                       const uint32_t* triangles, uint32_t n_triangles, uint32_t* out_id) {
@@ -569,6 +584,8 @@ int nr_scene_add_mesh(nr_scene* s, const float* positions, const float* normals,
   for (size_t i = 0; i < (size_t)n_triangles * 3; ++i)
     if (triangles[i] >= n_vertices)
       return fail(NR_ERR_INVALID, "nr_scene_add_mesh: triangle index out of range");
+  if (!all_finite(positions, 3 * (size_t)n_vertices))
+    return fail(NR_ERR_INVALID, "nr_scene_add_mesh: non-finite vertex position");
   HostMesh m;
   m.positions.assign(positions, positions + 3 * (size_t)n_vertices);
   m.normals = normals ? std::vector<float>(normals, normals + 3 * (size_t)n_vertices)
@@ -592,6 +609,8 @@ int nr_scene_load_obj(nr_scene* s, const char* path, uint32_t* out_id) {
   if (m.triangles.empty()) return fail(NR_ERR_INVALID, std::string("OBJ has no faces: ") + path);
   if (m.triangles.size() / 3 >= (1u << 22))
     return fail(NR_ERR_LIMIT, "nr_scene_load_obj: at most 4194303 triangles per mesh");
+  if (!all_finite(m.positions.data(), m.positions.size()))
+    return fail(NR_ERR_INVALID, std::string("OBJ has a non-finite vertex position: ") + path);
   s->meshes.push_back(std::move(m));
   if (out_id) *out_id = (uint32_t)(s->meshes.size() - 1);
   s->built = false;
@@ -606,6 +625,8 @@ int nr_scene_load_obj_device(nr_scene* s, const char* path, uint32_t* out_id) {
   if (raw.corners.empty()) return fail(NR_ERR_INVALID, std::string("OBJ has no faces: ") + path);
   if (raw.corners.size() / 9 >= (1u << 22))
     return fail(NR_ERR_LIMIT, "nr_scene_load_obj_device: at most 4194303 triangles per mesh");
+  if (!all_finite(raw.vpos.data(), raw.vpos.size()))
+    return fail(NR_ERR_INVALID, std::string("OBJ has a non-finite vertex position: ") + path);
   int dev_count = 0;
   if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0)
     return fail(NR_ERR_NO_DEVICE, "nr_scene_load_obj_device: no CUDA device");
@@ -647,6 +668,9 @@ int nr_scene_add_object(nr_scene* s, const nr_object_desc* d, uint32_t* out_id) 
     return fail(NR_ERR_INVALID, "nr_scene_add_object: unknown mesh id");
   if (d->material < 0 || (size_t)d->material >= s->materials.size())
     return fail(NR_ERR_INVALID, "nr_scene_add_object: unknown material id");
+  if (!all_finite(d->position, 3) || !all_finite(d->rotation, 3) || !all_finite(d->scale, 3) ||
+      !std::isfinite(d->radius) || !std::isfinite(d->density))
+    return fail(NR_ERR_INVALID, "nr_scene_add_object: non-finite transform, radius or density");
   s->objects.push_back(*d);
   if (out_id) *out_id = (uint32_t)(s->objects.size() - 1);
   s->built = false;
@@ -891,6 +915,8 @@ int nr_scene_build(nr_scene* s) {
 
   DevScene& ds = s->dev;
   ds = DevScene{};
+  ds.max_steps = kMaxTraversalSteps;  // renders set their own bounds (make_params)
+  ds.stack_limit = 0xffffffffu;
   ds.objects = s->d_objects;
   ds.n_objects = (uint32_t)objs.size();
   ds.materials = s->d_materials;
@@ -1012,7 +1038,7 @@ struct nr_render {
   float* layer[9] = {nullptr};
   uint32_t layer_c[9] = {0};
   double* beauty64 = nullptr;
-  uint32_t n64 = 0;
+  uint64_t n64 = 0;  // samples in the FP64 sum since the last reset
   float* raw[3] = {nullptr, nullptr, nullptr};
   uint32_t* raw_primary = nullptr;
   uint32_t* work = nullptr;
@@ -1220,6 +1246,8 @@ static KernelParams make_params(nr_render* r, uint32_t first, uint32_t count, bo
   memset(&P, 0, sizeof(P));
   P.scene = r->scene->dev;
   P.scene.use_bvh8 = 1;
+  P.scene.max_steps = r->cfg.max_traversal_steps ? r->cfg.max_traversal_steps : kMaxTraversalSteps;
+  P.scene.stack_limit = r->cfg.traversal_stack_limit ? r->cfg.traversal_stack_limit : 0xffffffffu;
   P.cam = r->dcam;
   P.W = r->W;
   P.H = r->H;
@@ -1484,7 +1512,7 @@ static int finish_kernel(nr_render* r, const KernelParams& P, const WaveTimer& t
   CU(cudaMemcpy(&herr, r->err, 4, cudaMemcpyDeviceToHost), "read error word");
   if (herr) {
     cudaMemset(r->err, 0, 4);
-    return fail(NR_ERR_DEVICE, "integrator error word 0x" + std::to_string(herr) +
+    return fail(NR_ERR_DEVICE, "integrator error word 0x" + hex_word(herr) +
                                    " (1: traversal stack overflow, 8: traversal step bound)");
   }
   if (r->counters_on) {
@@ -1516,7 +1544,7 @@ int nr_render_samples(nr_render* r, uint32_t first, uint32_t count) {
     return fail(NR_ERR_INVALID, "sample index beyond samples_per_pixel");
   KernelParams P = make_params(r, first, count, false);
   int rc = run_kernel(r, P);
-  if (rc == NR_OK) r->n64 = first + count - 1;
+  if (rc == NR_OK) r->n64 += count;
   return rc;
 }
 
@@ -1545,7 +1573,7 @@ int nr_render_samples_batch(nr_render* const* renders, uint32_t n, const uint32_
   for (uint32_t i = 0; i < queued; ++i) {
     if (count[i] == 0) continue;
     int ri = finish_kernel(renders[i], ps[i], tms[i]);
-    if (ri == NR_OK) renders[i]->n64 = first[i] + count[i] - 1;
+    if (ri == NR_OK) renders[i]->n64 += count[i];
     else if (rc == NR_OK) rc = ri;
   }
   return rc;
@@ -1610,7 +1638,7 @@ int nr_render_samples_static(nr_render* r, uint32_t first, uint32_t count) {
   CU(cudaMemcpy(&herr, r->err, 4, cudaMemcpyDeviceToHost), "read error word");
   if (herr) {
     cudaMemset(r->err, 0, 4);
-    return fail(NR_ERR_DEVICE, "integrator error word 0x" + std::to_string(herr));
+    return fail(NR_ERR_DEVICE, "integrator error word 0x" + hex_word(herr));
   }
   if (r->counters_on) {
     unsigned long long c[5];
@@ -1621,7 +1649,7 @@ int nr_render_samples_static(nr_render* r, uint32_t first, uint32_t count) {
     r->last.obj_tests = c[3];
     r->last.paths = (unsigned long long)count * N;
   }
-  r->n64 = first + count - 1;
+  r->n64 += count;
   return NR_OK;
 }
 
@@ -1635,7 +1663,7 @@ int nr_render_viewport(nr_render* r, int32_t show_axis_grid) {
   CU(cudaMemcpy(&herr, r->err, 4, cudaMemcpyDeviceToHost), "read error word");
   if (herr) {
     cudaMemset(r->err, 0, 4);
-    return fail(NR_ERR_DEVICE, "viewport error word 0x" + std::to_string(herr));
+    return fail(NR_ERR_DEVICE, "viewport error word 0x" + hex_word(herr));
   }
   return NR_OK;
 }
@@ -1730,6 +1758,15 @@ int nr_render_read_beauty_fp64(nr_render* r, double* host) {
   CU(cudaMemcpy(host, r->beauty64, sizeof(double) * n, cudaMemcpyDeviceToHost), "read fp64");
   double inv = r->n64 ? 1.0 / (double)r->n64 : 0.0;
   for (size_t i = 0; i < n; ++i) host[i] *= inv;
+  return NR_OK;
+}
+
+int nr_render_read_beauty_fp64_sum(nr_render* r, double* host, uint64_t* n_samples) {
+  if (!r || !host || !n_samples) return fail(NR_ERR_INVALID, "null argument");
+  if (!r->beauty64) return fail(NR_ERR_STATE, "fp64 accumulation is not enabled");
+  size_t n = (size_t)3 * r->W * r->H;
+  CU(cudaMemcpy(host, r->beauty64, sizeof(double) * n, cudaMemcpyDeviceToHost), "read fp64");
+  *n_samples = r->n64;
   return NR_OK;
 }
 

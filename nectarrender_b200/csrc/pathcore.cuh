@@ -194,15 +194,17 @@ constexpr uint32_t kMaxTraversalSteps = 1u << 20;
 __device__ __forceinline__ int mesh_closest_bvh2(const DevMesh& m, const Ray& r, float tmin,
                                                  float& tmax, float& bu, float& bv,
                                                  bool skip_flat, TraceStats& st,
-                                                 uint32_t* err) {
+                                                 uint32_t* err, uint32_t max_steps,
+                                                 uint32_t stack_limit) {
   int best = -1;
   V3 oinv = r.o * r.inv;
   uint32_t stack[NR_STACK];
+  const int cap = stack_limit < (uint32_t)NR_STACK ? (int)stack_limit : NR_STACK;
   int sp = 0;
   int cur = 0;
   if (m.n_bvh2 == 0) return -1;
   for (uint32_t steps = 0;; ++steps) {
-    if (steps >= kMaxTraversalSteps || (uint32_t)cur >= m.n_bvh2) {
+    if (steps >= max_steps || (uint32_t)cur >= m.n_bvh2) {
       atomicOr(err, 8u);
       break;
     }
@@ -240,7 +242,7 @@ __device__ __forceinline__ int mesh_closest_bvh2(const DevMesh& m, const Ray& r,
     if (h0 && h1) {
       bool near0 = tn0 <= tn1;
       int nearl = near0 ? D.x : D.y, farl = near0 ? D.y : D.x;
-      if (sp < NR_STACK) stack[sp++] = (uint32_t)farl;
+      if (sp < cap) stack[sp++] = (uint32_t)farl;
       else atomicOr(err, 1u);
       cur = nearl;
     } else if (h0) {
@@ -330,12 +332,14 @@ __device__ __forceinline__ uint32_t bvh8_intersect(const Bvh8Node* nd, const V3&
 __device__ __forceinline__ int mesh_closest_bvh8(const DevMesh& m, const Ray& r, float tmin,
                                                  float& tmax, float& bu, float& bv,
                                                  bool skip_flat, TraceStats& st,
-                                                 uint32_t* err) {
+                                                 uint32_t* err, uint32_t max_steps,
+                                                 uint32_t stack_limit) {
   if (m.n_bvh8 == 0) return -1;
   int best = -1;
   uint32_t oct = (r.d.x < 0.0f ? 4u : 0u) | (r.d.y < 0.0f ? 2u : 0u) | (r.d.z < 0.0f ? 1u : 0u);
   uint32_t oct_inv4 = (7u - oct) * 0x01010101u;
   uint2 stack[NR_STACK];
+  const int cap = stack_limit < (uint32_t)NR_STACK ? (int)stack_limit : NR_STACK;
   int sp = 0;
   // The root is the single inner child (bit 31) of a virtual group whose
   // child base is 0 and whose inner mask (low byte) is empty, so it resolves
@@ -343,7 +347,7 @@ __device__ __forceinline__ int mesh_closest_bvh8(const DevMesh& m, const Ray& r,
   uint2 ngroup = make_uint2(0u, 0x80000000u);
   const uint32_t oct_inv = 7u - oct;
   for (uint32_t steps = 0;; ++steps) {
-    if (steps >= kMaxTraversalSteps) {
+    if (steps >= max_steps) {
       atomicOr(err, 8u);
       break;
     }
@@ -359,7 +363,7 @@ __device__ __forceinline__ int mesh_closest_bvh8(const DevMesh& m, const Ray& r,
         break;
       }
       if (ngroup.y > 0x00ffffffu) {
-        if (sp < NR_STACK) stack[sp++] = ngroup;
+        if (sp < cap) stack[sp++] = ngroup;
         else atomicOr(err, 1u);
       }
       float4 n0;
@@ -401,8 +405,10 @@ __device__ __forceinline__ bool mesh_hit(const DevScene& sc, const DevObject& ob
                                          TraceStats& st, uint32_t* err) {
   const DevMesh& m = sc.meshes[ob.mesh];
   float u = 0.f, v = 0.f;
-  int slot = sc.use_bvh8 ? mesh_closest_bvh8(m, r, tmin, tmax, u, v, ref_mode, st, err)
-                         : mesh_closest_bvh2(m, r, tmin, tmax, u, v, ref_mode, st, err);
+  int slot = sc.use_bvh8 ? mesh_closest_bvh8(m, r, tmin, tmax, u, v, ref_mode, st, err,
+                                             sc.max_steps, sc.stack_limit)
+                         : mesh_closest_bvh2(m, r, tmin, tmax, u, v, ref_mode, st, err,
+                                             sc.max_steps, sc.stack_limit);
   if (slot < 0) return false;
   const TriRecord* tr = (sc.use_bvh8 ? m.tris8 : m.tris2) + slot;
   uint32_t tri = __float_as_uint(__ldg(&tr->v0.w));
@@ -532,10 +538,11 @@ __device__ __forceinline__ bool scene_hit(const DevScene& sc, const Ray& wr, Hit
   float inv_len = 1.0f / length(wr.d);
   float slack_base = (2.0f * EPS + 1e-4f * (fabsf(wr.o.x) + fabsf(wr.o.y) + fabsf(wr.o.z) + 1.0f));
   uint32_t stack[NR_STACK];
+  const int cap = sc.stack_limit < (uint32_t)NR_STACK ? (int)sc.stack_limit : NR_STACK;
   int sp = 0;
   int cur = 0;
   for (uint32_t steps = 0;; ++steps) {
-    if (steps >= kMaxTraversalSteps || (uint32_t)cur >= sc.n_tlas2) {
+    if (steps >= sc.max_steps || (uint32_t)cur >= sc.n_tlas2) {
       atomicOr(err, 8u);
       break;
     }
@@ -570,7 +577,7 @@ __device__ __forceinline__ bool scene_hit(const DevScene& sc, const Ray& wr, Hit
     if (h0 && h1) {
       bool near0 = tn0 <= tn1;
       int nearl = near0 ? D.x : D.y, farl = near0 ? D.y : D.x;
-      if (sp < NR_STACK) stack[sp++] = (uint32_t)farl;
+      if (sp < cap) stack[sp++] = (uint32_t)farl;
       else atomicOr(err, 1u);
       cur = nearl;
     } else if (h0) {

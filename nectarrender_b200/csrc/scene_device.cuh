@@ -143,6 +143,11 @@ struct DevScene {
   int32_t use_bvh8;
   const CubeFace* cube_faces;  // 6 faces
   DevSky sky;
+  // Bounds of one traversal: steps per query and entries per traversal stack
+  // (the smaller of this and the kernel's own stack). Exceeding either sets an
+  // error bit (8: steps, 1: stack) that the host reports as NR_ERR_DEVICE.
+  uint32_t max_steps;
+  uint32_t stack_limit;
 };
 
 }  // namespace nr

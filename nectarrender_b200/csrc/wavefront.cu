@@ -139,11 +139,13 @@ __device__ __forceinline__ void st8(float4* p, const float4& a, const float4& b)
 // ---------------------------------------------------------------------------
 // compressed 8-wide traversal with a shared-memory stack; `leaf(slot, tmax)`
 // is called for every primitive slot whose leaf box the ray enters.
+// `depth` bounds the stack entries and `max_steps` the loop (error bits 1 and 8).
 template <typename Leaf>
 __device__ __forceinline__ void cwbvh_trace(const Bvh8Node* __restrict__ nodes, uint32_t n_nodes,
                                             const V3& o, const V3& d, const V3& inv, float tmin,
                                             float& tmax, uint2* stk, uint32_t stride, int depth,
-                                            Leaf&& leaf, uint32_t& node_count, uint32_t* err) {
+                                            uint32_t max_steps, Leaf&& leaf, uint32_t& node_count,
+                                            uint32_t* err) {
   if (n_nodes == 0) return;
   uint32_t oct = (d.x < 0.0f ? 4u : 0u) | (d.y < 0.0f ? 2u : 0u) | (d.z < 0.0f ? 1u : 0u);
   const uint32_t oct_inv = 7u - oct;
@@ -151,7 +153,7 @@ __device__ __forceinline__ void cwbvh_trace(const Bvh8Node* __restrict__ nodes, 
   uint2 ngroup = make_uint2(0u, 0x80000000u);
   int sp = 0;
   for (uint32_t steps = 0;; ++steps) {
-    if (steps >= kMaxTraversalSteps) {
+    if (steps >= max_steps) {
       atomicOr(err, 8u);
       return;
     }
@@ -213,6 +215,11 @@ __device__ __forceinline__ V3 mesh_normal(const DevMesh& m, uint32_t tri, float 
   return normalize(n0 * w + n1 * u + n2 * v);
 }
 
+// A kernel's traversal stack depth under the render's stack limit.
+__device__ __forceinline__ int stack_cap(int depth, const DevScene& sc) {
+  return sc.stack_limit < (uint32_t)depth ? (int)sc.stack_limit : depth;
+}
+
 // Mesh::hit + interpolate_hit (mesh.h:239-292, 367-383) with the 8-wide tree
 // and a shared-memory stack.
 __device__ __forceinline__ bool mesh_hit8(const DevScene& sc, const DevObject& ob, const Ray& r,
@@ -235,8 +242,8 @@ __device__ __forceinline__ bool mesh_hit8(const DevScene& sc, const DevObject& o
       best = (int)ts;
     }
   };
-  cwbvh_trace(m.bvh8, m.n_bvh8, r.o, r.d, r.inv, tmin, tmax, stk, stride, kBlasStack, tri_leaf,
-              nodes, err);
+  cwbvh_trace(m.bvh8, m.n_bvh8, r.o, r.d, r.inv, tmin, tmax, stk, stride,
+              stack_cap(kBlasStack, sc), sc.max_steps, tri_leaf, nodes, err);
   if (best < 0) return false;
   uint32_t tri = __float_as_uint(__ldg(&m.tris8[best].v0.w));
   uint32_t i0 = __ldg(m.tri_vidx + 3 * tri), i1 = __ldg(m.tri_vidx + 3 * tri + 1),
@@ -298,8 +305,8 @@ __device__ __forceinline__ void trace_closest(const DevScene& sc, const Ray& wr,
           best_slot = (int)ts;
         }
       };
-      cwbvh_trace(m.bvh8, m.n_bvh8, r.o, r.d, r.inv, EPS, tmax, blas_stk, stride, kBlasStack,
-                  tri_leaf, nodes, err);
+      cwbvh_trace(m.bvh8, m.n_bvh8, r.o, r.d, r.inv, EPS, tmax, blas_stk, stride,
+                  stack_cap(kBlasStack, sc), sc.max_steps, tri_leaf, nodes, err);
       if (best_slot >= 0) {
         uint32_t tri = __float_as_uint(__ldg(&m.tris8[best_slot].v0.w));
         V3 p = ray_at(r, tmax);
@@ -333,8 +340,8 @@ __device__ __forceinline__ void trace_closest(const DevScene& sc, const Ray& wr,
     }
   };
   float tlas_tmax = best0;
-  cwbvh_trace(sc.tlas8, sc.n_tlas8, wr.o, wr.d, wr.inv, EPS, tlas_tmax, tlas_stk, stride, kTlasStack,
-              object_leaf, nodes, err);
+  cwbvh_trace(sc.tlas8, sc.n_tlas8, wr.o, wr.d, wr.inv, EPS, tlas_tmax, tlas_stk, stride,
+              stack_cap(kTlasStack, sc), sc.max_steps, object_leaf, nodes, err);
   if (kCount) st.nodes += nodes;
 }
 
@@ -585,7 +592,7 @@ __global__ void __launch_bounds__(kExtThreads, kMinBlocks) k_wf_extend_flat(WfPa
     if (__ballot_sync(0xffffffffu, active) == 0u) break;
     if (!active) continue;
 
-    if (++steps > kMaxTraversalSteps) {
+    if (++steps > sc.max_steps) {
       atomicOr(P.err, 8u);
       tg.y = 0u;
       ng.y = 0u;
@@ -678,7 +685,7 @@ __global__ void __launch_bounds__(kExtThreads, kMinBlocks) k_wf_extend_flat(WfPa
         sp = 0;
       } else {
         if (ng.y > 0x00ffffffu) {
-          const int depth = in_mesh ? kBlasStack : kTlasStack;
+          const int depth = in_mesh ? stack_cap(kBlasStack, sc) : stack_cap(kTlasStack, sc);
           uint2* stk = in_mesh ? bstk : tstk;
           if (sp < depth) stk[(sp++) * kExtThreads] = ng;
           else atomicOr(P.err, 1u);

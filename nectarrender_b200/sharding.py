@@ -37,3 +37,14 @@ def combine_sums(local_sum, total_count: int, all_reduce) -> object:
     `all_reduce` sums a tensor in place across ranks (torch.distributed)."""
     all_reduce(local_sum)
     return local_sum / float(total_count)
+
+
+def render_shard(render, first: int, count: int, world: int, rank: int):
+    """Renders this rank's shard of the sample indices [first, first+count)
+    with `render` (a capi.Render created with fp64_accumulate=1, nothing
+    rendered since its last reset) and returns (FP64 sum image, number of
+    samples in it): the rank's term of the sum over ranks."""
+    sh = shard_samples(first, count, world, rank)
+    if sh.count:
+        render.samples(sh.first, sh.count)
+    return render.beauty_fp64_sum()

@@ -47,7 +47,8 @@ RENDER_CONFIG_DEFAULTS = {"ray_depth": 8, "seed": 54321, "rr_enabled": 1, "rr_st
                           "rr_survival": 0.95, "mode": 0, "schedule": 1, "fp64_accumulate": 0,
                           "layer_mask": (1 << 0) | (1 << 1) | (1 << 4), "extend_variant": 0,
                           "samples_per_wave": 0, "use_graphs": 1, "tail_max_paths": 0,
-                          "shade_variant": 0, "sort_materials": 0}
+                          "shade_variant": 0, "sort_materials": 0, "max_traversal_steps": 0,
+                          "traversal_stack_limit": 0}
 
 
 def render_config(spec: SceneSpec, **over) -> RenderConfig:
@@ -375,6 +376,27 @@ class RefCUDA(_Lib):
         if rc != 0:
             raise RuntimeError(f"draw-order probe failed ({rc})")
         return a.value, b.value
+
+    def time_steps(self, spec, first: int, warmup: int, steps: int, spp_per_step: int,
+                   cfg=None) -> list[float]:
+        """Device ms of each of `steps` timed steps of the reference's render
+        loop (trace_full, accumulate, clear and a synchronise per sample;
+        `spp_per_step` sample indices per step, from `first`), after `warmup`
+        untimed steps, with L2 overwritten between steps."""
+        s = self.or_scene(spec)
+        cam = camera_desc(spec.camera)
+        cfg = cfg or render_config(spec)
+        H, W = int(spec.camera["resolution"][0]), int(spec.camera["resolution"][1])
+        if H % 16 or W % 16:
+            raise ValueError(f"reference CUDA build needs both sizes a multiple of 16, got {H}x{W}")
+        if first + (warmup + steps) * spp_per_step > spec.camera["samples_per_pixel"]:
+            raise ValueError("sample indices beyond samples_per_pixel")
+        out = (C.c_double * steps)()
+        rc = self.lib.refcuda_time_steps(C.byref(s), C.byref(cam), C.byref(cfg), first, warmup, steps,
+                                         spp_per_step, out)
+        if rc != 0:
+            raise RuntimeError(f"refcuda_time_steps failed ({rc})")
+        return list(out)
 
     def render(self, spec, first, count=1, mode=1, rows=None, threads=0, draw_rtl=1, fp64=False,
                cfg=None):

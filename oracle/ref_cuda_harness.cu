@@ -81,29 +81,10 @@ void read3(DataObject& o, float* host) {
   if (host) cudaMemcpy(host, o.data_ptr(), o.n_bytes(), cudaMemcpyDeviceToHost);
 }
 
-}  // namespace
-
-extern "C" {
-
-// Draw order of Vector3::random and Quad::random in device code:
-// 1 = right to left, 0 = left to right, -1 = neither.
-int refcuda_probe_draw_order(int* vec3_order, int* quad_order) {
-  float* d = nullptr;
-  if (cudaMalloc(&d, 16 * sizeof(float)) != cudaSuccess) return -1;
-  probe_kernel<<<1, 1>>>(d);
-  float h[16];
-  if (cudaMemcpy(h, d, sizeof(h), cudaMemcpyDeviceToHost) != cudaSuccess) return -2;
-  cudaFree(d);
-  *vec3_order = (h[0] == h[6] && h[2] == h[8]) ? 0 : ((h[0] == h[8] && h[2] == h[6]) ? 1 : -1);
-  float ra = h[3] + 0.5f;  // corner.x = -0.5, u = (1,0,0)
-  *quad_order = (ra == h[9]) ? 0 : ((ra == h[10]) ? 1 : -1);
-  return 0;
-}
-
-int refcuda_render(const or_scene* s, const nr_camera_desc* c, const nr_render_config* cfg,
-                   const or_request* req, double* elapsed_ms) {
-  cudaDeviceSetLimit(cudaLimitStackSize, CUDA_STACK_SIZE_LIMIT);
-  std::vector<std::unique_ptr<Hittable>> keep;
+// The reference's Scene for a checker scene description, built through its
+// own host API (Hittable factories, Scene, Scene::build). `keep` owns the
+// hittables the Scene points to.
+std::unique_ptr<Scene> build_ref_scene(const or_scene* s, std::vector<std::unique_ptr<Hittable>>& keep) {
   std::vector<Hittable*> hittables, lights;
   for (uint32_t i = 0; i < s->n_objects; ++i) {
     const nr_object_desc& d = s->objects[i];
@@ -134,12 +115,47 @@ int refcuda_render(const or_scene* s, const nr_camera_desc* c, const nr_render_c
   }
   auto scene = std::make_unique<Scene>(hittables, lights, std::move(sky));
   scene->build();
+  return scene;
+}
+
+// Built on the heap: the reference's Camera copy re-creates it from its
+// parameters only, so it is never copied once constructed.
+std::unique_ptr<Camera> make_camera(const nr_camera_desc* c, uint32_t seed) {
   CameraParams params(Vector2(c->resolution[0], c->resolution[1]),
                       Vector3(c->position[0], c->position[1], c->position[2]),
                       Vector3(c->rotation[0], c->rotation[1], c->rotation[2]), c->samples_per_pixel,
                       c->focal_length, c->focus_distance, c->aperture, c->sensor_width, c->shutter_speed);
-  Camera cam(params);
-  cam.__construct(cfg->seed);
+  auto cam = std::make_unique<Camera>(params);
+  cam->__construct(seed);
+  return cam;
+}
+
+}  // namespace
+
+extern "C" {
+
+// Draw order of Vector3::random and Quad::random in device code:
+// 1 = right to left, 0 = left to right, -1 = neither.
+int refcuda_probe_draw_order(int* vec3_order, int* quad_order) {
+  float* d = nullptr;
+  if (cudaMalloc(&d, 16 * sizeof(float)) != cudaSuccess) return -1;
+  probe_kernel<<<1, 1>>>(d);
+  float h[16];
+  if (cudaMemcpy(h, d, sizeof(h), cudaMemcpyDeviceToHost) != cudaSuccess) return -2;
+  cudaFree(d);
+  *vec3_order = (h[0] == h[6] && h[2] == h[8]) ? 0 : ((h[0] == h[8] && h[2] == h[6]) ? 1 : -1);
+  float ra = h[3] + 0.5f;  // corner.x = -0.5, u = (1,0,0)
+  *quad_order = (ra == h[9]) ? 0 : ((ra == h[10]) ? 1 : -1);
+  return 0;
+}
+
+int refcuda_render(const or_scene* s, const nr_camera_desc* c, const nr_render_config* cfg,
+                   const or_request* req, double* elapsed_ms) {
+  cudaDeviceSetLimit(cudaLimitStackSize, CUDA_STACK_SIZE_LIMIT);
+  std::vector<std::unique_ptr<Hittable>> keep;
+  auto scene = build_ref_scene(s, keep);
+  auto camp = make_camera(c, cfg->seed);
+  Camera& cam = *camp;
   RenderLayers aovs(cam.resolution());
   RenderLayers sample_aovs(&aovs);
   clear(aovs);
@@ -171,6 +187,58 @@ int refcuda_render(const or_scene* s, const nr_camera_desc* c, const nr_render_c
   read3(src.world_normal, req->normal);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  aovs.free_aovs();
+  sample_aovs.free_aovs();
+  return err == cudaSuccess ? 0 : (int)err;
+}
+
+// The reference's render loop (engine.cpp:42-74: trace_full, accumulate,
+// clear, synchronise per sample) timed in steps of `spp_per_step` sample
+// indices, after `warmup` untimed steps. A 256 MiB buffer is written between
+// steps so that no step starts with the previous one's data in L2. step_ms
+// receives each timed step's device time (CUDA events).
+int refcuda_time_steps(const or_scene* s, const nr_camera_desc* c, const nr_render_config* cfg,
+                       uint32_t first, uint32_t warmup, uint32_t steps, uint32_t spp_per_step,
+                       double* step_ms) {
+  cudaDeviceSetLimit(cudaLimitStackSize, CUDA_STACK_SIZE_LIMIT);
+  std::vector<std::unique_ptr<Hittable>> keep;
+  auto scene = build_ref_scene(s, keep);
+  auto camp = make_camera(c, cfg->seed);
+  Camera& cam = *camp;
+  RenderLayers aovs(cam.resolution());
+  RenderLayers sample_aovs(&aovs);
+  clear(aovs);
+  clear(sample_aovs);
+  void* flush = nullptr;
+  const size_t flush_bytes = size_t(256) << 20;
+  if (cudaMalloc(&flush, flush_bytes) != cudaSuccess) return -1;
+  cudaDeviceSynchronize();
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  uint32_t smp = first;
+  for (uint32_t k = 0; k < warmup + steps; ++k) {
+    cudaMemset(flush, k & 0xff, flush_bytes);
+    cudaDeviceSynchronize();
+    cudaEventRecord(e0);
+    for (uint32_t i = 0; i < spp_per_step; ++i, ++smp) {
+      TraceConfig tc{smp, cfg->ray_depth, cfg->seed, cfg->rr_enabled != 0, cfg->rr_start_bounce,
+                     cfg->rr_survival};
+      trace_full(cam, scene->graph, sample_aovs.aovs(), tc);
+      aovs.accumulate(sample_aovs, smp);
+      sample_aovs.clear();
+      cudaDeviceSynchronize();
+    }
+    cudaEventRecord(e1);
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (k >= warmup) step_ms[k - warmup] = ms;
+  }
+  cudaError_t err = cudaGetLastError();
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(flush);
   aovs.free_aovs();
   sample_aovs.free_aovs();
   return err == cudaSuccess ? 0 : (int)err;
