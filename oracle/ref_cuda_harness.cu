@@ -109,7 +109,14 @@ std::unique_ptr<Scene> build_ref_scene(const or_scene* s, std::vector<std::uniqu
     sky = Skylight::simple(Color(s->sky_start[0], s->sky_start[1], s->sky_start[2]),
                            Color(s->sky_end[0], s->sky_end[1], s->sky_end[2]));
   else if (s->sky_type == NR_SKY_HDRI) {
-    sky = Skylight::hdri(std::string(s->hdri_path));
+    // Skylight::hdri(path) copies an HDRISkylightConfig whose data_ptr is
+    // never initialised and then frees that pointer before loading
+    // (skylight.h:226-231, 205): whether that aborts depends on stale stack
+    // contents. The same loader is reached without it through hdri() and
+    // load_hdri_file once the pointer is cleared.
+    sky = Skylight::hdri();
+    sky.config_hdri().data_ptr = nullptr;
+    sky.load_hdri_file(std::string(s->hdri_path));
     sky.config_hdri().rotation = s->hdri_rotation;
     sky.config_hdri().intensity = s->hdri_intensity;
   }
