@@ -425,6 +425,19 @@ int nr_render_samples_static(nr_render* render, uint32_t first, uint32_t count);
  * any pointer may be NULL. Used for per-sample parity. */
 int nr_render_sample_layers(nr_render* render, uint32_t sample_idx, float* beauty_chw,
                             float* diffuse_chw, float* world_normal_chw, uint32_t* primary_prim);
+/* Per-bounce record of one sample index's paths, for diagnosing per-sample
+ * differences from the reference (no counterpart in the reference, whose
+ * trace_full_kernel, engine/src/trace.cu:47-79, keeps this state in
+ * registers). Renders sample_idx like nr_render_sample_layers (raw beauty to
+ * `beauty`, 3*H*W floats, may be NULL) and writes, per pixel and bounce b <
+ * max_bounces (<= 64), 16 floats at ((y*W + x) * max_bounces + b) * 16: the
+ * ray's origin and direction, the hit's registry object id and triangle
+ * index as uint32 bits (0xFFFFFFFF: none), its world t, the throughput and
+ * the beauty after the bounce, and 1 (as uint32 bits) if the path goes on.
+ * Bounces a path never reaches keep all-ones bits. NR_MODE_REFERENCE on the
+ * wavefront schedule only (NR_ERR_STATE otherwise). */
+int nr_render_trace_log(nr_render* render, uint32_t sample_idx, uint32_t max_bounces,
+                        float* host_log, float* beauty);
 /* Device pointer of an accumulated layer (DataObject::device_ptr,
  * nectar_render/csrc/data/include/data/data_object.h:163-166). */
 int nr_render_layer_device_ptr(nr_render* render, int32_t layer, uint64_t* out_ptr);

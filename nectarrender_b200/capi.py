@@ -109,7 +109,7 @@ EXPORTS = [
     "nr_denoiser_param_count", "nr_denoiser_get_params", "nr_denoiser_set_params",
     "nr_denoiser_layers", "nr_nrc_create", "nr_nrc_destroy", "nr_nrc_infer", "nr_nrc_train",
     "nr_nrc_count", "nr_nrc_get", "nr_nrc_set", "nr_render_set_nrc", "nr_render_nrc_stats",
-    "nr_render_sample_layers", "nr_render_layer_device_ptr", "nr_render_read_layer",
+    "nr_render_sample_layers", "nr_render_trace_log", "nr_render_layer_device_ptr", "nr_render_read_layer",
     "nr_render_read_beauty_fp64", "nr_render_read_beauty_fp64_sum", "nr_render_readback", "nr_render_display_float",
     "nr_render_dims", "nr_render_set_counters", "nr_render_get_counters", "nr_render_last_ms",
     "nr_render_stream", "nr_accumulate_device", "nr_display_device",
@@ -317,6 +317,15 @@ class Render:
                                                 p.ctypes.data_as(C.POINTER(C.c_uint32))),
                "nr_render_sample_layers")
         return b, d, n, p
+
+    def trace_log(self, sample_idx: int, max_bounces: int):
+        """(log, beauty) of nr_render_trace_log: log is (H, W, max_bounces,
+        16) float32, beauty the raw (3, H, W) sample."""
+        log = np.zeros((self.H, self.W, max_bounces, 16), np.float32)
+        b = np.zeros((3, self.H, self.W), np.float32)
+        _check(self.lib.nr_render_trace_log(self.h, sample_idx, max_bounces, _fptr(log), _fptr(b)),
+               "nr_render_trace_log")
+        return log, b
 
     def layer(self, layer: int = 0) -> np.ndarray:
         out = np.zeros((3, self.H, self.W), np.float32)

@@ -1040,6 +1040,8 @@ struct nr_render {
   double* beauty64 = nullptr;
   uint64_t n64 = 0;  // samples in the FP64 sum since the last reset
   float* raw[3] = {nullptr, nullptr, nullptr};
+  float* trace_log = nullptr;  // set only during nr_render_trace_log
+  uint32_t log_bounces = 0;
   uint32_t* raw_primary = nullptr;
   uint32_t* work = nullptr;
   uint32_t* err = nullptr;
@@ -1414,6 +1416,12 @@ static int launch(nr_render* r, const KernelParams& P, WaveTimer* tm) {
   W.shade_variant = r->cfg.shade_variant > 0 ? r->cfg.shade_variant : kDefaultShadeVariant;
   W.tail_max_paths = r->cfg.tail_max_paths == 0 ? kDefaultTailPaths
                      : (r->cfg.tail_max_paths == UINT32_MAX ? 0u : r->cfg.tail_max_paths);
+  if (r->trace_log) {
+    // per-bounce log: every bounce in k_wf_shade, so no hand-off to the tail
+    W.trace_log = r->trace_log;
+    W.log_bounces = r->log_bounces;
+    W.tail_max_paths = 0;
+  }
   const bool fused = r->fused_on && r->disp8 && !P.write_raw && P.beauty;
   if (fused) {
     W.disp8 = r->disp8;
@@ -1456,7 +1464,7 @@ static int launch(nr_render* r, const KernelParams& P, WaveTimer* tm) {
   for (uint32_t s = 0; s < P.n_samples; s += per) {
     W.base = P.first_sample + s;
     W.count = std::min(per, P.n_samples - s);
-    if (!r->counters_on && !tm && r->cfg.use_graphs && !nrc)
+    if (!r->counters_on && !tm && r->cfg.use_graphs && !nrc && !r->trace_log)
       CU(launch_wave_graph(r, W), "launch wavefront graph");
     else {
       cudaError_t e = wf_launch_wave(W, r->counters_on, r->stream, tm, nrc ? &hook : nullptr);
@@ -1735,6 +1743,41 @@ int nr_render_sample_layers(nr_render* r, uint32_t sample_idx, float* beauty, fl
   if (normal) CU(cudaMemcpy(normal, r->raw[2], sizeof(float) * 3 * hw, cudaMemcpyDeviceToHost), "read");
   if (primary) CU(cudaMemcpy(primary, r->raw_primary, sizeof(uint32_t) * hw, cudaMemcpyDeviceToHost), "read");
   return NR_OK;
+}
+
+int nr_render_trace_log(nr_render* r, uint32_t sample_idx, uint32_t max_bounces, float* host_log,
+                        float* beauty) {
+  if (!r || !host_log) return fail(NR_ERR_INVALID, "null argument");
+  if (sample_idx == 0 || sample_idx >= r->cam.samples_per_pixel)
+    return fail(NR_ERR_INVALID, "sample index outside 1 .. samples_per_pixel - 1");
+  if (max_bounces == 0 || max_bounces > 64) return fail(NR_ERR_INVALID, "max_bounces outside 1 .. 64");
+  if (r->cfg.mode != NR_MODE_REFERENCE || r->cfg.schedule != NR_SCHEDULE_WAVEFRONT)
+    return fail(NR_ERR_STATE, "the trace log covers the wavefront schedule in NR_MODE_REFERENCE");
+  size_t hw = (size_t)r->W * r->H;
+  for (int k = 0; k < 3; ++k)
+    if (!r->raw[k]) CU(cudaMalloc(&r->raw[k], sizeof(float) * 3 * hw), "alloc raw");
+  if (!r->raw_primary) CU(cudaMalloc(&r->raw_primary, sizeof(uint32_t) * hw), "alloc raw");
+  const size_t n = hw * max_bounces * kTraceLogFloats;
+  float* d = nullptr;
+  CU(cudaMalloc(&d, sizeof(float) * n), "alloc trace log");
+  // entries of bounces a path never reaches stay all-ones bits
+  cudaError_t e = cudaMemsetAsync(d, 0xff, sizeof(float) * n, r->stream);
+  int rc = NR_OK;
+  if (e != cudaSuccess) rc = cuda_fail(e, "clear trace log");
+  if (rc == NR_OK) {
+    r->trace_log = d;
+    r->log_bounces = max_bounces;
+    rc = run_kernel(r, make_params(r, sample_idx, 1, true));
+    r->trace_log = nullptr;
+    r->log_bounces = 0;
+  }
+  if (rc == NR_OK && (e = cudaMemcpy(host_log, d, sizeof(float) * n, cudaMemcpyDeviceToHost)) != cudaSuccess)
+    rc = cuda_fail(e, "read trace log");
+  if (rc == NR_OK && beauty &&
+      (e = cudaMemcpy(beauty, r->raw[0], sizeof(float) * 3 * hw, cudaMemcpyDeviceToHost)) != cudaSuccess)
+    rc = cuda_fail(e, "read beauty");
+  cudaFree(d);
+  return rc;
 }
 
 int nr_render_layer_device_ptr(nr_render* r, int32_t layer, uint64_t* out) {

@@ -918,6 +918,19 @@ __global__ void __launch_bounds__(kShadeThreads, kMinBlocks) k_wf_shade(WfParams
           if (kPerf) W.mis_pdf[p] = pdf_next;
         }
       }
+      if (!kPerf && W.trace_log && bounce < W.log_bounces && p < N) {
+        // ray, hit (registry object id, primitive, world t), throughput and
+        // beauty after this bounce, and whether the path goes on
+        float* L = W.trace_log + ((size_t)p * W.log_bounces + bounce) * kTraceLogFloats;
+        L[0] = o.x; L[1] = o.y; L[2] = o.z;
+        L[3] = d.x; L[4] = d.y; L[5] = d.z;
+        L[6] = __uint_as_float(hit ? sc.objects[rec.obj].object_id : 0xffffffffu);
+        L[7] = __uint_as_float(hit ? rec.prim : 0xffffffffu);
+        L[8] = hit ? rec.t : 0.0f;
+        L[9] = s.atten.x; L[10] = s.atten.y; L[11] = s.atten.z;
+        L[12] = s.beauty.x; L[13] = s.beauty.y; L[14] = s.beauty.z;
+        L[15] = __uint_as_float(alive ? 1u : 0u);
+      }
       if (bounce == 0u) {
         W.acc_d[p] = aov_d;
         W.acc_n[p] = aov_n;

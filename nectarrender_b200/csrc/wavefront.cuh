@@ -70,7 +70,13 @@ struct WfParams {
   // layer's display transform as uint8 CHW
   uint8_t* disp8;
   DisplayParams disp_p;
+  // per-bounce trace log of the wave's first sample index (null: off;
+  // NR_MODE_REFERENCE shading only): kTraceLogFloats floats per pixel and
+  // bounce, for bounces below log_bounces (see nr_render_trace_log)
+  float* trace_log;
+  uint32_t log_bounces;
 };
+constexpr int kTraceLogFloats = 16;
 
 size_t wf_state_bytes(uint32_t n_paths, bool perf = false, bool sort = false);
 cudaError_t wf_alloc(WfParams& W, uint32_t n_paths, bool perf = false, bool sort = false);

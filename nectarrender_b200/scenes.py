@@ -263,11 +263,11 @@ def mesh_stress(levels: int = 8, res_h: int = 1080, res_w: int = 1920, spp: int 
     hdr_path = ASSETS / f"sky_{hdri_size[0]}x{hdri_size[1]}_s{scene_seed}.hdr"
     if not obj_path.exists():
         v, f, n = displaced_icosphere(levels, scene_seed)
-        tmp = obj_path.with_suffix(".tmp")
+        tmp = obj_path.with_suffix(f".{os.getpid()}.tmp")  # unique per writer process
         write_obj(tmp, v, f, n)
         tmp.replace(obj_path)
     if not hdr_path.exists():
-        tmp = hdr_path.with_suffix(".tmp")
+        tmp = hdr_path.with_suffix(f".{os.getpid()}.tmp")
         write_hdr(tmp, procedural_hdri(hdri_size[0], hdri_size[1], scene_seed))
         tmp.replace(hdr_path)
     rng = np.random.default_rng(scene_seed + 1)

@@ -398,6 +398,24 @@ class RefCUDA(_Lib):
             raise RuntimeError(f"refcuda_time_steps failed ({rc})")
         return list(out)
 
+    def trace_log(self, spec, sample: int, max_bounces: int, cfg=None):
+        """(log, beauty): the per-bounce record of sample index `sample` from
+        the reference's own trace_ray (layout of nr_render_trace_log,
+        (H, W, max_bounces, 16) float32) and the raw beauty of the sample."""
+        s = self.or_scene(spec)
+        cam = camera_desc(spec.camera)
+        cfg = cfg or render_config(spec)
+        H, W = int(spec.camera["resolution"][0]), int(spec.camera["resolution"][1])
+        if H % 16 or W % 16:
+            raise ValueError(f"reference CUDA build needs both sizes a multiple of 16, got {H}x{W}")
+        log = np.zeros((H, W, max_bounces, 16), np.float32)
+        b = np.zeros((3, H, W), np.float32)
+        rc = self.lib.refcuda_trace_log(C.byref(s), C.byref(cam), C.byref(cfg), sample, max_bounces,
+                                        _f(log), _f(b))
+        if rc != 0:
+            raise RuntimeError(f"refcuda_trace_log failed ({rc})")
+        return log, b
+
     def render(self, spec, first, count=1, mode=1, rows=None, threads=0, draw_rtl=1, fp64=False,
                cfg=None):
         """Returns (beauty, diffuse, normal, elapsed_ms) of the reference's

@@ -26,6 +26,15 @@
 
 #include "oracle.h"
 
+// The reference's trace.cu compiled once more into this file, in its own
+// namespace (its headers are included above, so only its own definitions
+// land there): the per-bounce log below calls its trace_ray unchanged.
+#include "engine/include/engine/pdf.h"
+#include "engine/include/engine/ray.h"
+namespace refsrc {
+#include "engine/src/trace.cu"
+}  // namespace refsrc
+
 namespace {
 
 std::shared_ptr<Texture> tex(const nr_texture_desc& t) {
@@ -137,6 +146,54 @@ std::unique_ptr<Camera> make_camera(const nr_camera_desc* c, uint32_t seed) {
   return cam;
 }
 
+// trace_full_kernel (trace.cu:47-79) with a record of every bounce: the ray
+// before it, the hit's registry object id and world t (0xFFFFFFFF bits and 0
+// on a miss), the throughput and the pixel's beauty after it, and whether the
+// path goes on. 16 floats per pixel and bounce, the layout of
+// nr_render_trace_log (the reference records no triangle index: 0xFFFFFFFF).
+__global__ void trace_log_kernel(DeviceCamera* cam, SceneGraph* scene, AOVs* aovs, TraceConfig cfg,
+                                 uint32_t max_bounces, float* log) {
+  ProcessIndex p_idx = get_process_index();
+  if (p_idx.x >= cam->W || p_idx.y >= cam->H) return;
+  uint32_t pixel_idx = p_idx.y * cam->W + p_idx.x;
+  Color atten = Color::white();
+  Generator gen(cfg.seed, pixel_idx + cfg.sample_idx * (cam->W * cam->H));
+  Ray ray = cam->get_ray(p_idx.x, p_idx.y, pixel_idx, cfg.sample_idx, cfg.seed, gen);
+  ColorIndex ci(aovs->beauty.C, aovs->beauty.H, aovs->beauty.W);
+  for (int bounce = 0; bounce < cfg.ray_depth; bounce++) {
+    const Vector3 o = ray.origin(), d = ray.direction();
+    HitRecord rec;
+    rec.t = -1.0f;
+    bool go = refsrc::trace_ray(scene, aovs, ray, rec, atten, gen);
+    if (go) {
+      if (bounce == 0) {
+        aovs->diffuse += atten;
+        aovs->world_normal += Color(rec.n);
+      }
+      if (cfg.do_rr_termination && bounce >= cfg.rr_start_bounce) {
+        float survival = fmaxf(atten.r(), fmaxf(atten.g(), atten.b()));
+        survival = fminf(survival, cfg.rr_survival_chance);
+        if (gen.uniform() > survival) go = false;
+        else atten *= 1.0f / survival;
+      }
+    }
+    if ((uint32_t)bounce < max_bounces) {
+      float* L = log + ((size_t)pixel_idx * max_bounces + bounce) * 16;
+      const bool hit = rec.t >= 0.0f;
+      const Color b = ci.get_color(aovs->beauty.ptr);
+      L[0] = o.x(); L[1] = o.y(); L[2] = o.z();
+      L[3] = d.x(); L[4] = d.y(); L[5] = d.z();
+      L[6] = __uint_as_float(hit ? (uint32_t)rec.object_id : 0xffffffffu);
+      L[7] = __uint_as_float(0xffffffffu);
+      L[8] = hit ? rec.t : 0.0f;
+      L[9] = atten.r(); L[10] = atten.g(); L[11] = atten.b();
+      L[12] = b.r(); L[13] = b.g(); L[14] = b.b();
+      L[15] = __uint_as_float(go && bounce + 1 < cfg.ray_depth ? 1u : 0u);
+    }
+    if (!go) break;
+  }
+}
+
 }  // namespace
 
 extern "C" {
@@ -246,6 +303,39 @@ int refcuda_time_steps(const or_scene* s, const nr_camera_desc* c, const nr_rend
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   cudaFree(flush);
+  aovs.free_aovs();
+  sample_aovs.free_aovs();
+  return err == cudaSuccess ? 0 : (int)err;
+}
+
+// One sample index through trace_log_kernel: the per-bounce log (see the
+// kernel) and the raw beauty of the sample (3*H*W floats, may be null), which
+// equals what trace_full writes for that sample.
+int refcuda_trace_log(const or_scene* s, const nr_camera_desc* c, const nr_render_config* cfg,
+                      uint32_t sample, uint32_t max_bounces, float* host_log, float* beauty) {
+  cudaDeviceSetLimit(cudaLimitStackSize, CUDA_STACK_SIZE_LIMIT);
+  std::vector<std::unique_ptr<Hittable>> keep;
+  auto scene = build_ref_scene(s, keep);
+  auto camp = make_camera(c, cfg->seed);
+  Camera& cam = *camp;
+  RenderLayers aovs(cam.resolution());
+  RenderLayers sample_aovs(&aovs);
+  clear(sample_aovs);
+  const size_t n = (size_t)cam.width() * cam.height() * max_bounces * 16;
+  float* d_log = nullptr;
+  if (cudaMalloc(&d_log, n * sizeof(float)) != cudaSuccess) return -1;
+  cudaMemset(d_log, 0xff, n * sizeof(float));
+  TraceConfig tc{sample, cfg->ray_depth, cfg->seed, cfg->rr_enabled != 0, cfg->rr_start_bounce,
+                 cfg->rr_survival};
+  dim3 block(BS2D, BS2D, 1);
+  dim3 grid((cam.width() + BS2D - 1) / BS2D, (cam.height() + BS2D - 1) / BS2D, 1);
+  trace_log_kernel<<<grid, block>>>(cam.device_camera(), scene->graph, sample_aovs.aovs(), tc,
+                                    max_bounces, d_log);
+  cudaDeviceSynchronize();
+  cudaError_t err = cudaGetLastError();
+  if (err == cudaSuccess) cudaMemcpy(host_log, d_log, n * sizeof(float), cudaMemcpyDeviceToHost);
+  if (err == cudaSuccess) read3(sample_aovs.beauty, beauty);
+  cudaFree(d_log);
   aovs.free_aovs();
   sample_aovs.free_aovs();
   return err == cudaSuccess ? 0 : (int)err;

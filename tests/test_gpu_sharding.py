@@ -55,6 +55,7 @@ def _worker(rank, world, port, out):
 def test_two_rank_shards_combine_to_the_single_render(tmp_path):
     from nectarrender_b200 import capi
     out = str(tmp_path / "mean.npy")
+    _spec()  # writes the scene's files before the ranks read them
     mp.start_processes(_worker, args=(2, _free_port(), out), nprocs=2, start_method="spawn")
     r = capi.Render(capi.Scene(_spec()), fp64_accumulate=1)
     r.samples(FIRST, COUNT)
