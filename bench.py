@@ -74,6 +74,8 @@ def parse():
                    help="also render the 64-scene batched configuration and report every "
                         "scene's RMSE against an FP64 perf-mode render (about 2 minutes)")
     p.add_argument("--denoiser-seconds", type=float, default=40.0)
+    p.add_argument("--no-small", action="store_true",
+                   help="skip the small configuration (Cornell box 512x512, 64 spp, depth 8)")
     return p.parse_args()
 
 
@@ -394,6 +396,9 @@ def run_ours(args):
     cornell01 = None
     if rank == 0 and world == 1 and args.rmse_cornell:
         cornell01 = cornell_time_to_rmse(args)
+    small = None
+    if rank == 0 and world == 1 and not args.no_small:
+        small = small_config(args, local)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -431,6 +436,7 @@ def run_ours(args):
                 "multi_scene": multi,
                 "batch_rmse": batch,
                 "time_to_rmse_cornell": cornell01,
+                "small_config": small,
                 "scene": {"build_ms_device": stats["build_ms"], "build_wall_s": build_wall,
                           "obj_load_s": obj_load_times(spec) if rank == 0 else None,
                           "triangles": stats["n_triangles"], "wide_nodes": stats["wide_nodes"],
@@ -948,6 +954,93 @@ def time_to_rmse(args, target=0.01):
                 f"{plain[-1][0]} samples")
         info["reached_target"] = any(rr <= target for _, _, rr in curve)
         out["learned_denoiser"] = info
+    return out
+
+
+def l2_copy_gbs(mib: int = 24, reps: int = 200) -> float:
+    """Copy bandwidth (read + write bytes per second) of a buffer pair that
+    stays resident in L2 (2 x `mib` MiB against the 126 MB L2), best of 5
+    runs of `reps` back-to-back copies timed with CUDA events: the ceiling
+    of kernels whose working set lives in L2."""
+    import torch
+    a = torch.empty(mib << 20, dtype=torch.uint8, device="cuda")
+    b = torch.empty_like(a)
+    best = 0.0
+    for _ in range(5):
+        b.copy_(a)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            b.copy_(a)
+        e1.record()
+        torch.cuda.synchronize()
+        best = max(best, 2.0 * a.numel() * reps / (e0.elapsed_time(e1) * 1e-3) / 1e9)
+    return best
+
+
+def small_config(args, gpu: int, steps: int = 5, spp: int = 64, res: int = 512):
+    """The small configuration at its size: the Cornell box, 512x512, 64
+    samples per pixel, depth 8, seed 0. One step renders all 64 sample
+    indices of the frame (the reference's render() of that camera); one
+    warm-up step, then `steps` timed steps on fresh sample indices, CUDA
+    events on the render stream, clocks sampled. Its working set (9
+    objects, 17 top-level nodes, the 262,144-path wave state of 33 MB)
+    lives in L2, so the traversal roofline is taken against a measured L2
+    copy bandwidth. The reference's CUDA build runs the same steps."""
+    import ctypes
+    import torch
+    from nectarrender_b200 import capi
+    spec = scenes.cornell(res=res, spp=spp * (steps + 2) + 1, depth=8, seed=0)
+    sc = capi.Scene(spec)
+    r = capi.Render(sc)
+    sh = ctypes.c_uint64()
+    r.lib.nr_render_stream(r.h, ctypes.byref(sh))
+    stream = torch.cuda.ExternalStream(sh.value)
+    r.samples(1, spp)  # warm-up (allocates the wave state)
+    r.counters(True)
+    r.samples(1 + spp, spp)
+    counts = r.last_counters()
+    r.counters(False)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(steps)]
+    torch.cuda.synchronize()
+    with Clocks(gpu) as clk:
+        for k in range(steps):
+            ev[k][0].record(stream)
+            r.samples(1 + (k + 1) * spp, spp)
+            ev[k][1].record(stream)
+        torch.cuda.synchronize()
+    t = sum(a.elapsed_time(b) for a, b in ev) * 1e-3
+    samples = float(res * res * spp * steps)
+    r.profiling(True)
+    r.samples(1 + spp, spp)
+    prof = r.last_profile()
+    r.profiling(False)
+    ext_ms = prof["extend"][0]
+    trav_bytes = (counts["node_visits"] * 80 + counts["tri_tests"] * 48 +
+                  counts["obj_tests"] * 128 + counts["rays"] * 56)
+    l2 = l2_copy_gbs()
+    achieved = trav_bytes / (ext_ms * 1e-3) / 1e9
+    out = {"workload": f"cornell {res}x{res}, {spp} spp, depth 8, seed 0 (small configuration)",
+           "value": samples / t, "unit": "samples/s", "steps": steps, "warmup": 1,
+           "ms_per_step": 1e3 * t / steps, "clocks": clk.summary(),
+           "kernels_ms_per_step": {k: v[0] for k, v in prof.items() if v[1]},
+           "roofline": {"bound": "l2", "kernel": "extend", "achieved": achieved,
+                        "peak": l2, "unit": "GB/s", "frac": achieved / l2,
+                        "peak_source": "measured here: L2-resident copy, 2 x 24 MiB",
+                        "algorithmic_bytes_per_step": trav_bytes,
+                        "rays_per_step": counts["rays"]}}
+    if not args.no_reference_cuda:
+        try:
+            import oracle
+            with Clocks(gpu) as rclk:
+                ms = oracle.RefCUDA().time_steps(spec, 1, 1, steps, spp)
+            rt = sum(ms) * 1e-3
+            out["reference_cuda"] = {"value": samples / rt, "unit": "samples/s",
+                                     "ms_per_step": 1e3 * rt / steps, "clocks": rclk.summary(),
+                                     "ratio": (samples / t) / (samples / rt)}
+        except Exception as e:  # noqa: BLE001 - reported, not fatal
+            out["reference_cuda"] = {"unavailable": repr(e)[:200]}
     return out
 
 
