@@ -165,7 +165,13 @@ typedef struct nr_render_config {
   int32_t mode;             /* NR_MODE_*                                    */
   int32_t schedule;         /* NR_SCHEDULE_*                                */
   int32_t fp64_accumulate;  /* also keep an FP64 sum of the beauty layer    */
-  uint32_t layer_mask;      /* bit i enables LayerType i (default 0x13)      */
+  uint32_t layer_mask;      /* bit i enables LayerType i (default 0x13).
+                               DEPTH (bit 6, one channel) holds the running
+                               mean of the first hit's world distance (0 on
+                               a miss), written by the wavefront schedule;
+                               the reference allocates it but never writes
+                               it. The other optional layers stay zero, as
+                               in the reference (engine/src/trace.cu:47-79) */
   int32_t extend_variant;   /* wavefront traversal kernel: 4, 5, 6, 8 = nested
                                two-level traversal with that many CTAs per
                                SM; 14..18 = flattened traversal with lane
@@ -518,25 +524,29 @@ int nr_conv3x3_wgrad_device(const void* dy, int32_t dy_stride, int32_t dy_off, c
                             int32_t x_stride, int32_t x_off, float* dw, int32_t cin,
                             int32_t cout, int32_t B, int32_t H, int32_t W, uint64_t stream);
 
-/* Learned denoiser: a five-level U-Net on the beauty, diffuse and
- * world-normal layers (the inputs the reference hands to OIDN,
- * nectar_render/csrc/data/include/data/stream.h:160-170), convolutions on
- * the tcgen05 tensor cores, trained on the GPU. Images are device float
- * planar CHW, B images of H x W stacked ([B][3][H][W]); H and W multiples of
- * 16; B*H*W at most the max_pixels given at creation. */
+/* Learned denoiser: a five-level U-Net (32 -> 128 channels) on the beauty,
+ * diffuse and world-normal layers (the inputs the reference hands to OIDN,
+ * nectar_render/csrc/data/include/data/stream.h:160-170) plus the depth
+ * layer, convolutions on the tcgen05 tensor cores, trained on the GPU.
+ * Images are device float planar CHW, B images of H x W stacked
+ * ([B][3][H][W]; depth [B][1][H][W], may be NULL); H and W multiples of 16;
+ * B*H*W at most the max_pixels given at creation. */
 typedef struct nr_denoiser nr_denoiser;
 int nr_denoiser_create(uint32_t max_pixels, uint32_t seed, nr_denoiser** out);
 int nr_denoiser_destroy(nr_denoiser* d);
-/* One training step toward `target`: forward, squared-error loss in log
- * space, backward and (lr > 0) an Adam update; lr <= 0 only computes
- * gradients. *loss = mean 0.5 (log(1+out) - log(1+target))^2 before the
- * update. */
+/* Training loss in log space, per channel d = log(1+out) - log(1+target):
+ * 1 = absolute error |d| (the default), 0 = squared error 0.5 d^2. */
+int nr_denoiser_set_loss(nr_denoiser* d, int32_t kind);
+/* One training step toward `target`: forward, loss, backward and (lr > 0)
+ * an Adam update; lr <= 0 only computes gradients. *loss = the mean loss
+ * before the update. */
 int nr_denoiser_train_step(nr_denoiser* d, const float* beauty, const float* diffuse,
-                           const float* normal, const float* target, int32_t B, int32_t H,
-                           int32_t W, float lr, double* loss, uint64_t stream);
+                           const float* normal, const float* depth, const float* target,
+                           int32_t B, int32_t H, int32_t W, float lr, double* loss,
+                           uint64_t stream);
 int nr_denoiser_infer(nr_denoiser* d, const float* beauty, const float* diffuse,
-                      const float* normal, float* out, int32_t B, int32_t H, int32_t W,
-                      uint64_t stream);
+                      const float* normal, const float* depth, float* out, int32_t B, int32_t H,
+                      int32_t W, uint64_t stream);
 /* Parameters (what = 0) or the last step's gradients (what = 1) as host
  * float arrays, layer by layer: weights [9][cout][cin] then bias [cout]. */
 int nr_denoiser_param_count(const nr_denoiser* d, uint64_t* out);

@@ -105,7 +105,8 @@ EXPORTS = [
     "nr_render_get_profile",
     "nr_render_graph_stats", "nr_render_set_fused_display", "nr_host_alloc", "nr_host_free", "nr_render_viewport", "nr_render_pick", "nr_render_selection_mask",
     "nr_conv3x3_forward_device", "nr_conv3x3_wgrad_device",
-    "nr_denoiser_create", "nr_denoiser_destroy", "nr_denoiser_train_step", "nr_denoiser_infer",
+    "nr_denoiser_create", "nr_denoiser_destroy", "nr_denoiser_set_loss",
+    "nr_denoiser_train_step", "nr_denoiser_infer",
     "nr_denoiser_param_count", "nr_denoiser_get_params", "nr_denoiser_set_params",
     "nr_denoiser_layers", "nr_nrc_create", "nr_nrc_destroy", "nr_nrc_infer", "nr_nrc_train",
     "nr_nrc_count", "nr_nrc_get", "nr_nrc_set", "nr_render_set_nrc", "nr_render_nrc_stats",
@@ -329,6 +330,13 @@ class Render:
 
     def layer(self, layer: int = 0) -> np.ndarray:
         out = np.zeros((3, self.H, self.W), np.float32)
+        _check(self.lib.nr_render_read_layer(self.h, layer, _fptr(out)), "nr_render_read_layer")
+        return out
+
+    def layer_channels(self, layer: int) -> np.ndarray:
+        """An enabled layer of any channel count (the depth layer has one)."""
+        c = 1 if layer in (5, 6) else 3
+        out = np.zeros((c, self.H, self.W), np.float32)
         _check(self.lib.nr_render_read_layer(self.h, layer, _fptr(out)), "nr_render_read_layer")
         return out
 

@@ -1272,6 +1272,7 @@ static KernelParams make_params(nr_render* r, uint32_t first, uint32_t count, bo
     P.beauty = r->layer[NR_LAYER_BEAUTY];
     P.diffuse = r->layer[NR_LAYER_DIFFUSE];
     P.normal = r->layer[NR_LAYER_WORLD_NORMAL];
+    P.depth_layer = r->cfg.schedule == NR_SCHEDULE_WAVEFRONT ? r->layer[NR_LAYER_DEPTH] : nullptr;
     P.beauty64 = r->beauty64;
   }
   P.work_counter = r->work;
@@ -2027,22 +2028,28 @@ static int den_status(const std::string& e) {
   return fail(NR_ERR_CUDA, e);
 }
 
+int nr_denoiser_set_loss(nr_denoiser* d, int32_t kind) {
+  if (!d) return fail(NR_ERR_INVALID, "null argument");
+  return den_status(denoiser_set_loss(d->d, kind));
+}
+
 int nr_denoiser_train_step(nr_denoiser* d, const float* beauty, const float* diffuse,
-                           const float* normal, const float* target, int32_t B, int32_t H,
-                           int32_t W, float lr, double* loss, uint64_t stream) {
+                           const float* normal, const float* depth, const float* target,
+                           int32_t B, int32_t H, int32_t W, float lr, double* loss,
+                           uint64_t stream) {
   if (!d || !beauty || !target) return fail(NR_ERR_INVALID, "null argument");
   cudaStream_t st = (cudaStream_t)(uintptr_t)stream;
-  int rc = den_status(denoiser_forward_backward(d->d, beauty, diffuse, normal, target, B, H, W,
-                                                loss, st));
+  int rc = den_status(denoiser_forward_backward(d->d, beauty, diffuse, normal, depth, target, B,
+                                                H, W, loss, st));
   if (rc != NR_OK || lr <= 0.0f) return rc;
   return den_status(denoiser_adam(d->d, lr, st));
 }
 
 int nr_denoiser_infer(nr_denoiser* d, const float* beauty, const float* diffuse,
-                      const float* normal, float* out, int32_t B, int32_t H, int32_t W,
-                      uint64_t stream) {
+                      const float* normal, const float* depth, float* out, int32_t B, int32_t H,
+                      int32_t W, uint64_t stream) {
   if (!d || !beauty || !out) return fail(NR_ERR_INVALID, "null argument");
-  return den_status(denoiser_infer(d->d, beauty, diffuse, normal, out, B, H, W,
+  return den_status(denoiser_infer(d->d, beauty, diffuse, normal, depth, out, B, H, W,
                                    (cudaStream_t)(uintptr_t)stream));
 }
 

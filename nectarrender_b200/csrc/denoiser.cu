@@ -14,7 +14,7 @@ namespace nr {
 namespace {
 
 constexpr int kLevels = 5;
-constexpr int kEnc[kLevels] = {32, 48, 64, 80, 96};
+constexpr int kEnc[kLevels] = {32, 48, 64, 96, 128};
 constexpr int kIn = 16;
 constexpr int kOut = 16;
 
@@ -36,9 +36,10 @@ __device__ __forceinline__ void st(const View& v, size_t pix, int c, float x) {
 
 int blocks_for(size_t n) { return (int)std::min<size_t>((n + 255) / 256, 148 * 16); }
 
-// Network input: log(1 + beauty), diffuse, normal, zero padding to 16.
-__global__ void k_prep(const float* beauty, const float* diffuse, const float* normal, View out,
-                       int B, int H, int W) {
+// Network input: log(1 + beauty), diffuse, normal, log(1 + depth), zero
+// padding to 16.
+__global__ void k_prep(const float* beauty, const float* diffuse, const float* normal,
+                       const float* depth, View out, int B, int H, int W) {
   const size_t hw = (size_t)H * W, P = (size_t)B * hw;
   GRID_STRIDE(p, P) {
     const size_t b = p / hw, i = p - b * hw;
@@ -48,27 +49,27 @@ __global__ void k_prep(const float* beauty, const float* diffuse, const float* n
       st(out, p, 3 + c, diffuse ? diffuse[base + c * hw] : 0.0f);
       st(out, p, 6 + c, normal ? normal[base + c * hw] : 0.0f);
     }
-    for (int c = 9; c < out.ch; ++c) st(out, p, c, 0.0f);
+    st(out, p, 9, depth ? log1pf(fmaxf(depth[b * hw + i], 0.0f)) : 0.0f);
+    for (int c = 10; c < out.ch; ++c) st(out, p, c, 0.0f);
   }
 }
 
 // The prediction is residual in log space: pred = log(1 + noisy beauty) +
 // the network's first three output channels, so an untrained network (small
 // output layer) starts near the identity and a clean input needs only a small
-// correction. Loss: squared error in log space, 0.5 * (pred - log(1 +
-// target))^2; d(loss)/d(output) = pred - log(1 + target) on the first three
-// channels (Adam is invariant to the gradient scale, so the 1/N of the mean
-// is left out), zero on the others. A squared error estimates the
-// conditional mean of the noisy targets (an absolute error would estimate
-// their median, which sits below the mean under the heavy-tailed noise of
-// path tracing).
+// correction. Loss (per channel, d = pred - log(1 + target)): absolute error
+// |d| (kind 1, the default), gradient sign(d); or squared error 0.5 d^2
+// (kind 0), gradient d. Adam is invariant to the gradient scale, so the 1/N
+// of the mean is left out. The absolute error estimates the conditional
+// median of the targets, the squared error their mean (the two part where
+// the targets themselves still carry heavy-tailed noise).
 __device__ __forceinline__ float log_beauty(const float* beauty, size_t b, size_t hw, int c,
                                             size_t i) {
   return log1pf(fmaxf(beauty[b * 3 * hw + c * hw + i], 0.0f));
 }
 
 __global__ void k_loss(View out, const float* beauty, const float* target, View dout, int B, int H,
-                       int W, double* loss) {
+                       int W, int kind, double* loss) {
   const size_t hw = (size_t)H * W, P = (size_t)B * hw;
   double local = 0.0;
   GRID_STRIDE(p, P) {
@@ -76,8 +77,13 @@ __global__ void k_loss(View out, const float* beauty, const float* target, View 
     for (int c = 0; c < 3; ++c) {
       const float t = log_beauty(target, b, hw, c, i);
       const float d = (log_beauty(beauty, b, hw, c, i) + ld(out, p, c)) - t;
-      local += 0.5 * (double)d * (double)d;
-      st(dout, p, c, d);
+      if (kind == 1) {
+        local += fabs((double)d);
+        st(dout, p, c, d > 0.0f ? 1.0f : (d < 0.0f ? -1.0f : 0.0f));
+      } else {
+        local += 0.5 * (double)d * (double)d;
+        st(dout, p, c, d);
+      }
     }
     for (int c = 3; c < dout.ch; ++c) st(dout, p, c, 0.0f);
   }
@@ -230,6 +236,7 @@ struct DenoiserNet {
   std::vector<void*> allocs;
   int step = 0;
   int B = 0, H = 0, W = 0;  // shape of the last forward
+  int loss_kind = 1;        // 1: absolute error, 0: squared error (log space)
 };
 
 Denoiser::~Denoiser() {
@@ -387,11 +394,11 @@ std::string check_shape(const DenoiserNet& n, int B, int H, int W) {
 }
 
 cudaError_t forward(DenoiserNet& n, const float* beauty, const float* diffuse, const float* normal,
-                    int B, int H, int W, cudaStream_t st) {
+                    const float* depth, int B, int H, int W, cudaStream_t st) {
   auto& Ls = n.layers;
   cudaError_t e;
   const size_t P0 = (size_t)B * H * W;
-  k_prep<<<blocks_for(P0), 256, 0, st>>>(beauty, diffuse, normal, n.x[0].v(), B, H, W);
+  k_prep<<<blocks_for(P0), 256, 0, st>>>(beauty, diffuse, normal, depth, n.x[0].v(), B, H, W);
   for (int l = 0; l < kLevels; ++l) {
     const int h = H >> l, w = W >> l;
     const Layer& A = Ls[2 * l];
@@ -498,8 +505,8 @@ std::string finish(DenoiserNet& n, cudaStream_t st, const char* what) {
 }  // namespace
 
 std::string denoiser_forward_backward(Denoiser& d, const float* beauty, const float* diffuse,
-                                      const float* normal, const float* target, int B, int H, int W,
-                                      double* loss, cudaStream_t st) {
+                                      const float* normal, const float* depth, const float* target,
+                                      int B, int H, int W, double* loss, cudaStream_t st) {
   if (!d.net) return "denoiser: not created";
   DenoiserNet& n = *d.net;
   std::string s = check_shape(n, B, H, W);
@@ -509,18 +516,18 @@ std::string denoiser_forward_backward(Denoiser& d, const float* beauty, const fl
     cudaMemsetAsync(L.gb, 0, sizeof(float) * L.cout, st);
   }
   cudaMemsetAsync(n.d_loss, 0, sizeof(double), st);
-  cudaError_t e = forward(n, beauty, diffuse, normal, B, H, W, st);
+  cudaError_t e = forward(n, beauty, diffuse, normal, depth, B, H, W, st);
   if (e != cudaSuccess) return cuda_msg(e, "denoiser forward");
   const size_t P0 = (size_t)B * H * W;
   k_loss<<<blocks_for(P0), 256, 0, st>>>(n.out.v(), beauty, target, n.g_out.v(), B, H, W,
-                                         n.d_loss);
+                                         n.loss_kind, n.d_loss);
   e = backward(n, B, H, W, st);
   if (e != cudaSuccess) return cuda_msg(e, "denoiser backward");
   s = finish(n, st, "denoiser training step");
   if (!s.empty()) return s;
   double h = 0.0;
   cudaMemcpy(&h, n.d_loss, sizeof(double), cudaMemcpyDeviceToHost);
-  if (loss) *loss = h / (3.0 * (double)P0);
+  if (loss) *loss = h / (3.0 * (double)P0);  // mean |d| or mean 0.5 d^2
   n.B = B;
   n.H = H;
   n.W = W;
@@ -544,15 +551,23 @@ std::string denoiser_adam(Denoiser& d, float lr, cudaStream_t st) {
 }
 
 std::string denoiser_infer(Denoiser& d, const float* beauty, const float* diffuse,
-                           const float* normal, float* out, int B, int H, int W, cudaStream_t st) {
+                           const float* normal, const float* depth, float* out, int B, int H, int W,
+                           cudaStream_t st) {
   if (!d.net) return "denoiser: not created";
   DenoiserNet& n = *d.net;
   std::string s = check_shape(n, B, H, W);
   if (!s.empty()) return s;
-  cudaError_t e = forward(n, beauty, diffuse, normal, B, H, W, st);
+  cudaError_t e = forward(n, beauty, diffuse, normal, depth, B, H, W, st);
   if (e != cudaSuccess) return cuda_msg(e, "denoiser forward");
   k_output<<<blocks_for((size_t)B * H * W), 256, 0, st>>>(n.out.v(), beauty, out, B, H, W);
   return finish(n, st, "denoiser inference");
+}
+
+std::string denoiser_set_loss(Denoiser& d, int kind) {
+  if (!d.net) return "denoiser: not created";
+  if (kind != 0 && kind != 1) return "denoiser: loss kind must be 0 (squared) or 1 (absolute)";
+  d.net->loss_kind = kind;
+  return {};
 }
 
 size_t denoiser_param_count(const Denoiser& d) {

@@ -21,6 +21,7 @@ struct KernelParams {
   float* beauty;      // planar CHW, 3 channels
   float* diffuse;
   float* normal;
+  float* depth_layer; // planar 1-channel first-hit distance (wavefront only), or null
   double* beauty64;   // FP64 running sum of beauty, or null
   uint32_t* primary;  // raw mode: primary hit id per pixel, or null
   uint32_t* work_counter;

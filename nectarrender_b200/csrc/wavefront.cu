@@ -832,6 +832,7 @@ __global__ void __launch_bounds__(kShadeThreads, kMinBlocks) k_wf_shade(WfParams
       } else {
         const DevMaterial& m = sc.materials[sc.objects[rec.obj].material];
         Ray r_in = s.ray;
+        if (bounce == 0u) aov_n.w = rec.t;  // DEPTH layer: world distance of the first hit
         if (kPerf && W.nrc_bounce && bounce >= 1u &&
             nrc_training_path(pix, wbase + k, W.nrc_train_one_in)) {
           const uint32_t ti = atomicAdd(&W.ctr[CTR_NT], 1u);
@@ -904,7 +905,7 @@ __global__ void __launch_bounds__(kShadeThreads, kMinBlocks) k_wf_shade(WfParams
             // the first-hit AOV sums start from zero (0 + x, as a running
             // sum from a cleared buffer computes it)
             aov_d = make_float4(0.f + s.atten.x, 0.f + s.atten.y, 0.f + s.atten.z, 0.f);
-            aov_n = make_float4(0.f + rec.n.x, 0.f + rec.n.y, 0.f + rec.n.z, 0.f);
+            aov_n = make_float4(0.f + rec.n.x, 0.f + rec.n.y, 0.f + rec.n.z, aov_n.w);
           }
           if (P.rr_enabled && bounce >= P.rr_start) {
             float survival = fmaxf(s.atten.x, fmaxf(s.atten.y, s.atten.z));
@@ -1002,7 +1003,7 @@ __global__ void __launch_bounds__(128) k_wf_tail(WfParams W, int qsel, uint32_t 
     }
     W.path[path_at(p, kRecBeauty)] = make_float4(s.beauty.x, s.beauty.y, s.beauty.z, __uint_as_float(s.primary));
     W.acc_d[p] = make_float4(s.diffuse.x, s.diffuse.y, s.diffuse.z, 0.f);
-    W.acc_n[p] = make_float4(s.normal.x, s.normal.y, s.normal.z, 0.f);
+    W.acc_n[p] = make_float4(s.normal.x, s.normal.y, s.normal.z, an.w);
   }
 }
 
@@ -1129,12 +1130,14 @@ __global__ void k_wf_accumulate(WfParams W) {
       if (P.beauty) store3(P.beauty, hw, pix, V3{b.x, b.y, b.z});
       if (P.diffuse) store3(P.diffuse, hw, pix, V3{d.x, d.y, d.z});
       if (P.normal) store3(P.normal, hw, pix, V3{n.x, n.y, n.z});
+      if (P.depth_layer) P.depth_layer[pix] = n.w;
       if (P.primary) P.primary[pix] = __float_as_uint(b.w);
       continue;
     }
     V3 ab = P.beauty ? load3(P.beauty, hw, pix) : V3{0, 0, 0};
     V3 ad = P.diffuse ? load3(P.diffuse, hw, pix) : V3{0, 0, 0};
     V3 an = P.normal ? load3(P.normal, hw, pix) : V3{0, 0, 0};
+    float az = P.depth_layer ? P.depth_layer[pix] : 0.0f;
     double s64[3] = {0, 0, 0};
     for (uint32_t k = 0; k < W.count; ++k) {
       uint32_t p = k * N + pix, smp = base + k;
@@ -1142,12 +1145,14 @@ __global__ void k_wf_accumulate(WfParams W) {
       ab = running_mean(ab, V3{b.x, b.y, b.z}, smp);
       ad = running_mean(ad, V3{d.x, d.y, d.z}, smp);
       an = running_mean(an, V3{n.x, n.y, n.z}, smp);
+      az = running_mean(V3{az, 0.f, 0.f}, V3{n.w, 0.f, 0.f}, smp).x;
       s64[0] += (double)b.x;
       s64[1] += (double)b.y;
       s64[2] += (double)b.z;
     }
     if (P.beauty) store3(P.beauty, hw, pix, ab);
     if (P.diffuse) store3(P.diffuse, hw, pix, ad);
+    if (P.depth_layer) P.depth_layer[pix] = az;
     if (P.normal) store3(P.normal, hw, pix, an);
     if (W.disp8) {  // the display transform of the new running mean, in the same pass
       const V3 c = display_pixel(ab, W.disp_p);

@@ -9,7 +9,7 @@ from nectarrender_b200 import capi, denoise, scenes
 pytestmark = pytest.mark.gpu
 torch = pytest.importorskip("torch")
 
-ENC = [32, 48, 64, 80, 96]
+ENC = [32, 48, 64, 96, 128]
 
 
 def bf(a):
@@ -54,10 +54,10 @@ def up_bwd(g):
     return g[0::2, 0::2] + g[1::2, 0::2] + g[0::2, 1::2] + g[1::2, 1::2]
 
 
-def unet_grads(params, x0, target, base):
+def unet_grads(params, x0, target, base, kind=1):
     """FP64 forward + backward of the network in denoiser.cuh (prediction =
-    base + the first three output channels); returns the loss and [(dw, db)]
-    in parameter order."""
+    base + the first three output channels; loss kind 1 = mean |d|, 0 =
+    mean 0.5 d^2); returns the loss and [(dw, db)] in parameter order."""
     P = [(w.astype(np.float64), b.astype(np.float64)) for w, b in params]
     acts = {}
     relu = lambda a: np.maximum(a, 0)
@@ -77,9 +77,9 @@ def unet_grads(params, x0, target, base):
         below = b
     out = conv(below, *P[i]); acts[i] = (below, out)
     d = (base + out[..., :3]) - target
-    loss = (0.5 * d * d).mean()
+    loss = np.abs(d).mean() if kind == 1 else (0.5 * d * d).mean()
     g_out = np.zeros_like(out)
-    g_out[..., :3] = d
+    g_out[..., :3] = np.sign(d) if kind == 1 else d
     grads = [None] * len(P)
     dskip = {}
     dw, db, dx = conv_bwd(g_out, acts[i][0], P[i][0]); grads[i] = (dw, db)
@@ -103,8 +103,10 @@ def unet_grads(params, x0, target, base):
     return loss, grads
 
 
-def test_gradients_match_fp64_network():
+@pytest.mark.parametrize("kind", [denoise.LOSS_ABSOLUTE, denoise.LOSS_SQUARED])
+def test_gradients_match_fp64_network(kind):
     den = denoise.Denoiser(max_pixels=32 * 32, seed=3)
+    den.set_loss(kind)
     params = den.params()
     # the GPU computes with BF16 weights: give the FP64 model the same values
     params64 = [(bf(w), b.astype(np.float64)) for w, b in params]
@@ -112,16 +114,18 @@ def test_gradients_match_fp64_network():
     beauty = rng.gamma(1.0, 0.5, (1, 3, 32, 32)).astype(np.float32)
     diffuse = rng.uniform(0, 1, (1, 3, 32, 32)).astype(np.float32)
     normal = rng.uniform(-1, 1, (1, 3, 32, 32)).astype(np.float32)
+    depth = rng.uniform(0.5, 8.0, (1, 1, 32, 32)).astype(np.float32)
     target = rng.gamma(1.0, 0.5, (1, 3, 32, 32)).astype(np.float32)
     t = lambda a: torch.from_numpy(a).cuda()
-    loss_gpu = den.train_step(t(beauty), t(diffuse), t(normal), t(target), lr=0.0)
+    loss_gpu = den.train_step(t(beauty), t(diffuse), t(normal), t(target), lr=0.0, depth=t(depth))
     grads = den.grads()
     x0 = np.zeros((32, 32, 16))
     x0[..., 0:3] = np.log1p(beauty[0].transpose(1, 2, 0))
     x0[..., 3:6] = diffuse[0].transpose(1, 2, 0)
     x0[..., 6:9] = normal[0].transpose(1, 2, 0)
+    x0[..., 9] = np.log1p(depth[0, 0])
     loss_ref, ref = unet_grads(params64, bf(x0), np.log1p(target[0].transpose(1, 2, 0).astype(np.float64)),
-                               np.log1p(beauty[0].transpose(1, 2, 0).astype(np.float64)))
+                               np.log1p(beauty[0].transpose(1, 2, 0).astype(np.float64)), kind)
     assert abs(loss_gpu - loss_ref) <= 0.02 * loss_ref
     for k, ((gw, gb), (rw, rb)) in enumerate(zip(grads, ref)):
         rw = rw.astype(np.float64)
@@ -136,16 +140,18 @@ def test_training_reduces_loss_and_error():
     spec = scenes.mesh_stress(levels=5, res_h=128, res_w=128, spp=257, depth=8, n_spheres=24,
                               hdri_size=(256, 128), scene_seed=4)
     sc = capi.Scene(spec)
-    noisy = capi.Render(sc, mode=capi.MODE_PERF)
+    noisy = capi.Render(sc, mode=capi.MODE_PERF, layer_mask=denoise.DENOISE_LAYERS)
     noisy.samples(1, 4)
     ref = capi.Render(sc, mode=capi.MODE_PERF, seed=99)
     ref.samples(1, 256)
     inp = denoise.render_layers(noisy)
+    assert inp[3] is not None and float(inp[3].max()) > 0   # the depth layer is rendered
     target = denoise.render_layers(ref)[0]
     den = denoise.Denoiser(max_pixels=4 * 64 * 64, seed=1)
-    first = den.train_step(*[a[:, :, :64, :64].contiguous() for a in inp],
-                           target[:, :, :64, :64].contiguous(), lr=0.0)
+    crop = lambda a: a[:, :, :64, :64].contiguous()
+    b, d, n, z = (crop(a) for a in inp)
+    first = den.train_step(b, d, n, crop(target), lr=0.0, depth=z)
     steps, secs, last = denoise.train(den, [(inp, target)], steps=300, crop=64, batch=4)
     assert np.isfinite(last) and last < 0.7 * first
-    out = denoise.Denoiser.infer(den, *[a[:, :, :64, :64].contiguous() for a in inp])
+    out = den.infer(b, d, n, depth=z)
     assert torch.isfinite(out).all()
