@@ -901,15 +901,27 @@ def time_to_rmse(args, target=0.01, top=2048):
     from nectarrender_b200 import capi, denoise
     h, w = 1080, 1920
     half = max(1, args.rmse_oracle_spp // 2)
-    spec = scenes.mesh_stress(levels=args.levels, res_h=h, res_w=w, spp=2 * half + top + 2)
+    # a render's sample streams are pixel + sample * W * H in 32 bits (the
+    # reference's Generator subsequence), about 2071 sample indices at
+    # 1920x1080: each oracle half is a sum of renders with other seeds
+    chunk = min(half, 2048)
+    spec = scenes.mesh_stress(levels=args.levels, res_h=h, res_w=w, spp=max(chunk, top) + 2)
     sc = capi.Scene(spec, mesh_leaf=args.mesh_leaf)
     halves = []
     t0 = time.perf_counter()
     for k in (1, 2):
-        orc = capi.Render(sc, mode=capi.MODE_PERF, fp64_accumulate=1, seed=spec.seed + 1000 * k)
-        orc.samples(1, half)
-        halves.append(orc.beauty_fp64())
-        del orc
+        acc, n_acc, j = None, 0, 0
+        while n_acc < half:
+            m = min(chunk, half - n_acc)
+            orc = capi.Render(sc, mode=capi.MODE_PERF, fp64_accumulate=1,
+                              seed=spec.seed + 1000 * k + 97 * j)
+            orc.samples(1, m)
+            s_, n_ = orc.beauty_fp64_sum()
+            acc = s_ if acc is None else acc + s_
+            n_acc += n_
+            j += 1
+            del orc
+        halves.append(acc / n_acc)
     oracle_s = time.perf_counter() - t0
     oracle = 0.5 * (halves[0] + halves[1])
     disp_o = _disp(oracle)
@@ -920,7 +932,8 @@ def time_to_rmse(args, target=0.01, top=2048):
     corr = lambda e: float(np.sqrt(max(e * e - e_or * e_or, 0.0)))
     out = {"workload": f"mesh_stress {w}x{h}, depth {spec.ray_depth} (the configuration's size)",
            "target_rmse": target, "domain": "sqrt(clamp(x,0,1)), all pixels x 3 channels",
-           "oracle": {"spp": 2 * half, "halves": 2, "mode": "perf, FP64 sums",
+           "oracle": {"spp": 2 * half, "halves": 2, "renders_per_half": -(-half // chunk),
+                      "mode": "perf, FP64 sums",
                       "wall_s": oracle_s, "rmse_between_halves": between,
                       "error_estimate": e_or},
            "curve_columns": ["spp", "device_ms", "rmse", "rmse_minus_oracle_error"]}

@@ -325,6 +325,11 @@ int nr_scene_set_hdri_params(nr_scene* scene, float rotation_deg, float intensit
 /* Leaf sizes of the 8-wide trees (1..3 primitives; defaults: meshes 1,
  * top level 1). Takes effect at the next nr_scene_build. */
 int nr_scene_set_tuning(nr_scene* scene, uint32_t mesh_leaf_max, uint32_t tlas_leaf_max);
+/* Children per wide node (4..8; default 8) of the mesh trees and of the top
+ * level: the node layout stays the 8-wide compressed one, a narrower tree
+ * uses fewer of its slots (more, smaller nodes, a deeper tree). Takes effect at the next
+ * nr_scene_build. No counterpart in the reference (its trees are binary). */
+int nr_scene_set_bvh_width(nr_scene* scene, uint32_t mesh_width, uint32_t tlas_width);
 /* Uploads the scene and builds every BVH on the GPU (Scene::build,
  * nectar_render/csrc/scene/src/scene.cpp:68-76). Must precede nr_render_create. */
 int nr_scene_build(nr_scene* scene);

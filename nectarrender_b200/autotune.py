@@ -5,6 +5,8 @@ speed but never the image:
 
   * ``mesh_leaf`` / ``tlas_leaf`` - primitives per 8-wide BVH leaf (1..3) of
     the mesh trees and of the top-level tree;
+  * ``mesh_width`` / ``tlas_width`` - children per wide BVH node (4 or 8)
+    of the same trees;
   * ``extend_variant`` - traversal kernel and the CTAs per SM its register
     budget targets: 4, 5, 6, 8 (nested two-level traversal; 128, 96, 80 or
     64 registers per thread) and 14, 15, 16, 18 (flattened traversal with lane
@@ -18,7 +20,8 @@ speed but never the image:
     (1) or in queue order (-1);
   * ``schedule`` - wavefront or the per-pixel megakernel.
 
-Every candidate renders the same samples (the parity tests cover each knob),
+Every candidate renders the same samples (the parity tests cover each knob;
+knobs that reshape a tree can only change which primitive wins an exact tie),
 so the record only trades time. A record is keyed by the scene's signature
 and can be saved and reused with :func:`load` / :func:`save`.
 """
@@ -39,6 +42,8 @@ VARIANTS = (5, 14, 514, 515, 414, 614)
 class Tuning:
     mesh_leaf: int = 1
     tlas_leaf: int = 1
+    mesh_width: int = 8
+    tlas_width: int = 8
     extend_variant: int = 514
     samples_per_wave: int = 0
     shade_variant: int = 6
@@ -53,7 +58,8 @@ class Tuning:
                 "schedule": self.schedule}
 
     def scene_overrides(self) -> dict:
-        return {"mesh_leaf": self.mesh_leaf, "tlas_leaf": self.tlas_leaf}
+        return {"mesh_leaf": self.mesh_leaf, "tlas_leaf": self.tlas_leaf,
+                "mesh_width": self.mesh_width, "tlas_width": self.tlas_width}
 
 
 def signature(spec: SceneSpec) -> str:
@@ -76,13 +82,14 @@ def _time(scene: capi.Scene, spec: SceneSpec, over: dict, samples: int, reps: in
 
 def tune(spec: SceneSpec, samples: int = 4, reps: int = 2, leaves=((1, 1), (2, 1), (3, 1), (1, 2)),
          variants=VARIANTS, waves=(0, 2, 4, 8), shades=(5, 6), sorts=(1, -1),
-         megakernel: bool = True) -> Tuning:
+         megakernel: bool = True, widths=((8, 8), (4, 8))) -> Tuning:
     """Times every candidate on `spec` (device time of `samples` sample
     indices, best of `reps`) and returns the fastest as a :class:`Tuning`."""
     table = []
     best = None
-    for mesh_leaf, tlas_leaf in leaves:
-        scene = capi.Scene(spec, mesh_leaf=mesh_leaf, tlas_leaf=tlas_leaf)
+    for (mesh_leaf, tlas_leaf), (mesh_width, tlas_width) in itertools.product(leaves, widths):
+        scene = capi.Scene(spec, mesh_leaf=mesh_leaf, tlas_leaf=tlas_leaf, mesh_width=mesh_width,
+                           tlas_width=tlas_width)
         cands = [dict(extend_variant=v, samples_per_wave=w, shade_variant=sv, sort_materials=so,
                       schedule=capi.SCHEDULE_WAVEFRONT)
                  for v, w, sv, so in itertools.product(variants, waves, shades, sorts)]
@@ -91,12 +98,14 @@ def tune(spec: SceneSpec, samples: int = 4, reps: int = 2, leaves=((1, 1), (2, 1
                               sort_materials=-1, schedule=capi.SCHEDULE_MEGAKERNEL))
         for over in cands:
             ms = _time(scene, spec, over, samples, reps)
-            row = dict(mesh_leaf=mesh_leaf, tlas_leaf=tlas_leaf, ms_per_sample=ms, **over)
+            row = dict(mesh_leaf=mesh_leaf, tlas_leaf=tlas_leaf, mesh_width=mesh_width,
+                       tlas_width=tlas_width, ms_per_sample=ms, **over)
             table.append(row)
             if best is None or ms < best["ms_per_sample"]:
                 best = row
         del scene
-    t = Tuning(**{k: best[k] for k in ("mesh_leaf", "tlas_leaf", "extend_variant",
+    t = Tuning(**{k: best[k] for k in ("mesh_leaf", "tlas_leaf", "mesh_width", "tlas_width",
+                                       "extend_variant",
                                        "samples_per_wave", "shade_variant", "sort_materials",
                                        "schedule", "ms_per_sample")})
     t.table = table

@@ -98,7 +98,7 @@ EXPORTS = [
     "nr_scene_load_obj", "nr_scene_load_obj_device",
     "nr_scene_add_object", "nr_scene_set_sky_null", "nr_scene_set_sky_simple",
     "nr_scene_set_sky_hdri", "nr_scene_load_hdr", "nr_scene_set_hdri_params",
-    "nr_scene_set_tuning", "nr_scene_build",
+    "nr_scene_set_tuning", "nr_scene_set_bvh_width", "nr_scene_build",
     "nr_scene_get_stats", "nr_scene_get_bounds", "nr_scene_get_sky_tables", "nr_scene_get_binary_bvh", "nr_render_config_default",
     "nr_render_create", "nr_render_destroy", "nr_render_reset", "nr_render_samples",
     "nr_render_samples_static", "nr_render_samples_batch", "nr_render_set_profiling",
@@ -201,14 +201,17 @@ class Scene:
     reference: one material per hittable, lights after hittables)."""
 
     def __init__(self, spec: SceneSpec, build: bool = True, mesh_leaf: int = 1, tlas_leaf: int = 1,
-                 obj_on_device: bool = False):
+                 obj_on_device: bool = False, mesh_width: int = 8, tlas_width: int = 8):
         """obj_on_device: assemble the OBJ meshes' vertices on the GPU
-        (nr_scene_load_obj_device; the same meshes as the host reader)."""
+        (nr_scene_load_obj_device; the same meshes as the host reader).
+        mesh_width / tlas_width: children per wide BVH node (4..8)."""
         self.lib = library()
         self.spec = spec
         self.h = C.c_void_p()
         _check(self.lib.nr_scene_create(C.byref(self.h)), "nr_scene_create")
         _check(self.lib.nr_scene_set_tuning(self.h, mesh_leaf, tlas_leaf), "nr_scene_set_tuning")
+        _check(self.lib.nr_scene_set_bvh_width(self.h, mesh_width, tlas_width),
+               "nr_scene_set_bvh_width")
         load = self.lib.nr_scene_load_obj_device if obj_on_device else self.lib.nr_scene_load_obj
         for path in spec.meshes:
             mid = C.c_uint32()

@@ -937,7 +937,7 @@ struct WideWork {
 __global__ void k_collapse(const BinNode* nodes, const uint32_t* order, const WideWork* cur,
                            uint32_t n_cur, WideWork* next, uint32_t* n_next,
                            uint32_t* wide_counter, uint32_t* prim_counter, Bvh8Node* wide,
-                           uint32_t* order8, uint32_t leaf_max) {
+                           uint32_t* order8, uint32_t leaf_max, uint32_t width) {
   uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= n_cur) return;
   WideWork item = cur[w];
@@ -949,7 +949,7 @@ __global__ void k_collapse(const BinNode* nodes, const uint32_t* order, const Wi
   } else {
     ch[n++] = P.left;
     ch[n++] = P.right;
-    while (n < 8) {
+    while (n < (int)width) {
       int best = -1;
       float best_a = -1.0f;
       for (int i = 0; i < n; ++i) {
@@ -1091,9 +1091,11 @@ void free_build(BuildResult& r) {
 }
 
 int build_bvh(const float4* d_lo, const float4* d_hi, uint32_t n, bool want_bvh8,
-              BuildResult& out, cudaStream_t st, uint32_t leaf_max) {
+              BuildResult& out, cudaStream_t st, uint32_t leaf_max, uint32_t width) {
   if (leaf_max < 1) leaf_max = 1;
   if (leaf_max > 3) leaf_max = 3;
+  if (width < 2) width = 2;
+  if (width > 8) width = 8;
   out = BuildResult{};
   if (n == 0) return 0;
   cudaEvent_t ev0, ev1;
@@ -1280,7 +1282,7 @@ int build_bvh(const float4* d_lo, const float4* d_hi, uint32_t n, bool want_bvh8
       NR_TRY(cudaMemsetAsync(counters + 6, 0, 4, st));
       k_collapse<<<(n_cur + 127) / 128, 128, 0, st>>>(nodes, order, wa, n_cur, wb, counters + 6,
                                                       counters + 4, counters + 5, out.d_bvh8,
-                                                      out.d_order8, leaf_max);
+                                                      out.d_order8, leaf_max, width);
       NR_TRY(cudaGetLastError());
       NR_TRY(cudaMemcpyAsync(&n_cur, counters + 6, 4, cudaMemcpyDeviceToHost, st));
       NR_TRY(cudaStreamSynchronize(st));

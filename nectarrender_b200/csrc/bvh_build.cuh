@@ -31,9 +31,11 @@ struct BuildResult {
 // Builds the binary SAH tree over `n` primitive boxes given as device arrays
 // lo[i] = (x, y, z, _), hi[i] = (x, y, z, _) and derives the 2-wide and
 // 8-wide traversal layouts; 8-wide leaves hold at most `leaf_max` (1..3)
-// primitives. Returns a cudaError_t value.
+// primitives, and each wide node at most `width` (2..8) children (the node
+// format stays 8-wide; a narrower tree leaves slots empty). Returns a
+// cudaError_t value.
 int build_bvh(const float4* d_lo, const float4* d_hi, uint32_t n, bool want_bvh8,
-              BuildResult& out, cudaStream_t st, uint32_t leaf_max = 3);
+              BuildResult& out, cudaStream_t st, uint32_t leaf_max = 3, uint32_t width = 8);
 
 void free_build(BuildResult& r);
 

@@ -394,6 +394,7 @@ struct nr_scene {
   float world_lo[3] = {0.f, 0.f, 0.f}, world_hi[3] = {0.f, 0.f, 0.f};  // union of object boxes
   int32_t light = -1;
   uint32_t mesh_leaf_max = 1, tlas_leaf_max = 1;
+  uint32_t mesh_width = 8, tlas_width = 8;
 
   void release_device() {
     for (auto p : d_images) cudaFree(p);
@@ -735,6 +736,17 @@ int nr_scene_set_hdri_params(nr_scene* s, float rotation, float intensity) {
   return NR_OK;
 }
 
+int nr_scene_set_bvh_width(nr_scene* s, uint32_t mesh_width, uint32_t tlas_width) {
+  // narrower trees are deeper: below 4 children their depth could outgrow
+  // the traversal kernels' fixed stacks
+  if (!s || mesh_width < 4 || mesh_width > 8 || tlas_width < 4 || tlas_width > 8)
+    return fail(NR_ERR_INVALID, "nr_scene_set_bvh_width: widths must be 4..8");
+  s->mesh_width = mesh_width;
+  s->tlas_width = tlas_width;
+  s->built = false;
+  return NR_OK;
+}
+
 int nr_scene_set_tuning(nr_scene* s, uint32_t mesh_leaf_max, uint32_t tlas_leaf_max) {
   if (!s || mesh_leaf_max < 1 || mesh_leaf_max > 3 || tlas_leaf_max < 1 || tlas_leaf_max > 3)
     return fail(NR_ERR_INVALID, "nr_scene_set_tuning: leaf sizes must be 1..3");
@@ -798,7 +810,7 @@ int nr_scene_build(nr_scene* s) {
     CU(cudaMalloc(&lo, sizeof(float4) * nt), "alloc boxes");
     CU(cudaMalloc(&hi, sizeof(float4) * nt), "alloc boxes");
     k_tri_boxes<<<(nt + 255) / 256, 256, 0, st>>>(g.pos, g.vidx, nt, lo, hi);
-    int be = build_bvh(lo, hi, nt, true, g.bvh, st, s->mesh_leaf_max);
+    int be = build_bvh(lo, hi, nt, true, g.bvh, st, s->mesh_leaf_max, s->mesh_width);
     cudaFree(lo);
     cudaFree(hi);
     if (be != 0) return cuda_fail((cudaError_t)be, "mesh BVH build");
@@ -867,7 +879,8 @@ int nr_scene_build(nr_scene* s) {
   float4 *dlo = nullptr, *dhi = nullptr;
   CU(upload(dlo, blo.data(), blo.size(), st), "upload boxes");
   CU(upload(dhi, bhi.data(), bhi.size(), st), "upload boxes");
-  int be = build_bvh(dlo, dhi, (uint32_t)objs.size(), true, s->tlas, st, s->tlas_leaf_max);
+  int be = build_bvh(dlo, dhi, (uint32_t)objs.size(), true, s->tlas, st, s->tlas_leaf_max,
+                     s->tlas_width);
   cudaFree(dlo);
   cudaFree(dhi);
   if (be != 0) return cuda_fail((cudaError_t)be, "top-level BVH build");
