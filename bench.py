@@ -378,27 +378,16 @@ def run_ours(args):
             # per GPU: this arm's value over N GPUs against the reference on one
             ref_cuda["ratio"] = value / world / ref_cuda["value"]
 
-    rmse = None
-    if rank == 0 and world == 1 and not args.no_rmse:
-        rmse = time_to_rmse(args)
-    multi = None
-    if rank == 0 and world == 1 and not args.no_multi:
-        multi = multi_scene(args)
-    learned = None
-    if rank == 0 and world == 1 and not args.no_denoiser:
-        learned = learned_kernels(peaks)
-    cache = None
-    if rank == 0 and world == 1 and not args.no_nrc:
-        cache = radiance_cache(args)
-    batch = None
-    if rank == 0 and world == 1 and args.batch_rmse:
-        batch = batch_rmse(args)
-    cornell01 = None
-    if rank == 0 and world == 1 and args.rmse_cornell:
-        cornell01 = cornell_time_to_rmse(args)
-    small = None
-    if rank == 0 and world == 1 and not args.no_small:
-        small = small_config(args, local)
+    # the sections after the headline: a failure is recorded in its place
+    # and does not cost the line
+    one = rank == 0 and world == 1
+    rmse = section(one and not args.no_rmse, time_to_rmse, args)
+    multi = section(one and not args.no_multi, multi_scene, args)
+    learned = section(one and not args.no_denoiser, learned_kernels, peaks)
+    cache = section(one and not args.no_nrc, radiance_cache, args)
+    batch = section(one and args.batch_rmse, batch_rmse, args)
+    cornell01 = section(one and args.rmse_cornell, cornell_time_to_rmse, args)
+    small = section(one and not args.no_small, small_config, args, local)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -448,6 +437,18 @@ def run_ours(args):
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def section(enabled, fn, *a):
+    """fn(*a) if enabled, else None; an exception becomes {"error": ...}."""
+    if not enabled:
+        return None
+    try:
+        return fn(*a)
+    except Exception as e:  # noqa: BLE001 - reported in the line, not fatal
+        import traceback
+        traceback.print_exc()
+        return {"error": repr(e)[:300]}
 
 
 def e2e_public_api(pt, spec, S, args):
@@ -872,7 +873,7 @@ def _disp(x):
 def _time_at(curve, err):
     """Time a (samples, ms, rmse) curve needs to reach `err` (log-log
     interpolation between the points around it), or None."""
-    for (s0, m0, e0), (s1, m1, e1) in zip(curve, curve[1:]):
+    for (s0, m0, e0, *_), (s1, m1, e1, *_) in zip(curve, curve[1:]):
         if e0 > err >= e1 and e1 < e0:
             f = (np.log(err) - np.log(e0)) / (np.log(e1) - np.log(e0))
             return float(np.exp(np.log(m0) + f * (np.log(m1) - np.log(m0))))

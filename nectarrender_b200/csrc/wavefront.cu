@@ -672,78 +672,82 @@ __global__ void __launch_bounds__(kExtThreads, kMinBlocks) k_wf_extend_flat(WfPa
           }
         }
       }
-    } else if (ng.y > 0x00ffffffu) {
-      // one wide node
-      const uint32_t hits = ng.y;
-      const uint32_t child_bit = 31u - __clz(hits);
-      ng.y &= ~(1u << child_bit);
-      const uint32_t cslot = (child_bit - 24u) ^ (oct4 & 7u);
-      const uint32_t node_index = ng.x + __popc((hits & 0xffu) & ~(0xffffffffu << cslot));
-      if (node_index >= cur_n) {
-        atomicOr(P.err, 8u);
-        ng.y = 0u;
-        sp = 0;
-      } else {
-        if (ng.y > 0x00ffffffu) {
-          const int depth = in_mesh ? stack_cap(kBlasStack, sc) : stack_cap(kTlasStack, sc);
-          uint2* stk = in_mesh ? bstk : tstk;
-          if (sp < depth) stk[(sp++) * kExtThreads] = ng;
-          else atomicOr(P.err, 1u);
-        }
-        float4 n0;
-        uint4 n1;
-        const uint32_t hm = bvh8_intersect(cur_nodes + node_index, o, inv, oct4, EPS, tmax, n0, n1);
-        if (kCount) nodes++;
-        ng = make_uint2(n1.x, (hm & 0xff000000u) | (__float_as_uint(n0.w) >> 24));
-        tg = make_uint2(n1.y, hm & 0x00ffffffu);
-      }
-    } else if (sp > 0) {
-      uint2* stk = in_mesh ? bstk : tstk;
-      ng = stk[(--sp) * kExtThreads];
-    } else if (in_mesh) {
-      // leave the mesh tree: the candidate competes in world space
-      const V3 wo{cf(FS_WO), cf(FS_WO + 1), cf(FS_WO + 2)};
-      const V3 wd{cf(FS_WD), cf(FS_WD + 1), cf(FS_WD + 2)};
-      float tl_tmax = cf(FS_TL_TMAX);
-      if (best_slot >= 0) {
-        const uint32_t oi = cu(FS_MESH_OI);
-        const DevObject& ob = sc.objects[oi];
-        const DevMesh& m = sc.meshes[ob.mesh];
-        const uint32_t tri = __float_as_uint(__ldg(&m.tris8[best_slot].v0.w));
-        Ray r;
-        r.o = o;
-        r.d = d;
-        r.inv = inv;
-        r.tm = 0.f;
-        const Ray wr = make_ray(wo, wd, 0.f);
-        const float tw = world_t(ray_at(r, tmax), mesh_normal(m, tri, bu, bv), ob, r, wr);
-        if (EPS < tw && tw < best) {
-          best = tw;
-          tl_tmax = best;
-          cu(FS_OUT_OBJ) = oi;
-          cu(FS_OUT_SLOT) = (uint32_t)best_slot;
-          cf(FS_OUT_T) = tmax;
-          cf(FS_OUT_U) = bu;
-          cf(FS_OUT_V) = bv;
-        }
-      }
-      ng = make_uint2(cu(FS_TL_NG), cu(FS_TL_NG + 1));
-      tg = make_uint2(cu(FS_TL_TG), cu(FS_TL_TG + 1));
-      sp = (int)cu(FS_TL_SP);
-      tmax = tl_tmax;
-      o = wo;
-      d = wd;
-      inv = V3{1.0f / d.x, 1.0f / d.y, 1.0f / d.z};
-      oct4 = octant_inv4(d);
-      in_mesh = false;
-      cur_nodes = sc.tlas8;
-      cur_n = sc.n_tlas8;
     } else {
-      const uint32_t p = cu(FS_PATH);
-      W.hit[p] = make_uint4(cu(FS_OUT_OBJ), cu(FS_OUT_SLOT), cu(FS_OUT_U), cu(FS_OUT_V));
-      W.hit_t[p] = cf(FS_OUT_T);
-      if (binned) kh.add(W, sc, p, cu(FS_OUT_OBJ));
-      active = false;
+      // a stack pop and the node it names share one iteration
+      if (ng.y <= 0x00ffffffu && sp > 0) {
+        uint2* stk = in_mesh ? bstk : tstk;
+        ng = stk[(--sp) * kExtThreads];
+      }
+      if (ng.y > 0x00ffffffu) {
+        // one wide node
+        const uint32_t hits = ng.y;
+        const uint32_t child_bit = 31u - __clz(hits);
+        ng.y &= ~(1u << child_bit);
+        const uint32_t cslot = (child_bit - 24u) ^ (oct4 & 7u);
+        const uint32_t node_index = ng.x + __popc((hits & 0xffu) & ~(0xffffffffu << cslot));
+        if (node_index >= cur_n) {
+          atomicOr(P.err, 8u);
+          ng.y = 0u;
+          sp = 0;
+        } else {
+          if (ng.y > 0x00ffffffu) {
+            const int depth = in_mesh ? stack_cap(kBlasStack, sc) : stack_cap(kTlasStack, sc);
+            uint2* stk = in_mesh ? bstk : tstk;
+            if (sp < depth) stk[(sp++) * kExtThreads] = ng;
+            else atomicOr(P.err, 1u);
+          }
+          float4 n0;
+          uint4 n1;
+          const uint32_t hm = bvh8_intersect(cur_nodes + node_index, o, inv, oct4, EPS, tmax, n0, n1);
+          if (kCount) nodes++;
+          ng = make_uint2(n1.x, (hm & 0xff000000u) | (__float_as_uint(n0.w) >> 24));
+          tg = make_uint2(n1.y, hm & 0x00ffffffu);
+        }
+      } else if (in_mesh) {
+        // leave the mesh tree: the candidate competes in world space
+        const V3 wo{cf(FS_WO), cf(FS_WO + 1), cf(FS_WO + 2)};
+        const V3 wd{cf(FS_WD), cf(FS_WD + 1), cf(FS_WD + 2)};
+        float tl_tmax = cf(FS_TL_TMAX);
+        if (best_slot >= 0) {
+          const uint32_t oi = cu(FS_MESH_OI);
+          const DevObject& ob = sc.objects[oi];
+          const DevMesh& m = sc.meshes[ob.mesh];
+          const uint32_t tri = __float_as_uint(__ldg(&m.tris8[best_slot].v0.w));
+          Ray r;
+          r.o = o;
+          r.d = d;
+          r.inv = inv;
+          r.tm = 0.f;
+          const Ray wr = make_ray(wo, wd, 0.f);
+          const float tw = world_t(ray_at(r, tmax), mesh_normal(m, tri, bu, bv), ob, r, wr);
+          if (EPS < tw && tw < best) {
+            best = tw;
+            tl_tmax = best;
+            cu(FS_OUT_OBJ) = oi;
+            cu(FS_OUT_SLOT) = (uint32_t)best_slot;
+            cf(FS_OUT_T) = tmax;
+            cf(FS_OUT_U) = bu;
+            cf(FS_OUT_V) = bv;
+          }
+        }
+        ng = make_uint2(cu(FS_TL_NG), cu(FS_TL_NG + 1));
+        tg = make_uint2(cu(FS_TL_TG), cu(FS_TL_TG + 1));
+        sp = (int)cu(FS_TL_SP);
+        tmax = tl_tmax;
+        o = wo;
+        d = wd;
+        inv = V3{1.0f / d.x, 1.0f / d.y, 1.0f / d.z};
+        oct4 = octant_inv4(d);
+        in_mesh = false;
+        cur_nodes = sc.tlas8;
+        cur_n = sc.n_tlas8;
+      } else {
+        const uint32_t p = cu(FS_PATH);
+        W.hit[p] = make_uint4(cu(FS_OUT_OBJ), cu(FS_OUT_SLOT), cu(FS_OUT_U), cu(FS_OUT_V));
+        W.hit_t[p] = cf(FS_OUT_T);
+        if (binned) kh.add(W, sc, p, cu(FS_OUT_OBJ));
+        active = false;
+      }
     }
   }
   if (binned) kh.flush(W);

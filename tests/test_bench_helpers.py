@@ -1,0 +1,20 @@
+"""Host-side helpers of bench.py (no GPU): the time-at-error interpolation of
+the time-to-RMSE curves and the section guard."""
+import bench
+
+
+def test_time_at_interpolates_in_log_log():
+    curve = [[1, 10.0, 0.4, 0.39], [2, 20.0, 0.1, 0.09], [4, 40.0, 0.05, 0.04]]
+    assert bench._time_at(curve, 0.4) == 10.0
+    t = bench._time_at(curve, 0.2)
+    assert 10.0 < t < 20.0 and abs(t - 10.0 * 2 ** 0.5) < 1e-9   # halfway in log error
+    assert bench._time_at(curve, 0.01) is None
+    assert bench._time_at([[1, 5.0, 0.001]], 0.01) == 5.0
+
+
+def test_section_records_failures():
+    def boom():
+        raise ValueError("x")
+    assert bench.section(False, boom) is None
+    assert "ValueError" in bench.section(True, boom)["error"]
+    assert bench.section(True, lambda a: a + 1, 1) == 2

@@ -60,4 +60,5 @@ def test_narrow_trees_render_the_same_hits(spec):
     st4 = capi.Scene(spec, mesh_width=4, tlas_width=4).stats()
     st8 = capi.Scene(spec).stats()
     assert st4["wide_nodes"] > st8["wide_nodes"]          # smaller nodes, more of them
-    assert st4["sah_cost_binary"] == st8["sah_cost_binary"]  # the same binary tree
+    # the same binary tree (its cost summed on the GPU in another order)
+    assert st4["sah_cost_binary"] == pytest.approx(st8["sah_cost_binary"], rel=1e-9)
