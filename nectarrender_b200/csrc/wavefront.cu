@@ -507,7 +507,11 @@ enum : uint32_t {
 constexpr size_t kExtStackBytes = sizeof(uint2) * (kTlasStack + kBlasStack) * kExtThreads;
 constexpr size_t kFlatSmemBytes = kExtStackBytes + sizeof(uint32_t) * FS_COUNT * kExtThreads;
 
-template <bool kCount, int kMinBlocks, uint32_t kRefill = 12>
+// kVote: each iteration a warp runs one kind of work, primitive tests or
+// the rest (nodes, mesh exits, ends of rays), whichever more of its lanes
+// have next; the other lanes wait an iteration. Every ray still takes the
+// same steps in the same order, so the hits are the same.
+template <bool kCount, int kMinBlocks, uint32_t kRefill = 12, bool kVote = false>
 __global__ void __launch_bounds__(kExtThreads, kMinBlocks) k_wf_extend_flat(WfParams W, int qsel,
                                                                             int identity) {
   if (W.ctr[CTR_TAIL]) return;
@@ -589,7 +593,13 @@ __global__ void __launch_bounds__(kExtThreads, kMinBlocks) k_wf_extend_flat(WfPa
         }
       }
     }
-    if (__ballot_sync(0xffffffffu, active) == 0u) break;
+    const uint32_t act_mask = __ballot_sync(0xffffffffu, active);
+    if (act_mask == 0u) break;
+    if (kVote) {
+      const uint32_t prim_mask = __ballot_sync(0xffffffffu, active && tg.y != 0u);
+      const bool run_prims = __popc(prim_mask) >= __popc(act_mask & ~prim_mask);
+      if (active && (tg.y != 0u) != run_prims) continue;
+    }
     if (!active) continue;
 
     if (++steps > sc.max_steps) {
@@ -1325,6 +1335,9 @@ static ExtendFn extend_fn(bool counters, int variant) {
     case 24: return counters ? k_wf_extend_flat<true, 4, 8> : k_wf_extend_flat<false, 4, 8>;
     case 34: return counters ? k_wf_extend_flat<true, 4, 16> : k_wf_extend_flat<false, 4, 16>;
     case 44: return counters ? k_wf_extend_flat<true, 4, 24> : k_wf_extend_flat<false, 4, 24>;
+    // 64 / 65: as 14 / 15, each iteration running the kind of work most lanes have next
+    case 64: return counters ? k_wf_extend_flat<true, 4, 12, true> : k_wf_extend_flat<false, 4, 12, true>;
+    case 65: return counters ? k_wf_extend_flat<true, 5, 12, true> : k_wf_extend_flat<false, 5, 12, true>;
     default: return counters ? k_wf_extend<true, 4> : k_wf_extend<false, 4>;
   }
 }
