@@ -356,6 +356,27 @@ def run_ours(args):
         except (OSError, KeyError, ValueError):
             traffic = None
 
+    # L2 side of the roofline and SIMT efficiency, from one ncu capture of
+    # the two largest traversal launches (camera rays, first indirect
+    # bounce): L2 bytes (lts__t_sectors x 32) per launch against a live
+    # L2-resident read ceiling, threads per executed instruction
+    l2 = None
+    lp = HERE / "profiles" / "extend_l2_simt.json"
+    if lp.exists():
+        try:
+            prof = json.loads(lp.read_text())
+            ceiling = l2_read_gbs()
+            l2 = {"ceiling_gbs": ceiling, "ceiling_source": "measured here: L2-resident reads",
+                  "profile": "profiles/extend_l2_simt.json", "launches": {}}
+            for name, m in prof["launches"].items():
+                gbs = m["l2_bytes"] / (m["ms"] * 1e-3) / 1e9
+                l2["launches"][name] = {"l2_gbs": gbs, "frac_of_l2_ceiling": gbs / ceiling,
+                                        "simt_threads_per_instruction": m["threads_per_instruction"],
+                                        "simt_efficiency": m["threads_per_instruction"] / 32.0,
+                                        "issue_active_pct": m["issue_active_pct"]}
+        except (OSError, KeyError, ValueError, ZeroDivisionError):
+            l2 = None
+
     # end to end through the public API: render + display readback to host
     # end to end through the public API on every rank (weak scaling: each
     # rank's engine renders its own S samples per step); the job's value is
@@ -410,6 +431,7 @@ def run_ours(args):
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "traffic": traffic,
                              "kernel": dom, "peak_source": peak_src,
+                             "l2_and_simt": l2,
                              "algorithmic_bytes_per_launch": dom_bytes / dom_launches,
                              "launch_ms": dom_ms / dom_launches,
                              "counts_per_step": counts},
