@@ -507,11 +507,12 @@ enum : uint32_t {
 constexpr size_t kExtStackBytes = sizeof(uint2) * (kTlasStack + kBlasStack) * kExtThreads;
 constexpr size_t kFlatSmemBytes = kExtStackBytes + sizeof(uint32_t) * FS_COUNT * kExtThreads;
 
-// kVote: each iteration a warp runs one kind of work, primitive tests or
-// the rest (nodes, mesh exits, ends of rays), whichever more of its lanes
-// have next; the other lanes wait an iteration. Every ray still takes the
-// same steps in the same order, so the hits are the same.
-template <bool kCount, int kMinBlocks, uint32_t kRefill = 12, bool kVote = false>
+// kVote (1-3): each iteration a warp runs one kind of work, primitive tests
+// or the rest (nodes, mesh exits, ends of rays); the other lanes wait an
+// iteration. Primitive tests run when p lanes have one next and n lanes the
+// rest with p >= n (1), 2p >= n (2) or p >= 2n (3). Every ray still takes
+// the same steps in the same order, so the hits are the same.
+template <bool kCount, int kMinBlocks, uint32_t kRefill = 12, int kVote = 0>
 __global__ void __launch_bounds__(kExtThreads, kMinBlocks) k_wf_extend_flat(WfParams W, int qsel,
                                                                             int identity) {
   if (W.ctr[CTR_TAIL]) return;
@@ -597,7 +598,10 @@ __global__ void __launch_bounds__(kExtThreads, kMinBlocks) k_wf_extend_flat(WfPa
     if (act_mask == 0u) break;
     if (kVote) {
       const uint32_t prim_mask = __ballot_sync(0xffffffffu, active && tg.y != 0u);
-      const bool run_prims = __popc(prim_mask) >= __popc(act_mask & ~prim_mask);
+      const int np = __popc(prim_mask), nn = __popc(act_mask & ~prim_mask);
+      const bool run_prims = np > 0 && (kVote == 1   ? np >= nn
+                                        : kVote == 2 ? 2 * np >= nn
+                                                     : np >= 2 * nn || nn == 0);
       if (active && (tg.y != 0u) != run_prims) continue;
     }
     if (!active) continue;
@@ -1335,9 +1339,14 @@ static ExtendFn extend_fn(bool counters, int variant) {
     case 24: return counters ? k_wf_extend_flat<true, 4, 8> : k_wf_extend_flat<false, 4, 8>;
     case 34: return counters ? k_wf_extend_flat<true, 4, 16> : k_wf_extend_flat<false, 4, 16>;
     case 44: return counters ? k_wf_extend_flat<true, 4, 24> : k_wf_extend_flat<false, 4, 24>;
-    // 64 / 65: as 14 / 15, each iteration running the kind of work most lanes have next
-    case 64: return counters ? k_wf_extend_flat<true, 4, 12, true> : k_wf_extend_flat<false, 4, 12, true>;
-    case 65: return counters ? k_wf_extend_flat<true, 5, 12, true> : k_wf_extend_flat<false, 5, 12, true>;
+    // 64 / 74 / 84: as 14, each iteration running one kind of work (vote 1 / 2 / 3);
+    // 65: 64 at 5 CTAs per SM; 66 / 67: 64 refilling at 8 / 16 idle lanes
+    case 64: return counters ? k_wf_extend_flat<true, 4, 12, 1> : k_wf_extend_flat<false, 4, 12, 1>;
+    case 65: return counters ? k_wf_extend_flat<true, 5, 12, 1> : k_wf_extend_flat<false, 5, 12, 1>;
+    case 66: return counters ? k_wf_extend_flat<true, 4, 8, 1> : k_wf_extend_flat<false, 4, 8, 1>;
+    case 67: return counters ? k_wf_extend_flat<true, 4, 16, 1> : k_wf_extend_flat<false, 4, 16, 1>;
+    case 74: return counters ? k_wf_extend_flat<true, 4, 12, 2> : k_wf_extend_flat<false, 4, 12, 2>;
+    case 84: return counters ? k_wf_extend_flat<true, 4, 12, 3> : k_wf_extend_flat<false, 4, 12, 3>;
     default: return counters ? k_wf_extend<true, 4> : k_wf_extend<false, 4>;
   }
 }
