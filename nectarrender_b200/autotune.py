@@ -10,8 +10,9 @@ speed but never the image:
   * ``extend_variant`` - traversal kernel and the CTAs per SM its register
     budget targets: 4, 5, 6, 8 (nested two-level traversal; 128, 96, 80 or
     64 registers per thread) and 14, 15, 16, 18 (flattened traversal with lane
-    refill, same budgets); 100 * a + b runs a for the camera rays of bounce
-    0 and b for the later bounces;
+    refill, same budgets), 64 / 74 / 84 (14 with a per-iteration warp vote
+    between primitive tests and node work); 100 * a + b runs a for the
+    camera rays of bounce 0 and b for the later bounces;
   * ``samples_per_wave`` - sample indices in flight per wave, i.e. the length
     of the path queues (paths = W*H*samples_per_wave);
   * ``shade_variant`` - register budget of the shading kernel (5 or 6 CTAs
@@ -35,7 +36,7 @@ from pathlib import Path
 from . import capi
 from .scenes import SceneSpec
 
-VARIANTS = (5, 14, 514, 515, 414, 614)
+VARIANTS = (5, 14, 514, 564, 574, 584, 414, 474)
 
 
 @dataclass
@@ -44,7 +45,7 @@ class Tuning:
     tlas_leaf: int = 1
     mesh_width: int = 8
     tlas_width: int = 8
-    extend_variant: int = 514
+    extend_variant: int = 574
     samples_per_wave: int = 0
     shade_variant: int = 6
     sort_materials: int = 1

@@ -28,7 +28,7 @@ def _image(spec, t: autotune.Tuning):
 
 
 def test_tune_picks_the_fastest_candidate(spec, tmp_path):
-    t = autotune.tune(spec, samples=2, reps=1, leaves=((1, 1),), variants=(514, 14),
+    t = autotune.tune(spec, samples=2, reps=1, leaves=((1, 1),), variants=(574, 14),
                       waves=(0, 2), shades=(5, 6), sorts=(1,), megakernel=False,
                       widths=((8, 8), (4, 4)))
     assert len(t.table) == 2 * 2 * 2 * 2
@@ -45,7 +45,8 @@ def test_tune_picks_the_fastest_candidate(spec, tmp_path):
         assert (tuned == base).mean() >= 0.999
 
 
-@pytest.mark.parametrize("variant,wave,shade", [(14, 2, 5), (515, 0, 6), (5, 4, 5)])
+@pytest.mark.parametrize("variant,wave,shade", [(14, 2, 5), (515, 0, 6), (5, 4, 5), (564, 0, 6),
+                                                (84, 2, 6)])
 def test_launch_knobs_leave_samples_bit_identical(spec, variant, wave, shade):
     base = _image(spec, autotune.Tuning())
     t = autotune.Tuning(extend_variant=variant, samples_per_wave=wave, shade_variant=shade)

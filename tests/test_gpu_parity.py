@@ -101,6 +101,8 @@ def test_mesh_hdri_samples(mesh_scene, orc, refcuda, s):
     (15, 3, 2, 2, capi.SCHEDULE_WAVEFRONT),
     (16, 2, 1, 0, capi.SCHEDULE_WAVEFRONT),
     (515, 1, 1, 0, capi.SCHEDULE_WAVEFRONT),
+    (514, 1, 1, 0, capi.SCHEDULE_WAVEFRONT),    # the flattened traversal without the vote
+    (84, 2, 1, 2, capi.SCHEDULE_WAVEFRONT),
 ])
 def test_tuning_knobs_do_not_change_samples(mesh_scene, refcuda, variant, mesh_leaf, tlas_leaf,
                                             spw, schedule):
