@@ -892,6 +892,21 @@ def _disp(x):
     return np.sqrt(np.clip(np.nan_to_num(x, nan=0.0), 0.0, 1.0))
 
 
+def oracle_stats(h0, h1):
+    """(RMSE between two independent oracle halves, error estimate of their
+    mean, share of the squared difference carried by the worst 0.1% and 1%
+    of pixels) in the time-to-RMSE domain; h0, h1 are (3, H, W) images."""
+    dd = ((_disp(h0) - _disp(h1)) ** 2).sum(axis=0).ravel()
+    between = float(np.sqrt(dd.sum() / (3 * dd.size)))
+    ranked = np.sort(dd)[::-1]
+    share = {f"top_{q}pct_pixels": float(ranked[:max(1, int(dd.size * q / 100))].sum()
+                                         / max(ranked.sum(), 1e-300))
+             for q in (0.1, 1)}
+    # the mean of two independent halves has half the variance of one half,
+    # whose variance is half the squared difference between them
+    return between, 0.5 * between, share
+
+
 def _time_at(curve, err):
     """Time a (samples, ms, rmse) curve needs to reach `err` (log-log
     interpolation between the points around it), or None."""
@@ -949,14 +964,7 @@ def time_to_rmse(args, target=0.01, top=2048):
     oracle_s = time.perf_counter() - t0
     oracle = 0.5 * (halves[0] + halves[1])
     disp_o = _disp(oracle)
-    dd = ((_disp(halves[0]) - _disp(halves[1])) ** 2).sum(axis=0).ravel()
-    between = float(np.sqrt(dd.sum() / (3 * dd.size)))
-    e_or = 0.5 * between   # error of the mean of the two halves (independent halves)
-    # where the oracle's own error sits: share of the squared difference
-    # between the halves carried by the worst 0.1% and 1% of pixels
-    top = np.sort(dd)[::-1]
-    concentration = {f"top_{q}pct_pixels": float(top[:max(1, int(dd.size * q / 100))].sum() / top.sum())
-                     for q in (0.1, 1)}
+    between, e_or, concentration = oracle_stats(halves[0], halves[1])
     del halves
     rmse_of = lambda img: float(np.sqrt(np.mean((_disp(img) - disp_o) ** 2)))
     corr = lambda e: float(np.sqrt(max(e * e - e_or * e_or, 0.0)))

@@ -18,3 +18,18 @@ def test_section_records_failures():
     assert bench.section(False, boom) is None
     assert "ValueError" in bench.section(True, boom)["error"]
     assert bench.section(True, lambda a: a + 1, 1) == 2
+
+
+def test_oracle_stats():
+    import numpy as np
+    rng = np.random.default_rng(0)
+    truth = rng.uniform(0.1, 0.5, (3, 32, 32))
+    h0 = truth + rng.normal(0, 0.01, truth.shape)
+    h1 = truth + rng.normal(0, 0.01, truth.shape)
+    between, err, share = bench.oracle_stats(h0, h1)
+    assert between > 0 and err == 0.5 * between
+    assert 0.0 < share["top_0.1pct_pixels"] <= share["top_1pct_pixels"] <= 1.0
+    mean = 0.5 * (h0 + h1)
+    d = lambda x: np.sqrt(np.clip(x, 0, 1))
+    true_err = float(np.sqrt(np.mean((d(mean) - d(truth)) ** 2)))
+    assert 0.5 * err < true_err < 2.0 * err
