@@ -18,6 +18,8 @@
 // partial sums to dW with atomics.
 #include "conv_tc.cuh"
 
+#include <cuda.h>  // CUtensorMap and its enums; the encoder is fetched from the driver at run time
+
 #include <algorithm>
 #include "tcgen05.cuh"
 
@@ -670,6 +672,455 @@ __global__ void __launch_bounds__(kWgThreads) k_conv_wgrad_halo(ConvWgradArgs a,
   if (warp == 0) tc::tmem_dealloc(tmem, ncols);
 }
 
+// TMA-fed persistent forward. A CTA keeps the weights of all nine taps for
+// its slice of nco output channels (normally all of them: the MMA's time
+// hardly depends on N up to 128, so the widest slice is the fastest) and
+// streams the input halos of its 8 x 16 pixel tiles in slices of 16 input
+// channels through a ring of `ring` shared-memory slots. Warp 0 (one
+// thread) copies halo slices with TMA; warp 1 (all lanes, one elected
+// issuer) issues per slice the nine taps' MMAs (K = 16) into one of `accs`
+// tensor-memory accumulators and frees the slot with a commit; warps 2-5
+// (one per tensor-memory subpartition) read each finished accumulator back
+// and store it. Hand-overs are mbarriers: full[r] (a slice's bytes have
+// landed), empty[r] (the MMAs that read slot r are done), acc_full[q] (a
+// tile's MMAs are done), acc_empty[q] (its accumulator has been read). No
+// CTA-wide barrier sits inside the tile loop.
+//
+// Shared memory, 128-byte aligned regions:
+//  * weights [kg][tap][n][8] (kg: 8 input channels), copied once: B of tap t
+//    and slice p is K-major from 2p * 9 * nco * 16 + t * nco * 16 with LBO
+//    9 * nco * 16 (next 8 input channels) and SBO 128 (next 8 outputs);
+//  * `ring` halo slots of two 8-channel groups, each one TMA box (8
+//    channels x 10 x 18 pixels, zero outside the image) at kKgPitch: A of
+//    tap (dy, dx) is K-major from (dy * 10 + dx) * 16 with LBO kKgPitch and
+//    SBO 160 (one halo row), so no per-tap gather is needed.
+constexpr int kTmaThreads = 192;
+constexpr int kTmaMaxStages = 4, kTmaMaxAccs = 4, kTmaMaxRing = 16;
+constexpr uint32_t kKgPitch = 2944;  // 180 halo pixels x 16 bytes, rounded up to 128
+constexpr uint32_t kSlotBytes = 2u * kKgPitch;
+
+// Waits for `parity` on `bar`; gives up when `abort` is raised elsewhere, or
+// after kWaitLimit polls, when it raises `abort` itself.
+__device__ __forceinline__ bool wait_or_abort(uint64_t* bar, uint32_t parity, volatile int* abort) {
+  for (uint32_t i = 0; i < kWaitLimit; ++i) {
+    if (tc::mbar_test(bar, parity)) return true;
+    if (*abort) return false;
+  }
+  *abort = 1;
+  return false;
+}
+
+__global__ void __launch_bounds__(kTmaThreads, 1)
+    k_conv_fwd_tma(const __grid_constant__ CUtensorMap tm_x, ConvFwdArgs a, int nco, int ring, int accs,
+                   uint32_t ncols) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  __shared__ __align__(8) uint64_t full[kTmaMaxRing], empty[kTmaMaxRing];
+  __shared__ __align__(8) uint64_t acc_full[kTmaMaxAccs], acc_empty[kTmaMaxAccs];
+  __shared__ uint32_t tmem_base;
+  __shared__ int abort_flag, n_loaded, n_issued;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int cin = a.cin, kg_n = cin >> 3, np = cin >> 4;  // np: 16-channel slices per tile
+  const int co0 = blockIdx.y * nco;
+  const int tw = a.W / kTileW, th = a.H / kTileH, n_tiles = tw * th * a.B;
+  const int first = blockIdx.x, step = (int)gridDim.x;
+  const uint32_t base = (tc::smem_u32(smem) + 127u) & ~127u;
+  const uint32_t w_kg = 9u * (uint32_t)nco * 16u;  // one kg's weights
+  const uint32_t sw = base, sh0 = base + (uint32_t)kg_n * w_kg;
+  volatile int* abort_v = &abort_flag;
+
+  // the slice's weights, [kg][tap][n][8], by every thread
+  for (int i = tid; i < 9 * nco * kg_n; i += kTmaThreads) {
+    const int kg = i % kg_n, rest = i / kg_n, n = rest % nco, t = rest / nco;
+    cp_async16(sw + (uint32_t)kg * w_kg + (uint32_t)(t * nco + n) * 16u,
+               a.w + ((size_t)t * a.cout + co0 + n) * cin + kg * 8, true);
+  }
+  if (tid == 0) {
+    for (int r = 0; r < ring; ++r) {
+      tc::mbar_init(&full[r], 1);
+      tc::mbar_init(&empty[r], 1);
+    }
+    for (int q = 0; q < accs; ++q) {
+      tc::mbar_init(&acc_full[q], 1);
+      tc::mbar_init(&acc_empty[q], 4);  // one arrival per epilogue warp
+    }
+    abort_flag = 0;
+    n_loaded = 0;
+    n_issued = 0;
+  }
+  if (warp == 1) tc::tmem_alloc(&tmem_base, ncols);
+  cp_async_wait_all();
+  tc::fence_smem_to_async();
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tmem = tmem_base;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      tc::tma_prefetch_map(&tm_x);
+      int c = 0;  // slices copied so far
+      for (int t = first; t < n_tiles; t += step) {
+        const int b = t / (tw * th), rest = t % (tw * th);
+        const int y0 = (rest / tw) * kTileH, x0 = (rest % tw) * kTileW;
+        int p = 0;
+        for (; p < np; ++p, ++c) {
+          const int r = c % ring, u = c / ring;
+          if (u >= 1 && !wait_or_abort(&empty[r], (uint32_t)(u - 1) & 1u, abort_v)) break;
+          const uint32_t dst = sh0 + (uint32_t)r * kSlotBytes;
+          tc::mbar_arrive_expect_tx(&full[r], 2u * (uint32_t)kHalo * 16u);
+          tc::tma_load_5d(dst, &tm_x, &full[r], 0, 2 * p, x0 - 1, y0 - 1, b);
+          tc::tma_load_5d(dst + kKgPitch, &tm_x, &full[r], 0, 2 * p + 1, x0 - 1, y0 - 1, b);
+        }
+        if (p < np) break;
+      }
+      n_loaded = c;
+    }
+  } else if (warp == 1) {
+    // the whole warp runs the issue loop; the elected lane issues
+    int j = 0, c = 0, got = 1;
+    const uint32_t idesc = tc::idesc_bf16(128, (uint32_t)nco, false, false);
+    // descriptors advance by adding (byte offset >> 4) to the start-address
+    // field: every operand lies below 256 KB, so the field never carries
+    const uint64_t da0 = tc::smem_desc(sh0, kKgPitch, (uint32_t)kHaloW * 16u);
+    const uint64_t db0 = tc::smem_desc(sw, w_kg, 128u);
+    const uint64_t b_slice = (2u * w_kg) >> 4, b_tap = ((uint32_t)nco * 16u) >> 4;
+    for (int t = first; t < n_tiles; t += step, ++j) {
+      const int q = j % accs, uq = j / accs;
+      if (lane == 0) got = uq < 1 || wait_or_abort(&acc_empty[q], (uint32_t)(uq - 1) & 1u, abort_v);
+      if (!__shfl_sync(0xffffffffu, got, 0)) break;
+      const uint32_t d = tmem + (uint32_t)(q * nco);
+      int p = 0;
+      for (; p < np; ++p, ++c) {
+        const int r = c % ring, u = c / ring;
+        if (lane == 0) got = wait_or_abort(&full[r], (uint32_t)u & 1u, abort_v);
+        if (!__shfl_sync(0xffffffffu, got, 0)) break;
+        tc::fence_after_sync();
+        const uint64_t da = da0 + (uint64_t)((r * kSlotBytes) >> 4);
+        const uint64_t db = db0 + (uint64_t)p * b_slice;
+#pragma unroll
+        for (int tap = 0; tap < 9; ++tap)
+          if (tc::elect_one())
+            tc::mma_bf16(d, da + (uint64_t)((tap / 3) * kHaloW + (tap % 3)), db + (uint64_t)tap * b_tap, idesc,
+                         (p > 0 || tap > 0) ? 1u : 0u);
+        if (tc::elect_one()) tc::mma_commit(&empty[r]);
+        __syncwarp();
+      }
+      if (p < np) break;
+      if (tc::elect_one()) tc::mma_commit(&acc_full[q]);
+      __syncwarp();
+    }
+    if (lane == 0) n_issued = c;
+  } else {
+    // warps 2-5: warp w reads tensor-memory lanes 32 (w % 4) .. +31
+    const int sub = warp & 3, r = sub * 32 + lane;
+    const uint32_t lane_base = tmem + ((uint32_t)(sub * 32) << 16);
+    const int gend = nco >> 3;
+    int j = 0;
+    for (int t = first; t < n_tiles; t += step, ++j) {
+      const int q = j % accs, uq = j / accs;
+      int got = 0;
+      if (lane == 0) got = wait_or_abort(&acc_full[q], (uint32_t)uq & 1u, abort_v) ? 1 : 0;
+      if (!__shfl_sync(0xffffffffu, got, 0)) break;
+      tc::fence_after_sync();
+      const int b = t / (tw * th), rest = t % (tw * th);
+      const int y0 = (rest / tw) * kTileH, x0 = (rest % tw) * kTileW;
+      const size_t p = (size_t)(b * a.H + y0 + r / kTileW) * a.W + x0 + r % kTileW;
+      __nv_bfloat16* out = a.y + p * a.y_stride + a.y_off + co0;
+      for (int c0 = 0; c0 < gend; c0 += 8) {  // up to 64 columns in flight per wait
+        uint32_t v[8][8];
+        const int nc = min(8, gend - c0);
+#pragma unroll
+        for (int c = 0; c < 8; ++c)
+          if (c < nc) tc::tmem_ld8_nowait(lane_base + (uint32_t)(q * nco + (c0 + c) * 8), v[c]);
+        tc::tmem_wait_ld();
+        if (c0 + 8 >= gend) {  // the accumulator is read: hand it back before storing
+          tc::fence_before_sync();
+          __syncwarp();
+          if (lane == 0) tc::mbar_arrive(&acc_empty[q]);
+        }
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+          if (c >= nc) break;
+          float f[8];
+#pragma unroll
+          for (int e = 0; e < 8; ++e) {
+            f[e] = __uint_as_float(v[c][e]);
+            if (a.bias) f[e] += a.bias[co0 + (c0 + c) * 8 + e];
+            if (a.relu) f[e] = fmaxf(f[e], 0.0f);
+          }
+          *reinterpret_cast<uint4*>(out + (c0 + c) * 8) = pack_bf16x8(f);
+        }
+      }
+    }
+  }
+
+  tc::fence_before_sync();
+  __syncthreads();
+  if (abort_flag && tid == 0) {
+    atomicOr(a.err, 2u);
+    // bounded drain: slices copied but not consumed, and the last MMAs issued
+    for (int cc = n_issued; cc < n_loaded; ++cc)
+      tc::mbar_wait(&full[cc % ring], (uint32_t)(cc / ring) & 1u, kWaitLimit);
+    if (n_issued > 0)
+      tc::mbar_wait(&empty[(n_issued - 1) % ring], (uint32_t)((n_issued - 1) / ring) & 1u, kWaitLimit);
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  if (warp == 1) tc::tmem_dealloc(tmem, ncols);
+}
+
+// TMA-fed weight gradient: CTA (run of tiles, group of taps) as in
+// k_conv_wgrad_halo, with the copies made by TMA and no CTA-wide barrier
+// inside the tile loop. Warp 0 (one thread) copies each tile's dY rows and
+// input halo into one of `stages` stages; warp 1 (one thread) issues the
+// tile's ntap x 8 MMAs (K = 16 pixels each) and frees the stage with a
+// commit; at the end all four warps add the accumulators to dW. A stage:
+//  * dY: 16 groups of 8 output channels, [cg][py][px][8], 2048 bytes each,
+//    one TMA box (8 channels x 8 x 16 pixels) per group below cout; groups
+//    cout / 8 .. 15 stay zero (the M = 128 tile's padding rows). A is
+//    MN-major: LBO 128 (next 8 pixels), SBO 2048 (next 8 channels);
+//  * the input halo as in k_conv_fwd_tma; B of tap (dy, dx) is MN-major from
+//    (dy * 10 + dx) * 16 with LBO 160 (next tile row) and SBO kKgPitch.
+constexpr int kWgTmaThreads = 128;
+
+__global__ void __launch_bounds__(kWgTmaThreads, 1)
+    k_conv_wgrad_tma(const __grid_constant__ CUtensorMap tm_dy, const __grid_constant__ CUtensorMap tm_x,
+                     ConvWgradArgs a, int tpg, int tiles_per_cta, int stages) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  __shared__ __align__(8) uint64_t full[kTmaMaxStages], empty[kTmaMaxStages], done;
+  __shared__ uint32_t tmem_base;
+  __shared__ int abort_flag, n_loaded, n_issued;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int cin = a.cin, cout = a.cout, kg_n = cin >> 3, cg_n = cout >> 3;
+  const int tw = a.W / kTileW, th = a.H / kTileH, n_tiles = tw * th * a.B;
+  const int t0 = blockIdx.x * tiles_per_cta, t1 = min(n_tiles, t0 + tiles_per_cta);
+  const int tap0 = blockIdx.y * tpg, ntap = min(tpg, 9 - tap0);
+  const uint32_t a_bytes = 16u * 2048u, b_bytes = (uint32_t)kg_n * kKgPitch;
+  const uint32_t stage_bytes = a_bytes + b_bytes;
+  const uint32_t base = (tc::smem_u32(smem) + 127u) & ~127u;
+  unsigned char* gbase = smem + (base - tc::smem_u32(smem));
+  const uint32_t ncols = (uint32_t)ntap * cin <= 256u ? 256u : 512u;
+  volatile int* abort_v = &abort_flag;
+
+  // the dY padding rows of every stage are read by the MMAs: zero them
+  for (int s = 0; s < stages; ++s)
+    for (uint32_t i = (uint32_t)cg_n * 2048u + tid * 16u; i < a_bytes; i += kWgTmaThreads * 16u)
+      *reinterpret_cast<uint4*>(gbase + (size_t)s * stage_bytes + i) = make_uint4(0u, 0u, 0u, 0u);
+  tc::fence_smem_to_async();
+  if (tid == 0) {
+    for (int s = 0; s < stages; ++s) {
+      tc::mbar_init(&full[s], 1);
+      tc::mbar_init(&empty[s], 1);
+    }
+    tc::mbar_init(&done, 1);
+    abort_flag = 0;
+    n_loaded = 0;
+    n_issued = 0;
+  }
+  if (warp == 1) tc::tmem_alloc(&tmem_base, ncols);
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tmem = tmem_base;
+
+  if (warp == 0 && lane == 0) {
+    tc::tma_prefetch_map(&tm_dy);
+    tc::tma_prefetch_map(&tm_x);
+    int j = 0;
+    for (int t = t0; t < t1; ++t, ++j) {
+      const int s = j % stages, u = j / stages;
+      if (u >= 1 && !wait_or_abort(&empty[s], (uint32_t)(u - 1) & 1u, abort_v)) break;
+      const int b = t / (tw * th), rest = t % (tw * th);
+      const int y0 = (rest / tw) * kTileH, x0 = (rest % tw) * kTileW;
+      const uint32_t sa = base + (uint32_t)s * stage_bytes, sb = sa + a_bytes;
+      tc::mbar_arrive_expect_tx(&full[s], (uint32_t)cg_n * 2048u + (uint32_t)kg_n * (uint32_t)kHalo * 16u);
+      for (int cg = 0; cg < cg_n; ++cg)
+        tc::tma_load_5d(sa + (uint32_t)cg * 2048u, &tm_dy, &full[s], 0, cg, x0, y0, b);
+      for (int kg = 0; kg < kg_n; ++kg)
+        tc::tma_load_5d(sb + (uint32_t)kg * kKgPitch, &tm_x, &full[s], 0, kg, x0 - 1, y0 - 1, b);
+    }
+    n_loaded = j;
+  } else if (warp == 1) {
+    // the whole warp runs the issue loop; the elected lane issues
+    const uint32_t idesc = tc::idesc_bf16(128, (uint32_t)cin, true, true);
+    const uint64_t a_step = 256u >> 4, b_step = (2u * kHaloW * 16u) >> 4;
+    int j = 0;
+    for (int t = t0; t < t1; ++t, ++j) {
+      const int s = j % stages, u = j / stages;
+      int got = 0;
+      if (lane == 0) got = wait_or_abort(&full[s], (uint32_t)u & 1u, abort_v) ? 1 : 0;
+      if (!__shfl_sync(0xffffffffu, got, 0)) break;
+      tc::fence_after_sync();
+      const uint32_t sa = base + (uint32_t)s * stage_bytes, sb = sa + a_bytes;
+      const uint64_t da0 = tc::smem_desc(sa, 128u, 2048u);
+      const uint64_t db0 = tc::smem_desc(sb, kHaloW * 16u, kKgPitch);
+      for (int q = 0; q < ntap; ++q) {
+        const int tap = tap0 + q;
+        uint64_t da = da0, db = db0 + (uint64_t)((tap / 3) * kHaloW + (tap % 3));
+        const uint32_t d = tmem + (uint32_t)(q * cin);
+#pragma unroll
+        for (int kk = 0; kk < 8; ++kk, da += a_step, db += b_step)  // K = 128 pixels, 16 per MMA
+          if (tc::elect_one()) tc::mma_bf16(d, da, db, idesc, (j > 0 || kk > 0) ? 1u : 0u);
+      }
+      if (tc::elect_one()) tc::mma_commit(&empty[s]);
+      __syncwarp();
+    }
+    if (j > 0 && tc::elect_one()) tc::mma_commit(&done);
+    if (lane == 0) n_issued = j;
+  }
+  __syncwarp();
+  tc::fence_before_sync();
+  __syncthreads();
+  const int n_tiles_cta = t1 - t0;
+  bool ok = !abort_flag && n_issued == n_tiles_cta;
+  if (ok && n_tiles_cta > 0) {
+    int got = 0;
+    if (lane == 0) got = wait_or_abort(&done, 0u, abort_v) ? 1 : 0;
+    ok = __shfl_sync(0xffffffffu, got, 0) != 0;
+  }
+  ok = __syncthreads_and(ok);
+  tc::fence_after_sync();
+  if (ok && n_tiles_cta > 0) {
+    const int co = warp * 32 + lane;
+    for (int q = 0; q < ntap; ++q) {
+      if (warp * 32 >= cout) break;  // warp-uniform: tcgen05.ld is warp-wide
+      for (int cg = 0; cg < kg_n; ++cg) {
+        float v[8];
+        tc::tmem_ld8(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(q * cin + cg * 8), v);
+        if (co < cout) {
+          float4* dst = reinterpret_cast<float4*>(a.dw + ((size_t)(tap0 + q) * cout + co) * cin + cg * 8);
+          atomicAdd(dst, make_float4(v[0], v[1], v[2], v[3]));
+          atomicAdd(dst + 1, make_float4(v[4], v[5], v[6], v[7]));
+        }
+      }
+    }
+  } else if (!ok && tid == 0) {
+    atomicOr(a.err, 2u);
+    // bounded drain: copies not consumed, and the last MMAs issued
+    for (int jj = n_issued; jj < n_loaded; ++jj)
+      tc::mbar_wait(&full[jj % stages], (uint32_t)(jj / stages) & 1u, kWaitLimit);
+    if (n_issued > 0)
+      tc::mbar_wait(&empty[(n_issued - 1) % stages], (uint32_t)((n_issued - 1) / stages) & 1u, kWaitLimit);
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  if (warp == 1) tc::tmem_dealloc(tmem, ncols);
+}
+
+// cuTensorMapEncodeTiled, looked up through the runtime so that the library
+// needs no link against the driver library.
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*,
+                                   CUtensorMapInterleave, CUtensorMapSwizzle, CUtensorMapL2promotion,
+                                   CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_tiled() {
+  static const EncodeTiledFn fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) !=
+            cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      p = nullptr;
+    return reinterpret_cast<EncodeTiledFn>(p);
+  }();
+  return fn;
+}
+
+// Tensor map over BF16 rows of `stride` elements, `rank` - 1 outer
+// dimensions: dims[0] = 8 channels (16 bytes, always coordinate 0), then
+// dims[1..] with byte strides strides[0..]; no swizzle, zero fill outside.
+bool encode_map(CUtensorMap* m, const void* base, int rank, const cuuint64_t* dims,
+                const cuuint64_t* strides, const cuuint32_t* box) {
+  const EncodeTiledFn fn = encode_tiled();
+  if (!fn || (reinterpret_cast<uintptr_t>(base) & 15u)) return false;
+  const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+  return fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, (cuuint32_t)rank, const_cast<void*>(base), dims, strides,
+            box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+            CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// Activations [B][H][W][stride] seen as (8 channels, channel group, x, y,
+// image) with a box of one group x box_w x box_h pixels.
+bool map_activations(CUtensorMap* m, const __nv_bfloat16* base, int groups, int W, int H, int B, int stride,
+                     int box_w, int box_h) {
+  const cuuint64_t row = (cuuint64_t)stride * 2u;
+  const cuuint64_t dims[5] = {8, (cuuint64_t)groups, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)B};
+  const cuuint64_t strides[4] = {16, row, row * W, row * W * H};
+  const cuuint32_t box[5] = {8, 1, (cuuint32_t)box_w, (cuuint32_t)box_h, 1};
+  return encode_map(m, base, 5, dims, strides, box);
+}
+
+// TMA forward launch when the shape fits: the widest slice of output
+// channels whose resident weights leave room for a ring of at least one
+// tile's halo slices and two more.
+bool try_conv_fwd_tma(const ConvFwdArgs& a, cudaStream_t st, cudaError_t* err) {
+  if (a.taps == 1 || a.W % kTileW != 0 || a.H % kTileH != 0) return false;
+  constexpr size_t kBudget = 227u * 1024u - 1024u;  // dynamic shared memory, minus the static part
+  const int np = a.cin >> 4;
+  const size_t min_ring = (size_t)std::min(kTmaMaxRing, np + 2);
+  int nco = std::min(a.cout, 256);
+  while (nco >= 16 && (a.cout % nco != 0 || nco % 16 != 0 ||
+                       128u + 9u * (size_t)nco * a.cin * 2u + min_ring * kSlotBytes > kBudget))
+    nco -= 16;
+  if (nco < 16 || (nco < 32 && nco != a.cout) || min_ring < (size_t)np + 1) return false;
+  const size_t w_bytes = 9u * (size_t)nco * a.cin * 2u;
+  const int ring = (int)std::min<size_t>(kTmaMaxRing, (kBudget - 128u - w_bytes) / kSlotBytes);
+  const int accs = std::min(kTmaMaxAccs, 512 / nco);
+  uint32_t ncols = 32u;
+  while (ncols < (uint32_t)(accs * nco)) ncols <<= 1;
+  CUtensorMap mx;
+  if (!map_activations(&mx, a.x + a.x_off, a.cin >> 3, a.W, a.H, a.B, a.x_stride, kHaloW, kHaloH))
+    return false;
+  const size_t smem = 128u + w_bytes + (size_t)ring * kSlotBytes;
+  cudaError_t e = cudaFuncSetAttribute(k_conv_fwd_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess) {
+    int dev = 0, sms = 148, per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_conv_fwd_tma, kTmaThreads, smem);
+    per_sm = std::max(1, std::min(per_sm, (int)(512u / ncols)));  // tensor memory of resident CTAs
+    const int slices = a.cout / nco;
+    const int n_tiles = (a.W / kTileW) * (a.H / kTileH) * a.B;
+    const int workers = std::max(1, std::min(n_tiles, sms * per_sm / slices));
+    k_conv_fwd_tma<<<dim3(workers, slices), kTmaThreads, smem, st>>>(mx, a, nco, ring, accs, ncols);
+    e = cudaGetLastError();
+  }
+  *err = e;
+  return true;
+}
+
+// TMA weight-gradient launch when a stage pair fits.
+bool try_conv_wgrad_tma(const ConvWgradArgs& a, cudaStream_t st, cudaError_t* err) {
+  if (a.taps == 1 || a.W % kTileW != 0 || a.H % kTileH != 0) return false;
+  constexpr size_t kBudget = 227u * 1024u - 1024u;
+  const size_t stage = 16u * 2048u + (size_t)(a.cin >> 3) * kKgPitch;
+  const int stages = (int)std::min<size_t>(kTmaMaxStages, (kBudget - 128u) / stage);
+  if (stages < 2) return false;
+  CUtensorMap mdy, mx;
+  if (!map_activations(&mdy, a.dy + a.dy_off, a.cout >> 3, a.W, a.H, a.B, a.dy_stride, kTileW, kTileH) ||
+      !map_activations(&mx, a.x + a.x_off, a.cin >> 3, a.W, a.H, a.B, a.x_stride, kHaloW, kHaloH))
+    return false;
+  const size_t smem = 128u + (size_t)stages * stage;
+  cudaError_t e = cudaFuncSetAttribute(k_conv_wgrad_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess) {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int tpg = std::min(9, 512 / a.cin);  // taps whose accumulators fit in 512 columns
+    const int groups = (9 + tpg - 1) / tpg;
+    const int n_tiles = (a.W / kTileW) * (a.H / kTileH) * a.B;
+    const int ctas = std::max(1, std::min(n_tiles, sms / groups));  // one CTA per SM
+    const int per = (n_tiles + ctas - 1) / ctas;
+    dim3 grid((n_tiles + per - 1) / per, groups);
+    k_conv_wgrad_tma<<<grid, kWgTmaThreads, smem, st>>>(mdy, mx, a, tpg, per, stages);
+    e = cudaGetLastError();
+  }
+  *err = e;
+  return true;
+}
+
 }  // namespace
 
 size_t conv_fwd_smem_bytes(int cin, int cout) {
@@ -681,6 +1132,8 @@ cudaError_t launch_conv_fwd(const ConvFwdArgs& a, cudaStream_t st) {
   if (a.cin % 16 || a.cout % 16 || a.cin < 16 || a.cout < 16 || a.cin > 256 || a.cout > 256 ||
       a.x_stride % 8 || a.x_off % 8 || a.y_stride % 8 || a.y_off % 8)
     return cudaErrorInvalidValue;
+  cudaError_t tma_err = cudaSuccess;
+  if (try_conv_fwd_tma(a, st, &tma_err)) return tma_err;
   const bool tiles_fit = a.taps != 1 && a.W % kTileW == 0 && a.H % kTileH == 0;
   if (tiles_fit) {
     // resident weights: the widest output-channel slice whose nine taps and
@@ -729,6 +1182,8 @@ cudaError_t launch_conv_wgrad(const ConvWgradArgs& a, cudaStream_t st) {
   if (a.cin % 16 || a.cout % 16 || a.cin < 16 || a.cout < 16 || a.cin > 256 || a.cout > 128 ||
       a.x_stride % 8 || a.x_off % 8 || a.dy_stride % 8 || a.dy_off % 8 || a.chunks_per_cta < 1)
     return cudaErrorInvalidValue;
+  cudaError_t tma_err = cudaSuccess;
+  if (try_conv_wgrad_tma(a, st, &tma_err)) return tma_err;
   const size_t halo_smem = 2u * (16u * 2048u + (size_t)(a.cin >> 3) * kHalo * 16u);
   if (a.taps != 1 && a.W % kTileW == 0 && a.H % kTileH == 0 && halo_smem <= 200u * 1024u) {
     cudaError_t e = cudaFuncSetAttribute(k_conv_wgrad_halo,
