@@ -675,10 +675,11 @@ __global__ void __launch_bounds__(kWgThreads) k_conv_wgrad_halo(ConvWgradArgs a,
 // TMA-fed persistent forward. A CTA keeps the weights of all nine taps for
 // its slice of nco output channels (normally all of them: the MMA's time
 // hardly depends on N up to 128, so the widest slice is the fastest) and
-// streams the input halos of its 8 x 16 pixel tiles in slices of 16 input
-// channels through a ring of `ring` shared-memory slots. Warp 0 (one
-// thread) copies halo slices with TMA; warp 1 (all lanes, one elected
-// issuer) issues per slice the nine taps' MMAs (K = 16) into one of `accs`
+// streams the input halos of its 8 x 16 pixel tiles in slices of sc = 16,
+// 32 or 64 input channels through a ring of `ring` shared-memory slots.
+// Warp 0 (one thread) copies halo slices with TMA; warp 1 (all lanes, one
+// elected issuer) issues per slice the nine taps' MMAs (K = 16 each, sc / 16
+// per tap) into one of `accs`
 // tensor-memory accumulators and frees the slot with a commit; warps 2-5
 // (one per tensor-memory subpartition) read each finished accumulator back
 // and store it. Hand-overs are mbarriers: full[r] (a slice's bytes have
@@ -688,16 +689,28 @@ __global__ void __launch_bounds__(kWgThreads) k_conv_wgrad_halo(ConvWgradArgs a,
 //
 // Shared memory, 128-byte aligned regions:
 //  * weights [kg][tap][n][8] (kg: 8 input channels), copied once: B of tap t
-//    and slice p is K-major from 2p * 9 * nco * 16 + t * nco * 16 with LBO
-//    9 * nco * 16 (next 8 input channels) and SBO 128 (next 8 outputs);
-//  * `ring` halo slots of two 8-channel groups, each one TMA box (8
-//    channels x 10 x 18 pixels, zero outside the image) at kKgPitch: A of
-//    tap (dy, dx) is K-major from (dy * 10 + dx) * 16 with LBO kKgPitch and
-//    SBO 160 (one halo row), so no per-tap gather is needed.
+//    and input channels 16 k .. 16 k + 15 is K-major from 2k * 9 * nco * 16 +
+//    t * nco * 16 with LBO 9 * nco * 16 (next 8 input channels) and SBO 128
+//    (next 8 outputs);
+//  * `ring` 1024-byte aligned halo slots, each one TMA box (sc channels x
+//    10 x 18 pixels, zero outside the image) of 2 sc-byte pixel rows,
+//    swizzled by TMA in the mode of that row width (32, 64 or 128 bytes).
+//    A of tap (dy, dx) is K-major in the same swizzle mode from
+//    (dy * 10 + dx) * 2 sc (+ 32 bytes per further 16 channels) with SBO one
+//    halo row, 10 * 2 sc bytes: the tensor cores apply the swizzle to the
+//    absolute shared-memory address as TMA does, so a view that starts whole
+//    pixel rows into the box reads the box correctly, and no per-tap gather
+//    is needed.
 constexpr int kTmaThreads = 192;
 constexpr int kTmaMaxStages = 4, kTmaMaxAccs = 4, kTmaMaxRing = 16;
 constexpr uint32_t kKgPitch = 2944;  // 180 halo pixels x 16 bytes, rounded up to 128
-constexpr uint32_t kSlotBytes = 2u * kKgPitch;
+
+// Halo slot of sc channels: 180 pixel rows of 2 sc bytes, rounded up to 1 KB.
+__host__ __device__ constexpr uint32_t slot_bytes(int sc) {
+  return ((uint32_t)kHalo * 2u * (uint32_t)sc + 1023u) & ~1023u;
+}
+// Swizzle mode of the tensor-core descriptor for rows of 2 sc bytes.
+__host__ __device__ constexpr uint32_t umma_swizzle(int sc) { return sc == 64 ? 2u : (sc == 32 ? 4u : 6u); }
 
 // Waits for `parity` on `bar`; gives up when `abort` is raised elsewhere, or
 // after kWaitLimit polls, when it raises `abort` itself.
@@ -711,21 +724,22 @@ __device__ __forceinline__ bool wait_or_abort(uint64_t* bar, uint32_t parity, vo
 }
 
 __global__ void __launch_bounds__(kTmaThreads, 1)
-    k_conv_fwd_tma(const __grid_constant__ CUtensorMap tm_x, ConvFwdArgs a, int nco, int ring, int accs,
-                   uint32_t ncols) {
+    k_conv_fwd_tma(const __grid_constant__ CUtensorMap tm_x, ConvFwdArgs a, int nco, int sc, int ring,
+                   int accs, uint32_t ncols) {
   extern __shared__ __align__(1024) unsigned char smem[];
   __shared__ __align__(8) uint64_t full[kTmaMaxRing], empty[kTmaMaxRing];
   __shared__ __align__(8) uint64_t acc_full[kTmaMaxAccs], acc_empty[kTmaMaxAccs];
   __shared__ uint32_t tmem_base;
   __shared__ int abort_flag, n_loaded, n_issued;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int cin = a.cin, kg_n = cin >> 3, np = cin >> 4;  // np: 16-channel slices per tile
+  const int cin = a.cin, kg_n = cin >> 3, np = cin / sc, kps = sc >> 4;  // slices per tile, K steps per slice
   const int co0 = blockIdx.y * nco;
   const int tw = a.W / kTileW, th = a.H / kTileH, n_tiles = tw * th * a.B;
   const int first = blockIdx.x, step = (int)gridDim.x;
-  const uint32_t base = (tc::smem_u32(smem) + 127u) & ~127u;
+  const uint32_t base = (tc::smem_u32(smem) + 1023u) & ~1023u;
   const uint32_t w_kg = 9u * (uint32_t)nco * 16u;  // one kg's weights
-  const uint32_t sw = base, sh0 = base + (uint32_t)kg_n * w_kg;
+  const uint32_t sw = base, sh0 = (base + (uint32_t)kg_n * w_kg + 1023u) & ~1023u;
+  const uint32_t slot = slot_bytes(sc);
   volatile int* abort_v = &abort_flag;
 
   // the slice's weights, [kg][tap][n][8], by every thread
@@ -766,10 +780,8 @@ __global__ void __launch_bounds__(kTmaThreads, 1)
         for (; p < np; ++p, ++c) {
           const int r = c % ring, u = c / ring;
           if (u >= 1 && !wait_or_abort(&empty[r], (uint32_t)(u - 1) & 1u, abort_v)) break;
-          const uint32_t dst = sh0 + (uint32_t)r * kSlotBytes;
-          tc::mbar_arrive_expect_tx(&full[r], 2u * (uint32_t)kHalo * 16u);
-          tc::tma_load_5d(dst, &tm_x, &full[r], 0, 2 * p, x0 - 1, y0 - 1, b);
-          tc::tma_load_5d(dst + kKgPitch, &tm_x, &full[r], 0, 2 * p + 1, x0 - 1, y0 - 1, b);
+          tc::mbar_arrive_expect_tx(&full[r], (uint32_t)kHalo * 2u * (uint32_t)sc);
+          tc::tma_load_5d(sh0 + (uint32_t)r * slot, &tm_x, &full[r], 0, p, x0 - 1, y0 - 1, b);
         }
         if (p < np) break;
       }
@@ -781,9 +793,11 @@ __global__ void __launch_bounds__(kTmaThreads, 1)
     const uint32_t idesc = tc::idesc_bf16(128, (uint32_t)nco, false, false);
     // descriptors advance by adding (byte offset >> 4) to the start-address
     // field: every operand lies below 256 KB, so the field never carries
-    const uint64_t da0 = tc::smem_desc(sh0, kKgPitch, (uint32_t)kHaloW * 16u);
+    const uint64_t da0 =
+        tc::smem_desc(sh0, 16u, (uint32_t)kHaloW * 2u * (uint32_t)sc) | ((uint64_t)umma_swizzle(sc) << 61);
     const uint64_t db0 = tc::smem_desc(sw, w_kg, 128u);
-    const uint64_t b_slice = (2u * w_kg) >> 4, b_tap = ((uint32_t)nco * 16u) >> 4;
+    const uint64_t b_k = (2u * w_kg) >> 4, b_tap = ((uint32_t)nco * 16u) >> 4;
+    const uint32_t a_px = (2u * (uint32_t)sc) >> 4;  // one pixel row, in 16-byte units
     for (int t = first; t < n_tiles; t += step, ++j) {
       const int q = j % accs, uq = j / accs;
       if (lane == 0) got = uq < 1 || wait_or_abort(&acc_empty[q], (uint32_t)(uq - 1) & 1u, abort_v);
@@ -795,13 +809,15 @@ __global__ void __launch_bounds__(kTmaThreads, 1)
         if (lane == 0) got = wait_or_abort(&full[r], (uint32_t)u & 1u, abort_v);
         if (!__shfl_sync(0xffffffffu, got, 0)) break;
         tc::fence_after_sync();
-        const uint64_t da = da0 + (uint64_t)((r * kSlotBytes) >> 4);
-        const uint64_t db = db0 + (uint64_t)p * b_slice;
+        const uint64_t da = da0 + (uint64_t)(((uint32_t)r * slot) >> 4);
+        for (int kk = 0; kk < kps; ++kk) {
+          const uint64_t db = db0 + (uint64_t)(p * kps + kk) * b_k;
 #pragma unroll
-        for (int tap = 0; tap < 9; ++tap)
-          if (tc::elect_one())
-            tc::mma_bf16(d, da + (uint64_t)((tap / 3) * kHaloW + (tap % 3)), db + (uint64_t)tap * b_tap, idesc,
-                         (p > 0 || tap > 0) ? 1u : 0u);
+          for (int tap = 0; tap < 9; ++tap)
+            if (tc::elect_one())
+              tc::mma_bf16(d, da + (uint64_t)(((tap / 3) * kHaloW + (tap % 3)) * a_px + 2 * kk),
+                           db + (uint64_t)tap * b_tap, idesc, (p > 0 || kk > 0 || tap > 0) ? 1u : 0u);
+        }
         if (tc::elect_one()) tc::mma_commit(&empty[r]);
         __syncwarp();
       }
@@ -873,41 +889,41 @@ __global__ void __launch_bounds__(kTmaThreads, 1)
 // TMA-fed weight gradient: CTA (run of tiles, group of taps) as in
 // k_conv_wgrad_halo, with the copies made by TMA and no CTA-wide barrier
 // inside the tile loop. Warp 0 (one thread) copies each tile's dY rows and
-// input halo into one of `stages` stages; warp 1 (one thread) issues the
-// tile's ntap x 8 MMAs (K = 16 pixels each) and frees the stage with a
-// commit; at the end all four warps add the accumulators to dW. A stage:
-//  * dY: 16 groups of 8 output channels, [cg][py][px][8], 2048 bytes each,
-//    one TMA box (8 channels x 8 x 16 pixels) per group below cout; groups
-//    cout / 8 .. 15 stay zero (the M = 128 tile's padding rows). A is
-//    MN-major: LBO 128 (next 8 pixels), SBO 2048 (next 8 channels);
-//  * the input halo as in k_conv_fwd_tma; B of tap (dy, dx) is MN-major from
-//    (dy * 10 + dx) * 16 with LBO 160 (next tile row) and SBO kKgPitch.
+// input halo into one of `stages` stages; warp 1 (all lanes, one elected
+// issuer) issues the tile's ntap x 8 MMAs (K = 16 pixels each) and frees
+// the stage with a commit; at the end all four warps add the accumulators to
+// dW. Both operands are MN-major (channels contiguous within a pixel row)
+// in the swizzle mode of their row width, one TMA box per block of so
+// output or si input channels (32, 64 or 128-byte rows):
+//  * A (dY^T, M = 128 output channels, K = pixels): blocks of 128 pixel rows
+//    (the 8 x 16 tile) at 256 so bytes from each other (LBO); SBO 8 rows.
+//    Blocks past cout are never written: they only feed accumulator rows
+//    that are never read back;
+//  * B (the input halo, N = cin, K = pixels): blocks of the 10 x 18 halo at
+//    slot_bytes(si) (LBO); the view of tap (dy, dx) starts (dy * 10 + dx)
+//    pixel rows in, and its 8-pixel K groups are one halo row apart (SBO
+//    10 rows), so no per-tap gather is needed.
 constexpr int kWgTmaThreads = 128;
 
 __global__ void __launch_bounds__(kWgTmaThreads, 1)
     k_conv_wgrad_tma(const __grid_constant__ CUtensorMap tm_dy, const __grid_constant__ CUtensorMap tm_x,
-                     ConvWgradArgs a, int tpg, int tiles_per_cta, int stages) {
+                     ConvWgradArgs a, int tpg, int tiles_per_cta, int stages, int so, int si) {
   extern __shared__ __align__(1024) unsigned char smem[];
   __shared__ __align__(8) uint64_t full[kTmaMaxStages], empty[kTmaMaxStages], done;
   __shared__ uint32_t tmem_base;
   __shared__ int abort_flag, n_loaded, n_issued;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int cin = a.cin, cout = a.cout, kg_n = cin >> 3, cg_n = cout >> 3;
+  const int cin = a.cin, cout = a.cout, kg_n = cin >> 3;
+  const int ob_n = cout / so, ib_n = cin / si;  // channel blocks loaded per tile
   const int tw = a.W / kTileW, th = a.H / kTileH, n_tiles = tw * th * a.B;
   const int t0 = blockIdx.x * tiles_per_cta, t1 = min(n_tiles, t0 + tiles_per_cta);
   const int tap0 = blockIdx.y * tpg, ntap = min(tpg, 9 - tap0);
-  const uint32_t a_bytes = 16u * 2048u, b_bytes = (uint32_t)kg_n * kKgPitch;
-  const uint32_t stage_bytes = a_bytes + b_bytes;
-  const uint32_t base = (tc::smem_u32(smem) + 127u) & ~127u;
-  unsigned char* gbase = smem + (base - tc::smem_u32(smem));
+  const uint32_t a_blk = 256u * (uint32_t)so, b_blk = slot_bytes(si);
+  const uint32_t a_bytes = 128u / (uint32_t)so * a_blk, stage_bytes = a_bytes + (uint32_t)ib_n * b_blk;
+  const uint32_t base = (tc::smem_u32(smem) + 1023u) & ~1023u;
   const uint32_t ncols = (uint32_t)ntap * cin <= 256u ? 256u : 512u;
   volatile int* abort_v = &abort_flag;
 
-  // the dY padding rows of every stage are read by the MMAs: zero them
-  for (int s = 0; s < stages; ++s)
-    for (uint32_t i = (uint32_t)cg_n * 2048u + tid * 16u; i < a_bytes; i += kWgTmaThreads * 16u)
-      *reinterpret_cast<uint4*>(gbase + (size_t)s * stage_bytes + i) = make_uint4(0u, 0u, 0u, 0u);
-  tc::fence_smem_to_async();
   if (tid == 0) {
     for (int s = 0; s < stages; ++s) {
       tc::mbar_init(&full[s], 1);
@@ -934,17 +950,18 @@ __global__ void __launch_bounds__(kWgTmaThreads, 1)
       const int b = t / (tw * th), rest = t % (tw * th);
       const int y0 = (rest / tw) * kTileH, x0 = (rest % tw) * kTileW;
       const uint32_t sa = base + (uint32_t)s * stage_bytes, sb = sa + a_bytes;
-      tc::mbar_arrive_expect_tx(&full[s], (uint32_t)cg_n * 2048u + (uint32_t)kg_n * (uint32_t)kHalo * 16u);
-      for (int cg = 0; cg < cg_n; ++cg)
-        tc::tma_load_5d(sa + (uint32_t)cg * 2048u, &tm_dy, &full[s], 0, cg, x0, y0, b);
-      for (int kg = 0; kg < kg_n; ++kg)
-        tc::tma_load_5d(sb + (uint32_t)kg * kKgPitch, &tm_x, &full[s], 0, kg, x0 - 1, y0 - 1, b);
+      tc::mbar_arrive_expect_tx(&full[s], 256u * (uint32_t)cout + (uint32_t)kHalo * 2u * (uint32_t)cin);
+      for (int ob = 0; ob < ob_n; ++ob)
+        tc::tma_load_5d(sa + (uint32_t)ob * a_blk, &tm_dy, &full[s], 0, ob, x0, y0, b);
+      for (int ib = 0; ib < ib_n; ++ib)
+        tc::tma_load_5d(sb + (uint32_t)ib * b_blk, &tm_x, &full[s], 0, ib, x0 - 1, y0 - 1, b);
     }
     n_loaded = j;
   } else if (warp == 1) {
     // the whole warp runs the issue loop; the elected lane issues
     const uint32_t idesc = tc::idesc_bf16(128, (uint32_t)cin, true, true);
-    const uint64_t a_step = 256u >> 4, b_step = (2u * kHaloW * 16u) >> 4;
+    const uint32_t a_row = 2u * (uint32_t)so, b_row = 2u * (uint32_t)si;
+    const uint64_t a_step = (16u * a_row) >> 4, b_step = (2u * kHaloW * b_row) >> 4;  // 16 pixels
     int j = 0;
     for (int t = t0; t < t1; ++t, ++j) {
       const int s = j % stages, u = j / stages;
@@ -953,11 +970,11 @@ __global__ void __launch_bounds__(kWgTmaThreads, 1)
       if (!__shfl_sync(0xffffffffu, got, 0)) break;
       tc::fence_after_sync();
       const uint32_t sa = base + (uint32_t)s * stage_bytes, sb = sa + a_bytes;
-      const uint64_t da0 = tc::smem_desc(sa, 128u, 2048u);
-      const uint64_t db0 = tc::smem_desc(sb, kHaloW * 16u, kKgPitch);
+      const uint64_t da0 = tc::smem_desc(sa, a_blk, 8u * a_row) | ((uint64_t)umma_swizzle(so) << 61);
+      const uint64_t db0 = tc::smem_desc(sb, b_blk, (uint32_t)kHaloW * b_row) | ((uint64_t)umma_swizzle(si) << 61);
       for (int q = 0; q < ntap; ++q) {
         const int tap = tap0 + q;
-        uint64_t da = da0, db = db0 + (uint64_t)((tap / 3) * kHaloW + (tap % 3));
+        uint64_t da = da0, db = db0 + (uint64_t)((((tap / 3) * kHaloW + (tap % 3)) * b_row) >> 4);
         const uint32_t d = tmem + (uint32_t)(q * cin);
 #pragma unroll
         for (int kk = 0; kk < 8; ++kk, da += a_step, db += b_step)  // K = 128 pixels, 16 per MMA
@@ -1029,51 +1046,65 @@ EncodeTiledFn encode_tiled() {
 }
 
 // Tensor map over BF16 rows of `stride` elements, `rank` - 1 outer
-// dimensions: dims[0] = 8 channels (16 bytes, always coordinate 0), then
-// dims[1..] with byte strides strides[0..]; no swizzle, zero fill outside.
+// dimensions: dims[0] channels (16 to 128 bytes, always coordinate 0), then
+// dims[1..] with byte strides strides[0..]; zero fill outside.
 bool encode_map(CUtensorMap* m, const void* base, int rank, const cuuint64_t* dims,
-                const cuuint64_t* strides, const cuuint32_t* box) {
+                const cuuint64_t* strides, const cuuint32_t* box,
+                CUtensorMapSwizzle swizzle = CU_TENSOR_MAP_SWIZZLE_NONE) {
   const EncodeTiledFn fn = encode_tiled();
   if (!fn || (reinterpret_cast<uintptr_t>(base) & 15u)) return false;
   const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
   return fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, (cuuint32_t)rank, const_cast<void*>(base), dims, strides,
-            box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+            box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle,
             CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-// Activations [B][H][W][stride] seen as (8 channels, channel group, x, y,
-// image) with a box of one group x box_w x box_h pixels.
+// Activations [B][H][W][stride] seen as (gc channels, channel group, x, y,
+// image) with a box of one group x box_w x box_h pixels; rows of 32, 64 or
+// 128 bytes are swizzled in that mode, 16-byte rows are not.
 bool map_activations(CUtensorMap* m, const __nv_bfloat16* base, int groups, int W, int H, int B, int stride,
-                     int box_w, int box_h) {
+                     int box_w, int box_h, int gc = 8) {
   const cuuint64_t row = (cuuint64_t)stride * 2u;
-  const cuuint64_t dims[5] = {8, (cuuint64_t)groups, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)B};
-  const cuuint64_t strides[4] = {16, row, row * W, row * W * H};
-  const cuuint32_t box[5] = {8, 1, (cuuint32_t)box_w, (cuuint32_t)box_h, 1};
-  return encode_map(m, base, 5, dims, strides, box);
+  const cuuint64_t dims[5] = {(cuuint64_t)gc, (cuuint64_t)groups, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)B};
+  const cuuint64_t strides[4] = {(cuuint64_t)gc * 2u, row, row * W, row * W * H};
+  const cuuint32_t box[5] = {(cuuint32_t)gc, 1, (cuuint32_t)box_w, (cuuint32_t)box_h, 1};
+  const CUtensorMapSwizzle sw = gc == 64   ? CU_TENSOR_MAP_SWIZZLE_128B
+                                : gc == 32 ? CU_TENSOR_MAP_SWIZZLE_64B
+                                : gc == 16 ? CU_TENSOR_MAP_SWIZZLE_32B
+                                           : CU_TENSOR_MAP_SWIZZLE_NONE;
+  return encode_map(m, base, 5, dims, strides, box, sw);
 }
 
 // TMA forward launch when the shape fits: the widest slice of output
-// channels whose resident weights leave room for a ring of at least one
-// tile's halo slices and two more.
+// channels whose resident weights leave room for a ring of one tile's halo
+// slices and two more, with the widest halo slice (64, 32 or 16 channels)
+// that divides cin and fits.
 bool try_conv_fwd_tma(const ConvFwdArgs& a, cudaStream_t st, cudaError_t* err) {
   if (a.taps == 1 || a.W % kTileW != 0 || a.H % kTileH != 0) return false;
   constexpr size_t kBudget = 227u * 1024u - 1024u;  // dynamic shared memory, minus the static part
-  const int np = a.cin >> 4;
-  const size_t min_ring = (size_t)std::min(kTmaMaxRing, np + 2);
-  int nco = std::min(a.cout, 256);
-  while (nco >= 16 && (a.cout % nco != 0 || nco % 16 != 0 ||
-                       128u + 9u * (size_t)nco * a.cin * 2u + min_ring * kSlotBytes > kBudget))
-    nco -= 16;
-  if (nco < 16 || (nco < 32 && nco != a.cout) || min_ring < (size_t)np + 1) return false;
-  const size_t w_bytes = 9u * (size_t)nco * a.cin * 2u;
-  const int ring = (int)std::min<size_t>(kTmaMaxRing, (kBudget - 128u - w_bytes) / kSlotBytes);
+  auto w_bytes = [&](int nco) { return ((9u * (size_t)nco * a.cin * 2u) + 1023u) & ~(size_t)1023u; };
+  int nco = 0, sc = 0;
+  for (int n = std::min(a.cout, 256); n >= 16 && !nco; n -= 16) {
+    if (a.cout % n != 0 || (n < 32 && n != a.cout)) continue;
+    for (int c : {64, 32, 16}) {
+      const int np = a.cin / c;
+      if (a.cin % c != 0 || np + 2 > kTmaMaxRing) continue;
+      if (1024u + w_bytes(n) + (size_t)(np + 2) * slot_bytes(c) <= kBudget) {
+        nco = n;
+        sc = c;
+        break;
+      }
+    }
+  }
+  if (!nco) return false;
+  const int ring = (int)std::min<size_t>(kTmaMaxRing, (kBudget - 1024u - w_bytes(nco)) / slot_bytes(sc));
   const int accs = std::min(kTmaMaxAccs, 512 / nco);
   uint32_t ncols = 32u;
   while (ncols < (uint32_t)(accs * nco)) ncols <<= 1;
   CUtensorMap mx;
-  if (!map_activations(&mx, a.x + a.x_off, a.cin >> 3, a.W, a.H, a.B, a.x_stride, kHaloW, kHaloH))
+  if (!map_activations(&mx, a.x + a.x_off, a.cin / sc, a.W, a.H, a.B, a.x_stride, kHaloW, kHaloH, sc))
     return false;
-  const size_t smem = 128u + w_bytes + (size_t)ring * kSlotBytes;
+  const size_t smem = 1024u + w_bytes(nco) + (size_t)ring * slot_bytes(sc);
   cudaError_t e = cudaFuncSetAttribute(k_conv_fwd_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e == cudaSuccess) {
     int dev = 0, sms = 148, per_sm = 1;
@@ -1084,25 +1115,28 @@ bool try_conv_fwd_tma(const ConvFwdArgs& a, cudaStream_t st, cudaError_t* err) {
     const int slices = a.cout / nco;
     const int n_tiles = (a.W / kTileW) * (a.H / kTileH) * a.B;
     const int workers = std::max(1, std::min(n_tiles, sms * per_sm / slices));
-    k_conv_fwd_tma<<<dim3(workers, slices), kTmaThreads, smem, st>>>(mx, a, nco, ring, accs, ncols);
+    k_conv_fwd_tma<<<dim3(workers, slices), kTmaThreads, smem, st>>>(mx, a, nco, sc, ring, accs, ncols);
     e = cudaGetLastError();
   }
   *err = e;
   return true;
 }
 
-// TMA weight-gradient launch when a stage pair fits.
+// TMA weight-gradient launch when two stages fit, with the widest channel
+// blocks (64, 32 or 16) that divide cout and cin.
 bool try_conv_wgrad_tma(const ConvWgradArgs& a, cudaStream_t st, cudaError_t* err) {
   if (a.taps == 1 || a.W % kTileW != 0 || a.H % kTileH != 0) return false;
+  auto widest = [](int c) { return c % 64 == 0 ? 64 : (c % 32 == 0 ? 32 : 16); };
+  const int so = widest(a.cout), si = widest(a.cin);
   constexpr size_t kBudget = 227u * 1024u - 1024u;
-  const size_t stage = 16u * 2048u + (size_t)(a.cin >> 3) * kKgPitch;
-  const int stages = (int)std::min<size_t>(kTmaMaxStages, (kBudget - 128u) / stage);
+  const size_t stage = (size_t)(128 / so) * 256u * so + (size_t)(a.cin / si) * slot_bytes(si);
+  const int stages = (int)std::min<size_t>(kTmaMaxStages, (kBudget - 1024u) / stage);
   if (stages < 2) return false;
   CUtensorMap mdy, mx;
-  if (!map_activations(&mdy, a.dy + a.dy_off, a.cout >> 3, a.W, a.H, a.B, a.dy_stride, kTileW, kTileH) ||
-      !map_activations(&mx, a.x + a.x_off, a.cin >> 3, a.W, a.H, a.B, a.x_stride, kHaloW, kHaloH))
+  if (!map_activations(&mdy, a.dy + a.dy_off, a.cout / so, a.W, a.H, a.B, a.dy_stride, kTileW, kTileH, so) ||
+      !map_activations(&mx, a.x + a.x_off, a.cin / si, a.W, a.H, a.B, a.x_stride, kHaloW, kHaloH, si))
     return false;
-  const size_t smem = 128u + (size_t)stages * stage;
+  const size_t smem = 1024u + (size_t)stages * stage;
   cudaError_t e = cudaFuncSetAttribute(k_conv_wgrad_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e == cudaSuccess) {
     int dev = 0, sms = 148;
@@ -1114,7 +1148,7 @@ bool try_conv_wgrad_tma(const ConvWgradArgs& a, cudaStream_t st, cudaError_t* er
     const int ctas = std::max(1, std::min(n_tiles, sms / groups));  // one CTA per SM
     const int per = (n_tiles + ctas - 1) / ctas;
     dim3 grid((n_tiles + per - 1) / per, groups);
-    k_conv_wgrad_tma<<<grid, kWgTmaThreads, smem, st>>>(mdy, mx, a, tpg, per, stages);
+    k_conv_wgrad_tma<<<grid, kWgTmaThreads, smem, st>>>(mdy, mx, a, tpg, per, stages, so, si);
     e = cudaGetLastError();
   }
   *err = e;
