@@ -742,12 +742,6 @@ __global__ void __launch_bounds__(kTmaThreads, 1)
   const uint32_t slot = slot_bytes(sc);
   volatile int* abort_v = &abort_flag;
 
-  // the slice's weights, [kg][tap][n][8], by every thread
-  for (int i = tid; i < 9 * nco * kg_n; i += kTmaThreads) {
-    const int kg = i % kg_n, rest = i / kg_n, n = rest % nco, t = rest / nco;
-    cp_async16(sw + (uint32_t)kg * w_kg + (uint32_t)(t * nco + n) * 16u,
-               a.w + ((size_t)t * a.cout + co0 + n) * cin + kg * 8, true);
-  }
   if (tid == 0) {
     for (int r = 0; r < ring; ++r) {
       tc::mbar_init(&full[r], 1);
@@ -762,12 +756,26 @@ __global__ void __launch_bounds__(kTmaThreads, 1)
     n_issued = 0;
   }
   if (warp == 1) tc::tmem_alloc(&tmem_base, ncols);
-  cp_async_wait_all();
-  tc::fence_smem_to_async();
   tc::fence_before_sync();
   __syncthreads();
   tc::fence_after_sync();
   const uint32_t tmem = tmem_base;
+  if (warp >= 1) {
+    // warps 1-5 copy the slice's weights, [kg][tap][n][8], while warp 0
+    // already streams halos; each CTA starts at another offset so that the
+    // CTAs do not all read the same lines of L2 at once
+    const int total = 9 * nco * kg_n, rot = (int)((blockIdx.x * 613u + blockIdx.y * 97u) % (uint32_t)total);
+    for (int i = tid - 32; i < total; i += kTmaThreads - 32) {
+      int ii = i + rot;
+      if (ii >= total) ii -= total;
+      const int kg = ii % kg_n, rest = ii / kg_n, n = rest % nco, t = rest / nco;
+      cp_async16(sw + (uint32_t)kg * w_kg + (uint32_t)(t * nco + n) * 16u,
+                 a.w + ((size_t)t * a.cout + co0 + n) * cin + kg * 8, true);
+    }
+    cp_async_wait_all();
+    tc::fence_smem_to_async();
+    asm volatile("bar.sync 1, %0;" :: "r"(kTmaThreads - 32) : "memory");  // warps 1-5 only
+  }
 
   if (warp == 0) {
     if (lane == 0) {
