@@ -467,6 +467,323 @@ __global__ void k_pack(const float* w, __nv_bfloat16* wf, size_t n) {
   GRID_STRIDE(i, n) { wf[i] = __float2bfloat16(w[i]); }
 }
 
+// Training with two tiles in flight. The serial chain of one tile (5
+// forward and 5 backward steps, each a GEMM, a wait and a tcgen05.ld
+// epilogue) leaves the tensor core idle while the epilogue runs; here two
+// groups of four warps each carry their own tile through the chain and one
+// more warp issues every GEMM, so that one group's epilogue overlaps the
+// other group's GEMM. The issuing warp serves the groups in a fixed order
+// (step k of group 0, step k of group 1, step k + 1 of group 0, ...), which
+// also keeps all weight-gradient MMAs in one thread's issue order, as
+// accumulation into shared tensor-memory columns needs.
+//
+// Per group (kGrpBytes of shared memory): G (the output gradient, 128 x 16)
+// and four hidden tiles H0..H3. The encoded inputs X go to H3's tile (dead
+// until layer 3 writes H3) and are copied there again for the last backward
+// step; each backward step writes dZ_(j-1) over H_(j-1) in place, since the
+// mask is read by the same thread just before. Tensor memory: the group's
+// accumulator at 64 g, the weight gradients at 128 + 64 l.
+constexpr int kGroups = 2;
+constexpr int kTrainThreads = 32 * (4 * kGroups + 1);
+constexpr uint32_t kGOff = 0, kHOff = kRows * kOutCh * 2;  // within a group
+constexpr uint32_t kGrpBytes = kHOff + kHidden * kTileBytes;
+constexpr uint32_t kOffW2 = kGroups * kGrpBytes;
+constexpr uint32_t kSmemTrain = kOffW2 + kHidden * kWBytes + kOutCh * kWidth * 2;
+static_assert((kGroups - 1) * kGrpBytes + kHOff + (kHidden - 1) * kTileBytes + 32768u <= kSmemTrain,
+              "the padded weight-gradient reads stay inside the CTA's shared memory");
+static_assert(kSmemTrain <= 227u * 1024u, "shared memory per CTA");
+
+__device__ __forceinline__ bool wait_or_abort(uint64_t* bar, uint32_t parity, volatile int* abort) {
+  for (uint32_t i = 0; i < kWaitLimit; ++i) {
+    if (tc::mbar_test(bar, parity)) return true;
+    if (*abort) return false;
+  }
+  *abort = 1;
+  return false;
+}
+
+// D (+)= A * B^T over n MMAs of K = 16, issued by the elected lane of a
+// converged warp; the descriptors advance by a_inc / b_inc per MMA.
+__device__ __forceinline__ void issue_run(uint32_t d, uint64_t da, uint64_t a_inc, uint64_t db, uint64_t b_inc,
+                                          int n, uint32_t idesc, uint32_t acc0) {
+  for (int kk = 0; kk < n; ++kk, da += a_inc, db += b_inc)
+    if (tc::elect_one()) tc::mma_bf16(d, da, db, idesc, (acc0 || kk > 0) ? 1u : 0u);
+}
+
+__device__ __forceinline__ void group_sync(int g) {
+  asm volatile("bar.sync %0, %1;" :: "r"(1 + g), "r"(kRows) : "memory");
+}
+
+__global__ void __launch_bounds__(kTrainThreads, 1) k_mlp_train(MlpArgs a) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  __shared__ __align__(8) uint64_t ready[kGroups], done[kGroups], fin;
+  __shared__ uint32_t tmem_base;
+  __shared__ int abort_flag, grp_ok[kGroups];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint32_t base = tc::smem_u32(smem);
+  const uint32_t tiles = (a.count + kRows - 1) / kRows;
+  const uint32_t stride = gridDim.x * kGroups;
+  volatile int* abort_v = &abort_flag;
+  if (tid == 0) {
+    for (int g = 0; g < kGroups; ++g) {
+      tc::mbar_init(&ready[g], 1);
+      tc::mbar_init(&done[g], 1);
+    }
+    tc::mbar_init(&fin, 1);
+    abort_flag = 0;
+  }
+  if (warp == 0) tc::tmem_alloc(&tmem_base, 512);
+  // a group's first rows of encoded inputs are requested before the weights,
+  // so that the two loads overlap
+  uint4 xfirst[8];
+  if (warp < 4 * kGroups) {
+    const uint32_t r = (blockIdx.x * kGroups + warp / 4) * kRows + (warp % 4) * 32 + lane;
+#pragma unroll
+    for (int c = 0; c < 8; ++c)
+      xfirst[c] = r < a.count ? *reinterpret_cast<const uint4*>(a.x0 + (size_t)r * kWidth + c * 8)
+                              : make_uint4(0u, 0u, 0u, 0u);
+  }
+  for (int l = 0; l < kLayers; ++l) {
+    const int nout = l < kHidden ? kWidth : kOutCh;
+    unsigned char* wl = smem + kOffW2 + l * kWBytes;
+    for (int i = tid; i < nout * 8; i += kTrainThreads) {
+      const int o = i >> 3, g = i & 7;
+      *reinterpret_cast<uint4*>(wl + o * 16 + g * nout * 16) =
+          *reinterpret_cast<const uint4*>(a.w[l] + (size_t)o * kWidth + g * 8);
+    }
+  }
+  tc::fence_smem_to_async();
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tmem = tmem_base;
+  double loss = 0.0;
+
+  if (warp == 4 * kGroups) {
+    // the issuing warp: all lanes run the loop, the elected lane issues
+    uint32_t n_ready[kGroups] = {0u, 0u};
+    uint32_t wg_init = 0u;  // layers whose weight gradient has been started
+    bool ok = true;
+    for (uint32_t r = 0; ok; ++r) {
+      bool any = false;
+      for (int k = 0; k < 2 * kLayers && ok; ++k) {
+        for (int g = 0; g < kGroups; ++g) {
+          if (blockIdx.x * kGroups + g + r * stride >= tiles) continue;
+          any = true;
+          int got = 0;
+          if (lane == 0) got = wait_or_abort(&ready[g], n_ready[g] & 1u, abort_v) ? 1 : 0;
+          ++n_ready[g];
+          if (!__shfl_sync(0xffffffffu, got, 0)) {
+            ok = false;
+            break;
+          }
+          tc::fence_after_sync();
+          const uint32_t gb = base + (uint32_t)g * kGrpBytes, d = tmem + 64u * (uint32_t)g;
+          // descriptors are formed before the issue loops and advance by adding
+          // (byte offset >> 4) to the start-address field, which never carries
+          if (k < kLayers) {  // forward layer l: D = In_l W_l^T
+            const int l = k;
+            const uint32_t nout = l < kHidden ? kWidth : kOutCh;
+            const uint32_t in = l == 0 ? gb + kHOff + 3u * kTileBytes : gb + kHOff + (uint32_t)(l - 1) * kTileBytes;
+            const uint32_t w = base + kOffW2 + (uint32_t)l * kWBytes;
+            issue_run(d, tc::smem_desc(in, kActLbo, 128u), (2u * kActLbo) >> 4,
+                      tc::smem_desc(w, nout * 16u, 128u), (2u * nout * 16u) >> 4, kWidth / 16,
+                      tc::idesc_bf16(128, nout, false, false), 0u);
+          } else {  // backward layer j: dIn = dZ_j W_j, dW_j += dZ_j^T In_j
+            const int j = 2 * kLayers - 1 - k;
+            const uint32_t nout = j == kHidden ? kOutCh : kWidth;
+            const uint32_t dz = j == kHidden ? gb + kGOff : gb + kHOff + (uint32_t)j * kTileBytes;
+            const uint32_t in = j == 0 ? gb + kHOff + 3u * kTileBytes : gb + kHOff + (uint32_t)(j - 1) * kTileBytes;
+            const uint32_t w = base + kOffW2 + (uint32_t)j * kWBytes;
+            issue_run(d, tc::smem_desc(dz, kActLbo, 128u), (2u * kActLbo) >> 4,
+                      tc::smem_desc(w, 128u, nout * 16u), 256u >> 4, (int)nout / 16,
+                      tc::idesc_bf16(128, kWidth, false, true), 0u);
+            const uint32_t acc0 = (wg_init >> j) & 1u;
+            wg_init |= 1u << j;
+            issue_run(tmem + 128u + 64u * (uint32_t)j, tc::smem_desc(dz, 128u, kActLbo), 256u >> 4,
+                      tc::smem_desc(in, 128u, kActLbo), 256u >> 4, kRows / 16,
+                      tc::idesc_bf16(128, kWidth, true, true), acc0);
+          }
+          if (tc::elect_one()) tc::mma_commit(&done[g]);
+          __syncwarp();
+        }
+      }
+      if (!any) break;
+    }
+    if (tc::elect_one()) tc::mma_commit(&fin);
+    __syncwarp();
+  } else {
+    // a group: warp gw of group g reads tensor-memory lanes 32 gw .. +31
+    const int g = warp / 4, gw = warp % 4, row = gw * 32 + lane;
+    unsigned char* gp = smem + (size_t)g * kGrpBytes;
+    unsigned char* h3 = gp + kHOff + 3 * kTileBytes;
+    const uint32_t my_lane = tmem + ((uint32_t)(gw * 32) << 16) + 64u * (uint32_t)g;
+    uint32_t n_done = 0;
+    // the encoded inputs of a tile's rows: fetched into registers one tile
+    // ahead, and kept for the copy that the last backward step reads
+    uint4 xcur[8], xnext[8];
+    auto fetch_x = [&](uint32_t t, uint4 (&dst)[8]) {
+      const uint32_t r = t * kRows + row;
+#pragma unroll
+      for (int c = 0; c < 8; ++c)
+        dst[c] = r < a.count ? *reinterpret_cast<const uint4*>(a.x0 + (size_t)r * kWidth + c * 8)
+                             : make_uint4(0u, 0u, 0u, 0u);
+    };
+    auto store_x = [&]() {
+#pragma unroll
+      for (int c = 0; c < 8; ++c) *reinterpret_cast<uint4*>(h3 + act_off(row, c * 8)) = xcur[c];
+    };
+    // all 64 accumulator columns of this thread's row, one wait
+    auto load_acc = [&](float (&v)[64]) {
+      uint32_t r[8][8];
+#pragma unroll
+      for (int c = 0; c < 8; ++c) tc::tmem_ld8_nowait(my_lane + (uint32_t)(c * 8), r[c]);
+      tc::tmem_wait_ld();
+#pragma unroll
+      for (int c = 0; c < 8; ++c)
+#pragma unroll
+        for (int e = 0; e < 8; ++e) v[c * 8 + e] = __uint_as_float(r[c][e]);
+    };
+    // operands written: hand the next GEMM to the issuing warp
+    auto hand_over = [&]() {
+      tc::fence_smem_to_async();
+      tc::fence_before_sync();
+      group_sync(g);
+      if (row == 0) tc::mbar_arrive(&ready[g]);
+    };
+    // the group's GEMM is done (one poller, the result shared group-wide)
+    auto gemm_done = [&]() {
+      if (row == 0) grp_ok[g] = wait_or_abort(&done[g], n_done & 1u, abort_v) ? 1 : 0;
+      ++n_done;
+      group_sync(g);
+      tc::fence_after_sync();
+      return grp_ok[g] != 0;
+    };
+    bool ok = true;
+    uint32_t tile = blockIdx.x * kGroups + g;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) xnext[c] = xfirst[c];
+    for (; tile < tiles && ok; tile += stride) {
+      const uint32_t grow = tile * kRows + row;
+      const bool valid = grow < a.count;
+#pragma unroll
+      for (int c = 0; c < 8; ++c) xcur[c] = xnext[c];
+      store_x();
+      hand_over();
+      for (int l = 0; l < kLayers && ok; ++l) {
+        if (!(ok = gemm_done())) break;
+        if (l < kHidden) {
+          unsigned char* h = gp + kHOff + l * kTileBytes;
+          float v[64];
+          load_acc(v);
+#pragma unroll
+          for (int c = 0; c < kWidth / 8; ++c) {
+            float f[8];
+#pragma unroll
+            for (int e = 0; e < 8; ++e) f[e] = fmaxf(v[c * 8 + e], 0.0f);
+            *reinterpret_cast<uint4*>(h + act_off(row, c * 8)) = pack_bf16x8(f);
+          }
+        } else {
+          float o[16], gr[16];
+          uint32_t r[2][8];
+          tc::tmem_ld8_nowait(my_lane, r[0]);
+          tc::tmem_ld8_nowait(my_lane + 8u, r[1]);
+          tc::tmem_wait_ld();
+#pragma unroll
+          for (int c = 0; c < 16; ++c) {
+            o[c] = __uint_as_float(r[c >> 3][c & 7]);
+            gr[c] = 0.0f;
+          }
+          if (valid)
+            for (int c = 0; c < 3; ++c) {
+              const float oc = round_bf16(o[c]), t = a.target[(size_t)grow * 3 + c];
+              const float den = oc * oc + 0.01f, dd = oc - t;
+              loss += (double)(dd * dd / den);
+              gr[c] = 2.0f * dd / den;
+            }
+          *reinterpret_cast<uint4*>(gp + kGOff + act_off(row, 0)) = pack_bf16x8(*reinterpret_cast<float(*)[8]>(gr));
+          *reinterpret_cast<uint4*>(gp + kGOff + act_off(row, 8)) =
+              pack_bf16x8(*reinterpret_cast<float(*)[8]>(gr + 8));
+        }
+        hand_over();
+      }
+      for (int j = kHidden; j >= 0 && ok; --j) {
+        if (!(ok = gemm_done())) break;
+        if (j > 0) {
+          // dZ_(j-1) = BF16(dIn) where H_(j-1) > 0, over H_(j-1) in place
+          unsigned char* h = gp + kHOff + (j - 1) * kTileBytes;
+          float v[64];
+          load_acc(v);
+#pragma unroll
+          for (int c = 0; c < kWidth / 8; ++c) {
+            float f[8], hv[8];
+            unpack_bf16x8(*reinterpret_cast<const uint4*>(h + act_off(row, c * 8)), hv);
+#pragma unroll
+            for (int e = 0; e < 8; ++e) f[e] = hv[e] > 0.0f ? v[c * 8 + e] : 0.0f;
+            *reinterpret_cast<uint4*>(h + act_off(row, c * 8)) = pack_bf16x8(f);
+          }
+          if (j == 3 && tile + stride < tiles) fetch_x(tile + stride, xnext);
+          if (j == 1) store_x();  // In_0 for the last step; H3's tile is free again
+          hand_over();
+        } else {
+          // gradient of the grid features, rounded to BF16, for k_encode_bwd
+          uint32_t r[4][8];
+#pragma unroll
+          for (int c = 0; c < 4; ++c) tc::tmem_ld8_nowait(my_lane + (uint32_t)(c * 8), r[c]);
+          tc::tmem_wait_ld();
+          if (valid)
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+              float f[8];
+#pragma unroll
+              for (int e = 0; e < 8; ++e) f[e] = __uint_as_float(r[c][e]);
+              *reinterpret_cast<uint4*>(a.dx + (size_t)grow * 32 + c * 8) = pack_bf16x8(f);
+            }
+          tc::fence_before_sync();
+          group_sync(g);  // every row's accumulator is read before the next tile's GEMMs
+        }
+      }
+    }
+  }
+
+  tc::fence_before_sync();
+  __syncthreads();
+  bool fin_ok = false;
+  if (warp < 4) {
+    int got = 0;
+    if (lane == 0) got = (!abort_flag && wait_or_abort(&fin, 0u, abort_v)) ? 1 : 0;
+    fin_ok = __shfl_sync(0xffffffffu, got, 0) != 0;
+  }
+  tc::fence_after_sync();
+  if (warp < 4 && fin_ok) {
+    // weight gradients: accumulator row o (lane) holds dW[o][0..64)
+    for (int j = 0; j < kLayers; ++j) {
+      const int nout = j < kHidden ? kWidth : kOutCh;
+      if (warp * 32 >= nout) continue;  // warp-uniform: tcgen05.ld is warp-wide
+      for (int c = 0; c < kWidth / 8; ++c) {
+        float v[8];
+        tc::tmem_ld8(tmem + ((uint32_t)(warp * 32) << 16) + 128u + 64u * (uint32_t)j + (uint32_t)(c * 8), v);
+        if (tid < nout) {  // two 16-byte vector atomics
+          float4* dst = reinterpret_cast<float4*>(a.gw[j] + tid * kWidth + c * 8);
+          atomicAdd(dst, make_float4(v[0], v[1], v[2], v[3]));
+          atomicAdd(dst + 1, make_float4(v[4], v[5], v[6], v[7]));
+        }
+      }
+    }
+  }
+  if (a.loss && warp < 4 * kGroups) {
+    for (int off = 16; off > 0; off >>= 1) loss += __shfl_down_sync(0xffffffffu, loss, off);
+    if (lane == 0) atomicAdd(a.loss, loss);
+  }
+  if (abort_flag && tid == 0) {
+    atomicOr(a.err, 4u);
+    tc::mbar_wait(&fin, 0u, kWaitLimit);  // MMAs that may still be in flight
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) tc::tmem_dealloc(tmem, 512);
+}
+
 }  // namespace
 
 struct NrcNet {
@@ -522,6 +839,19 @@ int sm_count() {
 
 template <bool kTrain>
 cudaError_t launch_mlp(const MlpArgs& a, cudaStream_t st) {
+  if (kTrain) {
+    static bool attr_train = false;
+    if (!attr_train) {
+      cudaError_t e = cudaFuncSetAttribute(k_mlp_train, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)kSmemTrain);
+      if (e != cudaSuccess) return e;
+      attr_train = true;
+    }
+    const uint32_t tiles = (a.count + kRows - 1) / kRows;
+    const int grid = (int)std::min<uint32_t>((tiles + kGroups - 1) / kGroups, (uint32_t)sm_count());
+    k_mlp_train<<<grid, kTrainThreads, kSmemTrain, st>>>(a);
+    return cudaGetLastError();
+  }
   static bool attr = false;
   if (!attr) {
     cudaError_t e = cudaFuncSetAttribute(k_mlp<kTrain>, cudaFuncAttributeMaxDynamicSharedMemorySize,
