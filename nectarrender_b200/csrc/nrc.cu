@@ -7,22 +7,21 @@
 // the first three outputs are the radiance), no biases. Loss: relative squared error
 // (o - t)^2 / (o^2 + 0.01) with o held constant in the denominator.
 //
-// The whole MLP is one fused tcgen05 kernel per call (k_mlp): a CTA of 128
-// threads takes 128 queries at a time, one row per thread and one
+// The whole MLP is one fused tcgen05 kernel per call (k_mlp_infer,
+// k_mlp_train): 128 queries per tile, one row per thread and one
 // tensor-memory lane per row. The five weight matrices and every activation
 // tile stay in shared memory (BF16, no-swizzle canonical layouts), each layer
-// is 1-4 MMAs of M = 128, N = 64 (16 for the output layer), K = 16 issued by
-// one thread into a tensor-memory accumulator, and the epilogues (ReLU, the
-// loss gradient, the ReLU mask of the backward pass) run on the rows the
-// threads load back with tcgen05.ld. In training the backward-data GEMM of
-// each layer and its weight-gradient GEMM (dW += dZ^T X over the tile's rows,
-// both operands read MN-major from the same tiles) are issued together; the
-// weight gradients accumulate in tensor memory over all the CTA's tiles and
-// are added to the FP32 gradient with vector atomics once at the end; the
-// input-gradient rows go to global memory for the hash-grid scatter. A
-// training step is: encode, k_mlp, grid scatter, one Adam launch for the MLP
-// and one for the grid. The encoding and the scatter run one thread per
-// (query, level).
+// is 1-4 MMAs of M = 128, N = 64 (16 for the output layer), K = 16 into a
+// tensor-memory accumulator, and the epilogues (ReLU, the loss gradient, the
+// ReLU mask of the backward pass) run on the rows the threads load back with
+// tcgen05.ld. In training the backward-data GEMM of each layer and its
+// weight-gradient GEMM (dW += dZ^T X over the tile's rows, both operands read
+// MN-major from the same tiles) are issued together; the weight gradients
+// accumulate in tensor memory over all the CTA's tiles and are added to the
+// FP32 gradient with vector atomics once at the end; the input-gradient rows
+// go to global memory for the hash-grid scatter. A training step is: encode,
+// k_mlp_train, grid scatter, one Adam launch for the MLP and one for the
+// grid. The encoding and the scatter run one thread per (query, level).
 #include "nrc.cuh"
 
 #include <cmath>
@@ -39,7 +38,7 @@ constexpr int kLevels = 16, kFeat = 2, kLog2T = 19;
 constexpr uint32_t kT = 1u << kLog2T;
 constexpr int kWidth = 64, kOutCh = 16;
 constexpr int kHidden = 4, kLayers = kHidden + 1;
-constexpr int kRows = 128;  // queries per tile = threads per CTA of k_mlp
+constexpr int kRows = 128;  // queries per tile = threads per CTA of k_mlp_infer
 constexpr uint32_t kWaitLimit = 1u << 26;
 constexpr float kNmin = 16.0f, kNmax = 2048.0f;
 
@@ -184,34 +183,24 @@ __device__ __forceinline__ void unpack_bf16x8(const uint4& r, float (&v)[8]) {
 }
 __device__ __forceinline__ float round_bf16(float x) { return __bfloat162float(__float2bfloat16(x)); }
 
-// Shared memory of k_mlp (bytes from the dynamic base). An activation tile
-// holds 128 rows x C columns (C = 64, or 16 for the output gradient) in the
-// K-major no-swizzle layout with the 8-row core matrices stacked along the
-// rows: element (r, c) at r * 16 + (c / 8) * 2048 + (c % 8) * 2, i.e.
-// LBO = 2048 (next 8 columns) and SBO = 128 (next 8 rows) when the rows are
-// the M dimension. Read as an MN-major operand over (column, row) the same
-// bytes have LBO = 128 and SBO = 2048: the weight-gradient GEMMs use that
-// view. Their A operand is M = 128 wide over at most 64 real columns and so
-// reads up to 32 KB past the tile start (rows of the accumulator that are
-// never read back): those tiles (dZ, G) come first.
+// Shared-memory layouts of the MLP kernels. An activation tile holds 128
+// rows x C columns (C = 64, or 16 for the output gradient) in the K-major
+// no-swizzle layout with the 8-row core matrices stacked along the rows:
+// element (r, c) at r * 16 + (c / 8) * 2048 + (c % 8) * 2, i.e. LBO = 2048
+// (next 8 columns) and SBO = 128 (next 8 rows) when the rows are the M
+// dimension. Read as an MN-major operand over (column, row) the same bytes
+// have LBO = 128 and SBO = 2048: the weight-gradient GEMMs use that view.
+// Their A operand is M = 128 wide over at most 64 real columns and so reads
+// up to 32 KB past the tile start (rows of the accumulator that are never
+// read back), which must stay inside the CTA's shared memory.
 // A weight matrix W[o][i] (nout x 64) is the K-major B operand of the forward
 // GEMM (N = o, K = i): element (o, i) at o * 16 + (i / 8) * nout * 16 +
 // (i % 8) * 2 (SBO = 128, LBO = nout * 16); the backward-data GEMM reads it
 // MN-major over (i, o) (LBO = 128, SBO = nout * 16).
 constexpr uint32_t kTileBytes = kRows * kWidth * 2;        // 16 KB
 constexpr uint32_t kActLbo = kRows * 16;                   // 2048
-constexpr uint32_t kOffDz = 0;                             // dZ of a hidden layer
-constexpr uint32_t kOffG = kOffDz + kTileBytes;            // dZ of the output layer (4 KB)
-constexpr uint32_t kOffX = kOffG + kRows * kOutCh * 2;     // encoded inputs
-constexpr uint32_t kOffH = kOffX + kTileBytes;             // H0..H3
-constexpr uint32_t kOffW = kOffH + kHidden * kTileBytes;   // W0..W3, then W4
 constexpr uint32_t kWBytes = kWidth * kWidth * 2;          // 8 KB
-constexpr uint32_t kSmemBytes = kOffW + kHidden * kWBytes + kOutCh * kWidth * 2;  // 134 KB
-static_assert(kOffG + 32768u <= kSmemBytes && kOffDz + 32768u <= kSmemBytes,
-              "the padded weight-gradient reads stay inside the CTA's shared memory");
-static_assert(kSmemBytes <= 227u * 1024u, "shared memory per CTA");
-// Inference needs no gradient tiles and only two hidden tiles (ping-pong):
-// X, H(even), H(odd), weights = 82 KB, two CTAs per SM.
+// Inference: X, H(even), H(odd) (ping-pong), weights = 82 KB, two CTAs per SM.
 constexpr uint32_t kInferSmemBytes = 3 * kTileBytes + kHidden * kWBytes + kOutCh * kWidth * 2;
 
 __device__ __forceinline__ uint32_t act_off(uint32_t r, uint32_t c) {
@@ -232,28 +221,26 @@ struct MlpArgs {
   GridGeo geo;
 };
 
-// D[tmem_col] (+)= A * B^T over K = 16 * nk (one thread).
-__device__ __forceinline__ void issue_gemm(uint32_t d, uint32_t a, uint32_t a_lbo, uint32_t a_sbo,
-                                           uint32_t a_step, uint32_t b, uint32_t b_lbo,
-                                           uint32_t b_sbo, uint32_t b_step, int nk, uint32_t idesc,
-                                           bool acc) {
-  for (int k = 0; k < nk; ++k)
-    tc::mma_bf16(d, tc::smem_desc(a + k * a_step, a_lbo, a_sbo),
-                 tc::smem_desc(b + k * b_step, b_lbo, b_sbo), idesc, (acc || k > 0) ? 1u : 0u);
+// D (+)= A * B^T over n MMAs of K = 16, issued by the elected lane of a
+// converged warp; the descriptors advance by a_inc / b_inc per MMA (added to
+// the start-address field, which never carries: operands lie below 256 KB).
+__device__ __forceinline__ void issue_run(uint32_t d, uint64_t da, uint64_t a_inc, uint64_t db, uint64_t b_inc,
+                                          int n, uint32_t idesc, uint32_t acc0) {
+  for (int kk = 0; kk < n; ++kk, da += a_inc, db += b_inc)
+    if (tc::elect_one()) tc::mma_bf16(d, da, db, idesc, (acc0 || kk > 0) ? 1u : 0u);
 }
 
-template <bool kTrain>
-__global__ void __launch_bounds__(kRows, kTrain ? 1 : 2) k_mlp(MlpArgs a) {
+// Inference: one CTA of 128 threads takes 128 queries at a time, one row per
+// thread and one tensor-memory lane per row; warp 0 issues each layer's
+// GEMM, the CTA waits on its commit, applies ReLU to the accumulator rows it
+// loads back and writes the next layer's input tile. Two CTAs per SM overlap
+// one CTA's epilogues with the other's GEMMs.
+__global__ void __launch_bounds__(kRows, 2) k_mlp_infer(MlpArgs a) {
   extern __shared__ __align__(1024) unsigned char smem[];
   __shared__ __align__(8) uint64_t bar;
   __shared__ uint32_t tmem_base;
-  constexpr uint32_t kCols = kTrain ? 512u : 64u;  // D at 0; weight gradients at 64 + 64 * l
-  constexpr uint32_t oX = kTrain ? kOffX : 0u;
-  constexpr uint32_t oW = kTrain ? kOffW : 3u * kTileBytes;
-  // hidden tile l: one per layer in training, ping-pong in inference
-  auto h_tile = [](int l) -> uint32_t {
-    return kTrain ? kOffH + (uint32_t)l * kTileBytes : kTileBytes * (1u + (uint32_t)(l & 1));
-  };
+  constexpr uint32_t kCols = 64u;
+  constexpr uint32_t oX = 0u, oW = 3u * kTileBytes;
   const int tid = threadIdx.x, warp = tid >> 5;
   const uint32_t base = tc::smem_u32(smem);
   if (tid == 0) tc::mbar_init(&bar, 1);
@@ -273,23 +260,7 @@ __global__ void __launch_bounds__(kRows, kTrain ? 1 : 2) k_mlp(MlpArgs a) {
   const uint32_t tmem = tmem_base;
   const uint32_t my_lane = tmem + ((uint32_t)(warp * 32) << 16);
   uint32_t phase = 0;
-  bool ok = true, wg_acc = false;
-  double loss = 0.0;
-  // operands written, accumulators read: hand the tensor core the next GEMM
-  auto to_mma = [&]() {
-    tc::fence_smem_to_async();
-    tc::fence_before_sync();
-    __syncthreads();
-  };
-  // CTA-uniform wait for the last commit
-  auto wait = [&]() {
-    const bool w = tc::mbar_wait(&bar, phase, kWaitLimit);
-    ok = __syncthreads_and(w) != 0;
-    if (ok) phase ^= 1u;
-    tc::fence_after_sync();
-    return ok;
-  };
-
+  bool ok = true;
   const uint32_t tiles = (a.count + kRows - 1) / kRows;
   for (uint32_t tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
     const uint32_t row = tile * kRows + tid;
@@ -299,115 +270,46 @@ __global__ void __launch_bounds__(kRows, kTrain ? 1 : 2) k_mlp(MlpArgs a) {
       if (valid) v = *reinterpret_cast<const uint4*>(a.x0 + (size_t)row * kWidth + g * 8);
       *reinterpret_cast<uint4*>(smem + oX + act_off(tid, g * 8)) = v;
     }
-    // forward
     uint32_t in_off = oX;
     for (int l = 0; l < kLayers && ok; ++l) {
       const uint32_t nout = l < kHidden ? kWidth : kOutCh;
-      to_mma();
-      if (tid == 0) {
+      // operands written, accumulator read: hand the tensor core the layer
+      tc::fence_smem_to_async();
+      tc::fence_before_sync();
+      __syncthreads();
+      if (warp == 0) {
         tc::fence_after_sync();
-        issue_gemm(tmem, base + in_off, kActLbo, 128u, 2u * kActLbo, base + oW + l * kWBytes,
-                   nout * 16u, 128u, 2u * nout * 16u, kWidth / 16,
-                   tc::idesc_bf16(128, nout, false, false), false);
-        tc::mma_commit(&bar);
+        issue_run(tmem, tc::smem_desc(base + in_off, kActLbo, 128u), (2u * kActLbo) >> 4,
+                  tc::smem_desc(base + oW + (uint32_t)l * kWBytes, nout * 16u, 128u), (2u * nout * 16u) >> 4,
+                  kWidth / 16, tc::idesc_bf16(128, nout, false, false), 0u);
+        if (tc::elect_one()) tc::mma_commit(&bar);
+        __syncwarp();
       }
-      if (!wait()) break;
+      ok = __syncthreads_and(tc::mbar_wait(&bar, phase, kWaitLimit)) != 0;
+      if (!ok) break;
+      phase ^= 1u;
+      tc::fence_after_sync();
       if (l < kHidden) {
-        const uint32_t h_off = h_tile(l);
+        const uint32_t h_off = kTileBytes * (1u + (uint32_t)(l & 1));
+        uint32_t r[8][8];
+#pragma unroll
+        for (int c = 0; c < 8; ++c) tc::tmem_ld8_nowait(my_lane + (uint32_t)(c * 8), r[c]);
+        tc::tmem_wait_ld();
+#pragma unroll
         for (int c = 0; c < kWidth / 8; ++c) {
           float v[8];
-          tc::tmem_ld8(my_lane + (uint32_t)(c * 8), v);
 #pragma unroll
-          for (int k = 0; k < 8; ++k) v[k] = fmaxf(v[k], 0.0f);
+          for (int k = 0; k < 8; ++k) v[k] = fmaxf(__uint_as_float(r[c][k]), 0.0f);
           *reinterpret_cast<uint4*>(smem + h_off + act_off(tid, c * 8)) = pack_bf16x8(v);
         }
         in_off = h_off;
       } else {
-        float o[16];
-        tc::tmem_ld8(my_lane, *reinterpret_cast<float(*)[8]>(o));
-        tc::tmem_ld8(my_lane + 8u, *reinterpret_cast<float(*)[8]>(o + 8));
-        if (!kTrain) {
-          if (valid)
-            for (int c = 0; c < 3; ++c) a.out[(size_t)row * 3 + c] = fmaxf(round_bf16(o[c]), 0.0f);
-        } else {
-          float g[16];
-#pragma unroll
-          for (int c = 0; c < 16; ++c) g[c] = 0.0f;
-          if (valid)
-            for (int c = 0; c < 3; ++c) {
-              const float oc = round_bf16(o[c]), t = a.target[(size_t)row * 3 + c];
-              const float den = oc * oc + 0.01f, d = oc - t;
-              loss += (double)(d * d / den);
-              g[c] = 2.0f * d / den;
-            }
-          *reinterpret_cast<uint4*>(smem + kOffG + act_off(tid, 0)) =
-              pack_bf16x8(*reinterpret_cast<float(*)[8]>(g));
-          *reinterpret_cast<uint4*>(smem + kOffG + act_off(tid, 8)) =
-              pack_bf16x8(*reinterpret_cast<float(*)[8]>(g + 8));
-        }
+        float o[8];
+        tc::tmem_ld8(my_lane, o);
+        if (valid)
+          for (int c = 0; c < 3; ++c) a.out[(size_t)row * 3 + c] = fmaxf(round_bf16(o[c]), 0.0f);
       }
     }
-    if (!kTrain || !ok) continue;
-    // backward: layer j from the output layer down
-    for (int j = kHidden; j >= 0 && ok; --j) {
-      const uint32_t nout = j == kHidden ? kOutCh : kWidth;
-      const uint32_t dz = j == kHidden ? kOffG : kOffDz;
-      const uint32_t in_j = j == 0 ? kOffX : kOffH + (j - 1) * kTileBytes;
-      to_mma();
-      if (tid == 0) {
-        tc::fence_after_sync();
-        // dIn = dZ_j W_j: A = dZ_j (M = rows, K = nout), B = W_j seen as N = 64 inputs x K = nout
-        issue_gemm(tmem, base + dz, kActLbo, 128u, 2u * kActLbo, base + kOffW + j * kWBytes, 128u,
-                   nout * 16u, 256u, (int)nout / 16, tc::idesc_bf16(128, kWidth, false, true),
-                   false);
-        // dW_j += dZ_j^T In_j over the rows: A = dZ_j seen as M = 128 (nout real) x K = rows,
-        // B = In_j seen as N = 64 x K = rows, both MN-major
-        issue_gemm(tmem + 64u + 64u * (uint32_t)j, base + dz, 128u, kActLbo, 256u, base + in_j, 128u,
-                   kActLbo, 256u, kRows / 16, tc::idesc_bf16(128, kWidth, true, true), wg_acc);
-        tc::mma_commit(&bar);
-      }
-      if (!wait()) break;
-      if (j > 0) {
-        // dZ_(j-1) = BF16(dH) where H_(j-1) > 0
-        const uint32_t h_off = kOffH + (j - 1) * kTileBytes;
-        for (int c = 0; c < kWidth / 8; ++c) {
-          float v[8], h[8];
-          tc::tmem_ld8(my_lane + (uint32_t)(c * 8), v);
-          unpack_bf16x8(*reinterpret_cast<const uint4*>(smem + h_off + act_off(tid, c * 8)), h);
-#pragma unroll
-          for (int k = 0; k < 8; ++k) v[k] = h[k] > 0.0f ? v[k] : 0.0f;
-          *reinterpret_cast<uint4*>(smem + kOffDz + act_off(tid, c * 8)) = pack_bf16x8(v);
-        }
-      } else {
-        // gradient of the grid features, rounded to BF16, for k_encode_bwd
-        for (int c = 0; c < 4; ++c) {
-          float v[8];
-          tc::tmem_ld8(my_lane + (uint32_t)(c * 8), v);
-          if (valid) *reinterpret_cast<uint4*>(a.dx + (size_t)row * 32 + c * 8) = pack_bf16x8(v);
-        }
-      }
-    }
-    wg_acc = true;
-  }
-  if (kTrain && ok && wg_acc) {
-    // weight gradients: accumulator row o (lane) holds dW[o][0..64)
-    for (int j = 0; j < kLayers; ++j) {
-      const int nout = j < kHidden ? kWidth : kOutCh;
-      if (warp * 32 >= nout) continue;  // warp-uniform: tcgen05.ld is warp-wide
-      for (int c = 0; c < kWidth / 8; ++c) {
-        float v[8];
-        tc::tmem_ld8(my_lane + 64u + 64u * (uint32_t)j + (uint32_t)(c * 8), v);
-        if (tid < nout) {  // two 16-byte vector atomics
-          float4* dst = reinterpret_cast<float4*>(a.gw[j] + tid * kWidth + c * 8);
-          atomicAdd(dst, make_float4(v[0], v[1], v[2], v[3]));
-          atomicAdd(dst + 1, make_float4(v[4], v[5], v[6], v[7]));
-        }
-      }
-    }
-  }
-  if (kTrain && a.loss) {
-    for (int off = 16; off > 0; off >>= 1) loss += __shfl_down_sync(0xffffffffu, loss, off);
-    if ((tid & 31) == 0) atomicAdd(a.loss, loss);
   }
   if (!ok) {
     if (tid == 0) atomicOr(a.err, 4u);
@@ -500,14 +402,6 @@ __device__ __forceinline__ bool wait_or_abort(uint64_t* bar, uint32_t parity, vo
   }
   *abort = 1;
   return false;
-}
-
-// D (+)= A * B^T over n MMAs of K = 16, issued by the elected lane of a
-// converged warp; the descriptors advance by a_inc / b_inc per MMA.
-__device__ __forceinline__ void issue_run(uint32_t d, uint64_t da, uint64_t a_inc, uint64_t db, uint64_t b_inc,
-                                          int n, uint32_t idesc, uint32_t acc0) {
-  for (int kk = 0; kk < n; ++kk, da += a_inc, db += b_inc)
-    if (tc::elect_one()) tc::mma_bf16(d, da, db, idesc, (acc0 || kk > 0) ? 1u : 0u);
 }
 
 __device__ __forceinline__ void group_sync(int g) {
@@ -837,32 +731,30 @@ int sm_count() {
   return sms;
 }
 
-template <bool kTrain>
-cudaError_t launch_mlp(const MlpArgs& a, cudaStream_t st) {
-  if (kTrain) {
-    static bool attr_train = false;
-    if (!attr_train) {
-      cudaError_t e = cudaFuncSetAttribute(k_mlp_train, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)kSmemTrain);
-      if (e != cudaSuccess) return e;
-      attr_train = true;
-    }
-    const uint32_t tiles = (a.count + kRows - 1) / kRows;
-    const int grid = (int)std::min<uint32_t>((tiles + kGroups - 1) / kGroups, (uint32_t)sm_count());
-    k_mlp_train<<<grid, kTrainThreads, kSmemTrain, st>>>(a);
-    return cudaGetLastError();
-  }
+cudaError_t launch_mlp_train(const MlpArgs& a, cudaStream_t st) {
   static bool attr = false;
   if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(k_mlp<kTrain>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)(kTrain ? kSmemBytes : kInferSmemBytes));
+    cudaError_t e = cudaFuncSetAttribute(k_mlp_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemTrain);
     if (e != cudaSuccess) return e;
     attr = true;
   }
   const uint32_t tiles = (a.count + kRows - 1) / kRows;
-  const uint32_t bytes = kTrain ? kSmemBytes : kInferSmemBytes;
-  const int grid = (int)std::min<uint32_t>(tiles, (uint32_t)sm_count() * (kTrain ? 1u : 2u));
-  k_mlp<kTrain><<<grid, kRows, bytes, st>>>(a);
+  const int grid = (int)std::min<uint32_t>((tiles + kGroups - 1) / kGroups, (uint32_t)sm_count());
+  k_mlp_train<<<grid, kTrainThreads, kSmemTrain, st>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mlp_infer(const MlpArgs& a, cudaStream_t st) {
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e =
+        cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kInferSmemBytes);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  const uint32_t tiles = (a.count + kRows - 1) / kRows;
+  const int grid = (int)std::min<uint32_t>(tiles, (uint32_t)sm_count() * 2u);
+  k_mlp_infer<<<grid, kRows, kInferSmemBytes, st>>>(a);
   return cudaGetLastError();
 }
 
@@ -960,7 +852,7 @@ std::string nrc_infer(Nrc& c, const NrcQuery* q, uint32_t count, float* out, cud
   k_encode<<<blocks_for((size_t)count * kLevels), 256, 0, st>>>(n.geo, q, n.grid, n.x0, count);
   MlpArgs a = mlp_args(n, count);
   a.out = out;
-  cudaError_t e = launch_mlp<false>(a, st);
+  cudaError_t e = launch_mlp_infer(a, st);
   return e == cudaSuccess ? std::string() : cuda_msg(e, "nrc inference");
 }
 
@@ -981,7 +873,7 @@ std::string nrc_train(Nrc& c, const NrcQuery* q, const float* target, uint32_t c
   a.target = target;
   a.q = q;
   a.loss = n.d_loss;
-  cudaError_t e = launch_mlp<true>(a, st);
+  cudaError_t e = launch_mlp_train(a, st);
   if (e != cudaSuccess) return cuda_msg(e, "nrc training");
   k_encode_bwd<<<blocks_for((size_t)count * kLevels), 256, 0, st>>>(
       n.geo, q, reinterpret_cast<const __nv_bfloat162*>(n.dx), n.gg, count);
