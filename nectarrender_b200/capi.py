@@ -136,10 +136,13 @@ def material_desc(d: dict) -> MaterialDesc:
     m.tint = c_float3(*d.get("tint", (1.0, 1.0, 1.0)))
     for k in range(5):
         t = TextureDesc()
-        t.type = 0
-        t.image = -1
-        t.scale = 1.0
-        t.rgb = c_float3(*d["tex"][k])
+        slot = d["tex"][k]
+        if isinstance(slot, dict):  # IMAGE: an index into the spec's images
+            t.type, t.image, t.scale = 1, int(slot["image"]), float(slot.get("scale", 1.0))
+            t.rgb = c_float3(0.0, 0.0, 0.0)
+        else:
+            t.type, t.image, t.scale = 0, -1, 1.0
+            t.rgb = c_float3(*slot)
         m.tex[k] = t
     return m
 
@@ -216,6 +219,10 @@ class Scene:
         for path in spec.meshes:
             mid = C.c_uint32()
             _check(load(self.h, path.encode(), C.byref(mid)), "nr_scene_load_obj")
+        for im in spec.images:
+            im = np.ascontiguousarray(im, np.uint8)
+            _check(self.lib.nr_scene_add_image(self.h, im.ctypes.data_as(C.POINTER(C.c_uint8)), im.shape[0],
+                                               im.shape[1], im.shape[2], None), "nr_scene_add_image")
         for o in spec.objects:
             mid = C.c_uint32()
             _check(self.lib.nr_scene_add_material(self.h, C.byref(material_desc(o["material"])),

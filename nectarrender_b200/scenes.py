@@ -52,6 +52,9 @@ class SceneSpec:
     sky: dict = field(default_factory=lambda: {"type": SKY_NULL})
     meshes: list[str] = field(default_factory=list)   # OBJ paths, indexed by object["mesh"]
     name: str = ""
+    # uint8 planar CHW images (C >= 3) of IMAGE textures: a material's texture
+    # slot is an RGB tuple (a constant colour) or {"image": index, "scale": s}
+    images: list = field(default_factory=list)
 
 
 def _mat(type_, **kw) -> dict:
@@ -120,6 +123,66 @@ def cornell(res: int = 512, spp: int = 64, depth: int = 8, seed: int = 0) -> Sce
     ]
     cam = camera(res, res, (0, 0, 2), (0, 0, 0), spp + 1)
     return SceneSpec(objects=objs, camera=cam, ray_depth=depth, seed=seed, name=f"cornell{res}")
+
+
+def cornell_cubes(res: int = 64, spp: int = 4, depth: int = 8, seed: int = 0, aperture: float = 0.08,
+                  focus_distance: float = 2.0) -> SceneSpec:
+    """The Cornell box with its spheres replaced by rotated cubes (Lambertian,
+    rough metal, glass) and a camera with a finite aperture (thin-lens
+    defocus, camera.h): the cube's six quads under an arbitrary rotation and
+    the lens sampling, which the other test scenes do not exercise."""
+    spec = cornell(res=res, spp=spp, depth=depth, seed=seed)
+    light = spec.objects[-1]
+    spec.objects = spec.objects[:5] + [
+        obj(CUBE, lambertian((0.8, 0.8, 0.8)), (-0.22, -0.3, -0.15), (15, 30, 5), (0.3, 0.4, 0.3)),
+        obj(CUBE, pbr((0.9, 0.7, 0.4), roughness=0.35, metallic=0.8), (0.22, -0.3, -0.2), (-10, -40, 20),
+            (0.25, 0.25, 0.25)),
+        obj(CUBE, dielectric(ior=1.5), (0.02, -0.28, 0.22), (30, 45, 0), (0.2, 0.2, 0.2)),
+        light,
+    ]
+    spec.camera["aperture"] = float(aperture)
+    spec.camera["focus_distance"] = float(focus_distance)
+    spec.name = f"cornell_cubes{res}"
+    return spec
+
+
+def image_tex(index: int, scale: float = 1.0) -> dict:
+    """An IMAGE texture slot: spec.images[index] at texture_scale `scale`."""
+    return {"image": int(index), "scale": float(scale)}
+
+
+def cornell_textured(res: int = 64, spp: int = 4, depth: int = 8, seed: int = 0) -> SceneSpec:
+    """The Cornell box with image textures: a checker albedo on the back
+    wall (scale 0.5, so the uvs wrap), a PBR sphere and a PBR cube whose
+    albedo, roughness, metallic and normal come from images (the normal map
+    tilts the shading normal through the tangent frame), generated from a
+    fixed seed."""
+    spec = cornell(res=res, spp=spp, depth=depth, seed=seed)
+    rng = np.random.default_rng(7)
+    n = 16
+    yy, xx = np.mgrid[0:n, 0:n]
+    checker = ((xx // 4 + yy // 4) % 2).astype(np.float64)
+    albedo = np.stack([40 + 200 * checker, 60 + 150 * (1 - checker), 90 + 0 * checker]).astype(np.uint8)
+    rough = np.repeat((40 + 180 * rng.random((1, n, n))).astype(np.uint8), 3, axis=0)
+    metal = np.repeat((255 * (rng.random((1, n, n)) > 0.5)).astype(np.uint8), 3, axis=0)
+    # tangent-space normals: a bumpy field around +z, stored as n * 0.5 + 0.5
+    ang = rng.random((2, n, n)) * 0.6 - 0.3
+    nz = np.sqrt(np.maximum(1.0 - ang[0] ** 2 - ang[1] ** 2, 0.0))
+    normal = np.clip(np.stack([ang[0], ang[1], nz]) * 127.5 + 127.5, 0, 255).astype(np.uint8)
+    colour = (40 + 200 * rng.random((3, n, n))).astype(np.uint8)
+    spec.images = [albedo, rough, metal, normal, colour]
+    back = dict(spec.objects[4])
+    back["material"] = _mat(LAMBERTIAN, tex=[image_tex(0, 0.5)] + [(0.0, 0.0, 0.0)] * 4)
+    textured_pbr = _mat(PBR, tex=[image_tex(4), image_tex(1), image_tex(2), (0.0, 0.0, 0.0), image_tex(3)])
+    light = spec.objects[-1]
+    spec.objects = spec.objects[:4] + [back] + [
+        obj(SPHERE, textured_pbr, (-0.22, -0.2, -0.15), radius=0.3),
+        obj(CUBE, textured_pbr, (0.22, -0.3, -0.2), (10, -35, 5), (0.3, 0.3, 0.3)),
+        obj(SPHERE, dielectric(ior=1.5), (0.02, -0.25, 0.22), radius=0.3),
+        light,
+    ]
+    spec.name = f"cornell_textured{res}"
+    return spec
 
 
 # ---------------------------------------------------------------------------
@@ -362,6 +425,9 @@ def to_pathtracer(spec: SceneSpec, pt=None):
 
     def material(d):
         t = d["type"]
+        if any(isinstance(c, dict) for c in d["tex"]):
+            raise NotImplementedError("image texture slots of a spec go through capi.Scene "
+                                      "(Texture.from_image reads image files)")
         tex = [T.from_color(C(*c)) for c in d["tex"]]
         if t == LAMBERTIAN:
             return M.lambertian(tex[0])
@@ -461,12 +527,14 @@ def from_pathtracer(scene, camera, ray_depth: int, seed: int, name: str = "") ->
 
 
 def spec_to_json(spec: SceneSpec) -> dict:
-    """A JSON-ready dict of a spec (tuples become lists)."""
+    """A JSON-ready dict of a spec (tuples and arrays become lists)."""
     import dataclasses
     return json_ready(dataclasses.asdict(spec))
 
 
 def json_ready(x):
+    if isinstance(x, np.ndarray):
+        return x.tolist()
     if isinstance(x, dict):
         return {k: json_ready(v) for k, v in x.items()}
     if isinstance(x, (list, tuple)):
@@ -488,8 +556,9 @@ def spec_from_json(d: dict) -> SceneSpec:
         objects.append(o)
     cam = {k: tup(v) for k, v in d["camera"].items()}
     sky = {k: tup(v) for k, v in d["sky"].items()}
+    images = [np.asarray(im, np.uint8) for im in d.get("images", [])]
     return SceneSpec(objects=objects, camera=cam, ray_depth=d["ray_depth"], seed=d["seed"],
-                     sky=sky, meshes=list(d["meshes"]), name=d.get("name", ""))
+                     sky=sky, meshes=list(d["meshes"]), name=d.get("name", ""), images=images)
 
 
 def scene_set(n: int = 16, seed: int = 0, max_level: int = 6) -> list[SceneSpec]:

@@ -95,6 +95,10 @@ class OrMesh(C.Structure):
                 ("triangles", C.POINTER(C.c_uint32)), ("n_triangles", C.c_uint32)]
 
 
+class OrImage(C.Structure):
+    _fields_ = [("chw", C.POINTER(C.c_uint8)), ("C", C.c_uint32), ("H", C.c_uint32), ("W", C.c_uint32)]
+
+
 class OrScene(C.Structure):
     _fields_ = [("materials", C.POINTER(MaterialDesc)), ("n_materials", C.c_uint32),
                 ("objects", C.POINTER(ObjectDesc)), ("n_objects", C.c_uint32),
@@ -102,7 +106,7 @@ class OrScene(C.Structure):
                 ("sky_type", C.c_int32), ("sky_start", C.c_float * 3), ("sky_end", C.c_float * 3),
                 ("hdri", C.POINTER(C.c_float)), ("hdri_C", C.c_uint32), ("hdri_H", C.c_uint32),
                 ("hdri_W", C.c_uint32), ("hdri_rotation", C.c_float), ("hdri_intensity", C.c_float),
-                ("hdri_path", C.c_char_p)]
+                ("hdri_path", C.c_char_p), ("images", C.POINTER(OrImage)), ("n_images", C.c_uint32)]
 
 
 class OrRequest(C.Structure):
@@ -191,7 +195,14 @@ class _Lib:
             s.hdri_rotation = spec.sky.get("rotation", 0.0)
             s.hdri_intensity = spec.sky.get("intensity", 1.0)
             s.hdri_path = spec.sky["path"].encode()
-        keep += [mat_arr, obj_arr, mesh_arr]
+        imgs = []
+        for im in spec.images:
+            im = np.ascontiguousarray(im, np.uint8)
+            keep.append(im)
+            imgs.append(OrImage(im.ctypes.data_as(C.POINTER(C.c_uint8)), *im.shape))
+        img_arr = (OrImage * max(1, len(imgs)))(*imgs)
+        s.images, s.n_images = img_arr, len(imgs)
+        keep += [mat_arr, obj_arr, mesh_arr, img_arr]
         self._keep = keep
         return s
 

@@ -451,6 +451,9 @@ struct Obj {
 struct Tex {
   int type;
   V rgb;
+  const uint8_t* img = nullptr;  // IMAGE: planar CHW, 3 channels read
+  uint32_t H = 0, W = 0;
+  float scale = 1.0f;
 };
 struct Mat {
   int type;
@@ -687,7 +690,22 @@ bool scene_hit(const Scene& S, const Ray& ray, Hit& rec) {  // scene/include/gra
 }
 
 // ---- textures, materials, PDFs -----------------------------------------------
-inline V tex(const Tex& t) { return t.rgb; }  // constant textures (texture.h:58-65)
+// TextureView::sample (texture.h:58-90): constant colour, or the image texel
+// at the scaled, wrapped and clamped uv (nearest texel, v flipped), / 255.
+V tex(const Tex& t, V2 uv) {
+  if (t.type != NR_TEXTURE_IMAGE) return t.rgb;
+  const float inv = 1.0f / fmaxf(1e-8f, t.scale);  // FMIN (core/constants.h:9)
+  float su = fmodf(uv.x * inv, 1.0f), sv = fmodf(uv.y * inv, 1.0f);
+  float u = su < 0.0f ? 0.0f : (su > 1.0f ? 1.0f : su);
+  float v = 1.0f - (sv < 0.0f ? 0.0f : (sv > 1.0f ? 1.0f : sv));
+  int i = (int)(u * (float)t.W);
+  if (i >= (int)t.W) i = (int)t.W - 1;
+  int j = (int)(v * (float)t.H);
+  if (j >= (int)t.H) j = (int)t.H - 1;
+  const size_t px = (size_t)j * t.W + i, hw = (size_t)t.H * t.W;
+  const float k = 1.0f / 255.0f;  // Color / 255.0f multiplies by the reciprocal (core/vector.h:251-253)
+  return V{(float)t.img[px] * k, (float)t.img[hw + px] * k, (float)t.img[2 * hw + px] * k};
+}
 
 struct ONB {
   V u, v, w;
@@ -821,15 +839,15 @@ V light_random(const Scene& S, V origin, Rng& g, bool rtl) {  // primitives.h:61
 }
 
 V pbr_normal(const Mat& m, const Hit& h) {  // material.h:113-125
-  V tn = tex(m.tex[4]);
+  V tn = tex(m.tex[4], h.uv);
   V map = normalize(V{tn.x * 2.0f - 1.0f, tn.y * 2.0f - 1.0f, tn.z * 2.0f - 1.0f});
   V t = normalize(h.tangent - h.n * dot(h.tangent, h.n));
   V b = cross(h.n, t);
   return normalize(t * map.x + b * map.y + h.n * map.z);
 }
 V emitted(const Mat& m, const Hit& h) {
-  if (m.type == NR_MATERIAL_PBR) return h.front_face ? tex(m.tex[3]) : V{0, 0, 0};
-  if (m.type == NR_MATERIAL_EMISSIVE) return h.front_face ? tex(m.tex[0]) * m.brightness : V{0, 0, 0};
+  if (m.type == NR_MATERIAL_PBR) return h.front_face ? tex(m.tex[3], h.uv) : V{0, 0, 0};
+  if (m.type == NR_MATERIAL_EMISSIVE) return h.front_face ? tex(m.tex[0], h.uv) * m.brightness : V{0, 0, 0};
   return V{0, 0, 0};
 }
 float reflectance(float c, float ri) {
@@ -846,15 +864,15 @@ struct Scat {
 bool scatter(const Mat& m, const Hit& h, const Ray& ray, Scat& s, Rng& g) {
   switch (m.type) {
     case NR_MATERIAL_LAMBERTIAN:
-      s.atten = tex(m.tex[0]);
+      s.atten = tex(m.tex[0], h.uv);
       s.pdf.kind = 0;
       s.pdf.uvw = onb(h.n);
       s.skip = false;
       return true;
     case NR_MATERIAL_PBR: {
       V n = pbr_normal(m, h);
-      V albedo = tex(m.tex[0]);
-      float metallic = tex(m.tex[2]).x;
+      V albedo = tex(m.tex[0], h.uv);
+      float metallic = tex(m.tex[2], h.uv).x;
       V F0 = V{0.04f, 0.04f, 0.04f} * (1.0f - metallic) + albedo * metallic;
       float spec = fminf(0.9f, fmaxf(0.1f, fmaxf(F0.x, fmaxf(F0.y, F0.z))));
       s.atten = V{1, 1, 1};
@@ -862,7 +880,7 @@ bool scatter(const Mat& m, const Hit& h, const Ray& ray, Scat& s, Rng& g) {
       s.pdf.kind = 5;
       s.pdf.uvw = onb(n);
       s.pdf.view = normalize(-ray.d);
-      float rough = tex(m.tex[1]).x;
+      float rough = tex(m.tex[1], h.uv).x;
       s.pdf.alpha = fmaxf(rough * rough, 1e-3f);
       s.pdf.spec = spec;
       return true;
@@ -882,7 +900,7 @@ bool scatter(const Mat& m, const Hit& h, const Ray& ray, Scat& s, Rng& g) {
       return true;
     }
     case NR_MATERIAL_ISOTROPIC:
-      s.atten = tex(m.tex[0]);
+      s.atten = tex(m.tex[0], h.uv);
       s.pdf.kind = 1;
       s.skip = false;
       return true;
@@ -893,14 +911,14 @@ V evaluate(const Mat& m, const Hit& h, V view, V light) {
   if (m.type == NR_MATERIAL_LAMBERTIAN) {
     float ct = dot(h.n, normalize(light));
     if (ct <= 0.0f) return V{0, 0, 0};
-    return tex(m.tex[0]) * (ct / PI);
+    return tex(m.tex[0], h.uv) * (ct / PI);
   }
   if (m.type == NR_MATERIAL_PBR) {
     V n = pbr_normal(m, h);
     float ndl = dot(n, light), ndv = dot(n, view);
     if (ndl <= 0.0f || ndv <= 0.0f) return V{0, 0, 0};
-    V albedo = tex(m.tex[0]);
-    float rough = tex(m.tex[1]).x, metallic = tex(m.tex[2]).x;
+    V albedo = tex(m.tex[0], h.uv);
+    float rough = tex(m.tex[1], h.uv).x, metallic = tex(m.tex[2], h.uv).x;
     float alpha = fmaxf(rough * rough, 1e-3f);
     V hv = normalize(view + light);
     float ndh = fmaxf(dot(n, hv), 0.0f), vdh = fmaxf(dot(view, hv), 0.0f);
@@ -912,7 +930,7 @@ V evaluate(const Mat& m, const Hit& h, V view, V light) {
     V diff = albedo * (1.0f - metallic) * (1.0f / PI);
     return (diff + spec) * ndl;
   }
-  if (m.type == NR_MATERIAL_ISOTROPIC) return tex(m.tex[0]) * (1.0f / PI4);
+  if (m.type == NR_MATERIAL_ISOTROPIC) return tex(m.tex[0], h.uv) * (1.0f / PI4);
   return V{0, 0, 0};
 }
 
@@ -1310,9 +1328,19 @@ bool build_scene(const or_scene* in, bool rtl, Scene& S) {
     m.brightness = d.brightness;
     m.tint = V{d.tint[0], d.tint[1], d.tint[2]};
     for (int k = 0; k < 5; ++k) {
-      if (d.tex[k].type != NR_TEXTURE_CONSTANT) return false;  // image textures unsupported here
-      m.tex[k].type = 0;
+      m.tex[k].type = d.tex[k].type;
       m.tex[k].rgb = V{d.tex[k].rgb[0], d.tex[k].rgb[1], d.tex[k].rgb[2]};
+      if (d.tex[k].type == NR_TEXTURE_IMAGE) {
+        if (d.tex[k].image < 0 || (uint32_t)d.tex[k].image >= in->n_images) return false;
+        const or_image& im = in->images[d.tex[k].image];
+        if (!im.chw || im.C < 3) return false;
+        m.tex[k].img = im.chw;
+        m.tex[k].H = im.H;
+        m.tex[k].W = im.W;
+        m.tex[k].scale = d.tex[k].scale;
+      } else if (d.tex[k].type != NR_TEXTURE_CONSTANT) {
+        return false;
+      }
     }
   }
   const float P[6][3] = {{0, 0, 0.5f}, {0, 0, -0.5f}, {0.5f, 0, 0}, {-0.5f, 0, 0}, {0, 0.5f, 0}, {0, -0.5f, 0}};
@@ -1458,9 +1486,9 @@ bool vp_triplanar(const Ray& r, V& color, float& alpha) {  // axis_grid.cu:55-72
          vp_axis_grid(r, FMAX, 1, V{0.3f, 1.0f, 0.3f}, color, alpha) ||
          vp_axis_grid(r, FMAX, 2, V{0.3f, 0.3f, 1.0f}, color, alpha);
 }
-V vp_color(const Mat& m) {  // material.h viewport_color
+V vp_color(const Mat& m, V2 uv) {  // material.h viewport_color
   if (m.type == NR_MATERIAL_DIELECTRIC) return m.tint;
-  if (m.type >= 1 && m.type <= 5) return tex(m.tex[0]);
+  if (m.type >= 1 && m.type <= 5) return tex(m.tex[0], uv);
   return V{0, 0, 0};
 }
 Ray vp_center_ray(const Cam& c, uint32_t x, uint32_t y) {  // camera.h:181-184
@@ -1570,7 +1598,7 @@ int oracle_scene_viewport(void* handle, const nr_camera_desc* cam, uint32_t seed
         head = fminf(0.75f, head);
         float dir = (dot(V{1.0f, 1.0f, 1.0f}, rec.n) + 1.0f) * 0.5f;
         dir = fmaxf(0.1f, dir);
-        V col = vp_color(S.mats[S.objs[rec.obj].mat]);
+        V col = vp_color(S.mats[S.objs[rec.obj].mat], rec.uv);
         b = col * fmaxf(head, dir);
         d = col;
         n = rec.n;

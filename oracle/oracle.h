@@ -28,6 +28,12 @@ typedef struct or_mesh {
   uint32_t n_triangles;
 } or_mesh;
 
+/* uint8 planar CHW image of an IMAGE texture (texture.h:8-26), C >= 3. */
+typedef struct or_image {
+  const uint8_t* chw;
+  uint32_t C, H, W;
+} or_image;
+
 typedef struct or_scene {
   const nr_material_desc* materials; /* [0] is the default purple Lambertian */
   uint32_t n_materials;
@@ -41,6 +47,8 @@ typedef struct or_scene {
   uint32_t hdri_C, hdri_H, hdri_W;
   float hdri_rotation, hdri_intensity;
   const char* hdri_path; /* Radiance file the HDRI was read from (reference harnesses load it) */
+  const or_image* images; /* indexed by nr_texture_desc.image */
+  uint32_t n_images;
 } or_scene;
 
 /* Output buffers: planar CHW float (3 x H x W) or NULL. primary: one uint32

@@ -77,7 +77,10 @@ struct RefScene {
   std::vector<std::unique_ptr<MeshData>> meshes;
 };
 
-TextureView view_of(const nr_texture_desc& t) {
+// A texture view as Texture::view() builds it (texture.h:187-191); an IMAGE
+// texture points at the caller's host copy of the CHW bytes, which the
+// reference's sample_image then reads as it reads device memory.
+TextureView texture_view(const nr_texture_desc& t, const or_scene* in) {
   TextureView v{};
   v.type = TextureType::CONSTANT;
   v.d_tex_ptr = nullptr;
@@ -86,10 +89,19 @@ TextureView view_of(const nr_texture_desc& t) {
   v.H = 0;
   v.W = 0;
   v.scale = t.scale;
+  if (t.type == NR_TEXTURE_IMAGE && t.image >= 0 && (uint32_t)t.image < in->n_images) {
+    const or_image& im = in->images[t.image];
+    v.type = TextureType::IMAGE;
+    v.d_tex_ptr = const_cast<uint8_t*>(im.chw);
+    v.C = im.C;
+    v.H = im.H;
+    v.W = im.W;
+  }
   return v;
 }
 
-Material* make_material(const nr_material_desc& d, RefScene& S) {
+Material* make_material(const nr_material_desc& d, RefScene& S, const or_scene* in) {
+  auto view_of = [in](const nr_texture_desc& t) { return texture_view(t, in); };
   void* core = nullptr;
   MaterialType type = (MaterialType)d.type;
   switch (d.type) {
@@ -160,7 +172,7 @@ AABB local_box(int type, const nr_object_desc& d, RefScene& S) {
 std::unique_ptr<RefScene> build(const or_scene* in) {
   auto S = std::make_unique<RefScene>();
   for (uint32_t i = 0; i < in->n_meshes; ++i) S->meshes.push_back(load_mesh(in->meshes[i]));
-  for (uint32_t i = 0; i < in->n_materials; ++i) S->mat_ptrs.push_back(make_material(in->materials[i], *S));
+  for (uint32_t i = 0; i < in->n_materials; ++i) S->mat_ptrs.push_back(make_material(in->materials[i], *S, in));
   std::vector<Hittable*> reg(in->n_objects);
   std::vector<int> reg_mesh(in->n_objects, -1);
   std::vector<AABB> boxes(in->n_objects);

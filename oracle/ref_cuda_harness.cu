@@ -37,11 +37,29 @@ namespace refsrc {
 
 namespace {
 
-std::shared_ptr<Texture> tex(const nr_texture_desc& t) {
+// Texture::from_color, or an IMAGE texture set up as Texture::from_image
+// does (texture.h:158-176) from CHW bytes already in memory instead of a
+// file: device copy, channel count and size, scale.
+std::shared_ptr<Texture> tex(const nr_texture_desc& t, const or_scene* s) {
+  if (t.type == NR_TEXTURE_IMAGE && t.image >= 0 && (uint32_t)t.image < s->n_images) {
+    const or_image& im = s->images[t.image];
+    Texture tx(TextureType::IMAGE);
+    tx.texture_scale = t.scale;
+    tx.C = im.C;
+    tx.H = im.H;
+    tx.W = im.W;
+    const size_t n = (size_t)im.C * im.H * im.W;
+    uint8_t* d = nullptr;
+    if (cudaMalloc(&d, n) != cudaSuccess || cudaMemcpy(d, im.chw, n, cudaMemcpyHostToDevice) != cudaSuccess)
+      throw std::runtime_error("image texture upload failed");
+    tx.d_texture_ptr = d;
+    return std::make_shared<Texture>(std::move(tx));
+  }
   return Texture::from_color(Color(t.rgb[0], t.rgb[1], t.rgb[2]));
 }
 
-Material material(const nr_material_desc& d) {
+Material material(const nr_material_desc& d, const or_scene* s) {
+  auto tex = [s](const nr_texture_desc& t) { return ::tex(t, s); };
   switch (d.type) {
     case NR_MATERIAL_LAMBERTIAN: return Material::lambertian(tex(d.tex[0]));
     case NR_MATERIAL_PBR:
@@ -102,14 +120,14 @@ std::unique_ptr<Scene> build_ref_scene(const or_scene* s, std::vector<std::uniqu
       keep.emplace_back(new Hittable(shape(d.wrapped_type, d, s, Material())));
       Hittable& bound = *keep.back();
       if (d.type == NR_HITTABLE_OBJECT_LIGHT) {
-        keep.emplace_back(new Hittable(Hittable::object_light(bound, md.brightness, tex(md.tex[0]))));
+        keep.emplace_back(new Hittable(Hittable::object_light(bound, md.brightness, tex(md.tex[0], s))));
         lights.push_back(keep.back().get());
       } else {
-        keep.emplace_back(new Hittable(Hittable::constant_medium(bound, d.density, tex(md.tex[0]))));
+        keep.emplace_back(new Hittable(Hittable::constant_medium(bound, d.density, tex(md.tex[0], s))));
         hittables.push_back(keep.back().get());
       }
     } else {
-      keep.emplace_back(new Hittable(shape(d.type, d, s, material(md))));
+      keep.emplace_back(new Hittable(shape(d.type, d, s, material(md, s))));
       hittables.push_back(keep.back().get());
     }
   }
@@ -213,8 +231,17 @@ int refcuda_probe_draw_order(int* vec3_order, int* quad_order) {
   return 0;
 }
 
+// The previous scene's teardown frees each image texture twice (the
+// material registry's teardown frees it, material.h:572 via texture.h:181-183,
+// then ~Texture frees the same pointer again, texture.h:109): the second
+// cudaFree fails with cudaErrorInvalidValue after the entry point returned.
+// That error is not sticky; clear it so that it is not reported as this
+// call's.
+void clear_stale_error() { (void)cudaGetLastError(); }
+
 int refcuda_render(const or_scene* s, const nr_camera_desc* c, const nr_render_config* cfg,
                    const or_request* req, double* elapsed_ms) {
+  clear_stale_error();
   cudaDeviceSetLimit(cudaLimitStackSize, CUDA_STACK_SIZE_LIMIT);
   std::vector<std::unique_ptr<Hittable>> keep;
   auto scene = build_ref_scene(s, keep);
@@ -264,6 +291,7 @@ int refcuda_render(const or_scene* s, const nr_camera_desc* c, const nr_render_c
 int refcuda_time_steps(const or_scene* s, const nr_camera_desc* c, const nr_render_config* cfg,
                        uint32_t first, uint32_t warmup, uint32_t steps, uint32_t spp_per_step,
                        double* step_ms) {
+  clear_stale_error();
   cudaDeviceSetLimit(cudaLimitStackSize, CUDA_STACK_SIZE_LIMIT);
   std::vector<std::unique_ptr<Hittable>> keep;
   auto scene = build_ref_scene(s, keep);
@@ -313,6 +341,7 @@ int refcuda_time_steps(const or_scene* s, const nr_camera_desc* c, const nr_rend
 // equals what trace_full writes for that sample.
 int refcuda_trace_log(const or_scene* s, const nr_camera_desc* c, const nr_render_config* cfg,
                       uint32_t sample, uint32_t max_bounces, float* host_log, float* beauty) {
+  clear_stale_error();
   cudaDeviceSetLimit(cudaLimitStackSize, CUDA_STACK_SIZE_LIMIT);
   std::vector<std::unique_ptr<Hittable>> keep;
   auto scene = build_ref_scene(s, keep);

@@ -168,6 +168,40 @@ def test_participating_medium_samples(orc, refcuda):
     assert frac_close(b, rb) >= 0.98
 
 
+@pytest.mark.parametrize("s", [1, 2])
+def test_defocus_and_rotated_cubes(orc, refcuda, s):
+    """Thin-lens defocus and rotated cubes (Lambertian, rough metal, glass)
+    per sample, against the oracle and the reference's CUDA build."""
+    spec = scenes.cornell_cubes(res=64, spp=3)
+    r = capi.Render(capi.Scene(spec))
+    b, d, n, p = r.sample_layers(s)
+    ob, od, on, op, _ = orc.render(spec, s, mode=0, draw_rtl=RTL)
+    assert frac_close(b, ob) >= 0.99
+    assert frac_close(n, on) >= 0.99
+    assert (p == op).mean() >= 0.999
+    rb, rd, rn, _ = refcuda.render(spec, s, mode=0)
+    assert frac_close(b, rb) >= 0.99
+    assert frac_close(d, rd) >= 0.99
+    assert frac_close(n, rn) >= 0.999
+
+
+@pytest.mark.parametrize("s", [1, 2])
+def test_image_textures_and_normal_maps(orc, refcuda, s):
+    """Image textures and normal maps per sample, against the oracle and the
+    reference's CUDA build (its Texture set up from the same bytes)."""
+    spec = scenes.cornell_textured(res=64, spp=3)
+    r = capi.Render(capi.Scene(spec))
+    b, d, n, p = r.sample_layers(s)
+    ob, od, on, op, _ = orc.render(spec, s, mode=0, draw_rtl=RTL)
+    assert frac_close(b, ob) >= 0.99
+    assert frac_close(d, od) >= 0.999
+    assert (p == op).mean() >= 0.999
+    rb, rd, rn, _ = refcuda.render(spec, s, mode=0)
+    assert frac_close(b, rb) >= 0.99
+    assert frac_close(d, rd) >= 0.999
+    assert frac_close(n, rn) >= 0.999
+
+
 def test_edge_sizes_not_multiple_of_tiles(orc):
     spec = scenes.cornell(res=37, spp=2)
     spec.camera["resolution"] = (37.0, 37.0)
