@@ -86,8 +86,12 @@ def parse():
 def workload(args):
     h, w = (int(x) for x in args.res.split("x"))
     total = args.warmup + args.steps + 1
+    # a render's sample streams are pixel + sample x W x H in 32 bits: at most
+    # (2^32 - 1) / (W H) sample indices (2071 at 1920x1080); longer runs on
+    # more ranks reuse indices (first_index wraps), which changes no timing
+    cap = 0xFFFFFFFF // (h * w) - 1  # the camera's samples_per_pixel is spp + 1
     spec = scenes.mesh_stress(levels=args.levels, res_h=h, res_w=w,
-                              spp=max(256, args.spp_per_step * total * max(1, args.gpus)))
+                              spp=min(cap, max(256, args.spp_per_step * total * max(1, args.gpus))))
     return spec, h, w
 
 
@@ -254,9 +258,15 @@ def run_ours(args):
     lib.nr_render_stream(render.h, ctypes.byref(stream_handle))
     stream = torch.cuda.ExternalStream(stream_handle.value)
     S = args.spp_per_step
-    # sample indices of this rank: disjoint slices per step
+    # sample indices of this rank: disjoint slices per step, wrapping around
+    # the camera's sample range (1 .. spp - 1) when a run needs more slices
+    n_slots = (spec.camera["samples_per_pixel"] - 1) // S
+    if n_slots < world:
+        raise SystemExit(f"{world} ranks need {world * S + 1} sample indices, the frame allows "
+                         f"{spec.camera['samples_per_pixel']}")
+
     def first_index(step):
-        return 1 + (step * world + rank) * S
+        return 1 + ((step * world + rank) % n_slots) * S
 
     # warm-up
     for i in range(args.warmup):
@@ -282,8 +292,9 @@ def run_ours(args):
             ev[k][1].record(stream)
         torch.cuda.synchronize()
     graphs = render.graph_stats()
-    # this rank's FP64 sum over the sample indices it rendered so far (each
-    # index once): combined across ranks after the profiling pass below
+    # this rank's FP64 sum over the samples it rendered so far (warm-up,
+    # counting and timed launches; an index that wrapped around counts once
+    # per render): combined across ranks after the profiling pass below
     rank_sum, rank_n = render.beauty_fp64_sum()
     # Per-kernel device time: the same steps again with an event recorded
     # after every launch on the render stream (direct launches instead of
