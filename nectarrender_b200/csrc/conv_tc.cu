@@ -1,21 +1,33 @@
 // conv_tc.cu — tcgen05 implicit-GEMM 3x3 convolutions (see conv_tc.cuh).
 //
-// Forward / backward-data: one CTA of 128 threads computes a 128-pixel x cout
-// tile. The K loop runs over the 9 taps; per tap the 128 shifted input rows
-// (zero outside the image) and the tap's cout x cin weights are copied into
-// shared memory with cp.async (16-byte chunks, zero-fill at the borders) in
-// the K-major no-swizzle canonical layout, and one thread issues cin / 16
-// MMAs (M = 128, N = cout, K = 16) into a tensor-memory accumulator. Two
-// shared-memory stages alternate: the copy of tap t overlaps the MMAs of tap
-// t - 1; a stage is refilled after the tcgen05.commit of its previous MMAs
-// has arrived on that stage's mbarrier. The epilogue loads the accumulator
-// (tcgen05.ld, one pixel row per thread), adds the bias, applies ReLU and
-// stores BF16.
+// Which kernel runs (launch_conv_fwd / launch_conv_wgrad pick the first that
+// fits the shape):
+//  * k_conv_fwd_tma / k_conv_wgrad_tma — images whose height is a multiple
+//    of 16 and width a multiple of 8, weights (forward) or two stages
+//    (weight gradient) within shared memory: 8 x 16 pixel tiles copied by
+//    TMA in swizzled layouts, warp-specialised issue and mbarrier
+//    hand-overs (the main path; described at the kernels);
+//  * k_conv_fwd_res / k_conv_fwd_halo / k_conv_wgrad_halo — the same tiles
+//    copied with cp.async, for shapes whose TMA stages do not fit;
+//  * k_conv_fwd / k_conv_wgrad — any image size: per-tap gathers, described
+//    next.
 //
-// Backward-weights: CTA (g, tap) reduces chunks of 128 pixels: D[co, ci] +=
-// dY^T[co, p] * Xshift^T[ci, p] with both operands MN-major in shared memory
-// (cout rows padded to the M = 128 tile with zeros), then adds its FP32
-// partial sums to dW with atomics.
+// Forward / backward-data (k_conv_fwd): one CTA of 128 threads computes a
+// 128-pixel x cout tile. The K loop runs over the 9 taps; per tap the 128
+// shifted input rows (zero outside the image) and the tap's cout x cin
+// weights are copied into shared memory with cp.async (16-byte chunks,
+// zero-fill at the borders) in the K-major no-swizzle canonical layout, and
+// one thread issues cin / 16 MMAs (M = 128, N = cout, K = 16) into a
+// tensor-memory accumulator. Two shared-memory stages alternate: the copy of
+// tap t overlaps the MMAs of tap t - 1; a stage is refilled after the
+// tcgen05.commit of its previous MMAs has arrived on that stage's mbarrier.
+// The epilogue loads the accumulator (tcgen05.ld, one pixel row per thread),
+// adds the bias, applies ReLU and stores BF16.
+//
+// Backward-weights (k_conv_wgrad): CTA (g, tap) reduces chunks of 128
+// pixels: D[co, ci] += dY^T[co, p] * Xshift^T[ci, p] with both operands
+// MN-major in shared memory (cout rows padded to the M = 128 tile with
+// zeros), then adds its FP32 partial sums to dW with atomics.
 #include "conv_tc.cuh"
 
 #include <cuda.h>  // CUtensorMap and its enums; the encoder is fetched from the driver at run time
