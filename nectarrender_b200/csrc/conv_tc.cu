@@ -724,15 +724,8 @@ __host__ __device__ constexpr uint32_t slot_bytes(int sc) {
 // Swizzle mode of the tensor-core descriptor for rows of 2 sc bytes.
 __host__ __device__ constexpr uint32_t umma_swizzle(int sc) { return sc == 64 ? 2u : (sc == 32 ? 4u : 6u); }
 
-// Waits for `parity` on `bar`; gives up when `abort` is raised elsewhere, or
-// after kWaitLimit polls, when it raises `abort` itself.
 __device__ __forceinline__ bool wait_or_abort(uint64_t* bar, uint32_t parity, volatile int* abort) {
-  for (uint32_t i = 0; i < kWaitLimit; ++i) {
-    if (tc::mbar_test(bar, parity)) return true;
-    if (*abort) return false;
-  }
-  *abort = 1;
-  return false;
+  return tc::mbar_wait_or_abort(bar, parity, abort, kWaitLimit);
 }
 
 __global__ void __launch_bounds__(kTmaThreads, 1)

@@ -396,12 +396,7 @@ static_assert((kGroups - 1) * kGrpBytes + kHOff + (kHidden - 1) * kTileBytes + 3
 static_assert(kSmemTrain <= 227u * 1024u, "shared memory per CTA");
 
 __device__ __forceinline__ bool wait_or_abort(uint64_t* bar, uint32_t parity, volatile int* abort) {
-  for (uint32_t i = 0; i < kWaitLimit; ++i) {
-    if (tc::mbar_test(bar, parity)) return true;
-    if (*abort) return false;
-  }
-  *abort = 1;
-  return false;
+  return tc::mbar_wait_or_abort(bar, parity, abort, kWaitLimit);
 }
 
 __device__ __forceinline__ void group_sync(int g) {

@@ -1,7 +1,9 @@
 // tcgen05.cuh — the fifth-generation tensor-core primitives used by the
 // learned kernels, as inline PTX for sm_100a: tensor-memory allocation,
-// shared-memory matrix descriptors in the no-swizzle canonical layouts,
-// BF16 x BF16 -> FP32 MMA issue, commit to an mbarrier and accumulator loads.
+// shared-memory matrix descriptors (no-swizzle canonical layouts; callers OR
+// a swizzle mode into bits 61-63 for the 32/64/128-byte swizzled layouts that
+// TMA writes), BF16 x BF16 -> FP32 MMA issue, commit to an mbarrier,
+// mbarrier waits and arrivals, TMA tiled loads and accumulator loads.
 //
 // Canonical no-swizzle layouts (one "core matrix" = 8 rows of 16 bytes):
 //  * K-major operand (rows along M or N, K contiguous): element (r, k) of a
@@ -21,7 +23,9 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return (uint32_t)__cvta_generic_to_shared(p);
 }
 
-// Shared-memory matrix descriptor (SWIZZLE_NONE, version 1, base offset 0).
+// Shared-memory matrix descriptor (SWIZZLE_NONE, version 1, base offset 0:
+// the tensor cores apply a swizzle to the absolute address, as TMA does, so
+// no base offset is needed for views that start inside a swizzle atom).
 __device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo_bytes, uint32_t sbo_bytes) {
   uint64_t d = 0;
   d |= (uint64_t)((addr >> 4) & 0x3FFFu);
@@ -141,6 +145,19 @@ __device__ __forceinline__ bool mbar_test(uint64_t* bar, uint32_t parity) {
       "selp.u32 %0, 1, 0, p;\n\t}\n"
       : "=r"(done) : "r"(smem_u32(bar)), "r"(parity) : "memory");
   return done != 0;
+}
+
+// Waits for `parity` on `bar`; gives up when `abort` is raised elsewhere, or
+// after `limit` polls, when it raises `abort` itself. For kernels whose warps
+// wait on one another's hand-overs: one failed wait releases them all.
+__device__ __forceinline__ bool mbar_wait_or_abort(uint64_t* bar, uint32_t parity, volatile int* abort,
+                                                   uint32_t limit) {
+  for (uint32_t i = 0; i < limit; ++i) {
+    if (mbar_test(bar, parity)) return true;
+    if (*abort) return false;
+  }
+  *abort = 1;
+  return false;
 }
 
 // Tensor-memory-access (TMA) tiled loads from a tensor map in this GPU's
