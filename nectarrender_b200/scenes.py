@@ -246,11 +246,21 @@ def value_noise(p: np.ndarray, seed: int, octaves: int = 4, base_freq: float = 2
     return out / norm
 
 
-def write_obj(path: Path, v: np.ndarray, f: np.ndarray, n: np.ndarray | None = None) -> None:
+def write_obj(path: Path, v: np.ndarray, f: np.ndarray, n: np.ndarray | None = None,
+              uv: np.ndarray | None = None) -> None:
+    """OBJ with positions, optional normals and optional texture coordinates
+    (with uv, faces are written v/vt/vn, or v/vt without normals)."""
     v32 = v.astype(np.float32)
     lines = ["# nectarrender_b200 generated mesh"]
     lines += [f"v {a:.9g} {b:.9g} {c:.9g}" for a, b, c in v32]
-    if n is not None:
+    if uv is not None:
+        lines += [f"vt {a:.9g} {b:.9g}" for a, b in uv.astype(np.float32)]
+        if n is not None:
+            lines += [f"vn {a:.9g} {b:.9g} {c:.9g}" for a, b, c in n.astype(np.float32)]
+            lines += [f"f {a}/{a}/{a} {b}/{b}/{b} {c}/{c}/{c}" for a, b, c in (f + 1)]
+        else:
+            lines += [f"f {a}/{a} {b}/{b} {c}/{c}" for a, b, c in (f + 1)]
+    elif n is not None:
         lines += [f"vn {a:.9g} {b:.9g} {c:.9g}" for a, b, c in n.astype(np.float32)]
         lines += [f"f {a}//{a} {b}//{b} {c}//{c}" for a, b, c in (f + 1)]
     else:
@@ -316,6 +326,49 @@ def procedural_hdri(width: int, height: int, seed: int, sun_radiance: float = 1e
     sun = cosang > math.cos(math.radians(0.6))
     sky[sun] = sun_radiance
     return sky.astype(np.float32)
+
+
+def uv_sphere(n_lat: int = 24, n_lon: int = 48):
+    """Latitude-longitude unit sphere with texture coordinates (u along the
+    longitude, v along the latitude; the seam and the poles duplicate
+    vertices) and normals: (v, f, n, uv)."""
+    lat = np.linspace(0.0, math.pi, n_lat + 1)
+    lon = np.linspace(0.0, 2.0 * math.pi, n_lon + 1)
+    th, ph = np.meshgrid(lat, lon, indexing="ij")
+    v = np.stack([np.sin(th) * np.cos(ph), np.cos(th), np.sin(th) * np.sin(ph)], -1).reshape(-1, 3)
+    uv = np.stack([ph / (2.0 * math.pi), 1.0 - th / math.pi], -1).reshape(-1, 2)
+    idx = np.arange((n_lat + 1) * (n_lon + 1)).reshape(n_lat + 1, n_lon + 1)
+    a, b = idx[:-1, :-1].ravel(), idx[:-1, 1:].ravel()
+    c, d = idx[1:, :-1].ravel(), idx[1:, 1:].ravel()
+    f = np.concatenate([np.stack([a, c, b], 1), np.stack([b, c, d], 1)])
+    # drop the zero-area triangles at the poles
+    area = np.linalg.norm(np.cross(v[f[:, 1]] - v[f[:, 0]], v[f[:, 2]] - v[f[:, 0]]), axis=1)
+    return v, f[area > 1e-9], v.copy(), uv
+
+
+def cornell_textured_mesh(res: int = 64, spp: int = 4, depth: int = 8, seed: int = 0) -> SceneSpec:
+    """The textured Cornell box with a uv-mapped sphere mesh (OBJ with vt
+    and vn) carrying the image-textured PBR material: mesh texture
+    coordinates, the tangents the mesh loader derives from them, and normal
+    maps on a mesh."""
+    spec = cornell_textured(res=res, spp=spp, depth=depth, seed=seed)
+    ASSETS.mkdir(parents=True, exist_ok=True)
+    obj_path = ASSETS / "uv_sphere_24x48.obj"
+    if not obj_path.exists():
+        v, f, n, uv = uv_sphere()
+        tmp = obj_path.with_suffix(f".{os.getpid()}.tmp")  # unique per writer process
+        write_obj(tmp, v, f, n, uv)
+        tmp.replace(obj_path)
+    spec.meshes = [str(obj_path)]
+    textured_pbr = spec.objects[5]["material"]
+    light = spec.objects[-1]
+    spec.objects = spec.objects[:5] + [
+        obj(MESH, textured_pbr, (-0.2, -0.22, -0.1), (20, 30, 0), (0.28, 0.28, 0.28), mesh=0),
+        spec.objects[6],
+        light,
+    ]
+    spec.name = f"cornell_textured_mesh{res}"
+    return spec
 
 
 def mesh_stress(levels: int = 8, res_h: int = 1080, res_w: int = 1920, spp: int = 256,

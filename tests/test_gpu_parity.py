@@ -185,11 +185,13 @@ def test_defocus_and_rotated_cubes(orc, refcuda, s):
     assert frac_close(n, rn) >= 0.999
 
 
+@pytest.mark.parametrize("make", [scenes.cornell_textured, scenes.cornell_textured_mesh])
 @pytest.mark.parametrize("s", [1, 2])
-def test_image_textures_and_normal_maps(orc, refcuda, s):
-    """Image textures and normal maps per sample, against the oracle and the
-    reference's CUDA build (its Texture set up from the same bytes)."""
-    spec = scenes.cornell_textured(res=64, spp=3)
+def test_image_textures_and_normal_maps(orc, refcuda, s, make):
+    """Image textures and normal maps per sample (on analytic shapes, and on
+    a uv-mapped OBJ mesh), against the oracle and the reference's CUDA build
+    (its Texture set up from the same bytes)."""
+    spec = make(res=64, spp=3)
     r = capi.Render(capi.Scene(spec))
     b, d, n, p = r.sample_layers(s)
     ob, od, on, op, _ = orc.render(spec, s, mode=0, draw_rtl=RTL)

@@ -101,12 +101,14 @@ def test_oracle_matches_reference_defocus_and_rotated_cubes(orc):
 
 
 @pytest.mark.skipif(not oracle.REF_CPU_SO.exists(), reason="reference host build not present")
-def test_oracle_matches_reference_image_textures(orc):
+@pytest.mark.parametrize("make", [scenes.cornell_textured, scenes.cornell_textured_mesh])
+def test_oracle_matches_reference_image_textures(orc, make):
     """Image textures (wrapped checker albedo, PBR albedo, roughness,
-    metallic and normal maps on a sphere and a rotated cube), against the
-    reference build, bit for bit."""
+    metallic and normal maps on a sphere, a rotated cube and a uv-mapped
+    mesh read from an OBJ with texture coordinates), against the reference
+    build, bit for bit."""
     ref = oracle.RefCPU()
-    spec = scenes.cornell_textured(res=16, spp=3)
+    spec = make(res=16, spp=3)
     for s in (1, 2):
         a = orc.render(spec, s, mode=0, draw_rtl=1)
         b = ref.render(spec, s, mode=0)
