@@ -109,10 +109,24 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
 
+// Non-blocking test of a phase (mbarrier.test_wait): the cheap first probe
+// when the phase has usually completed already (the blocking try_wait took
+// some hundred cycles to report a completed phase in measurements on B200).
+__device__ __forceinline__ bool mbar_test_now(uint64_t* bar, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(done) : "r"(smem_u32(bar)), "r"(parity) : "memory");
+  return done != 0;
+}
+
 // Waits for the phase with the given parity to complete; gives up after
 // `limit` polls and returns false (the caller reports an error instead of
 // hanging).
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32_t limit) {
+  if (mbar_test_now(bar, parity)) return true;
   const uint32_t a = smem_u32(bar);
   for (uint32_t i = 0; i < limit; ++i) {
     uint32_t done;
@@ -147,21 +161,11 @@ __device__ __forceinline__ bool mbar_test(uint64_t* bar, uint32_t parity) {
   return done != 0;
 }
 
-// Non-blocking test of a phase (mbarrier.test_wait): the cheap first probe
-// when the phase has usually completed already.
-__device__ __forceinline__ bool mbar_test_now(uint64_t* bar, uint32_t parity) {
-  uint32_t done;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}\n"
-      : "=r"(done) : "r"(smem_u32(bar)), "r"(parity) : "memory");
-  return done != 0;
-}
-
 // Waits for `parity` on `bar`; gives up when `abort` is raised elsewhere, or
 // after `limit` polls, when it raises `abort` itself. For kernels whose warps
-// wait on one another's hand-overs: one failed wait releases them all.
+// wait on one another's hand-overs: one failed wait releases them all. The
+// first probe does not block; the later ones use the blocking try_wait
+// (spinning on the non-blocking test was slower in measurements on B200).
 __device__ __forceinline__ bool mbar_wait_or_abort(uint64_t* bar, uint32_t parity, volatile int* abort,
                                                    uint32_t limit) {
   if (mbar_test_now(bar, parity)) return true;
