@@ -83,15 +83,32 @@ def parse():
     return p.parse_args()
 
 
+def sample_cap(h: int, w: int) -> int:
+    """Largest spp for a mesh-stress camera of h x w pixels: its
+    samples_per_pixel is spp + 1 and a render's sample streams are
+    pixel + sample x W x H in 32 bits."""
+    return 0xFFFFFFFF // (h * w) - 1
+
+
+def sample_first(step: int, rank: int, world: int, spp_per_step: int, samples_per_pixel: int) -> int:
+    """First sample index of a rank's step: disjoint slices of spp_per_step
+    indices per step and rank, wrapping around 1 .. samples_per_pixel - 1
+    when a run needs more slices than the camera has."""
+    n_slots = (samples_per_pixel - 1) // spp_per_step
+    if n_slots < world:
+        raise ValueError(f"{world} ranks need {world * spp_per_step + 1} sample indices, the frame "
+                         f"allows {samples_per_pixel}")
+    return 1 + ((step * world + rank) % n_slots) * spp_per_step
+
+
 def workload(args):
     h, w = (int(x) for x in args.res.split("x"))
     total = args.warmup + args.steps + 1
     # a render's sample streams are pixel + sample x W x H in 32 bits: at most
     # (2^32 - 1) / (W H) sample indices (2071 at 1920x1080); longer runs on
     # more ranks reuse indices (first_index wraps), which changes no timing
-    cap = 0xFFFFFFFF // (h * w) - 1  # the camera's samples_per_pixel is spp + 1
     spec = scenes.mesh_stress(levels=args.levels, res_h=h, res_w=w,
-                              spp=min(cap, max(256, args.spp_per_step * total * max(1, args.gpus))))
+                              spp=min(sample_cap(h, w), max(256, args.spp_per_step * total * max(1, args.gpus))))
     return spec, h, w
 
 
@@ -258,15 +275,11 @@ def run_ours(args):
     lib.nr_render_stream(render.h, ctypes.byref(stream_handle))
     stream = torch.cuda.ExternalStream(stream_handle.value)
     S = args.spp_per_step
-    # sample indices of this rank: disjoint slices per step, wrapping around
-    # the camera's sample range (1 .. spp - 1) when a run needs more slices
-    n_slots = (spec.camera["samples_per_pixel"] - 1) // S
-    if n_slots < world:
-        raise SystemExit(f"{world} ranks need {world * S + 1} sample indices, the frame allows "
-                         f"{spec.camera['samples_per_pixel']}")
+    # sample indices of this rank: disjoint slices per step (sample_first)
+    spp_cam = spec.camera["samples_per_pixel"]
 
     def first_index(step):
-        return 1 + ((step * world + rank) % n_slots) * S
+        return sample_first(step, rank, world, S, spp_cam)
 
     # warm-up
     for i in range(args.warmup):

@@ -1,5 +1,6 @@
 """Host-side helpers of bench.py (no GPU): the time-at-error interpolation of
-the time-to-RMSE curves and the section guard."""
+the time-to-RMSE curves, the section guard, the oracle statistics and the
+sample-index slices of the ranks."""
 import bench
 
 
@@ -33,3 +34,22 @@ def test_oracle_stats():
     d = lambda x: np.sqrt(np.clip(x, 0, 1))
     true_err = float(np.sqrt(np.mean((d(mean) - d(truth)) ** 2)))
     assert 0.5 * err < true_err < 2.0 * err
+
+
+def test_sample_slices_stay_in_the_32_bit_streams():
+    import pytest
+    h, w, S = 1080, 1920, 4
+    cap = bench.sample_cap(h, w)
+    assert w * h * (cap + 1) <= 0xFFFFFFFF < w * h * (cap + 2)
+    for world in (1, 2, 4, 8):
+        for steps in (5, 64, 300):
+            spp = min(cap, max(256, S * steps * world)) + 1
+            for step in range(steps):
+                firsts = [bench.sample_first(step, r, world, S, spp) for r in range(world)]
+                assert len(set(firsts)) == world                     # disjoint within a step
+                assert min(firsts) >= 1 and max(firsts) + S <= spp   # inside the camera's range
+    # no wrap while the run fits: every slice once
+    seen = {bench.sample_first(k, r, 2, S, 2 * S * 10 + 1) for k in range(10) for r in range(2)}
+    assert len(seen) == 20
+    with pytest.raises(ValueError):
+        bench.sample_first(0, 0, 8, S, 8)
