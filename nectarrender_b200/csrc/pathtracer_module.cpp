@@ -113,12 +113,20 @@ struct Texture {
     return t;
   }
   static std::shared_ptr<Texture> from_image(const std::string& path, float scale) {
-    // decode with Pillow; planar CHW uint8 of the first 3 channels is what the
-    // reference's sampler reads (texture.h:69-89)
+    // Decoded with Pillow into the file's own channels, as stb_image does
+    // (req_comp 0). The reference then builds its planes as
+    // chw[c * H * W + i] = data[i * 3 + c] whatever the channel count
+    // (texture.h:17-22): RGB images come out right and RGBA images come out
+    // shifted, which is kept here; grey images would be read past their
+    // data, so those (and palette images) are expanded to RGB instead.
     py::gil_scoped_acquire gil;
     py::module_ np = py::module_::import("numpy");
     py::module_ image = py::module_::import("PIL.Image");
-    py::object img = image.attr("open")(path).attr("convert")("RGB");
+    py::object img = image.attr("open")(path);
+    const std::string mode = py::str(img.attr("mode"));
+    if (mode != "RGB" && mode != "RGBA") img = img.attr("convert")(mode == "P" || mode == "PA" ? "RGBA" : "RGB");
+    if (mode == "P" && !py::bool_(img.attr("info").attr("__contains__")("transparency")))
+      img = img.attr("convert")("RGB");
     py::array_t<uint8_t> hwc = np.attr("ascontiguousarray")(np.attr("asarray")(img));
     auto t = std::make_shared<Texture>();
     t->type = TextureType::IMAGE;
@@ -126,12 +134,12 @@ struct Texture {
     t->scale = scale;
     t->H = hwc.shape(0);
     t->W = hwc.shape(1);
-    t->C = 3;
-    t->chw.resize(3 * t->H * t->W);
-    auto a = hwc.unchecked<3>();
-    for (size_t c = 0; c < 3; ++c)
-      for (size_t y = 0; y < t->H; ++y)
-        for (size_t x = 0; x < t->W; ++x) t->chw[c * t->H * t->W + y * t->W + x] = a(y, x, c);
+    t->C = hwc.ndim() == 3 ? hwc.shape(2) : 1;
+    const size_t hw = t->H * t->W;
+    const uint8_t* data = hwc.data();  // interleaved, C bytes per pixel
+    t->chw.resize(t->C * hw);
+    for (size_t c = 0; c < t->C; ++c)
+      for (size_t i = 0; i < hw; ++i) t->chw[c * hw + i] = data[i * 3 + c];
     return t;
   }
 };
@@ -973,7 +981,13 @@ PYBIND11_MODULE(_pathtracer, m) {
       .def_readonly("constant_color", &Texture::constant_color)
       .def_readonly("C", &Texture::C)
       .def_readonly("H", &Texture::H)
-      .def_readonly("W", &Texture::W);
+      .def_readonly("W", &Texture::W)
+      .def_property_readonly("texels", [](const Texture& t) {
+        // planar CHW uint8 copy of an IMAGE texture's planes (empty otherwise)
+        py::array_t<uint8_t> a({(py::ssize_t)t.C, (py::ssize_t)t.H, (py::ssize_t)t.W});
+        if (!t.chw.empty()) std::memcpy(a.mutable_data(), t.chw.data(), t.chw.size());
+        return a;
+      });
   py::enum_<MaterialType>(m_material, "MaterialType")
       .value("Lambertian", MaterialType::Lambertian)
       .value("PBR", MaterialType::PBR)

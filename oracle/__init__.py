@@ -356,6 +356,19 @@ class RefCPU(_Lib):
         self.lib.refcpu_n_rooks(n, seed, _f(out))
         return out.reshape(n, 2)
 
+    def load_image_uint8(self, path: str) -> np.ndarray:
+        """The reference's image-texture loader: its planes (C, H, W) as it
+        builds them from the decoded file."""
+        C_, H_, W_ = C.c_uint32(), C.c_uint32(), C.c_uint32()
+        cap = 1 << 26
+        buf = np.zeros(cap, np.uint8)
+        rc = self.lib.refcpu_load_image_uint8(path.encode(), buf.ctypes.data_as(C.POINTER(C.c_uint8)),
+                                              C.byref(C_), C.byref(H_), C.byref(W_), C.c_uint64(cap))
+        if rc != 0:
+            raise RuntimeError(f"refcpu_load_image_uint8 failed ({rc})")
+        n = C_.value * H_.value * W_.value
+        return buf[:n].reshape(C_.value, H_.value, W_.value).copy()
+
     def render(self, spec, first, count=1, mode=1, rows=None, threads=0, draw_rtl=1, fp64=False,
                cfg=None):
         # the reference's host build evaluates multi-draw arguments right to left

@@ -584,4 +584,23 @@ int refcpu_load_hdr(const char* path, float* chw, uint32_t* C, uint32_t* H, uint
   return 0;
 }
 
+// The reference's image-texture loader (texture.h:8-26, stbi_load with the
+// file's own channel count): its C planes as it builds them.
+int refcpu_load_image_uint8(const char* path, uint8_t* chw, uint32_t* C, uint32_t* H, uint32_t* W,
+                            uint64_t cap) {
+  int c, h, w;
+  std::vector<uint8_t> d;
+  try {
+    d = load_image_uint8(path, c, h, w);
+  } catch (const std::exception&) {
+    return -1;
+  }
+  *C = c;
+  *H = h;
+  *W = w;
+  if (d.size() > cap) return 1;
+  std::copy(d.begin(), d.end(), chw);
+  return 0;
+}
+
 }  // extern "C"

@@ -53,3 +53,28 @@ def test_scene_and_engine_surface(pt):
     if nb.device_count() == 0:
         with pytest.raises(RuntimeError, match="no CUDA device"):
             eng.set_scene(scene)
+
+
+@pytest.mark.parametrize("mode", ["RGB", "RGBA"])
+def test_image_texture_planes_match_the_reference_loader(pt, tmp_path, mode):
+    """Texture.from_image builds its planes as the reference's loader does
+    (texture.h:8-26): right for RGB, and for RGBA with the reference's
+    i * 3 + c indexing of four-channel pixels."""
+    import numpy as np
+    import oracle
+    Image = pytest.importorskip("PIL.Image")
+    if not oracle.REF_CPU_SO.exists():
+        pytest.skip("reference host build not present")
+    rng = np.random.default_rng(5)
+    nch = len(mode)
+    px = rng.integers(0, 256, (5, 7, nch), dtype=np.uint8)
+    path = tmp_path / f"t_{mode}.png"
+    Image.fromarray(px, mode).save(path)
+    ours = pt.material.texture.Texture.from_image(str(path), 0.5)
+    ref = oracle.RefCPU().load_image_uint8(str(path))
+    assert (ours.C, ours.H, ours.W) == ref.shape == (nch, 5, 7)
+    assert np.array_equal(ours.texels, ref)
+    if mode == "RGB":   # planes are the image's channels
+        assert np.array_equal(ref, px.transpose(2, 0, 1))
+    else:               # the reference's four-channel quirk: shifted planes
+        assert not np.array_equal(ref[:3], px[..., :3].transpose(2, 0, 1))
