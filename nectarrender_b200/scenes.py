@@ -155,8 +155,8 @@ def cornell_textured(res: int = 64, spp: int = 4, depth: int = 8, seed: int = 0)
     """The Cornell box with image textures: a checker albedo on the back
     wall (scale 0.5, so the uvs wrap), a PBR sphere and a PBR cube whose
     albedo, roughness, metallic and normal come from images (the normal map
-    tilts the shading normal through the tangent frame), generated from a
-    fixed seed."""
+    tilts the shading normal through the tangent frame), and the ceiling
+    light's emission from an image, generated from a fixed seed."""
     spec = cornell(res=res, spp=spp, depth=depth, seed=seed)
     rng = np.random.default_rng(7)
     n = 16
@@ -174,7 +174,8 @@ def cornell_textured(res: int = 64, spp: int = 4, depth: int = 8, seed: int = 0)
     back = dict(spec.objects[4])
     back["material"] = _mat(LAMBERTIAN, tex=[image_tex(0, 0.5)] + [(0.0, 0.0, 0.0)] * 4)
     textured_pbr = _mat(PBR, tex=[image_tex(4), image_tex(1), image_tex(2), (0.0, 0.0, 0.0), image_tex(3)])
-    light = spec.objects[-1]
+    light = dict(spec.objects[-1])  # the ceiling light's emission from an image too
+    light["material"] = dict(light["material"], tex=[image_tex(4)] + list(light["material"]["tex"][1:]))
     spec.objects = spec.objects[:4] + [back] + [
         obj(SPHERE, textured_pbr, (-0.22, -0.2, -0.15), radius=0.3),
         obj(CUBE, textured_pbr, (0.22, -0.3, -0.2), (10, -35, 5), (0.3, 0.3, 0.3)),
