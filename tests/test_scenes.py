@@ -50,3 +50,26 @@ def test_mesh_stress_spheres_do_not_overlap():
         assert np.linalg.norm(p) >= 1.06 + r
         for q, s in sph[:i]:
             assert np.linalg.norm(p - q) >= r + s
+
+
+def test_spec_json_roundtrip_keeps_images_and_texture_slots():
+    import json
+    import numpy as np
+    spec = scenes.cornell_textured_mesh(res=16, spp=2)
+    d = json.loads(json.dumps(scenes.spec_to_json(spec)))
+    back = scenes.spec_from_json(d)
+    assert len(back.images) == len(spec.images)
+    for a, b in zip(spec.images, back.images):
+        assert b.dtype == np.uint8 and np.array_equal(a, b)
+    assert back.meshes == spec.meshes
+    for o, p in zip(spec.objects, back.objects):
+        assert o["material"]["tex"] == p["material"]["tex"]
+    assert scenes.spec_to_json(back) == d
+
+
+def test_uv_sphere_mesh():
+    import numpy as np
+    v, f, n, uv = scenes.uv_sphere(8, 16)
+    assert np.allclose(np.linalg.norm(v, axis=1), 1.0)
+    assert uv.min() >= 0.0 and uv.max() <= 1.0
+    assert f.max() < len(v) and len(f) == 2 * 8 * 16 - 2 * 16  # the pole rows lose one triangle per quad
