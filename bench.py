@@ -74,6 +74,10 @@ def parse():
                    help="also render the 64-scene batched configuration and report every "
                         "scene's RMSE against an FP64 perf-mode render (about 2 minutes)")
     p.add_argument("--denoiser-seconds", type=float, default=40.0)
+    p.add_argument("--denoiser-scenes", type=int, default=24,
+                   help="training scenes for the denoiser (the configuration's set has 2000)")
+    p.add_argument("--denoiser-target-spp", type=int, default=1024,
+                   help="samples of the denoiser's training targets (the configuration's: 4096)")
     p.add_argument("--no-small", action="store_true",
                    help="skip the small configuration (Cornell box 512x512, 64 spp, depth 8)")
     p.add_argument("--learned-only", action="store_true",
@@ -1037,7 +1041,7 @@ def time_to_rmse(args, target=0.01, top=2048):
         out[name] = summary(curve(r))
         del r
     if not args.no_denoiser:
-        den, info = train_denoiser(args)
+        den, info = train_denoiser(args, n_scenes=args.denoiser_scenes, target_spp=args.denoiser_target_spp)
         r = capi.Render(sc, mode=capi.MODE_PERF, seed=spec.seed, layer_mask=denoise.DENOISE_LAYERS)
         r.samples(1, 1)
         r.reset()
